@@ -1,0 +1,133 @@
+/*
+ * qcmpodmrg_b200 -- C ABI of the B200 two-site MPO-DMRG hot path.
+ *
+ * Two shared libraries are built from qcmpodmrg_b200/csrc:
+ *   libqsym.so   drop-in for the reference's ctypes/qsym.c (same symbol, same
+ *                signature), loaded by source/sysutil_include.py:14-17.
+ *   libqcgpu.so  block maps, plan compiler and the sm_100a kernels.
+ *
+ * Conventions: plain pointers and sizes; device pointers are CUDA device
+ * addresses; `stream` is a cudaStream_t passed as void*.  Every function
+ * returns an int status (QC_OK = 0, negative on error) except where a count is
+ * documented; qc_last_error() returns the message of the last failure on the
+ * calling thread.  Nothing here calls exit().
+ */
+#ifndef QCMPODMRG_B200_H
+#define QCMPODMRG_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QC_OK 0
+#define QC_ERR_ARG -1
+#define QC_ERR_CAPACITY -2
+#define QC_ERR_CUDA -3
+#define QC_ERR_LAYOUT -4
+#define QC_ERR_HALFINT -5
+
+/* ---------------------------------------------------------------- libqsym.so */
+
+/* Replaces ctypes/qsym.c:5-22 symAllowed (and symAllowed2..8, :24-480).
+ * allowed[idx] = 1 iff sum_{status[i]==0} q_i - sum_{status[i]==1} q_i == 0
+ * over the row-major Cartesian product of the sectors of a0..a(rank-1)
+ * (each a_i is [ndims[i]][nqnum] doubles).  Quantum numbers must be
+ * multiples of 1/2; the comparison is done exactly on 2q as integers.
+ * Unlike the reference, rank 8 iterates its last index over ndims[7]
+ * (qsym.c:436 loops over ndims[6]).  Returns 0, or QC_ERR_* without exiting. */
+int symAllowed(int rank, int nqnum, int *ndims, int *status, int *allowed,
+               double *a0, double *a1, double *a2, double *a3,
+               double *a4, double *a5, double *a6, double *a7);
+
+/* ---------------------------------------------------------------- libqcgpu.so */
+
+int qc_version(void);
+const char *qc_last_error(void);
+
+/* Integer allowed-block mask (the same map as symAllowed, on 2q as int32).
+ * qsyms2: concatenation over i of [nsyms[i]][nqnum] int32 values of 2q.
+ * Replaces qtensor_util.blks_allowed1 (source/qtensor/qtensor_util.py:70-90). */
+int qc_sym_allowed(int rank, int nqnum, const int *nsyms, const int *status,
+                   const int *qsyms2, int *allowed);
+
+/* Same mask computed on the GPU (qsyms2_dev, allowed_dev device pointers). */
+int qc_sym_allowed_gpu(int rank, int nqnum, const int *nsyms, const int *status,
+                       const int *qsyms2_dev, int *allowed_dev, void *stream);
+
+/* Packed layout of a block-sparse tensor: replaces qtensor.fromQsyms
+ * (source/qtensor/qtensor.py:272-346).  ndims: concatenation over i of the
+ * nsyms[i] sector dimensions.  Outputs over nblks = prod(nsyms):
+ * iblks (1-based index of allowed blocks, 0 otherwise), ioff (packed offset,
+ * 0 for forbidden blocks), ndim (block size, for all blocks).
+ * *size_allowed and *nallowed receive the totals. */
+int qc_block_layout(int rank, const int *nsyms, const long long *ndims,
+                    const int *allowed, int *iblks, long long *ioff, long long *ndim,
+                    long long *size_allowed, long long *nallowed);
+
+/* Block-pair list of a contraction: replaces the pair loop of
+ * qtensor.tensordotSYM (source/qtensor/qtensor.py:617-636).  For every
+ * allowed output block (out_iblks over the external sectors e1+e2, row-major)
+ * and every internal sector tuple (row-major over the contracted axes in the
+ * order of ax1) with both input blocks allowed, writes one triple
+ * (out_block, in1_block, in2_block) of flat block indices.
+ * Returns the number of triples (written only if <= cap), or < 0 on error. */
+long long qc_contract_pairs(int r1, const int *nsyms1, const int *iblks1,
+                            int r2, const int *nsyms2, const int *iblks2,
+                            int nax, const int *ax1, const int *ax2,
+                            const int *out_iblks, long long *triples, long long cap);
+
+/* Plan compiler: turns pair triples into GPU work items for qc_bgemm_*.
+ * Each operand (1, 2, out) is described by its sector grid nsyms[rank], the
+ * concatenated sector dimensions ndims (int64) and the per-block packed
+ * offsets off[nblks] (from qc_block_layout).  For each operator o (nops of
+ * them) the element offsets base1[o], base2[o], baseo[o] are added and the
+ * product is scaled by alpha[o].  group_ops != 0 merges the contributions of
+ * all operators into one output (sum over o, used for sigma).  tile_m/tile_n
+ * is the output tile.  Writes up to task_cap tasks (qc_task, 64 B) and
+ * contrib_cap contributions (qc_contrib, 80 B).  Returns the number of
+ * contributions and stores the number of tasks in *ntasks and the algorithmic
+ * FLOP count (2*M*N*K summed over contributions) in *flops; if a capacity is
+ * too small nothing is written and the required counts are returned. */
+long long qc_compile_pairs(int r1, const int *nsyms1, const long long *ndims1, const long long *off1,
+                           int r2, const int *nsyms2, const long long *ndims2, const long long *off2,
+                           int ro, const int *nsymso, const long long *ndimso, const long long *offo,
+                           int nax, const int *ax1, const int *ax2,
+                           long long npairs, const long long *triples,
+                           int nops, const long long *base1, const long long *base2,
+                           const long long *baseo, const double *alpha, int group_ops,
+                           int tile_m, int tile_n,
+                           void *tasks, long long task_cap, void *contribs, long long contrib_cap,
+                           long long *ntasks, double *flops);
+
+/* Grouped block GEMM, FP64 (DFMA): the engine behind one stage of HVecQt /
+ * renormQt_H00 / HDiagQt (source/mpo_dmrg_kernelQt.py:238-317, 642-697,
+ * 77-119), i.e. the tensordotCAL loop (source/qtensor/qtensor.py:642-659) for
+ * all operators and block pairs of a stage in one launch.
+ * tasks (qc_task, 64 B), contribs (qc_contrib, 80 B) and ops (qc_op, 32 B:
+ * a_base, b_base, c_base, alpha per operator) are device arrays; the layout
+ * is documented in qcmpodmrg_b200/csrc/qc_types.h.
+ * summed == 0: each task writes one tile per operator of its range;
+ * summed != 0: each task writes one tile summed over the operators of every
+ * contribution's range (sigma's sum over p).
+ * tile_cfg: 0 = 64x64, 1 = 128x32, 2 = 256x16 output tiles. */
+int qc_bgemm_f64(const void *tasks_dev, long long ntasks, const void *contribs_dev, const void *ops_dev,
+                 int summed, const double *A, const double *B, double *C, int tile_cfg, void *stream);
+
+/* Same engine with FP32 operands and FP32 accumulation (mixed-precision sigma). */
+int qc_bgemm_f32(const void *tasks_dev, long long ntasks, const void *contribs_dev, const void *ops_dev,
+                 int summed, const float *A, const float *B, float *C, int tile_cfg, void *stream);
+
+/* dst[i] = src[idx[i]] (FP64), i < n.  Used for diag[prjmap] (kernelQt.py:122). */
+int qc_gather_f64(const double *src, const long long *idx, double *dst, long long n, void *stream);
+/* dst[idx[i]] = src[i] (FP64) after zeroing dst[0..ndst). */
+int qc_scatter_f64(const double *src, const long long *idx, double *dst, long long n,
+                   long long ndst, void *stream);
+
+/* Precision conversions used by the mixed-precision path. */
+int qc_convert_f64_to_f32(const double *src, float *dst, long long n, void *stream);
+int qc_convert_f32_to_f64(const float *src, double *dst, long long n, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

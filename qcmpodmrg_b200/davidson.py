@@ -1,0 +1,111 @@
+"""Davidson eigensolver on the GPU in FP64 (pdvdson.eigenSolver.solve_iter).
+
+Follows source/tools/pdvdson.py:90-330: start vector from the diagonal
+(genV0, :81-87) or the guess, Rayleigh-Ritz in the subspace, residuals,
+convergence when every residual norm <= crit_vec or its eigenvalue changed by
+<= crit_e, restart to span{x, x_old - x} once the subspace exceeds nfac*neig,
+preconditioner iop=4  r / (|diag - e| + 1e-4)  (:275-278) unless a
+preconditioner object is supplied, and 5-pass Gram-Schmidt (dvdson_ortho,
+:350-390).  All vectors stay on the device; the subspace eigenproblem is a
+cuSOLVER eigh.  The matrix-vector product is called one vector at a time, as
+the reference's HVecs does (:67-78).
+"""
+import torch
+
+
+def _ortho(vbas, rbas, crit_indp, times=5):
+    rbas = rbas.clone()
+    for _ in range(times):
+        rbas = rbas - (rbas @ vbas.T) @ vbas
+    out = []
+    for i in range(rbas.shape[0]):
+        r = rbas[i].clone()
+        n = torch.linalg.norm(r)
+        if float(n) <= crit_indp:
+            continue
+        r = r / n
+        r = r / torch.linalg.norm(r)
+        out.append(r)
+        v2 = torch.stack(out)
+        for _ in range(times):
+            rbas[i:] -= (rbas[i:] @ vbas.T) @ vbas
+            rbas[i:] -= (rbas[i:] @ v2.T) @ v2
+    if not out:
+        return 0, None
+    return len(out), torch.stack(out)
+
+
+def gen_v0(diag, neig):
+    n = diag.numel()
+    d = diag + 1.e-12 * torch.arange(1, 1 + n, dtype=diag.dtype, device=diag.device) / float(n)
+    idx = torch.argsort(d)[:neig]
+    v0 = torch.zeros((neig, n), dtype=diag.dtype, device=diag.device)
+    v0[torch.arange(neig, device=diag.device), idx] = 1.0
+    return v0
+
+
+class DavidsonResult(object):
+    def __init__(self, eigs, vecs, nmvp, niter, rnorms):
+        self.eigs, self.vecs, self.nmvp, self.niter, self.rnorms = eigs, vecs, nmvp, niter, rnorms
+
+
+def davidson(hvec, diag, neig=1, v0=None, crit_e=1.e-8, crit_vec=1.e-8, maxcycle=20, crit_indp=1.e-12,
+             lshift=1.e-4, nfac=10, precond=None, record=None):
+    """Lowest ``neig`` eigenpairs of the operator ``hvec`` (device FP64 vectors)."""
+    ndim = diag.numel()
+    if neig > ndim:
+        raise ValueError("neig > ndim")
+    vbas = gen_v0(diag, neig) if v0 is None else v0.reshape(neig, ndim).to(torch.float64).clone()
+    vbas[0] = vbas[0] / torch.linalg.norm(vbas[0])
+    if neig > 1:
+        n, v2 = _ortho(vbas[0:1], vbas[1:], crit_indp)
+        if n + 1 != neig:
+            raise RuntimeError("insufficient orthonormal start basis")
+        vbas[1:] = v2
+    wbas = torch.stack([hvec(v) for v in vbas])
+    nmvp = neig
+    eigs = torch.full((neig,), 1.e3, dtype=torch.float64, device=diag.device)
+    rnorms = []
+    for niter in range(1, maxcycle):
+        h = vbas @ wbas.T
+        h = 0.5 * (h + h.T)
+        e, u = torch.linalg.eigh(h)
+        vr = u[:, :neig].T.contiguous()
+        teig = e[:neig]
+        econv = (teig - eigs).abs() <= crit_e
+        eigs = teig.clone()
+        xbas = vr @ vbas
+        rbas = vr @ wbas - eigs[:, None] * xbas
+        rn = torch.linalg.norm(rbas, dim=1)
+        rn_h = rn.cpu().tolist()
+        ec_h = econv.cpu().tolist()
+        rnorms.append(rn_h)
+        rconv = [x <= crit_vec for x in rn_h]
+        rindx = [i for i in range(neig) if not rconv[i] and not ec_h[i]]
+        if len(rindx) == 0 or niter == maxcycle - 1:
+            return DavidsonResult(eigs.cpu().numpy(), xbas, nmvp, niter, rnorms)
+        nsub = vbas.shape[0]
+        if nsub > nfac * neig:
+            pr = torch.eye(nsub, dtype=torch.float64, device=diag.device)[:neig, :] - vr
+            nindp, vr2 = _ortho(vr, pr[rindx, :], crit_indp)
+            if nindp:
+                vr = torch.cat([vr, vr2])
+            vbas = vr @ vbas
+            wbas = vr @ wbas
+        for i in range(neig):
+            if rconv[i]:
+                continue
+            if precond is None:
+                rbas[i] = rbas[i] / ((diag - eigs[i]).abs() + lshift)
+            else:
+                rbas[i] = precond(rbas[i], diag, eigs[i], xbas[i])
+            if record is not None:
+                record(rbas[i], diag, eigs[i], xbas[i])
+        nindp, vbas2 = _ortho(vbas, rbas[rindx, :], crit_indp)
+        if nindp == 0:
+            raise RuntimeError("Davidson: unable to generate a new direction")
+        wbas2 = torch.stack([hvec(v) for v in vbas2])
+        nmvp += nindp
+        vbas = torch.cat([vbas, vbas2])
+        wbas = torch.cat([wbas, wbas2])
+    return DavidsonResult(eigs.cpu().numpy(), vr @ vbas, nmvp, maxcycle, rnorms)

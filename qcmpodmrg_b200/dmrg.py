@@ -1,0 +1,299 @@
+"""Two-site Qt DMRG driver with device-resident environments.
+
+Mirrors the reference's control flow around the hot path (ifQt=True,
+ncsite=2, one symmetry sector):
+  default(sc, fmps)     source/mpo_dmrg_class.py:329-434  -> DMRG.run
+  initOps / genHopsQt   source/mpo_dmrg_util.py:193-214, mpo_dmrg_initQt.py:88-271 -> load_mps
+  sweep                 source/mpo_dmrg_opt.py:31-101 (+ updateSite :319-350, updateBoundary :353-383)
+  ci_solver             source/mpo_dmrg_dot.py:24-112 (setupQtmpCI dotutil.py:173-184)
+  decimation            source/mpo_dmrg_dotutil.py:269-476 with rdm_blkdiag (mpo_dmrg_qparser.py:106-183)
+  genGuess              source/mpo_dmrg_dotutil.py:479-540
+Environments L_p / R_p of every operator live in HBM (TensorSet) instead of
+per-site HDF5 files; the sigma/diagonal/renormalisation plans are built once
+per dot.  Davidson, the RDM and its eigendecomposition run in FP64 on the GPU;
+the global sort of RDM eigenvalues runs on the host with NumPy so ties break
+exactly as in the reference.
+"""
+import time
+
+import numpy
+import torch
+
+from .kernels import SigmaOperator, DiagOperator, Renormalizer, TensorSet, Workspace
+from .mpo import QPHYS, build_mpo
+from .qtensor import Layout, classification
+from .davidson import davidson
+
+L_STATUS = numpy.array([False, False, True])
+R_STATUS = numpy.array([True, False, False])
+PSI_STATUS = numpy.array([False, False, False, True])
+
+
+def dpt(q1, q2):
+    q1 = numpy.asarray(q1, dtype=numpy.float64)
+    q2 = numpy.asarray(q2, dtype=numpy.float64)
+    return (q1[:, None, :] + q2[None, :, :]).reshape(-1, q1.shape[1])
+
+
+class SiteTensor(object):
+    """A site tensor in packed layout on the device (plus its dense form)."""
+
+    def __init__(self, dense, qnums, status, device):
+        cls = [classification(q) for q in qnums]
+        self.layout = Layout(status, [c[0] for c in cls], [c[1] for c in cls])
+        self.idlst = [c[2] for c in cls]
+        prj = torch.from_numpy(self.layout.prjmap(self.idlst)).to(device)
+        if not torch.is_tensor(dense):
+            dense = torch.from_numpy(numpy.ascontiguousarray(dense, dtype=numpy.float64)).to(device)
+        self.dense = dense.reshape(tuple(int(n) for n in self.layout.shape))
+        self.values = self.dense.reshape(-1)[prj].contiguous()
+
+
+def boundary_set(nops, device):
+    lay = Layout([True, False, True], [numpy.zeros((1, 2))] * 3, [numpy.ones(1, dtype=numpy.int64)] * 3)
+    return TensorSet([lay] * nops, [numpy.ones(1)] * nops, device=device)
+
+
+class DMRG(object):
+    """Two-site MPO-DMRG with every hot-path contraction on the GPU."""
+
+    def __init__(self, ham, device="cuda", precision="f64", preconditioner=None):
+        self.ham = ham
+        self.device = torch.device(device)
+        self.nsite = ham.nsite
+        self.nops = ham.sbas
+        self.opers = list(range(ham.sbas))
+        self.hpwts = numpy.ones(self.nops)
+        self.qkey = numpy.array([float(ham.nelec), 0.0])
+        self.precision = precision
+        self.preconditioner = preconditioner
+        self.crit_vec = 1.e-8
+        self.thresh = -1.e-14
+        self.ifguess = True
+        self.ws = Workspace(self.device)
+        t0 = time.time()
+        mpo = build_mpo(ham)
+        self.mpo = {i: TensorSet(l, v, device=self.device) for i, (l, v) in mpo.items()}
+        self.t_mpo = time.time() - t0
+        self.log = []
+        self.stats = {"hvec_s": 0.0, "hdiag_s": 0.0, "renorm_s": 0.0, "decim_s": 0.0, "plan_s": 0.0,
+                      "nmvp": 0, "sigma_flops": 0.0, "renorm_flops": 0.0, "diag_flops": 0.0}
+        self.events = False
+
+    # ------------------------------------------------------------- set-up
+    def load_mps(self, init):
+        K = self.nsite
+        dev = self.device
+        self.qnuml = [numpy.array(init["qnum%d" % i], dtype=numpy.float64).reshape(-1, 2) for i in range(K + 1)]
+        self.qnumr = [None] * (K + 1)
+        self.qnumr[K] = numpy.zeros((1, 2))
+        self.lmps = [SiteTensor(init["site%d" % i], [self.qnuml[i], QPHYS, self.qnuml[i + 1]], L_STATUS, dev)
+                     for i in range(K)]
+        self.rmps = [None] * K
+        self.lenv = {-1: boundary_set(self.nops, dev)}
+        self.renv = {K: boundary_set(self.nops, dev)}
+        for i in range(K):
+            rn = Renormalizer(self.ws, i, "L", self.lmps[i].layout, self.lenv[i - 1], self.mpo[i], self.opers)
+            self.lenv[i] = rn(self.lmps[i].values)
+        self.psi0 = None
+
+    # ------------------------------------------------------------- one dot
+    def dot_operators(self, isite):
+        ql, qr = self.qnuml[isite], self.qnumr[isite + 2]
+        cls = [classification(q) for q in (ql, QPHYS, QPHYS, self.qkey - qr)]
+        lay = Layout(PSI_STATUS, [c[0] for c in cls], [c[1] for c in cls])
+        idl = [c[2] for c in cls]
+        L, R = self.lenv[isite - 1], self.renv[isite + 2]
+        Wi, Wj = self.mpo[isite], self.mpo[isite + 1]
+        sig = SigmaOperator(self.ws, isite, lay, L, R, Wi, Wj, self.qkey, self.opers, self.hpwts, self.precision)
+        dg = DiagOperator(self.ws, isite, lay, L, R, Wi, Wj, self.qkey, self.opers, self.hpwts)
+        return lay, idl, sig, dg
+
+    def solve_dot(self, isite, status, dmax, crit_e):
+        dev = self.device
+        t0 = time.time()
+        lay, idl, sig, dg = self.dot_operators(isite)
+        prj = torch.from_numpy(lay.prjmap(idl)).to(dev)
+        self.stats["plan_s"] += time.time() - t0
+        ldim, rdim = len(self.qnuml[isite]), len(self.qnumr[isite + 2])
+        dims = (ldim, 16, rdim, ldim * 16 * rdim)
+        torch.cuda.synchronize(dev)
+        t0 = time.time()
+        diag = dg()
+        torch.cuda.synchronize(dev)
+        self.stats["hdiag_s"] += time.time() - t0
+        self.stats["diag_flops"] += dg.flops
+        nmv = [0]
+
+        def hv(x):
+            nmv[0] += 1
+            return sig(x)
+
+        v0 = None
+        if self.psi0 is not None:
+            v0 = self.psi0[0:1].reshape(1, -1)[:, prj].contiguous()
+        t0 = time.time()
+        res = davidson(hv, diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec, precond=self.preconditioner)
+        torch.cuda.synchronize(dev)
+        self.stats["hvec_s"] += time.time() - t0
+        self.stats["nmvp"] += res.nmvp
+        self.stats["sigma_flops"] += res.nmvp * sig.flops
+        civec = torch.zeros((1, dims[3]), dtype=torch.float64, device=dev)
+        civec[:, prj] = res.vecs
+        t0 = time.time()
+        out = self.decimate(civec, isite, status, dims, dmax)
+        torch.cuda.synchronize(dev)
+        self.stats["decim_s"] += time.time() - t0
+        return res, out, dims, sig
+
+    def decimate(self, civecs, isite, status, dims, dmax):
+        ldim, cdim, rdim, ndim = dims
+        neig = civecs.shape[0]
+        lcdim, crdim = ldim * 4, 4 * rdim
+        c = civecs.reshape(neig, lcdim, crdim)
+        if status == "L":
+            rdm = sum(c[i] @ c[i].T for i in range(neig))
+            classes = dpt(self.qnuml[isite], QPHYS)
+        else:
+            rdm = sum(c[i].T @ c[i] for i in range(neig))
+            classes = dpt(QPHYS, self.qnumr[isite + 2])
+        tr = float(torch.trace(rdm))
+        if abs(tr) < 1.e-12:
+            rdm = rdm + torch.eye(rdm.shape[0], dtype=rdm.dtype, device=rdm.device) / float(rdm.shape[0])
+        else:
+            rdm = rdm / tr
+        dwts, qred, rot, sigs = self.rdm_blkdiag(rdm, classes, dmax)
+        nres = len(qred)
+        if status == "L":
+            site = rot.reshape(ldim, 4, nres)
+            srotR = torch.stack([(rot.T @ c[i]).reshape(nres, 4, rdim) for i in range(neig)])
+        else:
+            site = rot.reshape(4, rdim, nres).permute(2, 0, 1).contiguous()
+            srotR = torch.stack([(c[i] @ rot).reshape(ldim, 4, nres) for i in range(neig)])
+        return dwts, qred, site, srotR, civecs
+
+    def rdm_blkdiag(self, rho, classes, dcut):
+        """Block eigh per (N, Sz) class on the GPU; global sort/truncation on the host."""
+        q2 = numpy.rint(2 * classes).astype(numpy.int64)
+        keys, first = [], {}
+        for i, k in enumerate(map(tuple, q2)):
+            if k not in first:
+                first[k] = []
+                keys.append(k)
+            first[k].append(i)
+        nrows = rho.shape[0]
+        qsym, cols, sig = [], [], []
+        for k in keys:
+            rows = torch.tensor(first[k], dtype=torch.int64, device=rho.device)
+            blk = rho[rows][:, rows]
+            s2, u = torch.linalg.eigh(blk)
+            qsym += [list(numpy.array(k) / 2.0)] * len(first[k])
+            col = torch.zeros((nrows, len(first[k])), dtype=rho.dtype, device=rho.device)
+            col[rows, :] = u
+            cols.append(col)
+            sig.append(s2.abs())
+        rot = torch.cat(cols, dim=1)
+        sig_h = torch.cat(sig).cpu().numpy()
+        sig_h = sig_h / numpy.sum(sig_h)
+        indx = numpy.argsort(sig_h)[::-1]
+        nres = len(sig_h)
+        tsig = sig_h[indx]
+        for i in range(nres):
+            if tsig[i] < self.thresh * 1.01:
+                nres = i
+                break
+        if nres == 0:
+            nres = 1
+        if dcut > 0:
+            nres = min(nres, dcut)
+        indx = indx[:nres]
+        s = sig_h[indx].copy()
+        dwts = 1.0 - numpy.sum(s)
+        qk = [qsym[i] for i in indx]
+        o = sorted(range(nres), key=lambda x: qk[x])
+        sel = numpy.asarray(indx)[o].copy()
+        qred = numpy.array([qk[i] for i in o], dtype=numpy.float64)
+        rot = rot[:, torch.from_numpy(sel).to(rot.device)].contiguous()
+        return dwts, qred, rot, s[o]
+
+    # ------------------------------------------------------------- sweeps
+    def sweep(self, status, dmax, crit_e):
+        K = self.nsite
+        dev = self.device
+        actlst = list(range(0, K - 1)) if status == "L" else list(range(K - 2, -1, -1))
+        elst, dlst, nmvp = [], [], 0
+        for isite in actlst:
+            res, (dwts, qred, site, srotR, civecs), dims, sig = self.solve_dot(isite, status, dmax, crit_e)
+            nmvp += res.nmvp
+            elst.append(float(res.eigs[0]))
+            dlst.append(float(dwts))
+            t0 = time.time()
+            if status == "L":
+                self.qnuml[isite + 1] = qred
+                st = SiteTensor(site, [self.qnuml[isite], QPHYS, qred], L_STATUS, dev)
+                self.lmps[isite] = st
+                rn = Renormalizer(self.ws, isite, "L", st.layout, self.lenv[isite - 1], self.mpo[isite], self.opers)
+                self.lenv[isite] = rn(st.values)
+            else:
+                j = isite + 1
+                self.qnumr[j] = qred
+                st = SiteTensor(site, [qred, QPHYS, self.qnumr[j + 1]], R_STATUS, dev)
+                self.rmps[j] = st
+                rn = Renormalizer(self.ws, j, "R", st.layout, self.renv[j + 1], self.mpo[j], self.opers)
+                self.renv[j] = rn(st.values)
+            torch.cuda.synchronize(dev)
+            self.stats["renorm_s"] += time.time() - t0
+            self.stats["renorm_flops"] += rn.flops
+            self.guess(isite, status, actlst, civecs, srotR)
+            self.log.append({"status": status, "isite": isite, "e": elst[-1], "dwt": dlst[-1],
+                             "nmvp": int(res.nmvp), "bond": int(len(qred)), "ndim0": int(sig.ndim0),
+                             "sigma_gflop": sig.flops / 1e9})
+        smat = srotR[0] / torch.linalg.norm(srotR[0])
+        qk = self.qkey.reshape(1, 2).copy()
+        if status == "L":
+            self.lmps[K - 1] = SiteTensor(smat, [qred, QPHYS, qk], L_STATUS, dev)
+            self.qnuml[K] = qk
+        else:
+            self.rmps[0] = SiteTensor(smat, [qk, QPHYS, qred], R_STATUS, dev)
+            self.qnumr[0] = qk
+        i = int(numpy.argmin(elst))
+        return nmvp, elst[i], dlst[i], elst, dlst
+
+    def guess(self, isite, status, actlst, civecs, srotR):
+        if not self.ifguess:
+            return
+        if isite == actlst[-1]:
+            self.psi0 = civecs.clone()
+        elif status == "R":
+            t = self.lmps[isite - 1].dense
+            self.psi0 = torch.stack([torch.tensordot(t, srotR[i], dims=([2], [0])).reshape(-1)
+                                     for i in range(srotR.shape[0])])
+        else:
+            t = self.rmps[isite + 2].dense
+            self.psi0 = torch.stack([torch.tensordot(srotR[i], t, dims=([2], [0])).reshape(-1)
+                                     for i in range(srotR.shape[0])])
+
+    def run(self, init_mps, dmax, nsweeps, tol=1.e-7, callback=None):
+        """schedule.fixed(ncsite=2, maxM=dmax, tol=tol, noise=0): sweeps R then L until |dE| < tol."""
+        self.load_mps(init_mps)
+        eav, dwt, esweeps, nmvps = [], [], [], []
+        eold = 1.e3
+        for isweep in range(nsweeps):
+            t0 = time.time()
+            n1, e1, d1, el1, dl1 = self.sweep("R", dmax, tol)
+            n2, e2, d2, el2, dl2 = self.sweep("L", dmax, tol)
+            nmvps.append(n1 + n2)
+            esweeps += el1 + el2
+            if e1 < e2:
+                eav.append(e1)
+                dwt.append(d1)
+            else:
+                eav.append(e2)
+                dwt.append(d2)
+            if callback is not None:
+                callback(isweep, eav[-1], time.time() - t0)
+            if abs(eav[-1] - eold) < tol:
+                break
+            eold = eav[-1]
+        return {"eav": numpy.array(eav), "dwt": numpy.array(dwt), "esweeps": numpy.array(esweeps),
+                "nmvp": numpy.array(nmvps)}

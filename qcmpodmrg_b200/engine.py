@@ -1,0 +1,195 @@
+"""Device execution of block-pair contraction stages.
+
+A *stage* is one contraction (one tensordotSYM/tensordotCAL pair of the
+reference) applied to every operator at once: its block-pair lists are
+compiled into GPU work items (one task per output tile, one contribution per
+block pair) by the native plan compiler and executed by one launch of the
+grouped block GEMM (qc_bgemm_*).  Plans are built once per dot and reused for
+every Davidson iteration.
+"""
+import numpy
+import torch
+
+from . import native
+from .native import ptr, check
+from .qtensor import Contraction
+
+TASK_DT = numpy.dtype([("c_off", "<i8"), ("M", "<i4"), ("N", "<i4"), ("m0", "<i4"), ("n0", "<i4"),
+                       ("mlo", "<i4"), ("nlo", "<i4"), ("c_mh", "<i4"), ("c_ml", "<i4"), ("c_nh", "<i4"),
+                       ("c_nl", "<i4"), ("cb", "<i4"), ("ce", "<i4"), ("op_b", "<i4"), ("op_e", "<i4")])
+CONTRIB_DT = numpy.dtype([("a_off", "<i8"), ("b_off", "<i8"), ("alpha", "<f8"), ("K", "<i4"), ("klo", "<i4"),
+                          ("a_mh", "<i4"), ("a_ml", "<i4"), ("a_kh", "<i4"), ("a_kl", "<i4"), ("b_kh", "<i4"),
+                          ("b_kl", "<i4"), ("b_nh", "<i4"), ("b_nl", "<i4"), ("op_b", "<i4"), ("op_e", "<i4"),
+                          ("pad2", "<i4"), ("pad3", "<i4")])
+OP_DT = numpy.dtype([("a_base", "<i8"), ("b_base", "<i8"), ("c_base", "<i8"), ("alpha", "<f8")])
+assert TASK_DT.itemsize == native.TASK_BYTES and CONTRIB_DT.itemsize == native.CONTRIB_BYTES
+assert OP_DT.itemsize == native.OP_BYTES
+
+TILES = {0: (64, 64), 1: (128, 32), 2: (256, 16)}
+
+
+def pick_tile(ns):
+    """Choose the output tile shape from the typical N (columns) of a stage."""
+    n = float(numpy.median(ns)) if len(ns) else 64.0
+    if n <= 16:
+        return 2
+    if n <= 32:
+        return 1
+    return 0
+
+
+def compile_template(l1, l2, lo, axes, triples, tile_cfg):
+    """Work items of one contraction for a single operator with zero base offsets.
+
+    The operator loop is added afterwards through op ranges into an operator table.
+    """
+    return compile_pairs(l1, l2, lo, axes, triples, [0], [0], [0], [1.0], 0, tile_cfg)
+
+
+def compile_pairs(l1, l2, lo, axes, triples, base1, base2, baseo, alpha, group_ops, tile_cfg):
+    """Native plan compiler wrapper -> (tasks, contribs, flops)."""
+    lib = native.lib()
+    tm, tn = TILES[tile_cfg]
+    ax1 = numpy.array(axes[0], dtype=numpy.int32)
+    ax2 = numpy.array(axes[1], dtype=numpy.int32)
+    tri = numpy.ascontiguousarray(triples, dtype=numpy.int64)
+    b1 = numpy.ascontiguousarray(base1, dtype=numpy.int64)
+    b2 = numpy.ascontiguousarray(base2, dtype=numpy.int64)
+    bo = numpy.ascontiguousarray(baseo, dtype=numpy.int64)
+    al = numpy.ascontiguousarray(alpha, dtype=numpy.float64)
+    nt = numpy.zeros(1, dtype=numpy.int64)
+    fl = numpy.zeros(1, dtype=numpy.float64)
+    head = (l1.rank, ptr(l1.nsyms), ptr(l1.ndims_cat), ptr(l1.ioff), l2.rank, ptr(l2.nsyms), ptr(l2.ndims_cat),
+            ptr(l2.ioff), lo.rank, ptr(lo.nsyms), ptr(lo.ndims_cat), ptr(lo.ioff), len(axes[0]), ptr(ax1), ptr(ax2), len(tri), ptr(tri), len(b1), ptr(b1), ptr(b2), ptr(bo),
+            ptr(al), int(group_ops), tm, tn)
+    nc = check(lib.qc_compile_pairs(*(head + (None, 0, None, 0, ptr(nt), ptr(fl)))), "qc_compile_pairs")
+    ntask = int(nt[0])
+    tasks = numpy.zeros(max(ntask, 1), dtype=TASK_DT)
+    contribs = numpy.zeros(max(nc, 1), dtype=CONTRIB_DT)
+    nc2 = check(lib.qc_compile_pairs(*(head + (ptr(tasks), ntask, ptr(contribs), nc, ptr(nt), ptr(fl)))),
+                "qc_compile_pairs")
+    assert nc2 == nc and int(nt[0]) == ntask
+    return tasks[:ntask], contribs[:nc], float(fl[0])
+
+
+def merge_grouped(parts):
+    """Merge per-class task lists that write the same output blocks (sigma's sum over operators).
+
+    Tasks of one output block (same c_off) share one contribution range within a
+    part.  The merged list has, per output block, the contributions of all parts
+    (in part order) and the tiles of that block once.
+    """
+    parts = [p for p in parts if len(p[0])]
+    flops = sum(p[2] for p in parts)
+    if not parts:
+        return numpy.zeros(0, TASK_DT), numpy.zeros(0, CONTRIB_DT), flops
+    cbase = numpy.cumsum([0] + [len(p[1]) for p in parts])
+    tbase = numpy.cumsum([0] + [len(p[0]) for p in parts])
+    all_t = numpy.concatenate([p[0] for p in parts])
+    all_c = numpy.concatenate([p[1] for p in parts])
+    part_of = numpy.repeat(numpy.arange(len(parts)), [len(p[0]) for p in parts])
+    coff = all_t["c_off"]
+    first = numpy.ones(len(all_t), dtype=bool)
+    first[1:] = (coff[1:] != coff[:-1]) | (part_of[1:] != part_of[:-1])
+    fidx = numpy.flatnonzero(first)
+    # records: one per (part, output block)
+    r_coff = coff[fidx]
+    r_part = part_of[fidx]
+    r_cb = all_t["cb"][fidx] + cbase[r_part]
+    r_ce = all_t["ce"][fidx] + cbase[r_part]
+    r_ntile = numpy.diff(numpy.append(fidx, len(all_t)))
+    order = numpy.lexsort((r_part, r_coff))
+    r_coff, r_part, r_cb, r_ce, r_ntile, fidx = (x[order] for x in (r_coff, r_part, r_cb, r_ce, r_ntile, fidx))
+    lens = r_ce - r_cb
+    # contribution gather index: concatenation of [cb, ce) in record order
+    starts = numpy.repeat(r_cb - numpy.cumsum(numpy.append(0, lens[:-1])), lens)
+    gidx = starts + numpy.arange(lens.sum())
+    new_c = all_c[gidx]
+    # one group per output block
+    gfirst = numpy.ones(len(r_coff), dtype=bool)
+    gfirst[1:] = r_coff[1:] != r_coff[:-1]
+    gstart = numpy.flatnonzero(gfirst)
+    cum = numpy.append(0, numpy.cumsum(lens))
+    g_cb = cum[gstart]
+    g_ce = cum[numpy.append(gstart[1:], len(r_coff))]
+    # tiles: those of the first record of each group
+    g_t0 = fidx[gstart]
+    g_nt = r_ntile[gstart]
+    tix = numpy.repeat(g_t0 - numpy.cumsum(numpy.append(0, g_nt[:-1])), g_nt) + numpy.arange(g_nt.sum())
+    new_t = all_t[tix].copy()
+    new_t["cb"] = numpy.repeat(g_cb, g_nt)
+    new_t["ce"] = numpy.repeat(g_ce, g_nt)
+    return new_t, new_c, flops
+
+
+class Stage(object):
+    """A compiled stage resident on the device.
+
+    parts: list of (tasks, contribs, flops) whose op ranges index ``ops`` (OP_DT).
+    summed: tasks accumulate over the operators of each contribution (sigma's
+    last contraction) instead of writing one tile per operator.
+    """
+
+    def __init__(self, parts, tile_cfg, device, name="", ops=None, summed=False):
+        tasks, contribs = [], []
+        nc = 0
+        flops = 0.0
+        for (t, c, f) in parts:
+            if len(t):
+                t = t.copy()
+                t["cb"] += nc
+                t["ce"] += nc
+                tasks.append(t)
+                contribs.append(c)
+                nc += len(c)
+            flops += f
+        if ops is None:
+            ops = numpy.zeros(1, dtype=OP_DT)
+            ops["alpha"] = 1.0
+        self.name = name
+        self.tile_cfg = tile_cfg
+        self.summed = bool(summed)
+        self.flops = flops
+        self.ntasks = int(sum(len(t) for t in tasks))
+        self.ncontribs = nc
+        tk = numpy.concatenate(tasks) if tasks else numpy.zeros(0, TASK_DT)
+        ct = numpy.concatenate(contribs) if contribs else numpy.zeros(0, CONTRIB_DT)
+        self.host_tasks, self.host_contribs, self.host_ops = tk, ct, ops
+        self.d_tasks = torch.from_numpy(tk.view(numpy.uint8).copy()).to(device)
+        self.d_contribs = torch.from_numpy(ct.view(numpy.uint8).copy()).to(device)
+        self.d_ops = torch.from_numpy(ops.view(numpy.uint8).copy()).to(device)
+
+    def run(self, A, B, C, kind="f64", stream=None):
+        if self.ntasks == 0:
+            return
+        lib = native.lib()
+        s = stream if stream is not None else torch.cuda.current_stream(C.device).cuda_stream
+        fn = {"f64": lib.qc_bgemm_f64, "f32": lib.qc_bgemm_f32, "tf32": getattr(lib, "qc_bgemm_tf32", None)}[kind]
+        check(fn(self.d_tasks.data_ptr(), self.ntasks, self.d_contribs.data_ptr(), self.d_ops.data_ptr(),
+                 int(self.summed), A.data_ptr(), B.data_ptr(), C.data_ptr(), self.tile_cfg, s), "qc_bgemm_" + kind)
+
+
+def op_table(a_base, b_base, c_base, alpha):
+    n = max(numpy.size(x) for x in (a_base, b_base, c_base, alpha))
+    t = numpy.zeros(n, dtype=OP_DT)
+    t["a_base"] = a_base
+    t["b_base"] = b_base
+    t["c_base"] = c_base
+    t["alpha"] = alpha
+    return t
+
+
+def live_blocks(layout, triples):
+    live = numpy.zeros(layout.nblks, dtype=bool)
+    if len(triples):
+        live[triples[:, 0]] = True
+    return live
+
+
+def prune(triples, live1=None, live2=None):
+    keep = numpy.ones(len(triples), dtype=bool)
+    if live1 is not None and len(triples):
+        keep &= live1[triples[:, 1]]
+    if live2 is not None and len(triples):
+        keep &= live2[triples[:, 2]]
+    return triples[keep]

@@ -1,0 +1,457 @@
+"""Device operators of the two-site hot path: sigma, diagonal, renormalisation.
+
+  SigmaOperator  <- HVecQt        source/mpo_dmrg_kernelQt.py:153-319 (two-site :238-317)
+  DiagOperator   <- HDiagQt       source/mpo_dmrg_kernelQt.py:30-127  (two-site :77-119)
+  Renormalizer   <- renormQt_H00  source/mpo_dmrg_kernelQt.py:633-767 (also genHopsQt,
+                                  source/mpo_dmrg_initQt.py:88-271, which is the same chain)
+
+The reference loops over operators p, MPO slices and block pairs in Python and
+calls numpy.tensordot per pair.  Here the operator loop is folded into the
+work lists: each of the four sigma contractions (L.psi, .W_i, .W_{i+1}, .R) is
+one launch over all operators and all block pairs, with intermediates in HBM
+scratch and the sum over operators done inside the last launch (no atomics).
+Block-pair lists are built per symmetry class of the operator, as the
+reference caches its templates per class.
+"""
+import numpy
+import torch
+
+from . import native
+from .native import check
+from .engine import (Stage, compile_template, merge_grouped, live_blocks, prune, pick_tile, op_table,
+                     TASK_DT, CONTRIB_DT)
+from .mpo import case
+from .qtensor import Contraction, flip_right, flip_horizontal
+
+
+class Workspace(object):
+    """Grow-only device scratch buffers shared by all operators of a context."""
+
+    def __init__(self, device):
+        self.device = device
+        self.bufs = {}
+
+    def get(self, name, numel, dtype):
+        b = self.bufs.get((name, dtype))
+        if b is None or b.numel() < numel:
+            self.bufs.pop((name, dtype), None)
+            b = torch.empty(max(int(numel), 1) + 64, dtype=dtype, device=self.device)
+            self.bufs[(name, dtype)] = b
+        return b
+
+
+class TensorSet(object):
+    """Per-operator block tensors (environments or site operators) back to back in one buffer."""
+
+    def __init__(self, layouts, values, offsets=None, device=None):
+        self.layouts = list(layouts)
+        if offsets is None:
+            sizes = numpy.array([l.size for l in self.layouts], dtype=numpy.int64)
+            offsets = numpy.concatenate([[0], numpy.cumsum(sizes)[:-1]]).astype(numpy.int64)
+        self.offsets = numpy.asarray(offsets, dtype=numpy.int64)
+        self.total = int(self.offsets[-1] + self.layouts[-1].size) if self.layouts else 0
+        if isinstance(values, (list, tuple)):
+            host = numpy.concatenate([numpy.asarray(v, dtype=numpy.float64) for v in values]) \
+                if values else numpy.zeros(0)
+            values = torch.from_numpy(host).to(device)
+        self.values = values
+        self._f32 = None
+
+    def f32(self):
+        if self._f32 is None or self._f32.data_ptr() == 0:
+            self._f32 = self.values.to(torch.float32)
+        return self._f32
+
+    def op_values(self, i):
+        o = int(self.offsets[i])
+        return self.values[o:o + self.layouts[i].size]
+
+    def nbytes(self):
+        return self.values.numel() * self.values.element_size()
+
+
+def _stream(device):
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def gather(src, idx, out):
+    """out[i] = src[idx[i]] on the device (qc_gather_f64)."""
+    check(native.lib().qc_gather_f64(src.data_ptr(), idx.data_ptr(), out.data_ptr(), out.numel(),
+                                     _stream(out.device)), "qc_gather_f64")
+    return out
+
+
+def convert(src, out):
+    """FP64 <-> FP32 conversion on the device."""
+    lib = native.lib()
+    n = min(src.numel(), out.numel())
+    if src.dtype == torch.float64:
+        check(lib.qc_convert_f64_to_f32(src.data_ptr(), out.data_ptr(), n, _stream(out.device)), "convert")
+    else:
+        check(lib.qc_convert_f32_to_f64(src.data_ptr(), out.data_ptr(), n, _stream(out.device)), "convert")
+    return out
+
+
+def _groups(opers, isite, ncsite):
+    g = {}
+    for iop, p in enumerate(opers):
+        g.setdefault(case(p, isite, ncsite), []).append(iop)
+    return g
+
+
+def _ncols(c, triples):
+    """N extent (product of the operand-2 external dims) of the output blocks a stage writes."""
+    if len(triples) == 0:
+        return numpy.array([64])
+    ne1 = c.l1.rank - len(c.axes[0])
+    ob = numpy.unique(triples[:, 0])
+    return numpy.prod(c.out.block_dims(ob)[:, ne1:], axis=1)
+
+
+class SigmaOperator(object):
+    """sigma = sum_p w_p R_p W_p[i+1] W_p[i] L_p psi for the dot (isite, isite+1)."""
+
+    def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts, precision="f64"):
+        self.ws, self.psi, self.precision = ws, psi_layout, precision
+        self.L, self.R, self.Wi, self.Wj = L, R, Wi, Wj
+        dev = ws.device
+        groups = _groups(opers, isite, 2)
+        nops = len(opers)
+        ax = (([2], [0]), ([0, 2], [0, 3]), ([1, 3], [3, 0]), ([1, 3], [2, 0]))
+        bases = [numpy.zeros(nops, dtype=numpy.int64) for _ in range(3)]
+        tot = [0, 0, 0]
+        plans = {}
+        for key, ops in sorted(groups.items()):
+            i0 = ops[0]
+            Ll, W1, W2 = L.layouts[i0], Wi.layouts[i0], Wj.layouts[i0]
+            Rl = flip_right(R.layouts[i0], qkey)
+            for i in ops:
+                if (L.layouts[i] is not Ll or Wi.layouts[i] is not W1 or Wj.layouts[i] is not W2
+                        or flip_right(R.layouts[i], qkey) is not Rl):
+                    raise ValueError("operators of one symmetry class must share their block structure")
+            c1 = Contraction(Ll, psi_layout, ax[0])
+            t1 = c1.triples
+            c2 = Contraction(c1.out, W1, ax[1])
+            t2 = prune(c2.triples, live1=live_blocks(c1.out, t1))
+            c3 = Contraction(c2.out, W2, ax[2])
+            t3 = prune(c3.triples, live1=live_blocks(c2.out, t2))
+            c4 = Contraction(c3.out, Rl, ax[3])
+            t4 = prune(c4.triples, live1=live_blocks(c3.out, t3))
+            if c4.out is not psi_layout:
+                raise ValueError("sigma output layout differs from the wavefunction template")
+            plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3), (c4, t4), Rl)
+            for s, c in enumerate((c1, c2, c3)):
+                for i in ops:
+                    bases[s][i] = tot[s]
+                    tot[s] += c.out.size
+        self.tot = tot
+        hp = numpy.asarray(hpwts, dtype=numpy.float64)
+        ncols = [[], [], [], []]
+        for key, (ops, *cs, Rl) in sorted(plans.items()):
+            for si, (c, t) in enumerate(cs):
+                ncols[si].append(_ncols(c, t))
+        self.tiles = [pick_tile(numpy.concatenate(n)) for n in ncols]
+        # operator tables: operators ordered class by class
+        order = numpy.concatenate([numpy.array(plans[k][0]) for k in sorted(plans)])
+        tabs = [op_table(L.offsets[order], 0, bases[0][order], 1.0),
+                op_table(bases[0][order], Wi.offsets[order], bases[1][order], 1.0),
+                op_table(bases[1][order], Wj.offsets[order], bases[2][order], 1.0),
+                op_table(bases[2][order], R.offsets[order], 0, hp[order])]
+        st = [[], [], [], []]
+        pos = 0
+        for key, (ops, *cs, Rl) in sorted(plans.items()):
+            ob, oe = pos, pos + len(ops)
+            pos = oe
+            for si, (c, t) in enumerate(cs):
+                tk, ct, fl = compile_template(c.l1, c.l2, c.out, ax[si], t, self.tiles[si])
+                if si < 3:
+                    tk["op_b"], tk["op_e"] = ob, oe
+                else:
+                    ct["op_b"], ct["op_e"] = ob, oe
+                st[si].append((tk, ct, fl * len(ops)))
+        self.stages = [Stage(st[si], self.tiles[si], dev, "sigma%d" % (si + 1), tabs[si]) for si in range(3)]
+        self.stages.append(Stage([merge_grouped(st[3])], self.tiles[3], dev, "sigma4", tabs[3], summed=True))
+        self.flops = sum(s.flops for s in self.stages)
+        self.ndim0 = psi_layout.size
+
+    def scratch_bytes(self):
+        return 8 * sum(self.tot)
+
+    def __call__(self, x, y=None):
+        """x: device tensor (ndim0,) float64 -> y = H x (float64)."""
+        ws = self.ws
+        if y is None:
+            y = torch.empty(self.ndim0, dtype=torch.float64, device=ws.device)
+        if self.precision == "f64":
+            T1 = ws.get("t1", self.tot[0], torch.float64)
+            T2 = ws.get("t2", self.tot[1], torch.float64)
+            T3 = ws.get("t3", self.tot[2], torch.float64)
+            s = self.stages
+            s[0].run(self.L.values, x, T1, "f64")
+            s[1].run(T1, self.Wi.values, T2, "f64")
+            s[2].run(T2, self.Wj.values, T3, "f64")
+            y.zero_()
+            s[3].run(T3, self.R.values, y, "f64")
+            return y
+        kind = "tf32" if self.precision == "tf32" else "f32"
+        T1 = ws.get("t1", self.tot[0], torch.float32)
+        T2 = ws.get("t2", self.tot[1], torch.float32)
+        T3 = ws.get("t3", self.tot[2], torch.float32)
+        x32 = ws.get("x32", self.ndim0, torch.float32)
+        y32 = ws.get("y32", self.ndim0, torch.float32)
+        convert(x, x32)
+        s = self.stages
+        s[0].run(self.L.f32(), x32, T1, kind)
+        s[1].run(T1, self.Wi.f32(), T2, "f32")
+        s[2].run(T2, self.Wj.f32(), T3, "f32")
+        y32[:self.ndim0].zero_()
+        s[3].run(T3, self.R.f32(), y32, kind)
+        convert(y32, y)
+        return y
+
+
+def _dense_tasks(M, N, K, a_off, a_m, a_k, b_off, b_k, b_n, c_off, c_m, alpha, groups, tile_cfg):
+    """Work items for dense GEMMs C_g = sum_{j in group g} alpha_j A_j B_j.
+
+    a_off/b_off/alpha are per contribution; groups is a list of (c_off, [contribution ids]).
+    """
+    from .engine import TILES
+    tm, tn = TILES[tile_cfg]
+    ncontr = len(a_off)
+    contribs = numpy.zeros(ncontr, dtype=CONTRIB_DT)
+    contribs["a_off"] = a_off
+    contribs["b_off"] = b_off
+    contribs["alpha"] = alpha
+    contribs["K"] = K
+    contribs["klo"] = K
+    contribs["a_ml"] = a_m
+    contribs["a_kl"] = a_k
+    contribs["b_kl"] = b_k
+    contribs["b_nl"] = b_n
+    contribs["op_b"] = 0
+    contribs["op_e"] = 1
+    tasks = []
+    order = []
+    for (co, ids) in groups:
+        cb = len(order)
+        order.extend(ids)
+        for m0 in range(0, M, tm):
+            for n0 in range(0, N, tn):
+                tasks.append((co, M, N, m0, n0, M, N, 0, c_m, 0, 1, cb, len(order), 0, 1))
+    t = numpy.array(tasks, dtype=TASK_DT)
+    return t, contribs[numpy.array(order, dtype=numpy.int64)], 2.0 * M * N * K * ncontr
+
+
+class DiagOperator(object):
+    """Davidson diagonal in the packed wavefunction layout (HDiagQt, two-site)."""
+
+    def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts):
+        dev = ws.device
+        self.ws = ws
+        nops = len(opers)
+        ql = psi_layout
+        ldim = int(ql.shape[0])
+        rdim = int(ql.shape[3])
+        A = int(L.layouts[0].shape[0])
+        Ab = int(Wi.layouts[0].shape[1])
+        Ac = int(R.layouts[0].shape[0])
+        self.dims = (A, Ab, Ac, ldim, rdim)
+        # ---- index maps for the diagonal elements (host, once per dot) ----
+        Lsrc, Ldst = [], []
+        Rsrc, Rdst = [], []
+        Wsrc1, Wdst1, Wsrc2, Wdst2 = [], [], [], []
+        cache = {}
+
+        def env_diag(lay, off, opi, nrow, ncol, into_s, into_d):
+            key = ("e", id(lay))
+            if key not in cache:
+                s, d = [], []
+                for idx in lay.idx_allowed:
+                    sa, s1, s2 = numpy.unravel_index(idx, tuple(lay.nsyms))
+                    if s1 != s2:
+                        continue
+                    da, dl, _ = lay.block_dims(idx)[0]
+                    w, u = numpy.meshgrid(numpy.arange(da), numpy.arange(dl), indexing="ij")
+                    s.append(lay.ioff[idx] + w * dl * dl + u * dl + u)
+                    d.append((lay.secoff[0][sa] + w) * ncol + lay.secoff[1][s1] + u)
+                cache[key] = (numpy.concatenate([x.ravel() for x in s]) if s else numpy.zeros(0, numpy.int64),
+                              numpy.concatenate([x.ravel() for x in d]) if d else numpy.zeros(0, numpy.int64))
+            s, d = cache[key]
+            into_s.append(s + off)
+            into_d.append(d + opi * nrow * ncol)
+
+        def w_diag(lay, off, opi, n1, n2, into_s, into_d):
+            key = ("w", id(lay))
+            if key not in cache:
+                s, d = [], []
+                for idx in lay.idx_allowed:
+                    sa, sb, n, n_ = numpy.unravel_index(idx, tuple(lay.nsyms))
+                    if n != n_:
+                        continue
+                    da, db = lay.block_dims(idx)[0][:2]
+                    w, v = numpy.meshgrid(numpy.arange(da), numpy.arange(db), indexing="ij")
+                    s.append(lay.ioff[idx] + w * db + v)
+                    d.append(((lay.secoff[0][sa] + w) * n2 + lay.secoff[1][sb] + v) * 4 + n)
+                cache[key] = (numpy.concatenate([x.ravel() for x in s]) if s else numpy.zeros(0, numpy.int64),
+                              numpy.concatenate([x.ravel() for x in d]) if d else numpy.zeros(0, numpy.int64))
+            s, d = cache[key]
+            into_s.append(s + off)
+            into_d.append(d + opi * n1 * n2 * 4)
+
+        for i in range(nops):
+            env_diag(L.layouts[i], L.offsets[i], i, A, ldim, Lsrc, Ldst)
+            env_diag(R.layouts[i], R.offsets[i], i, Ac, rdim, Rsrc, Rdst)
+            w_diag(Wi.layouts[i], Wi.offsets[i], i, A, Ab, Wsrc1, Wdst1)
+            w_diag(Wj.layouts[i], Wj.offsets[i], i, Ab, Ac, Wsrc2, Wdst2)
+        cat = lambda x: torch.from_numpy(numpy.concatenate(x).astype(numpy.int64)).to(dev)
+        self.maps = [(cat(Lsrc), cat(Ldst), nops * A * ldim, "ld", L),
+                     (cat(Rsrc), cat(Rdst), nops * Ac * rdim, "rd", R),
+                     (cat(Wsrc1), cat(Wdst1), nops * A * Ab * 4, "w1", Wi),
+                     (cat(Wsrc2), cat(Wdst2), nops * Ab * Ac * 4, "w2", Wj)]
+        # ---- packed output gather: psi block (sl, n, m, sr), element (u, v) ----
+        gat = numpy.empty(ql.size, dtype=numpy.int64)
+        for idx in ql.idx_allowed:
+            sl, n, m, sr = numpy.unravel_index(idx, tuple(ql.nsyms))
+            bd = ql.block_dims(idx)[0]
+            dl, dr = bd[0], bd[3]
+            u, v = numpy.meshgrid(numpy.arange(dl), numpy.arange(dr), indexing="ij")
+            o = int(ql.ioff[idx])
+            gat[o:o + dl * dr] = ((n * 4 + m) * ldim * rdim + (ql.secoff[0][sl] + u) * rdim
+                                  + ql.secoff[3][sr] + v).ravel()
+        self.gather = torch.from_numpy(gat).to(dev)
+        self.ndim0 = ql.size
+        # ---- three dense GEMM stages ----
+        hp = numpy.asarray(hpwts, dtype=numpy.float64)
+        # X[p, n, m, a, c] = sum_b W1[p, a, b, n] W2[p, b, c, m]
+        a_off, b_off, al, grp = [], [], [], []
+        for p in range(nops):
+            for n in range(4):
+                for m in range(4):
+                    grp.append((((p * 16 + n * 4 + m) * A * Ac), [len(a_off)]))
+                    a_off.append(p * A * Ab * 4 + n)
+                    b_off.append(p * Ab * Ac * 4 + m)
+                    al.append(1.0)
+        sX = _dense_tasks(A, Ac, Ab, a_off, Ab * 4, 4, b_off, Ac * 4, 4, None, Ac, al, grp, 0)
+        # T[p, nm, c, l] = sum_a X[p, nm, a, c] Ld[p, a, l]
+        a_off, b_off, al, grp = [], [], [], []
+        for p in range(nops):
+            for nm in range(16):
+                grp.append(((p * 16 + nm) * Ac * ldim, [len(a_off)]))
+                a_off.append((p * 16 + nm) * A * Ac)
+                b_off.append(p * A * ldim)
+                al.append(1.0)
+        sT = _dense_tasks(Ac, ldim, A, a_off, 1, Ac, b_off, ldim, 1, None, ldim, al, grp, 0)
+        # D[nm, l, r] = sum_p w_p sum_c T[p, nm, c, l] Rd[p, c, r]
+        a_off, b_off, al, grp = [], [], [], []
+        for nm in range(16):
+            ids = []
+            for p in range(nops):
+                ids.append(len(a_off))
+                a_off.append((p * 16 + nm) * Ac * ldim)
+                b_off.append(p * Ac * rdim)
+                al.append(hp[p])
+            grp.append((nm * ldim * rdim, ids))
+        sD = _dense_tasks(ldim, rdim, Ac, a_off, 1, ldim, b_off, rdim, 1, None, rdim, al, grp, 0)
+        self.sX = Stage([sX], 0, dev, "diagX")
+        self.sT = Stage([sT], 0, dev, "diagT")
+        self.sD = Stage([sD], 0, dev, "diagD")
+        self.nX = nops * 16 * A * Ac
+        self.nT = nops * 16 * Ac * ldim
+        self.nD = 16 * ldim * rdim
+        self.flops = self.sX.flops + self.sT.flops + self.sD.flops
+
+    def __call__(self):
+        ws = self.ws
+        bufs = {}
+        for (src, dst, n, name, tset) in self.maps:
+            b = ws.get("diag_" + name, n, torch.float64)
+            b[:n].zero_()
+            if src.numel():
+                b[dst] = tset.values[src]
+            bufs[name] = b
+        X = ws.get("diag_x", self.nX, torch.float64)
+        T = ws.get("diag_t", self.nT, torch.float64)
+        D = ws.get("diag_d", self.nD, torch.float64)
+        self.sX.run(bufs["w1"], bufs["w2"], X, "f64")
+        self.sT.run(X, bufs["ld"], T, "f64")
+        self.sD.run(T, bufs["rd"], D, "f64")
+        out = torch.empty(self.ndim0, dtype=torch.float64, device=ws.device)
+        return gather(D, self.gather, out)
+
+
+class Renormalizer(object):
+    """New environments of every operator after a decimation (renormQt_H00).
+
+    status 'L': L'[b, r, r'] = sum site*[l, n, r] L[a, l, l'] W[a, b, n, n'] site[l', n', r']
+    status 'R': the mirror image with W's bond indices flipped (kernelQt.py:723-740).
+    """
+
+    def __init__(self, ws, isite, status, site_layout, E, W, opers):
+        self.ws, self.status = ws, status
+        dev = ws.device
+        groups = _groups(opers, isite, 1)
+        nops = len(opers)
+        if status == "L":
+            ax = (([0], [1]), ([0, 2], [2, 0]), ([1, 3], [1, 0]))
+        else:
+            ax = (([2], [1]), ([1, 2], [2, 1]), ([1, 3], [1, 2]))
+        bases = [numpy.zeros(nops, dtype=numpy.int64) for _ in range(3)]
+        tot = [0, 0, 0]
+        plans = {}
+        out_layouts = [None] * nops
+        for key, ops in sorted(groups.items()):
+            i0 = ops[0]
+            El = E.layouts[i0]
+            Wl = W.layouts[i0] if status == "L" else flip_horizontal(W.layouts[i0])
+            for i in ops:
+                if E.layouts[i] is not El or W.layouts[i] is not W.layouts[i0]:
+                    raise ValueError("operators of one symmetry class must share their block structure")
+            c1 = Contraction(site_layout, El, ax[0])
+            t1 = c1.triples
+            c2 = Contraction(Wl, c1.out, ax[1])
+            t2 = prune(c2.triples, live2=live_blocks(c1.out, t1))
+            c3 = Contraction(c2.out, site_layout, ax[2])
+            t3 = prune(c3.triples, live1=live_blocks(c2.out, t2))
+            plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3))
+            for s, c in enumerate((c1, c2, c3)):
+                for i in ops:
+                    bases[s][i] = tot[s]
+                    tot[s] += c.out.size
+                    if s == 2:
+                        out_layouts[i] = c.out
+        self.out_layouts = out_layouts
+        self.out_offsets = bases[2].copy()
+        self.tot = tot
+        ncols = [[], [], []]
+        for key, (ops, *cs) in sorted(plans.items()):
+            for si, (c, t) in enumerate(cs):
+                ncols[si].append(_ncols(c, t))
+        self.tiles = [pick_tile(numpy.concatenate(n)) for n in ncols]
+        order = numpy.concatenate([numpy.array(plans[k][0]) for k in sorted(plans)])
+        tabs = [op_table(0, E.offsets[order], bases[0][order], 1.0),
+                op_table(W.offsets[order], bases[0][order], bases[1][order], 1.0),
+                op_table(bases[1][order], 0, bases[2][order], 1.0)]
+        st = [[], [], []]
+        pos = 0
+        for key, (ops, *cs) in sorted(plans.items()):
+            ob, oe = pos, pos + len(ops)
+            pos = oe
+            for si, (c, t) in enumerate(cs):
+                tk, ct, fl = compile_template(c.l1, c.l2, c.out, ax[si], t, self.tiles[si])
+                tk["op_b"], tk["op_e"] = ob, oe
+                st[si].append((tk, ct, fl * len(ops)))
+        self.stages = [Stage(st[si], self.tiles[si], dev, "renorm%d" % (si + 1), tabs[si]) for si in range(3)]
+        self.flops = sum(s.flops for s in self.stages)
+        self.E, self.W = E, W
+
+    def __call__(self, site_values):
+        """site_values: packed site tensor (float64, device) -> new TensorSet."""
+        ws = self.ws
+        T1 = ws.get("r1", self.tot[0], torch.float64)
+        T2 = ws.get("r2", self.tot[1], torch.float64)
+        out = torch.zeros(max(self.tot[2], 1), dtype=torch.float64, device=ws.device)
+        s = self.stages
+        s[0].run(site_values, self.E.values, T1, "f64")
+        s[1].run(self.W.values, T1, T2, "f64")
+        s[2].run(T2, site_values, out, "f64")
+        return TensorSet(self.out_layouts, out, self.out_offsets)

@@ -1,0 +1,65 @@
+"""NumPy interpreter of the qc_bgemm work-item semantics (test infrastructure).
+
+Lets the plan compiler (task/contribution lists) be checked on a machine without
+a GPU: C[tile] = sum_c alpha_c * A_c[M-tile, :] @ B_c[:, N-tile], with the
+two-level index maps documented in qcmpodmrg_b200/csrc/qc_types.h.
+"""
+import numpy
+
+
+def _idx(i, lo, s_hi, s_lo):
+    return (i // lo) * s_hi + (i % lo) * s_lo
+
+
+def patch_stage_run(monkeypatch):
+    """Route Stage.run through the interpreter (tile extents follow the stage's tile config)."""
+    import torch
+    from qcmpodmrg_b200 import engine
+
+    def run(self, A, B, C, kind="f64", stream=None):
+        if self.ntasks == 0:
+            return
+        tm, tn = engine.TILES[self.tile_cfg]
+        a = A.detach().cpu().numpy().astype(numpy.float64)
+        b = B.detach().cpu().numpy().astype(numpy.float64)
+        c = C.detach().cpu().numpy().astype(numpy.float64)
+        _run_tiled(self.host_tasks, self.host_contribs, self.host_ops, self.summed, a, b, c, tm, tn)
+        C.copy_(torch.from_numpy(c).to(C.dtype))
+
+    monkeypatch.setattr(engine.Stage, "run", run)
+    from qcmpodmrg_b200 import kernels
+
+    def gather(src, idx, out):
+        out.copy_(src[idx])
+        return out
+
+    def convert(src, out):
+        n = min(src.numel(), out.numel())
+        out[:n].copy_(src[:n].to(out.dtype))
+        return out
+
+    monkeypatch.setattr(kernels, "gather", gather)
+    monkeypatch.setattr(kernels, "convert", convert)
+
+
+def _run_tiled(tasks, contribs, ops, summed, A, B, C, tm, tn):
+    for t in tasks:
+        ms = numpy.arange(t["m0"], min(t["m0"] + tm, t["M"]))
+        ns = numpy.arange(t["n0"], min(t["n0"] + tn, t["N"]))
+        outer = [None] if summed else list(range(t["op_b"], t["op_e"]))
+        for oi in outer:
+            acc = numpy.zeros((len(ms), len(ns)))
+            for c in contribs[t["cb"]:t["ce"]]:
+                ks = numpy.arange(c["K"])
+                ao = c["a_off"] + _idx(ms, t["mlo"], c["a_mh"], c["a_ml"])[:, None] + \
+                    _idx(ks, c["klo"], c["a_kh"], c["a_kl"])[None, :]
+                bo = c["b_off"] + _idx(ks, c["klo"], c["b_kh"], c["b_kl"])[:, None] + \
+                    _idx(ns, t["nlo"], c["b_nh"], c["b_nl"])[None, :]
+                oprange = range(c["op_b"], c["op_e"]) if summed else [oi]
+                for op in oprange:
+                    o = ops[op]
+                    acc += o["alpha"] * c["alpha"] * (A[o["a_base"] + ao] @ B[o["b_base"] + bo])
+            cbase = 0 if summed else ops[oi]["c_base"]
+            co = cbase + t["c_off"] + _idx(ms, t["mlo"], t["c_mh"], t["c_ml"])[:, None] + \
+                _idx(ns, t["nlo"], t["c_nh"], t["c_nl"])[None, :]
+            C[co] = acc

@@ -1,0 +1,82 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Requires the converted reference (python tests/golden/convert_reference.py)
+and /root/reference; run here, not on the GPU box:
+
+    python tests/golden/make_golden.py            # small fixtures (seconds)
+    python tests/golden/make_golden.py --config1  # K=12, N=12, D=100, 6 sweeps (~30 min CPU)
+
+Outputs:
+  qsym_cases.npz       symAllowed masks from the reference's own libqsym.so
+  kernels_<tag>.npz    HVecQt/HDiagQt/renormQt_H00 inputs and outputs at chosen dots
+  sweep_<tag>.npz      sweep energies/discarded weights/matvec counts + initial Qt L-MPS
+"""
+import argparse
+import ctypes
+import os
+import sys
+
+import numpy
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import reference_runner as rr  # noqa: E402
+import fixtures  # noqa: E402
+
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def qsym_cases(seed=7):
+    lib = ctypes.CDLL(os.path.join(REPO, "baseline", "_ref", "qcmpodmrg", "libs", "libqsym.so"))
+    rng = numpy.random.default_rng(seed)
+    cases = []
+    for rank in [2, 3, 3, 4, 4, 5, 6, 7, 8]:
+        nqnum = int(rng.integers(1, 3))
+        ndims = rng.integers(1, 6, size=rank).astype(numpy.int32)
+        if rank == 8:   # the reference's rank-8 loop runs its last index over ndims[6] (qsym.c:436)
+            ndims[7] = ndims[6]
+        status = rng.integers(0, 2, size=rank).astype(numpy.int32)
+        qs = [(rng.integers(-4, 5, size=(int(n), nqnum)) / 2.0).astype(numpy.float64) for n in ndims]
+        nblks = int(numpy.prod(ndims))
+        allowed = numpy.zeros(nblks, dtype=numpy.int32)
+        args = [q.ctypes.data_as(ctypes.c_void_p) for q in qs] + [None] * (8 - rank)
+        lib.symAllowed(ctypes.c_int(rank), ctypes.c_int(nqnum), ndims.ctypes.data_as(ctypes.c_void_p),
+                       status.ctypes.data_as(ctypes.c_void_p), allowed.ctypes.data_as(ctypes.c_void_p), *args)
+        cases.append({"rank": rank, "nqnum": nqnum, "ndims": ndims, "status": status,
+                      "qsyms": qs, "allowed": allowed.copy()})
+    fixtures.save(os.path.join(HERE, "qsym_cases.npz"), {"cases": cases})
+    print("qsym cases:", len(cases), "allowed counts", [int(c["allowed"].sum()) for c in cases])
+
+
+def run_case(tag, K, N, D, nsweeps, seed, decay, targets, record_envs=True):
+    res, rec = rr.run_reference(K=K, N=N, D=D, nsweeps=nsweeps, seed=seed, decay=decay, targets=targets,
+                                record_envs=record_envs)
+    sweep = {"K": K, "N": N, "D": D, "seed": seed, "decay": -1.0 if decay is None else float(decay),
+             "nsweeps": nsweeps, "eav": res["eav"], "dwt": res["dwt"], "esweeps": res["esweeps"],
+             "nmvp": res["nmvp"], "init_mps": {k: v for k, v in res["init_mps"].items() if k != "nsite"}}
+    fixtures.save(os.path.join(HERE, "sweep_%s.npz" % tag), sweep)
+    if targets:
+        recs = []
+        for k in targets:
+            r = rec.records.get(k)
+            if r and "hvec_x" in r:
+                d = dict(r)
+                d["key"] = numpy.array([k[0], 0 if k[1] == "L" else 1, k[2]])
+                recs.append(d)
+        fixtures.save(os.path.join(HERE, "kernels_%s.npz" % tag),
+                      {"K": K, "N": N, "seed": seed, "decay": -1.0 if decay is None else float(decay),
+                       "records": recs})
+    print(tag, "eav", res["eav"], "nmvp", res["nmvp"])
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config1", action="store_true")
+    a = ap.parse_args()
+    if a.config1:
+        run_case("C1", 12, 12, 100, 6, 1, None, [], record_envs=False)
+        sys.exit(0)
+    qsym_cases()
+    run_case("K4", 4, 4, 16, 2, 1, None, [(0, "R", 1), (0, "L", 1), (0, "R", 0), (0, "L", 2), (1, "R", 2)])
+    run_case("K5", 5, 4, 12, 2, 2, 2.0, [(0, "R", 2), (0, "L", 1), (1, "L", 3)])
+    run_case("K6", 6, 6, 20, 3, 3, None, [(0, "R", 3), (1, "L", 2)])

@@ -1,0 +1,58 @@
+"""Shared test helpers: fixture tensors -> product layouts / device tensor sets."""
+import os
+
+import numpy
+
+import fixtures
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return fixtures.load(os.path.join(GOLDEN, name))
+
+
+def layout_of(d):
+    from qcmpodmrg_b200.qtensor import Layout
+    r = int(d["rank"])
+    return Layout(numpy.asarray(d["status"], dtype=bool), [d["qsyms%d" % i] for i in range(r)],
+                  [d["ndims%d" % i] for i in range(r)])
+
+
+def tensorset(dicts, device):
+    from qcmpodmrg_b200.kernels import TensorSet
+    return TensorSet([layout_of(d) for d in dicts], [numpy.asarray(d["value"], dtype=numpy.float64)
+                                                      for d in dicts], device=device)
+
+
+def record_operators(r, device, precision="f64"):
+    """SigmaOperator / DiagOperator for a recorded reference dot."""
+    from qcmpodmrg_b200.kernels import SigmaOperator, DiagOperator, Workspace
+    import torch
+    ws = Workspace(torch.device(device))
+    isite = int(r["key"][2])
+    psi = layout_of(r["qtmp"])
+    L, R = tensorset(r["envL"], device), tensorset(r["envR"], device)
+    Wi, Wj = tensorset(r["mpo_i"], device), tensorset(r["mpo_j"], device)
+    opers = [int(x) for x in numpy.atleast_1d(r["opers"])]
+    hp = numpy.atleast_1d(r["hpwts"]).astype(numpy.float64)
+    qkey = numpy.asarray(r["qkey"], dtype=numpy.float64)
+    sig = SigmaOperator(ws, isite, psi, L, R, Wi, Wj, qkey, opers, hp, precision)
+    dg = DiagOperator(ws, isite, psi, L, R, Wi, Wj, qkey, opers, hp)
+    return sig, dg, ws
+
+
+def record_renormalizer(r, device):
+    from qcmpodmrg_b200.kernels import Renormalizer, Workspace
+    import torch
+    ws = Workspace(torch.device(device))
+    isite = int(r["key"][2])
+    status = "L" if int(r["key"][1]) == 0 else "R"
+    site = layout_of(r["renorm_site"])
+    opers = [int(x) for x in numpy.atleast_1d(r["opers"])]
+    if status == "L":
+        E, W, j = tensorset(r["envL"], device), tensorset(r["mpo_i"], device), isite
+    else:
+        E, W, j = tensorset(r["envR"], device), tensorset(r["mpo_j"], device), isite + 1
+    rn = Renormalizer(ws, j, status, site, E, W, opers)
+    return rn, numpy.asarray(r["renorm_site"]["value"], dtype=numpy.float64)

@@ -1,0 +1,25 @@
+"""GPU end-to-end: FP64 two-site sweeps reproduce the reference's energies (1e-8 Eh)
+and discarded weights (1e-10) from the same initial MPS."""
+import os
+
+import numpy
+import pytest
+
+from helpers import load, GOLDEN
+from qcmpodmrg_b200.hamiltonian import make_hamiltonian
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("tag", ["K4", "K5", "K6", "C1"])
+def test_sweeps_match_reference(tag, cuda):
+    if not os.path.exists(os.path.join(GOLDEN, "sweep_%s.npz" % tag)):
+        pytest.skip("fixture not generated")
+    from qcmpodmrg_b200.dmrg import DMRG
+    fx = load("sweep_%s.npz" % tag)
+    decay = None if fx["decay"] < 0 else fx["decay"]
+    ham = make_hamiltonian(int(fx["K"]), int(fx["N"]), int(fx["seed"]), decay)
+    out = DMRG(ham, device=cuda).run(fx["init_mps"], int(fx["D"]), int(fx["nsweeps"]))
+    n = min(len(out["eav"]), len(fx["eav"]))
+    assert numpy.abs(out["eav"][:n] - fx["eav"][:n]).max() <= 1e-8
+    assert numpy.abs(out["dwt"][:n] - fx["dwt"][:n]).max() <= 1e-10

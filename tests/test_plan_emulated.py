@@ -1,0 +1,27 @@
+"""The plan compiler + work lists, executed by a NumPy interpreter of the kernel
+semantics, reproduce the reference's HVecQt / HDiagQt / renormQt_H00 (no GPU)."""
+import numpy
+import pytest
+import torch
+
+from helpers import load, record_operators, record_renormalizer
+from emulate import patch_stage_run
+
+
+@pytest.mark.parametrize("tag", ["K4", "K5", "K6"])
+def test_sigma_diag_renorm_emulated(tag, monkeypatch):
+    patch_stage_run(monkeypatch)
+    for r in load("kernels_%s.npz" % tag)["records"]:
+        sig, dg, ws = record_operators(r, "cpu")
+        x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))
+        y = sig(x).numpy()
+        ref = numpy.asarray(r["hvec_y"])
+        assert numpy.abs(y - ref).max() <= 1e-12 * max(1.0, numpy.abs(ref).max())
+        d = dg().numpy()
+        assert numpy.abs(d - numpy.asarray(r["hdiag"])).max() <= 1e-12
+        rn, site = record_renormalizer(r, "cpu")
+        out = rn(torch.from_numpy(site))
+        for i, b in enumerate(r["renorm_out"]):
+            got = out.op_values(i).numpy()
+            assert len(got) == len(b["value"])
+            assert numpy.abs(got - b["value"]).max() <= 1e-12
