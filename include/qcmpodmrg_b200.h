@@ -109,7 +109,8 @@ long long qc_compile_pairs(int r1, const int *nsyms1, const long long *ndims1, c
  * summed == 0: each task writes one tile per operator of its range;
  * summed != 0: each task writes one tile summed over the operators of every
  * contribution's range (sigma's sum over p).
- * tile_cfg: 0 = 64x64, 1 = 128x32, 2 = 256x16 output tiles. */
+ * tile_cfg: output tile / threads: 0 = 64x64/256, 1 = 128x32/256, 2 = 256x16/256,
+ * 3 = 32x32/64, 4 = 64x16/64. */
 int qc_bgemm_f64(const void *tasks_dev, long long ntasks, const void *contribs_dev, const void *ops_dev,
                  int summed, const double *A, const double *B, double *C, int tile_cfg, void *stream);
 
@@ -122,6 +123,11 @@ int qc_gather_f64(const double *src, const long long *idx, double *dst, long lon
 /* dst[idx[i]] = src[i] (FP64) after zeroing dst[0..ndst). */
 int qc_scatter_f64(const double *src, const long long *idx, double *dst, long long n,
                    long long ndst, void *stream);
+
+/* out[i] = sum_{o < nops} part[o*n + i] in fixed order (per-operator partial sigma
+ * vectors -> sigma; the sum over p of HVecQt, kernelQt.py:316). */
+int qc_reduce_ops_f64(const double *part, int nops, long long n, double *out, void *stream);
+int qc_reduce_ops_f32(const float *part, int nops, long long n, float *out, void *stream);
 
 /* Precision conversions used by the mixed-precision path. */
 int qc_convert_f64_to_f32(const double *src, float *dst, long long n, void *stream);

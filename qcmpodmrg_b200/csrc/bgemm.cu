@@ -25,13 +25,11 @@ extern "C" const char *qc_last_cuda_error(void) { return g_cuerr.c_str(); }
 
 namespace {
 
-constexpr int kThreads = 256;
-
 // SUMMED = false: the task computes one tile for each operator in [t.op_b, t.op_e)
 //                 of the operator table (same block structure, own base offsets).
 // SUMMED = true:  the task computes one tile; every contribution accumulates the
 //                 products of the operators in [c.op_b, c.op_e) (sum over p).
-template <typename T, int TM, int TN, int TK, int RM, int RN, bool SUMMED>
+template <typename T, int TM, int TN, int TK, int RM, int RN, bool SUMMED, int kThreads>
 __global__ void __launch_bounds__(kThreads)
 k_bgemm(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ contribs,
         const qc_op *__restrict__ ops, const T *__restrict__ A, const T *__restrict__ B, T *__restrict__ C) {
@@ -131,11 +129,13 @@ k_bgemm(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ contri
 template <typename T, bool S>
 int launch_mode(const qc_task *tk, long long ntasks, const qc_contrib *cb, const qc_op *ops, const T *A,
                 const T *B, T *C, int cfg, cudaStream_t s) {
-  dim3 grid((unsigned)ntasks), block(kThreads);
+  dim3 grid((unsigned)ntasks);
   switch (cfg) {
-    case 0: k_bgemm<T, 64, 64, 16, 4, 4, S><<<grid, block, 0, s>>>(tk, cb, ops, A, B, C); break;
-    case 1: k_bgemm<T, 128, 32, 16, 4, 4, S><<<grid, block, 0, s>>>(tk, cb, ops, A, B, C); break;
-    case 2: k_bgemm<T, 256, 16, 16, 4, 4, S><<<grid, block, 0, s>>>(tk, cb, ops, A, B, C); break;
+    case 0: k_bgemm<T, 64, 64, 16, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
+    case 1: k_bgemm<T, 128, 32, 16, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
+    case 2: k_bgemm<T, 256, 16, 16, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
+    case 3: k_bgemm<T, 32, 32, 16, 4, 4, S, 64><<<grid, 64, 0, s>>>(tk, cb, ops, A, B, C); break;
+    case 4: k_bgemm<T, 64, 16, 16, 4, 4, S, 64><<<grid, 64, 0, s>>>(tk, cb, ops, A, B, C); break;
     default: return QC_ERR_ARG;
   }
   return cuda_fail("qc_bgemm");
@@ -197,6 +197,15 @@ __global__ void k_f32_to_f64(const float *__restrict__ s, double *__restrict__ d
     d[i] = (double)s[i];
 }
 
+template <typename T>
+__global__ void k_reduce_ops(const T *__restrict__ part, int nops, long long n, T *__restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    T acc = T(0);
+    for (int o = 0; o < nops; ++o) acc += part[(long long)o * n + i];   // fixed order: reproducible
+    out[i] = acc;
+  }
+}
+
 inline unsigned grid_for(long long n) {
   long long g = (n + 255) / 256;
   if (g > 148LL * 32) g = 148LL * 32;   // a multiple of the 148 SMs
@@ -247,6 +256,18 @@ extern "C" int qc_scatter_f64(const double *src, const long long *idx, double *d
   if (n <= 0) return cuda_fail("qc_scatter_f64");
   k_scatter_f64<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(src, idx, dst, n);
   return cuda_fail("qc_scatter_f64");
+}
+
+extern "C" int qc_reduce_ops_f64(const double *part, int nops, long long n, double *out, void *stream) {
+  if (n <= 0) return QC_OK;
+  k_reduce_ops<double><<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(part, nops, n, out);
+  return cuda_fail("qc_reduce_ops_f64");
+}
+
+extern "C" int qc_reduce_ops_f32(const float *part, int nops, long long n, float *out, void *stream) {
+  if (n <= 0) return QC_OK;
+  k_reduce_ops<float><<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(part, nops, n, out);
+  return cuda_fail("qc_reduce_ops_f32");
 }
 
 extern "C" int qc_convert_f64_to_f32(const double *s, float *d, long long n, void *stream) {

@@ -25,17 +25,34 @@ OP_DT = numpy.dtype([("a_base", "<i8"), ("b_base", "<i8"), ("c_base", "<i8"), ("
 assert TASK_DT.itemsize == native.TASK_BYTES and CONTRIB_DT.itemsize == native.CONTRIB_BYTES
 assert OP_DT.itemsize == native.OP_BYTES
 
-TILES = {0: (64, 64), 1: (128, 32), 2: (256, 16)}
+TILES = {0: (64, 64), 1: (128, 32), 2: (256, 16), 3: (32, 32), 4: (64, 16)}
 
 
-def pick_tile(ns):
-    """Choose the output tile shape from the typical N (columns) of a stage."""
-    n = float(numpy.median(ns)) if len(ns) else 64.0
-    if n <= 16:
-        return 2
-    if n <= 32:
-        return 1
-    return 0
+def tile_class(M, N):
+    """Output-tile configuration for output blocks of extent M x N (vectorised)."""
+    M = numpy.asarray(M)
+    N = numpy.asarray(N)
+    return numpy.where(N <= 16, numpy.where(M <= 64, 4, 2),
+                       numpy.where(N <= 32, numpy.where(M <= 32, 3, 1), numpy.where(M <= 32, 3, 0)))
+
+
+def compile_classes(c, triples, axes):
+    """Compile one contraction's pair list, binned by output-block shape into tile classes.
+
+    Returns {tile_cfg: (tasks, contribs, flops)} for a single operator (template).
+    """
+    out = {}
+    if len(triples) == 0:
+        return out
+    ne1 = c.l1.rank - len(axes[0])
+    d = c.out.block_dims(triples[:, 0])
+    M = numpy.prod(d[:, :ne1], axis=1)
+    N = numpy.prod(d[:, ne1:], axis=1)
+    cls = tile_class(M, N)
+    for k in numpy.unique(cls):
+        sel = triples[cls == k]
+        out[int(k)] = compile_template(c.l1, c.l2, c.out, axes, sel, int(k))
+    return out
 
 
 def compile_template(l1, l2, lo, axes, triples, tile_cfg):
@@ -123,50 +140,69 @@ def merge_grouped(parts):
 
 
 class Stage(object):
-    """A compiled stage resident on the device.
+    """A compiled stage resident on the device: one launch per tile configuration.
 
-    parts: list of (tasks, contribs, flops) whose op ranges index ``ops`` (OP_DT).
-    summed: tasks accumulate over the operators of each contribution (sigma's
-    last contraction) instead of writing one tile per operator.
+    parts: {tile_cfg: [(tasks, contribs, flops), ...]} whose op ranges index
+    ``ops`` (OP_DT).  summed: tasks accumulate over the operators of each
+    contribution instead of writing one tile per operator.
     """
 
-    def __init__(self, parts, tile_cfg, device, name="", ops=None, summed=False):
-        tasks, contribs = [], []
-        nc = 0
-        flops = 0.0
-        for (t, c, f) in parts:
-            if len(t):
-                t = t.copy()
-                t["cb"] += nc
-                t["ce"] += nc
-                tasks.append(t)
-                contribs.append(c)
-                nc += len(c)
-            flops += f
+    def __init__(self, parts, device, name="", ops=None, summed=False):
         if ops is None:
             ops = numpy.zeros(1, dtype=OP_DT)
             ops["alpha"] = 1.0
         self.name = name
-        self.tile_cfg = tile_cfg
         self.summed = bool(summed)
-        self.flops = flops
-        self.ntasks = int(sum(len(t) for t in tasks))
-        self.ncontribs = nc
-        tk = numpy.concatenate(tasks) if tasks else numpy.zeros(0, TASK_DT)
-        ct = numpy.concatenate(contribs) if contribs else numpy.zeros(0, CONTRIB_DT)
-        self.host_tasks, self.host_contribs, self.host_ops = tk, ct, ops
-        self.d_tasks = torch.from_numpy(tk.view(numpy.uint8).copy()).to(device)
-        self.d_contribs = torch.from_numpy(ct.view(numpy.uint8).copy()).to(device)
+        self.host_ops = ops
         self.d_ops = torch.from_numpy(ops.view(numpy.uint8).copy()).to(device)
+        self.groups = []
+        self.flops = 0.0
+        self.ntasks = 0
+        self.ncontribs = 0
+        for cfg in sorted(parts):
+            tasks, contribs = [], []
+            nc = 0
+            for (t, c, f) in parts[cfg]:
+                self.flops += f
+                if len(t):
+                    t = t.copy()
+                    t["cb"] += nc
+                    t["ce"] += nc
+                    tasks.append(t)
+                    contribs.append(c)
+                    nc += len(c)
+            if not tasks:
+                continue
+            tk = numpy.concatenate(tasks)
+            ct = numpy.concatenate(contribs)
+            self.groups.append((cfg, tk, ct, torch.from_numpy(tk.view(numpy.uint8).copy()).to(device),
+                                torch.from_numpy(ct.view(numpy.uint8).copy()).to(device)))
+            self.ntasks += len(tk)
+            self.ncontribs += len(ct)
+
+    @property
+    def host_groups(self):
+        return [(cfg, tk, ct) for (cfg, tk, ct, _, _) in self.groups]
 
     def run(self, A, B, C, kind="f64", stream=None):
-        if self.ntasks == 0:
-            return
         lib = native.lib()
         s = stream if stream is not None else torch.cuda.current_stream(C.device).cuda_stream
         fn = {"f64": lib.qc_bgemm_f64, "f32": lib.qc_bgemm_f32, "tf32": getattr(lib, "qc_bgemm_tf32", None)}[kind]
-        check(fn(self.d_tasks.data_ptr(), self.ntasks, self.d_contribs.data_ptr(), self.d_ops.data_ptr(),
-                 int(self.summed), A.data_ptr(), B.data_ptr(), C.data_ptr(), self.tile_cfg, s), "qc_bgemm_" + kind)
+        for (cfg, tk, ct, dt, dc) in self.groups:
+            check(fn(dt.data_ptr(), len(tk), dc.data_ptr(), self.d_ops.data_ptr(), int(self.summed),
+                     A.data_ptr(), B.data_ptr(), C.data_ptr(), cfg, s), "qc_bgemm_" + kind)
+
+
+def add_parts(dst, parts, op_range=None, contrib_range=None):
+    """Append compiled class parts to {cfg: [...]}, stamping operator ranges."""
+    for cfg, (tk, ct, fl) in parts.items():
+        if op_range is not None:
+            tk["op_b"], tk["op_e"] = op_range
+        if contrib_range is not None:
+            ct["op_b"], ct["op_e"] = contrib_range
+        nops = (op_range or contrib_range)
+        mult = (nops[1] - nops[0]) if nops else 1
+        dst.setdefault(cfg, []).append((tk, ct, fl * mult))
 
 
 def op_table(a_base, b_base, c_base, alpha):

@@ -18,8 +18,7 @@ import torch
 
 from . import native
 from .native import check
-from .engine import (Stage, compile_template, merge_grouped, live_blocks, prune, pick_tile, op_table,
-                     TASK_DT, CONTRIB_DT)
+from .engine import (Stage, compile_classes, add_parts, live_blocks, prune, op_table, TASK_DT, CONTRIB_DT)
 from .mpo import case
 from .qtensor import Contraction, flip_right, flip_horizontal
 
@@ -92,6 +91,14 @@ def convert(src, out):
     return out
 
 
+def reduce_ops(part, nops, n, out):
+    """out = sum over operators of the per-operator partial vectors (qc_reduce_ops_*)."""
+    lib = native.lib()
+    fn = lib.qc_reduce_ops_f64 if part.dtype == torch.float64 else lib.qc_reduce_ops_f32
+    check(fn(part.data_ptr(), nops, n, out.data_ptr(), _stream(out.device)), "qc_reduce_ops")
+    return out
+
+
 def _groups(opers, isite, ncsite):
     g = {}
     for iop, p in enumerate(opers):
@@ -145,32 +152,24 @@ class SigmaOperator(object):
                     bases[s][i] = tot[s]
                     tot[s] += c.out.size
         self.tot = tot
+        self.nops = nops
         hp = numpy.asarray(hpwts, dtype=numpy.float64)
-        ncols = [[], [], [], []]
-        for key, (ops, *cs, Rl) in sorted(plans.items()):
-            for si, (c, t) in enumerate(cs):
-                ncols[si].append(_ncols(c, t))
-        self.tiles = [pick_tile(numpy.concatenate(n)) for n in ncols]
-        # operator tables: operators ordered class by class
+        # operator tables: operators ordered class by class; the last contraction
+        # writes one partial sigma per operator (slot = position in that order)
         order = numpy.concatenate([numpy.array(plans[k][0]) for k in sorted(plans)])
+        slot = numpy.arange(nops, dtype=numpy.int64) * psi_layout.size
         tabs = [op_table(L.offsets[order], 0, bases[0][order], 1.0),
                 op_table(bases[0][order], Wi.offsets[order], bases[1][order], 1.0),
                 op_table(bases[1][order], Wj.offsets[order], bases[2][order], 1.0),
-                op_table(bases[2][order], R.offsets[order], 0, hp[order])]
-        st = [[], [], [], []]
+                op_table(bases[2][order], R.offsets[order], slot, hp[order])]
+        st = [{}, {}, {}, {}]
         pos = 0
         for key, (ops, *cs, Rl) in sorted(plans.items()):
-            ob, oe = pos, pos + len(ops)
-            pos = oe
+            rng = (pos, pos + len(ops))
+            pos += len(ops)
             for si, (c, t) in enumerate(cs):
-                tk, ct, fl = compile_template(c.l1, c.l2, c.out, ax[si], t, self.tiles[si])
-                if si < 3:
-                    tk["op_b"], tk["op_e"] = ob, oe
-                else:
-                    ct["op_b"], ct["op_e"] = ob, oe
-                st[si].append((tk, ct, fl * len(ops)))
-        self.stages = [Stage(st[si], self.tiles[si], dev, "sigma%d" % (si + 1), tabs[si]) for si in range(3)]
-        self.stages.append(Stage([merge_grouped(st[3])], self.tiles[3], dev, "sigma4", tabs[3], summed=True))
+                add_parts(st[si], compile_classes(c, t, ax[si]), op_range=rng)
+        self.stages = [Stage(st[si], dev, "sigma%d" % (si + 1), tabs[si]) for si in range(4)]
         self.flops = sum(s.flops for s in self.stages)
         self.ndim0 = psi_layout.size
 
@@ -186,13 +185,14 @@ class SigmaOperator(object):
             T1 = ws.get("t1", self.tot[0], torch.float64)
             T2 = ws.get("t2", self.tot[1], torch.float64)
             T3 = ws.get("t3", self.tot[2], torch.float64)
+            P = ws.get("part", self.nops * self.ndim0, torch.float64)
             s = self.stages
             s[0].run(self.L.values, x, T1, "f64")
             s[1].run(T1, self.Wi.values, T2, "f64")
             s[2].run(T2, self.Wj.values, T3, "f64")
-            y.zero_()
-            s[3].run(T3, self.R.values, y, "f64")
-            return y
+            P[:self.nops * self.ndim0].zero_()
+            s[3].run(T3, self.R.values, P, "f64")
+            return reduce_ops(P, self.nops, self.ndim0, y)
         kind = "tf32" if self.precision == "tf32" else "f32"
         T1 = ws.get("t1", self.tot[0], torch.float32)
         T2 = ws.get("t2", self.tot[1], torch.float32)
@@ -200,12 +200,14 @@ class SigmaOperator(object):
         x32 = ws.get("x32", self.ndim0, torch.float32)
         y32 = ws.get("y32", self.ndim0, torch.float32)
         convert(x, x32)
+        P = ws.get("part32", self.nops * self.ndim0, torch.float32)
         s = self.stages
         s[0].run(self.L.f32(), x32, T1, kind)
         s[1].run(T1, self.Wi.f32(), T2, "f32")
         s[2].run(T2, self.Wj.f32(), T3, "f32")
-        y32[:self.ndim0].zero_()
-        s[3].run(T3, self.R.f32(), y32, kind)
+        P[:self.nops * self.ndim0].zero_()
+        s[3].run(T3, self.R.f32(), P, kind)
+        reduce_ops(P, self.nops, self.ndim0, y32)
         convert(y32, y)
         return y
 
@@ -352,9 +354,9 @@ class DiagOperator(object):
                 al.append(hp[p])
             grp.append((nm * ldim * rdim, ids))
         sD = _dense_tasks(ldim, rdim, Ac, a_off, 1, ldim, b_off, rdim, 1, None, rdim, al, grp, 0)
-        self.sX = Stage([sX], 0, dev, "diagX")
-        self.sT = Stage([sT], 0, dev, "diagT")
-        self.sD = Stage([sD], 0, dev, "diagD")
+        self.sX = Stage({0: [sX]}, dev, "diagX")
+        self.sT = Stage({0: [sT]}, dev, "diagT")
+        self.sD = Stage({0: [sD]}, dev, "diagD")
         self.nX = nops * 16 * A * Ac
         self.nT = nops * 16 * Ac * ldim
         self.nD = 16 * ldim * rdim
@@ -422,25 +424,18 @@ class Renormalizer(object):
         self.out_layouts = out_layouts
         self.out_offsets = bases[2].copy()
         self.tot = tot
-        ncols = [[], [], []]
-        for key, (ops, *cs) in sorted(plans.items()):
-            for si, (c, t) in enumerate(cs):
-                ncols[si].append(_ncols(c, t))
-        self.tiles = [pick_tile(numpy.concatenate(n)) for n in ncols]
         order = numpy.concatenate([numpy.array(plans[k][0]) for k in sorted(plans)])
         tabs = [op_table(0, E.offsets[order], bases[0][order], 1.0),
                 op_table(W.offsets[order], bases[0][order], bases[1][order], 1.0),
                 op_table(bases[1][order], 0, bases[2][order], 1.0)]
-        st = [[], [], []]
+        st = [{}, {}, {}]
         pos = 0
         for key, (ops, *cs) in sorted(plans.items()):
-            ob, oe = pos, pos + len(ops)
-            pos = oe
+            rng = (pos, pos + len(ops))
+            pos += len(ops)
             for si, (c, t) in enumerate(cs):
-                tk, ct, fl = compile_template(c.l1, c.l2, c.out, ax[si], t, self.tiles[si])
-                tk["op_b"], tk["op_e"] = ob, oe
-                st[si].append((tk, ct, fl * len(ops)))
-        self.stages = [Stage(st[si], self.tiles[si], dev, "renorm%d" % (si + 1), tabs[si]) for si in range(3)]
+                add_parts(st[si], compile_classes(c, t, ax[si]), op_range=rng)
+        self.stages = [Stage(st[si], dev, "renorm%d" % (si + 1), tabs[si]) for si in range(3)]
         self.flops = sum(s.flops for s in self.stages)
         self.E, self.W = E, W
 

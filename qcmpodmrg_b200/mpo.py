@@ -83,11 +83,12 @@ def _wfac(nsite, i, hq, v):
 
 def _hfac_spin(p, nsite, i, hq, v):
     e = SGN if i < p else (CRE if i == p else IDN)
-    return numpy.einsum("ij,abjk->abik", e, _wfac(nsite, i, hq, v))
+    return numpy.matmul(e, _wfac(nsite, i, hq, v))
 
 
 def _link(op1, op2):
-    t = numpy.einsum("abij,bckl->acikjl", op1, op2)
+    t = numpy.tensordot(op1, op2, axes=([1], [0]))        # a i j c k l
+    t = t.transpose(0, 3, 1, 4, 2, 5)                    # a c i k j l
     s = t.shape
     return t.reshape(s[0], s[1], s[2] * s[3], s[4] * s[5])
 

@@ -38,8 +38,8 @@ def random_mps(K, N, D, seed=0, width=1.2, szwidth=0.7):
                 w[s] = numpy.exp(-0.5 * ((n - nbar) / width) ** 2 - 0.5 * (sz / szwidth) ** 2)
             if w.sum() == 0:
                 raise ValueError("no admissible sector")
+            w[w < 1e-3 * w.max()] = 0.0
             cnt = numpy.minimum(avail, numpy.floor(D * w / w.sum() + 0.5).astype(numpy.int64))
-            cnt[(w > 0) & (cnt == 0) & (avail > 0)] = 1
             while cnt.sum() > D:
                 j = numpy.argmax(cnt)
                 cnt[j] -= 1
@@ -73,3 +73,31 @@ def random_mps(K, N, D, seed=0, width=1.2, szwidth=0.7):
     out = {"site%d" % i: s for i, s in enumerate(sites)}
     out.update({"qnum%d" % i: q for i, q in enumerate(qnum)})
     return out
+
+
+def product_mps(ham):
+    """The occupation-number (Hartree-Fock) product state as a bond-dimension-1 L-MPS
+    (the reference's mps0occun, source/mpo_dmrg_util.py:118-156)."""
+    K = ham.nsite
+    occ = ham.occun
+    qnum = [numpy.zeros((1, 2))]
+    sites = {}
+    n, sz = 0.0, 0.0
+    for i in range(K):
+        na, nb = occ[2 * i], occ[2 * i + 1]
+        t = numpy.zeros((1, 4, 1))
+        if na < 0.5 and nb < 0.5:
+            t[0, 0, 0] = 1.0
+        elif na < 0.5:
+            t[0, 1, 0] = 1.0
+            n, sz = n + 1, sz - 0.5
+        elif nb < 0.5:
+            t[0, 2, 0] = 1.0
+            n, sz = n + 1, sz + 0.5
+        else:
+            t[0, 3, 0] = 1.0
+            n += 2
+        sites["site%d" % i] = t
+        qnum.append(numpy.array([[n, sz]]))
+    sites.update({"qnum%d" % i: q for i, q in enumerate(qnum)})
+    return sites

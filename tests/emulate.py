@@ -19,11 +19,12 @@ def patch_stage_run(monkeypatch):
     def run(self, A, B, C, kind="f64", stream=None):
         if self.ntasks == 0:
             return
-        tm, tn = engine.TILES[self.tile_cfg]
         a = A.detach().cpu().numpy().astype(numpy.float64)
         b = B.detach().cpu().numpy().astype(numpy.float64)
         c = C.detach().cpu().numpy().astype(numpy.float64)
-        _run_tiled(self.host_tasks, self.host_contribs, self.host_ops, self.summed, a, b, c, tm, tn)
+        for cfg, tk, ct in self.host_groups:
+            tm, tn = engine.TILES[cfg]
+            _run_tiled(tk, ct, self.host_ops, self.summed, a, b, c, tm, tn)
         C.copy_(torch.from_numpy(c).to(C.dtype))
 
     monkeypatch.setattr(engine.Stage, "run", run)
@@ -39,6 +40,12 @@ def patch_stage_run(monkeypatch):
         return out
 
     monkeypatch.setattr(kernels, "gather", gather)
+
+    def reduce_ops(part, nops, n, out):
+        out[:n].copy_(part[:nops * n].reshape(nops, n).sum(0).to(out.dtype))
+        return out
+
+    monkeypatch.setattr(kernels, "reduce_ops", reduce_ops)
     monkeypatch.setattr(kernels, "convert", convert)
 
 
