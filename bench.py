@@ -1,0 +1,294 @@
+"""Benchmark: two-site MPO-DMRG sweeps at K=24, N=24, Sz=0, D=500 on one B200.
+
+Workload (the reference's config quoted by the metric): seeded synthetic
+integrals (K=24 spatial orbitals, N=24 electrons, locality decay 3, seed 1),
+the occupation-number product state as start, a bond-dimension ramp
+D = 50, 100, 200 (set-up, untimed), then W warm-up and K timed steps.  One
+step = one full two-site sweep (right-to-left then left-to-right) at D=500:
+per dot the sigma/diagonal plans, Davidson (FP64 Rayleigh-Ritz), RDM
+decimation and renormalisation of every operator's environment.
+
+  python bench.py [--steps K] [--warmup W] [--precision mixed|f64] [--gpus N]
+  python bench.py --impl reference      # the reference algorithm (oracle port) on the host CPU
+
+Prints one JSON line.  value = seconds per sweep (lower is better).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sweep sec & sigma TFLOP/s @K=24,D=500: mixed+learned vs FP64, |ΔE|≤1e-6 Eh"
+K_SITES, N_ELEC, DECAY, SEED, DMAX = 24, 24, 3.0, 1, 500
+RAMP = (50, 100, 200)
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler(object):
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(numpy.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        torch.cuda.set_device(local)
+        return dist, rank, ws, local
+    return None, 0, 1, 0
+
+
+def barrier(dist):
+    import torch
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def run_ours(args):
+    import torch
+    from qcmpodmrg_b200.hamiltonian import make_hamiltonian
+    from qcmpodmrg_b200.synthetic import product_mps
+    from qcmpodmrg_b200.dmrg import DMRG
+    from qcmpodmrg_b200.engine import LOG
+
+    dist, rank, world, local = dist_init()
+    dev = torch.device("cuda:%d" % local)
+    torch.cuda.set_device(dev)
+    prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32"}[args.precision]
+    ham = make_hamiltonian(args.sites, args.sites, SEED + rank * 0, DECAY)
+    d = DMRG(ham, device=dev, precision=prec)
+    d.load_mps(product_mps(ham))
+    for D in RAMP:
+        if D < args.dmax:
+            d.sweep("R", D, 1e-7)
+            d.sweep("L", D, 1e-7)
+
+    def step():
+        f0 = d.stats["sigma_flops"]
+        d.sweep("R", args.dmax, 1e-7)
+        n, e, dw, el, dl = d.sweep("L", args.dmax, 1e-7)
+        d.sweep_sigma_flops = d.stats["sigma_flops"] - f0
+        return e, dw
+
+    for _ in range(args.warmup):
+        step()
+    # ---- timed region (device events on the launching stream, barrier + sync both sides)
+    s0 = dict(d.stats)
+    LOG.reset()
+    LOG.enabled = True
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(dist)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    energies = []
+    for _ in range(args.steps):
+        energies.append(step())
+    ev1.record()
+    barrier(dist)
+    ck = clocks.stop()
+    LOG.enabled = False
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    stats = {k: d.stats[k] - s0[k] for k in d.stats}
+    # per-stage device time from the launch log
+    per = {}
+    for (name, e0, e1, fl, by) in LOG.records:
+        t = e0.elapsed_time(e1)
+        a = per.setdefault(name, [0, 0.0, 0.0, 0.0])
+        a[0] += 1
+        a[1] += t
+        a[2] += fl
+        a[3] += by
+    sig_ms = sum(v[1] for k, v in per.items() if k.startswith("sigma"))
+    sig_fl = sum(v[2] for k, v in per.items() if k.startswith("sigma"))
+    top = max(per.items(), key=lambda kv: kv[1][1])
+    pk, src = peaks()
+    n_l, t_l, f_l, b_l = top[1]
+    gbs = b_l / (t_l / 1e3) / 1e9
+    roof = {"kernel": "qc_bgemm (%s)" % top[0], "bound": "hbm", "achieved": round(gbs, 1),
+            "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(gbs / pk["hbm_gbs"], 4),
+            "peak_source": src, "traffic": None, "launches": n_l,
+            "achieved_tflops": round(f_l / (t_l / 1e3) / 1e12, 3)}
+    line = {
+        "metric": METRIC, "value": round(ms_per_step / 1e3, 3), "unit": "s/sweep", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 1),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"f64": "f64", "f32": "f32 (sigma), f64 (Davidson, decimation)",
+                  "tf32": "tf32 (sigma), f64 (Davidson, decimation)"}[prec],
+        "data": "synthetic: seeded integrals (K=24, N=24, decay 3, seed 1), product-state start, D ramp 50/100/200",
+        "config": {"workload": "two-site Qt DMRG sweep, K=24 N=24 Sz=0 D=500, 48 operators H_p", "K": args.sites,
+                   "N": args.sites, "D": args.dmax, "precision": args.precision,
+                   "l2": "inputs larger than L2: environments and sigma scratch are tens of GB per sweep",
+                   "parallelism": "replicas" if world > 1 else "1 GPU"},
+        "energy": energies[-1][0], "dwt": energies[-1][1],
+        "sigma_tflops": round(sig_fl / (sig_ms / 1e3) / 1e12, 3) if sig_ms else None,
+        "sigma_share": round(sig_ms / ms, 3) if ms else None,
+        "matvecs_per_step": stats["nmvp"] / args.steps,
+        "stage_ms_per_step": {k: round(v[1] / args.steps, 1) for k, v in sorted(per.items())},
+        "roofline": roof, "clocks": ck, "gpu_launches": LOG.launches,
+    }
+    if args.e2e:
+        line["e2e"] = e2e_leg(d, args)
+    if rank == 0 and args.cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(d, ms_per_step / 1e3)
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def e2e_leg(d, args):
+    """One sweep through the reference-facing API (mpo_dmrg_kernel.HVec/HDiag with host NumPy
+    vectors, Davidson on the host as in the reference's pdvdson); copies are in the timed region."""
+    import torch
+    d.host_api = True
+    d.h2d_bytes = d.d2h_bytes = 0
+    torch.cuda.synchronize()
+    t0 = time.time()
+    d.sweep("R", args.dmax, 1e-7)
+    d.sweep("L", args.dmax, 1e-7)
+    torch.cuda.synchronize()
+    dt = time.time() - t0
+    d.host_api = False
+    return {"value": round(dt, 3), "unit": "s/sweep", "h2d_bytes_per_step": int(d.h2d_bytes),
+            "d2h_bytes_per_step": int(d.d2h_bytes),
+            "path": "qcmpodmrg_b200.mpo_dmrg_kernel.HVec/HDiag with host buffers, host Davidson"}
+
+
+def cpu_baseline_sample(d, gpu_sweep_s):
+    """The oracle (NumPy restatement of the reference's HVecQt) timed on this host's cores on
+    one sigma matvec at the mid-chain dot of the same state; scaled to a sweep by algorithmic
+    sigma FLOPs (the same count the GPU reports)."""
+    from oracle.kernels import SigmaOracle
+    from oracle.bench_cpu import oracle_dot
+    isite = d.nsite // 2
+    ora, x, flops_dot = oracle_dot(d, isite)
+    t0 = time.time()
+    ora(x)
+    t = time.time() - t0
+    rate = flops_dot / t
+    est = d.sweep_sigma_flops / rate
+    return {"value": round(est, 1), "unit": "s/sweep", "cores": os.cpu_count(),
+            "kind": "port", "sample": "one oracle sigma matvec at the mid-chain dot (%.1f s, %.2f GFLOP/s), "
+                                      "scaled to the sweep's sigma FLOPs" % (t, rate / 1e9)}
+
+
+def run_reference(args):
+    """The reference algorithm (oracle port of HVecQt/HDiagQt/renormQt_H00) on the host cores."""
+    dist, rank, world, local = None, int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0
+    if rank != 0:
+        return
+    from oracle.bench_cpu import reference_step
+    for _ in range(args.warmup):
+        reference_step(args, warm=True)
+    t0 = time.time()
+    res = [reference_step(args) for _ in range(args.steps)]
+    wall = time.time() - t0
+    v = float(numpy.mean([r["sweep_s_est"] for r in res]))
+    line = {"metric": METRIC, "impl": "reference", "value": round(v, 1), "unit": "s/sweep", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * wall / args.steps, 1),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded integrals (K=24, N=24, decay 3, seed 1), synthetic D=500 state",
+            "config": {"workload": "two-site Qt DMRG sweep, K=24 N=24 Sz=0 D=500, 48 operators H_p",
+                       "K": args.sites, "N": args.sites, "D": args.dmax},
+            "cpu_baseline": {"value": round(v, 1), "unit": "s/sweep", "cores": res[0]["cores"], "kind": "port",
+                             "sample": res[0]["sample"]},
+            "e2e": {"value": round(v, 1), "unit": "s/sweep", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "f64", "tf32"])
+    ap.add_argument("--sites", type=int, default=K_SITES)
+    ap.add_argument("--dmax", type=int, default=DMAX)
+    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-cpu", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

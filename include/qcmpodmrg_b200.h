@@ -106,17 +106,20 @@ long long qc_compile_pairs(int r1, const int *nsyms1, const long long *ndims1, c
  * tasks (qc_task, 64 B), contribs (qc_contrib, 80 B) and ops (qc_op, 32 B:
  * a_base, b_base, c_base, alpha per operator) are device arrays; the layout
  * is documented in qcmpodmrg_b200/csrc/qc_types.h.
- * summed == 0: each task writes one tile per operator of its range;
+ * summed == 0: each task writes one tile per operator of its range; the grid
+ *              is ntasks x opspan CTAs, opspan = the longest operator range;
  * summed != 0: each task writes one tile summed over the operators of every
- * contribution's range (sigma's sum over p).
+ * contribution's range (opspan ignored).
  * tile_cfg: output tile / threads: 0 = 64x64/256, 1 = 128x32/256, 2 = 256x16/256,
  * 3 = 32x32/64, 4 = 64x16/64. */
-int qc_bgemm_f64(const void *tasks_dev, long long ntasks, const void *contribs_dev, const void *ops_dev,
-                 int summed, const double *A, const double *B, double *C, int tile_cfg, void *stream);
+int qc_bgemm_f64(const void *tasks_dev, long long ntasks, int opspan, const void *contribs_dev,
+                 const void *ops_dev, int summed, const double *A, const double *B, double *C,
+                 int tile_cfg, void *stream);
 
 /* Same engine with FP32 operands and FP32 accumulation (mixed-precision sigma). */
-int qc_bgemm_f32(const void *tasks_dev, long long ntasks, const void *contribs_dev, const void *ops_dev,
-                 int summed, const float *A, const float *B, float *C, int tile_cfg, void *stream);
+int qc_bgemm_f32(const void *tasks_dev, long long ntasks, int opspan, const void *contribs_dev,
+                 const void *ops_dev, int summed, const float *A, const float *B, float *C,
+                 int tile_cfg, void *stream);
 
 /* dst[i] = src[idx[i]] (FP64), i < n.  Used for diag[prjmap] (kernelQt.py:122). */
 int qc_gather_f64(const double *src, const long long *idx, double *dst, long long n, void *stream);

@@ -1,0 +1,108 @@
+"""ORACLE (test infrastructure): CPU timing samples for bench.py.
+
+Only bench.py's CPU-baseline leg and its --impl reference arm import this.
+Both time the oracle (the NumPy restatement of HVecQt / HDiagQt /
+renormQt_H00, source/mpo_dmrg_kernelQt.py) on this host's cores.
+"""
+import os
+import time
+
+import numpy
+
+from .blocks import QTensor, classification
+from .kernels import SigmaOracle, hdiag, RenormOracle, boundary_env
+from .mpo import QPHYS, build_mpo, site_operator
+
+# Davidson matrix-vector products per dot at K=24, D=500 (FP64 GPU sweeps of the
+# same workload: 398 products over the 46 dots of one sweep).
+MATVECS_PER_DOT = 8.7
+
+
+def _qt(status, qsyms, ndims, values=None, rng=None):
+    q = QTensor(status).from_qsyms(len(qsyms), qsyms, ndims, allocate=True)
+    if values is not None:
+        q.value = numpy.asarray(values, dtype=numpy.float64)
+    elif rng is not None:
+        q.value = rng.standard_normal(q.size_allowed)
+    return q
+
+
+def oracle_dot(d, isite):
+    """Oracle sigma of the product's current dot (its environments copied to the host)."""
+    L, R = d.lenv[isite - 1], d.renv[isite + 2]
+    Wi, Wj = d.mpo[isite], d.mpo[isite + 1]
+
+    def conv(ts, i):
+        l = ts.layouts[i]
+        return _qt(l.status, l.qsyms, l.ndims, ts.op_values(i).cpu().numpy())
+
+    ql, qr = d.qnuml[isite], d.qnumr[isite + 2]
+    cls = [classification(q) for q in (ql, QPHYS, QPHYS, d.qkey - qr)]
+    qtmp = QTensor([False, False, False, True]).from_qsyms(4, [c[0] for c in cls], [c[1] for c in cls],
+                                                           allocate=False)
+    n = d.nops
+    sig = SigmaOracle(qtmp, d.qkey, [conv(L, i) for i in range(n)], [conv(R, i) for i in range(n)],
+                      [conv(Wi, i) for i in range(n)], [conv(Wj, i) for i in range(n)],
+                      list(range(n)), numpy.ones(n), isite)
+    lay, idl, s, dg = d.dot_operators(isite)
+    x = numpy.random.default_rng(0).standard_normal(qtmp.size_allowed)
+    return sig, x, s.flops
+
+
+_CACHE = {}
+
+
+def reference_step(args, warm=False):
+    """One bounded sample of the K=24, D=500 sweep on the host: at the mid-chain dot of a
+    synthetic D=500 state, one sigma matvec, one diagonal and one renormalisation; the sweep
+    estimate is 2(K-1) dots x (MATVECS_PER_DOT sigma + diagonal + renormalisation)."""
+    from qcmpodmrg_b200.hamiltonian import make_hamiltonian
+    from qcmpodmrg_b200.synthetic import random_mps
+    K, D = args.sites, args.dmax
+    if "ham" not in _CACHE:
+        ham = make_hamiltonian(K, K, 1, 3.0)
+        isite = K // 2
+        _CACHE["ham"] = ham
+        _CACHE["W"] = {i: [site_operator(p, ham.sbas, i, ham.int1e, ham.int2e) for p in range(ham.sbas)]
+                       for i in (isite - 1, isite, isite + 1)}
+        _CACHE["mps"] = random_mps(K, K, D, seed=1)
+        _CACHE["rmps"] = random_mps(K, K, D, seed=2)
+    if warm:
+        return None
+    ham, W, mps, rm = _CACHE["ham"], _CACHE["W"], _CACHE["mps"], _CACHE["rmps"]
+    isite = K // 2
+    rng = numpy.random.default_rng(5)
+    qkey = numpy.array([float(K), 0.0])
+    nops = ham.sbas
+    ql = mps["qnum%d" % isite]
+    qr = rm["qnum%d" % (K - isite - 2)]
+    # environment layouts: a-bond of the neighbouring site operators, MPS bonds (status T,F,T)
+    cl, cr = classification(ql), classification(qr)
+    lenv = [_qt([True, False, True], [W[isite][p].qsyms[0], cl[0], cl[0]], [W[isite][p].ndims[0], cl[1], cl[1]],
+                rng=rng) for p in range(nops)]
+    renv = [_qt([True, False, True], [-W[isite + 1][p].qsyms[1], cr[0], cr[0]],
+                [W[isite + 1][p].ndims[1], cr[1], cr[1]], rng=rng) for p in range(nops)]
+    cls = [classification(q) for q in (ql, QPHYS, QPHYS, qkey - qr)]
+    qtmp = QTensor([False, False, False, True]).from_qsyms(4, [c[0] for c in cls], [c[1] for c in cls],
+                                                           allocate=False)
+    sig = SigmaOracle(qtmp, qkey, lenv, renv, W[isite], W[isite + 1], list(range(nops)), numpy.ones(nops), isite)
+    x = rng.standard_normal(qtmp.size_allowed)
+    t0 = time.time()
+    sig(x)
+    t_hvec = time.time() - t0
+    prj = qtmp.prjmap([c[2] for c in cls])
+    dims = (len(ql), 16, len(qr), len(ql) * 16 * len(qr))
+    t0 = time.time()
+    hdiag(prj, dims, lenv, renv, W[isite], W[isite + 1], numpy.ones(nops))
+    t_diag = time.time() - t0
+    site = QTensor([False, False, True]).from_dense(rng.standard_normal((len(ql), 4, len(ql) * 4)),
+                                                    [ql, QPHYS, (ql[:, None, :] + QPHYS[None]).reshape(-1, 2)])
+    t0 = time.time()
+    RenormOracle(list(range(nops)), isite, "L")(site, lenv, W[isite])
+    t_ren = time.time() - t0
+    ndots = 2 * (K - 1)
+    est = ndots * (MATVECS_PER_DOT * t_hvec + t_diag + t_ren)
+    return {"sweep_s_est": est, "cores": os.cpu_count(),
+            "sample": "mid-chain dot of a synthetic D=500 state: sigma %.1f s, diagonal %.1f s, renormalisation "
+                      "%.1f s; sweep = %d dots x (%.1f sigma + diagonal + renormalisation)"
+                      % (t_hvec, t_diag, t_ren, ndots, MATVECS_PER_DOT)}

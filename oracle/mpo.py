@@ -88,12 +88,12 @@ def elem_spin(p, i):
 
 def hfac_spin(p, nsite, i, hq, v):
     w = wfac_spin(nsite, i, hq, v)
-    return numpy.einsum("ij,abjk->abik", elem_spin(p, i), w)
+    return numpy.matmul(elem_spin(p, i), w)        # ij,abjk->abik
 
 
 def link(op1, op2):
     """abij,bckl -> a c (ik) (jl)  (mpo_dmrg_opers.linkTwoOpers)."""
-    t = numpy.einsum("abij,bckl->acikjl", op1, op2)
+    t = numpy.tensordot(op1, op2, axes=([1], [0])).transpose(0, 3, 1, 4, 2, 5)
     s = t.shape
     return t.reshape(s[0], s[1], s[2] * s[3], s[4] * s[5])
 

@@ -44,10 +44,12 @@ k_bgemm(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ contri
   __shared__ int bkoff[TK];
 
   const qc_task t = tasks[blockIdx.x];
+  // per-operator mode: blockIdx.y selects the operator of the task's range
+  if (!SUMMED && t.op_b + (int)blockIdx.y >= t.op_e) return;
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
-  const int nouter = SUMMED ? 1 : (t.op_e - t.op_b);
-  for (int oi = 0; oi < nouter; ++oi) {
+  {
+    const int oi = SUMMED ? 0 : (int)blockIdx.y;
     T acc[RM][RN];
 #pragma unroll
     for (int i = 0; i < RM; ++i)
@@ -127,9 +129,9 @@ k_bgemm(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ contri
 }
 
 template <typename T, bool S>
-int launch_mode(const qc_task *tk, long long ntasks, const qc_contrib *cb, const qc_op *ops, const T *A,
-                const T *B, T *C, int cfg, cudaStream_t s) {
-  dim3 grid((unsigned)ntasks);
+int launch_mode(const qc_task *tk, long long ntasks, int opspan, const qc_contrib *cb, const qc_op *ops,
+                const T *A, const T *B, T *C, int cfg, cudaStream_t s) {
+  dim3 grid((unsigned)ntasks, S ? 1u : (unsigned)opspan);
   switch (cfg) {
     case 0: k_bgemm<T, 64, 64, 16, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
     case 1: k_bgemm<T, 128, 32, 16, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
@@ -142,15 +144,15 @@ int launch_mode(const qc_task *tk, long long ntasks, const qc_contrib *cb, const
 }
 
 template <typename T>
-int launch_bgemm(const void *tasks, long long ntasks, const void *contribs, const void *ops, int summed,
-                 const T *A, const T *B, T *C, int cfg, cudaStream_t s) {
+int launch_bgemm(const void *tasks, long long ntasks, int opspan, const void *contribs, const void *ops,
+                 int summed, const T *A, const T *B, T *C, int cfg, cudaStream_t s) {
   if (ntasks <= 0) return QC_OK;
-  if (ntasks > 0x7fffffffLL) return QC_ERR_ARG;
+  if (ntasks > 0x7fffffffLL || opspan < 1 || opspan > 65535) return QC_ERR_ARG;
   const qc_task *tk = (const qc_task *)tasks;
   const qc_contrib *cb = (const qc_contrib *)contribs;
   const qc_op *op = (const qc_op *)ops;
-  return summed ? launch_mode<T, true>(tk, ntasks, cb, op, A, B, C, cfg, s)
-                : launch_mode<T, false>(tk, ntasks, cb, op, A, B, C, cfg, s);
+  return summed ? launch_mode<T, true>(tk, ntasks, 1, cb, op, A, B, C, cfg, s)
+                : launch_mode<T, false>(tk, ntasks, opspan, cb, op, A, B, C, cfg, s);
 }
 
 struct SymArgs {
@@ -214,14 +216,14 @@ inline unsigned grid_for(long long n) {
 
 }  // namespace
 
-extern "C" int qc_bgemm_f64(const void *tasks, long long ntasks, const void *contribs, const void *ops, int summed,
-                            const double *A, const double *B, double *C, int cfg, void *stream) {
-  return launch_bgemm<double>(tasks, ntasks, contribs, ops, summed, A, B, C, cfg, (cudaStream_t)stream);
+extern "C" int qc_bgemm_f64(const void *tasks, long long ntasks, int opspan, const void *contribs, const void *ops,
+                            int summed, const double *A, const double *B, double *C, int cfg, void *stream) {
+  return launch_bgemm<double>(tasks, ntasks, opspan, contribs, ops, summed, A, B, C, cfg, (cudaStream_t)stream);
 }
 
-extern "C" int qc_bgemm_f32(const void *tasks, long long ntasks, const void *contribs, const void *ops, int summed,
-                            const float *A, const float *B, float *C, int cfg, void *stream) {
-  return launch_bgemm<float>(tasks, ntasks, contribs, ops, summed, A, B, C, cfg, (cudaStream_t)stream);
+extern "C" int qc_bgemm_f32(const void *tasks, long long ntasks, int opspan, const void *contribs, const void *ops,
+                            int summed, const float *A, const float *B, float *C, int cfg, void *stream) {
+  return launch_bgemm<float>(tasks, ntasks, opspan, contribs, ops, summed, A, B, C, cfg, (cudaStream_t)stream);
 }
 
 extern "C" int qc_sym_allowed_gpu(int rank, int nqnum, const int *nsyms, const int *status, const int *q2,

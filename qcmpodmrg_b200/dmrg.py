@@ -79,6 +79,11 @@ class DMRG(object):
         self.stats = {"hvec_s": 0.0, "hdiag_s": 0.0, "renorm_s": 0.0, "decim_s": 0.0, "plan_s": 0.0,
                       "nmvp": 0, "sigma_flops": 0.0, "renorm_flops": 0.0, "diag_flops": 0.0}
         self.events = False
+        # host_api: drive the dot through the reference-facing functions with host
+        # (NumPy) vectors, as the reference's pdvdson does (used for end-to-end timing)
+        self.host_api = False
+        self.h2d_bytes = 0
+        self.d2h_bytes = 0
 
     # ------------------------------------------------------------- set-up
     def load_mps(self, init):
@@ -110,6 +115,8 @@ class DMRG(object):
         return lay, idl, sig, dg
 
     def solve_dot(self, isite, status, dmax, crit_e):
+        if self.host_api:
+            return self._solve_dot_host(isite, status, dmax, crit_e)
         dev = self.device
         t0 = time.time()
         lay, idl, sig, dg = self.dot_operators(isite)
@@ -140,6 +147,44 @@ class DMRG(object):
         self.stats["sigma_flops"] += res.nmvp * sig.flops
         civec = torch.zeros((1, dims[3]), dtype=torch.float64, device=dev)
         civec[:, prj] = res.vecs
+        t0 = time.time()
+        out = self.decimate(civec, isite, status, dims, dmax)
+        torch.cuda.synchronize(dev)
+        self.stats["decim_s"] += time.time() - t0
+        return res, out, dims, sig
+
+    def _solve_dot_host(self, isite, status, dmax, crit_e):
+        """The same dot, through mpo_dmrg_kernel.HDiag/HVec with host buffers."""
+        from . import mpo_dmrg_kernel as K
+        dev = self.device
+        info = [self, isite, 2, [[self.lenv[isite - 1], self.renv[isite + 2]]], status, True]
+        t0 = time.time()
+        lay, idl, sig, dg = K._ops(self, isite)
+        prj_h = lay.prjmap(idl)
+        self.stats["plan_s"] += time.time() - t0
+        ndim0 = lay.size
+        ldim, rdim = len(self.qnuml[isite]), len(self.qnumr[isite + 2])
+        dims = (ldim, 16, rdim, ldim * 16 * rdim)
+        diag = torch.from_numpy(K.HDiag(info, ndim0, prj_h))
+        self.d2h_bytes += 8 * ndim0
+
+        def hv(x):
+            y = K.HVec(x.numpy(), info, ndim0, prj_h)
+            self.h2d_bytes += 8 * ndim0
+            self.d2h_bytes += 8 * ndim0
+            return torch.from_numpy(y)
+
+        v0 = None
+        if self.psi0 is not None:
+            v0 = self.psi0[0:1].reshape(1, -1)[:, torch.from_numpy(prj_h).to(self.psi0.device)].cpu()
+        t0 = time.time()
+        res = davidson(hv, diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec)
+        self.stats["hvec_s"] += time.time() - t0
+        self.stats["nmvp"] += res.nmvp
+        self.stats["sigma_flops"] += res.nmvp * sig.flops
+        civec = torch.zeros((1, dims[3]), dtype=torch.float64, device=dev)
+        civec[:, torch.from_numpy(prj_h).to(dev)] = res.vecs.to(dev)
+        self.h2d_bytes += 8 * ndim0
         t0 = time.time()
         out = self.decimate(civec, isite, status, dims, dmax)
         torch.cuda.synchronize(dev)

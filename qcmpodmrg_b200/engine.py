@@ -139,6 +139,22 @@ def merge_grouped(parts):
     return new_t, new_c, flops
 
 
+class LaunchLog(object):
+    """Optional per-launch CUDA-event log (bench instrumentation) and launch counter."""
+
+    def __init__(self):
+        self.enabled = False
+        self.records = []
+        self.launches = 0
+
+    def reset(self):
+        self.records = []
+        self.launches = 0
+
+
+LOG = LaunchLog()
+
+
 class Stage(object):
     """A compiled stage resident on the device: one launch per tile configuration.
 
@@ -156,6 +172,7 @@ class Stage(object):
         self.host_ops = ops
         self.d_ops = torch.from_numpy(ops.view(numpy.uint8).copy()).to(device)
         self.groups = []
+        self.bytes = 0.0          # algorithmic bytes (operands read once, output written once)
         self.flops = 0.0
         self.ntasks = 0
         self.ncontribs = 0
@@ -175,22 +192,31 @@ class Stage(object):
                 continue
             tk = numpy.concatenate(tasks)
             ct = numpy.concatenate(contribs)
+            span = 1 if self.summed else int(max(1, (tk["op_e"] - tk["op_b"]).max()))
             self.groups.append((cfg, tk, ct, torch.from_numpy(tk.view(numpy.uint8).copy()).to(device),
-                                torch.from_numpy(ct.view(numpy.uint8).copy()).to(device)))
+                                torch.from_numpy(ct.view(numpy.uint8).copy()).to(device), span))
             self.ntasks += len(tk)
             self.ncontribs += len(ct)
 
     @property
     def host_groups(self):
-        return [(cfg, tk, ct) for (cfg, tk, ct, _, _) in self.groups]
+        return [(cfg, tk, ct) for (cfg, tk, ct, _, _, _) in self.groups]
 
     def run(self, A, B, C, kind="f64", stream=None):
         lib = native.lib()
         s = stream if stream is not None else torch.cuda.current_stream(C.device).cuda_stream
         fn = {"f64": lib.qc_bgemm_f64, "f32": lib.qc_bgemm_f32, "tf32": getattr(lib, "qc_bgemm_tf32", None)}[kind]
-        for (cfg, tk, ct, dt, dc) in self.groups:
-            check(fn(dt.data_ptr(), len(tk), dc.data_ptr(), self.d_ops.data_ptr(), int(self.summed),
+        if LOG.enabled:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+        for (cfg, tk, ct, dt, dc, span) in self.groups:
+            check(fn(dt.data_ptr(), len(tk), span, dc.data_ptr(), self.d_ops.data_ptr(), int(self.summed),
                      A.data_ptr(), B.data_ptr(), C.data_ptr(), cfg, s), "qc_bgemm_" + kind)
+            LOG.launches += 1
+        if LOG.enabled:
+            e1.record()
+            LOG.records.append((self.name, e0, e1, self.flops, self.bytes * (A.element_size() / 8.0)))
 
 
 def add_parts(dst, parts, op_range=None, contrib_range=None):

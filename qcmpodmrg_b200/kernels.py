@@ -18,7 +18,7 @@ import torch
 
 from . import native
 from .native import check
-from .engine import (Stage, compile_classes, add_parts, live_blocks, prune, op_table, TASK_DT, CONTRIB_DT)
+from .engine import (Stage, compile_classes, add_parts, live_blocks, prune, op_table, TASK_DT, CONTRIB_DT, LOG)
 from .mpo import case
 from .qtensor import Contraction, flip_right, flip_horizontal
 
@@ -77,6 +77,7 @@ def gather(src, idx, out):
     """out[i] = src[idx[i]] on the device (qc_gather_f64)."""
     check(native.lib().qc_gather_f64(src.data_ptr(), idx.data_ptr(), out.data_ptr(), out.numel(),
                                      _stream(out.device)), "qc_gather_f64")
+    LOG.launches += 1
     return out
 
 
@@ -88,6 +89,7 @@ def convert(src, out):
         check(lib.qc_convert_f64_to_f32(src.data_ptr(), out.data_ptr(), n, _stream(out.device)), "convert")
     else:
         check(lib.qc_convert_f32_to_f64(src.data_ptr(), out.data_ptr(), n, _stream(out.device)), "convert")
+    LOG.launches += 1
     return out
 
 
@@ -96,6 +98,7 @@ def reduce_ops(part, nops, n, out):
     lib = native.lib()
     fn = lib.qc_reduce_ops_f64 if part.dtype == torch.float64 else lib.qc_reduce_ops_f32
     check(fn(part.data_ptr(), nops, n, out.data_ptr(), _stream(out.device)), "qc_reduce_ops")
+    LOG.launches += 1
     return out
 
 
@@ -170,6 +173,22 @@ class SigmaOperator(object):
             for si, (c, t) in enumerate(cs):
                 add_parts(st[si], compile_classes(c, t, ax[si]), op_range=rng)
         self.stages = [Stage(st[si], dev, "sigma%d" % (si + 1), tabs[si]) for si in range(4)]
+        # algorithmic bytes per stage (FP64): every operand block read once, output written once
+        for si in range(4):
+            tot_b = 0
+            for key, (ops, *cs, Rl) in sorted(plans.items()):
+                c, t = cs[si]
+                if len(t) == 0:
+                    continue
+                u1 = numpy.unique(t[:, 1])
+                u2 = numpy.unique(t[:, 2])
+                uo = numpy.unique(t[:, 0])
+                shared2 = (si == 0)     # psi is read by every operator
+                b1 = c.l1.ndim[u1].sum() * len(ops)
+                b2 = c.l2.ndim[u2].sum() * (1 if shared2 else len(ops))
+                bo = c.out.ndim[uo].sum() * len(ops)
+                tot_b += 8 * (b1 + b2 + bo)
+            self.stages[si].bytes = float(tot_b)
         self.flops = sum(s.flops for s in self.stages)
         self.ndim0 = psi_layout.size
 

@@ -1,0 +1,96 @@
+"""Drop-in for the reference's kernel dispatch module (source/mpo_dmrg_kernel.py).
+
+Same function names, arguments and return conventions as the functions that
+mpo_dmrg_dot.ci_solver, dotutil.genHDiag and mpo_dmrg_opt.sweep call:
+
+  HDiag(info, ndim0, prjmap)                       source/mpo_dmrg_kernel.py:41-51
+  HVec(vec0, info, ndim0, prjmap)                  source/mpo_dmrg_kernel.py:117-136
+  renorm(dmrg, isite, ncsite, flst, flstN, site, status)   :347-377
+  pRDM(cimat, info)                                :278-282 (noise-free part)
+
+``info = [dmrg, isite, ncsite, flst, status, ifsym]`` as in mpo_dmrg_dot.py:31.
+Here ``dmrg`` is a qcmpodmrg_b200.dmrg.DMRG (device-resident environments);
+``flst[0][0:2]`` / ``flstN[0][0]`` are the device environment sets standing in
+for the reference's per-site HDF5 files.  Vectors may be NumPy arrays (host
+buffers, copied to and from the device inside the call) or CUDA tensors.  Only
+the two-site Qt path exists (ncsite == 2, ifQt); anything else raises.
+"""
+import numpy
+import torch
+
+from .kernels import Renormalizer
+
+
+def _check(info):
+    dmrg, isite, ncsite, flst, status, ifsym = info
+    if ncsite != 2:
+        raise NotImplementedError("only the two-site dot is implemented")
+    return dmrg, isite
+
+
+def _ops(dmrg, isite):
+    """Sigma/diagonal operators of the dot, cached on the DMRG object while the dot is active."""
+    key = (isite, id(dmrg.lenv[isite - 1]), id(dmrg.renv[isite + 2]))
+    cache = getattr(dmrg, "_dot_cache", None)
+    if cache is None or cache[0] != key:
+        lay, idl, sig, dg = dmrg.dot_operators(isite)
+        dmrg._dot_cache = (key, lay, idl, sig, dg)
+    return dmrg._dot_cache[1:]
+
+
+def _to_dev(v, dev):
+    if torch.is_tensor(v):
+        return v.to(dev, torch.float64)
+    return torch.from_numpy(numpy.ascontiguousarray(v, dtype=numpy.float64)).to(dev)
+
+
+def HVec(vec0, info, ndim0, prjmap):
+    """sigma = H_eff vec0 in the packed (qtmp) layout."""
+    dmrg, isite = _check(info)
+    lay, idl, sig, dg = _ops(dmrg, isite)
+    if ndim0 != sig.ndim0:
+        raise ValueError("ndim0 does not match the dot's wavefunction template")
+    y = sig(_to_dev(vec0, dmrg.device))
+    return y if torch.is_tensor(vec0) else y.cpu().numpy()
+
+
+def HDiag(info, ndim0, prjmap):
+    """Diagonal of H_eff in the packed layout (real)."""
+    dmrg, isite = _check(info)
+    lay, idl, sig, dg = _ops(dmrg, isite)
+    return dg().cpu().numpy()
+
+
+def renorm(dmrg, isite, ncsite, flst, flstN, site, status):
+    """New environments of every operator; stored in flstN[0][0] and in dmrg's env table.
+
+    ``site`` is a qcmpodmrg_b200.dmrg.SiteTensor (packed values on the device).
+    """
+    if ncsite != 2:
+        raise NotImplementedError("only the two-site dot is implemented")
+    if status == "L":
+        rn = Renormalizer(dmrg.ws, isite, "L", site.layout, dmrg.lenv[isite - 1], dmrg.mpo[isite], dmrg.opers)
+        new = rn(site.values)
+        dmrg.lenv[isite] = new
+    else:
+        j = isite + ncsite - 1
+        rn = Renormalizer(dmrg.ws, j, "R", site.layout, dmrg.renv[j + 1], dmrg.mpo[j], dmrg.opers)
+        new = rn(site.values)
+        dmrg.renv[j] = new
+    if flstN is not None:
+        flstN[0][0] = new
+    return 0
+
+
+def pRDM(cimat, info):
+    """Reduced density matrix of the superblock, sum_i C_i C_i^+ (noise = 0)."""
+    dmrg, isite, ncsite, flst, status, ifsym = info
+    c = _to_dev(cimat, dmrg.device)
+    neig = c.shape[0]
+    if status == "L":      # cimat [neig, ldim, dim, crdim] (dotutil.py:276-281)
+        m = c.reshape(neig, c.shape[1] * c.shape[2], -1)
+        rdm = sum(m[i] @ m[i].T for i in range(neig))
+    else:                  # cimat [neig, lcdim, dim, rdim] (dotutil.py:282-288)
+        m = c.reshape(neig, c.shape[1], -1)
+        rdm = sum(m[i].T @ m[i] for i in range(neig))
+    return rdm.cpu().numpy()

@@ -44,9 +44,9 @@ _SIGS = {
     "qc_compile_pairs": (c_ll, [c_int, c_vp, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp, c_vp, c_vp,
                                 c_int, c_vp, c_vp, c_ll, c_vp, c_int, c_vp, c_vp, c_vp, c_vp, c_int,
                                 c_int, c_int, c_vp, c_ll, c_vp, c_ll, c_vp, c_vp]),
-    "qc_bgemm_f64": (c_int, [c_vp, c_ll, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
-    "qc_bgemm_f32": (c_int, [c_vp, c_ll, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
-    "qc_bgemm_tf32": (c_int, [c_vp, c_ll, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
+    "qc_bgemm_f64": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
+    "qc_bgemm_f32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
+    "qc_bgemm_tf32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
     "qc_gather_f64": (c_int, [c_vp, c_vp, c_vp, c_ll, c_vp]),
     "qc_reduce_ops_f64": (c_int, [c_vp, c_int, c_ll, c_vp, c_vp]),
     "qc_reduce_ops_f32": (c_int, [c_vp, c_int, c_ll, c_vp, c_vp]),

@@ -13,7 +13,7 @@ import numpy
 QPHYS = numpy.array([[0., 0.], [1., -0.5], [1., 0.5], [2., 0.]])
 
 
-def random_mps(K, N, D, seed=0, width=1.2, szwidth=0.7):
+def random_mps(K, N, D, seed=0, width=0.9, szwidth=0.6):
     rng = numpy.random.default_rng(seed)
     qnum = [numpy.zeros((1, 2))]
     sites = []

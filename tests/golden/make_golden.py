@@ -78,5 +78,5 @@ if __name__ == "__main__":
         sys.exit(0)
     qsym_cases()
     run_case("K4", 4, 4, 16, 2, 1, None, [(0, "R", 1), (0, "L", 1), (0, "R", 0), (0, "L", 2), (1, "R", 2)])
-    run_case("K5", 5, 4, 12, 2, 2, 2.0, [(0, "R", 2), (0, "L", 1), (1, "L", 3)])
+    run_case("K5", 5, 4, 12, 6, 2, 2.0, [(0, "R", 2), (0, "L", 1), (1, "L", 3)])
     run_case("K6", 6, 6, 20, 3, 3, None, [(0, "R", 3), (1, "L", 2)])
