@@ -20,6 +20,11 @@ MATVECS_PER_DOT = 8.7
 
 def _qt(status, qsyms, ndims, values=None, rng=None):
     q = QTensor(status).from_qsyms(len(qsyms), qsyms, ndims, allocate=True)
+    # contiguous index lists: sector s of index i covers positions [off, off + ndims[i][s])
+    q.idlst = []
+    for nd in q.ndims:
+        off = numpy.concatenate([[0], numpy.cumsum(nd)[:-1]])
+        q.idlst.append([list(range(int(o), int(o + n))) for o, n in zip(off, nd)])
     if values is not None:
         q.value = numpy.asarray(values, dtype=numpy.float64)
     elif rng is not None:
@@ -52,6 +57,15 @@ def oracle_dot(d, isite):
 _CACHE = {}
 
 
+def _with_idlst(q):
+    if q.idlst is None:
+        q.idlst = []
+        for nd in q.ndims:
+            off = numpy.concatenate([[0], numpy.cumsum(nd)[:-1]])
+            q.idlst.append([list(range(int(o), int(o + n))) for o, n in zip(off, nd)])
+    return q
+
+
 def reference_step(args, warm=False):
     """One bounded sample of the K=24, D=500 sweep on the host: at the mid-chain dot of a
     synthetic D=500 state, one sigma matvec, one diagonal and one renormalisation; the sweep
@@ -63,7 +77,7 @@ def reference_step(args, warm=False):
         ham = make_hamiltonian(K, K, 1, 3.0)
         isite = K // 2
         _CACHE["ham"] = ham
-        _CACHE["W"] = {i: [site_operator(p, ham.sbas, i, ham.int1e, ham.int2e) for p in range(ham.sbas)]
+        _CACHE["W"] = {i: [_with_idlst(site_operator(p, ham.sbas, i, ham.int1e, ham.int2e)) for p in range(ham.sbas)]
                        for i in (isite - 1, isite, isite + 1)}
         _CACHE["mps"] = random_mps(K, K, D, seed=1)
         _CACHE["rmps"] = random_mps(K, K, D, seed=2)
@@ -103,6 +117,6 @@ def reference_step(args, warm=False):
     ndots = 2 * (K - 1)
     est = ndots * (MATVECS_PER_DOT * t_hvec + t_diag + t_ren)
     return {"sweep_s_est": est, "cores": os.cpu_count(),
-            "sample": "mid-chain dot of a synthetic D=500 state: sigma %.1f s, diagonal %.1f s, renormalisation "
+            "sample": "mid-chain dot of a synthetic D=%d state: sigma %.1f s, diagonal %.1f s, renormalisation "
                       "%.1f s; sweep = %d dots x (%.1f sigma + diagonal + renormalisation)"
-                      % (t_hvec, t_diag, t_ren, ndots, MATVECS_PER_DOT)}
+                      % (D, t_hvec, t_diag, t_ren, ndots, MATVECS_PER_DOT)}
