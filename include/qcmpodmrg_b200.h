@@ -136,6 +136,32 @@ int qc_reduce_ops_f32(const float *part, int nops, long long n, float *out, void
 int qc_convert_f64_to_f32(const double *src, float *dst, long long n, void *stream);
 int qc_convert_f32_to_f64(const float *src, double *dst, long long n, void *stream);
 
+/* Sigma without any device allocation.  This entry point has no counterpart in
+ * the reference; it exists for host codes that own the GPU memory budget and
+ * cannot hand out intermediate buffers (or must not trigger cudaMalloc's
+ * device-wide synchronisation mid-iteration).  It runs the same four
+ * qc_bgemm_f64 contractions and the operator sum as the regular path, with the
+ * intermediates held in a fixed 32 MiB device array inside the library
+ * (present on every GPU that loads it, until process exit).
+ *   groups: ngroups work-item groups of the compiled sigma plan, ordered by
+ *     stage 0..3 (L.psi, .W_i, .W_{i+1}, .R); for each: stage, device task and
+ *     contribution arrays, task count, operator span, tile configuration;
+ *   stage_ops[4]: device operator tables of the four stages;
+ *   L, Wi, Wj, R: device environment / site-operator values; x: device input;
+ *   y: device output (ndim0 doubles); t1, t2, t3: intermediate sizes (doubles).
+ * Needs t1 + t2 + t3 + nops*ndim0 doubles (each region padded to 256 bytes);
+ * larger dots return QC_ERR_CAPACITY before queueing any work.  All calls on a
+ * device share the array and leave their data in it: calls that overlap on the
+ * GPU race and must be serialised by the caller.  The first call on each device
+ * looks up the array's device address with that device current; make it before
+ * any stream capture.  Allocates nothing (no cudaMalloc/cudaFree). */
+int qc_sigma_f64_noalloc(int ngroups, const int *group_stage, const void *const *group_tasks,
+                         const long long *group_ntasks, const int *group_opspan,
+                         const void *const *group_contribs, const int *group_cfg,
+                         const void *const *stage_ops, const double *L, const double *Wi,
+                         const double *Wj, const double *R, const double *x, double *y, int nops,
+                         long long ndim0, long long t1, long long t2, long long t3, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

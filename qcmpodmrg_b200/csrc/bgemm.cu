@@ -216,6 +216,21 @@ inline unsigned grid_for(long long n) {
 
 }  // namespace
 
+// Internal launchers shared with sigma_noalloc.cu (not part of the C ABI).
+__attribute__((visibility("hidden"))) int qc_internal_bgemm_f64(const void *tasks, long long ntasks, int opspan,
+                                                                const void *contribs, const void *ops, int summed,
+                                                                const double *A, const double *B, double *C,
+                                                                int cfg, cudaStream_t s) {
+  return launch_bgemm<double>(tasks, ntasks, opspan, contribs, ops, summed, A, B, C, cfg, s);
+}
+
+__attribute__((visibility("hidden"))) int qc_internal_reduce_f64(const double *part, int nops, long long n,
+                                                                 double *out, cudaStream_t s) {
+  if (n <= 0) return QC_OK;
+  k_reduce_ops<double><<<grid_for(n), 256, 0, s>>>(part, nops, n, out);
+  return cuda_fail("qc_internal_reduce_f64");
+}
+
 extern "C" int qc_bgemm_f64(const void *tasks, long long ntasks, int opspan, const void *contribs, const void *ops,
                             int summed, const double *A, const double *B, double *C, int cfg, void *stream) {
   return launch_bgemm<double>(tasks, ntasks, opspan, contribs, ops, summed, A, B, C, cfg, (cudaStream_t)stream);

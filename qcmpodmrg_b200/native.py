@@ -49,6 +49,8 @@ _SIGS = {
     "qc_bgemm_tf32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
     "qc_gather_f64": (c_int, [c_vp, c_vp, c_vp, c_ll, c_vp]),
     "qc_reduce_ops_f64": (c_int, [c_vp, c_int, c_ll, c_vp, c_vp]),
+    "qc_sigma_f64_noalloc": (c_int, [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                     c_vp, c_vp, c_int, c_ll, c_ll, c_ll, c_ll, c_vp]),
     "qc_reduce_ops_f32": (c_int, [c_vp, c_int, c_ll, c_vp, c_vp]),
     "qc_scatter_f64": (c_int, [c_vp, c_vp, c_vp, c_ll, c_ll, c_vp]),
     "qc_convert_f64_to_f32": (c_int, [c_vp, c_vp, c_ll, c_vp]),
