@@ -111,7 +111,7 @@ long long qc_compile_pairs(int r1, const int *nsyms1, const long long *ndims1, c
  * summed != 0: each task writes one tile summed over the operators of every
  * contribution's range (opspan ignored).
  * tile_cfg: output tile / threads: 0 = 64x64/256, 1 = 128x32/256, 2 = 256x16/256,
- * 3 = 32x32/64, 4 = 64x16/64. */
+ * 3 = 32x32/64, 4 = 64x16/64, 5 = 128x64/256. */
 int qc_bgemm_f64(const void *tasks_dev, long long ntasks, int opspan, const void *contribs_dev,
                  const void *ops_dev, int summed, const double *A, const double *B, double *C,
                  int tile_cfg, void *stream);
@@ -120,6 +120,19 @@ int qc_bgemm_f64(const void *tasks_dev, long long ntasks, int opspan, const void
 int qc_bgemm_f32(const void *tasks_dev, long long ntasks, int opspan, const void *contribs_dev,
                  const void *ops_dev, int summed, const float *A, const float *B, float *C,
                  int tile_cfg, void *stream);
+
+/* The same contraction on the 5th-generation tensor cores: tcgen05.mma
+ * kind::tf32 with FP32 accumulators in tensor memory, FP32 operands rounded to
+ * TF32 when staged in shared memory, FP32 output.  Per-operator mode only
+ * (summed must be 0) and only tile_cfg 5 (128 x 64 output tiles).  Waits are
+ * bounded; a timed-out wait is reported by qc_tc_status(). */
+int qc_bgemm_tf32(const void *tasks_dev, long long ntasks, int opspan, const void *contribs_dev,
+                  const void *ops_dev, int summed, const float *A, const float *B, float *C,
+                  int tile_cfg, void *stream);
+
+/* 0 if no tensor-core launch has reported a timed-out wait, 1 otherwise
+ * (synchronous: reads a device flag), negative on a CUDA error. */
+int qc_tc_status(void);
 
 /* dst[i] = src[idx[i]] (FP64), i < n.  Used for diag[prjmap] (kernelQt.py:122). */
 int qc_gather_f64(const double *src, const long long *idx, double *dst, long long n, void *stream);

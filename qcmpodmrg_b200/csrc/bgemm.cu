@@ -138,6 +138,7 @@ int launch_mode(const qc_task *tk, long long ntasks, int opspan, const qc_contri
     case 2: k_bgemm<T, 256, 16, 16, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
     case 3: k_bgemm<T, 32, 32, 16, 4, 4, S, 64><<<grid, 64, 0, s>>>(tk, cb, ops, A, B, C); break;
     case 4: k_bgemm<T, 64, 16, 16, 4, 4, S, 64><<<grid, 64, 0, s>>>(tk, cb, ops, A, B, C); break;
+    case 5: k_bgemm<T, 128, 64, 16, 8, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
     default: return QC_ERR_ARG;
   }
   return cuda_fail("qc_bgemm");

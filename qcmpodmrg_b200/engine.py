@@ -25,7 +25,8 @@ OP_DT = numpy.dtype([("a_base", "<i8"), ("b_base", "<i8"), ("c_base", "<i8"), ("
 assert TASK_DT.itemsize == native.TASK_BYTES and CONTRIB_DT.itemsize == native.CONTRIB_BYTES
 assert OP_DT.itemsize == native.OP_BYTES
 
-TILES = {0: (64, 64), 1: (128, 32), 2: (256, 16), 3: (32, 32), 4: (64, 16)}
+TILES = {0: (64, 64), 1: (128, 32), 2: (256, 16), 3: (32, 32), 4: (64, 16), 5: (128, 64)}
+TC_CFG = 5      # output tile of the tensor-core kernel (qc_bgemm_tf32)
 
 
 def tile_class(M, N):
@@ -36,10 +37,18 @@ def tile_class(M, N):
                        numpy.where(N <= 32, numpy.where(M <= 32, 3, 1), numpy.where(M <= 32, 3, 0)))
 
 
-def compile_classes(c, triples, axes):
+def tile_class_tc(M, N, K):
+    """Tensor-core tiles for output blocks that fill a useful part of a 128 x 64 tile."""
+    base = tile_class(M, N)
+    return numpy.where((numpy.asarray(M) > 64) & (numpy.asarray(N) > 24) & (numpy.asarray(K) >= 16), TC_CFG, base)
+
+
+def compile_classes(c, triples, axes, tensor_cores=False):
     """Compile one contraction's pair list, binned by output-block shape into tile classes.
 
     Returns {tile_cfg: (tasks, contribs, flops)} for a single operator (template).
+    tensor_cores: route large output blocks to the tcgen05 tile class (TC_CFG);
+    tensor_cores == "all" routes every block there (tests).
     """
     out = {}
     if len(triples) == 0:
@@ -48,7 +57,19 @@ def compile_classes(c, triples, axes):
     d = c.out.block_dims(triples[:, 0])
     M = numpy.prod(d[:, :ne1], axis=1)
     N = numpy.prod(d[:, ne1:], axis=1)
-    cls = tile_class(M, N)
+    if tensor_cores == "all":
+        cls = numpy.full(len(M), TC_CFG)
+    elif tensor_cores:
+        d1 = c.l1.block_dims(triples[:, 1])
+        K = numpy.prod(d1[:, axes[0]], axis=1)
+        # every pair of one output block must land in the same class
+        cls = tile_class_tc(M, N, K)
+        ob = triples[:, 0]
+        first = numpy.unique(ob, return_index=True)[1]
+        cmap = dict(zip(ob[first].tolist(), cls[first].tolist()))
+        cls = numpy.array([cmap[x] for x in ob.tolist()])
+    else:
+        cls = tile_class(M, N)
     for k in numpy.unique(cls):
         sel = triples[cls == k]
         out[int(k)] = compile_template(c.l1, c.l2, c.out, axes, sel, int(k))
@@ -205,14 +226,15 @@ class Stage(object):
     def run(self, A, B, C, kind="f64", stream=None):
         lib = native.lib()
         s = stream if stream is not None else torch.cuda.current_stream(C.device).cuda_stream
-        fn = {"f64": lib.qc_bgemm_f64, "f32": lib.qc_bgemm_f32, "tf32": getattr(lib, "qc_bgemm_tf32", None)}[kind]
+        fn = {"f64": lib.qc_bgemm_f64, "f32": lib.qc_bgemm_f32, "tf32": lib.qc_bgemm_f32}[kind]
         if LOG.enabled:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
         for (cfg, tk, ct, dt, dc, span) in self.groups:
-            check(fn(dt.data_ptr(), len(tk), span, dc.data_ptr(), self.d_ops.data_ptr(), int(self.summed),
-                     A.data_ptr(), B.data_ptr(), C.data_ptr(), cfg, s), "qc_bgemm_" + kind)
+            f = lib.qc_bgemm_tf32 if (kind == "tf32" and cfg == TC_CFG) else fn
+            check(f(dt.data_ptr(), len(tk), span, dc.data_ptr(), self.d_ops.data_ptr(), int(self.summed),
+                    A.data_ptr(), B.data_ptr(), C.data_ptr(), cfg, s), "qc_bgemm_" + kind)
             LOG.launches += 1
         if LOG.enabled:
             e1.record()

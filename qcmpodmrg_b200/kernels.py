@@ -121,8 +121,11 @@ def _ncols(c, triples):
 class SigmaOperator(object):
     """sigma = sum_p w_p R_p W_p[i+1] W_p[i] L_p psi for the dot (isite, isite+1)."""
 
-    def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts, precision="f64"):
+    def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts, precision="f64",
+                 tensor_cores=None):
         self.ws, self.psi, self.precision = ws, psi_layout, precision
+        # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 mode
+        tc = (precision == "tf32") if tensor_cores is None else tensor_cores
         self.L, self.R, self.Wi, self.Wj = L, R, Wi, Wj
         dev = ws.device
         groups = _groups(opers, isite, 2)
@@ -171,7 +174,8 @@ class SigmaOperator(object):
             rng = (pos, pos + len(ops))
             pos += len(ops)
             for si, (c, t) in enumerate(cs):
-                add_parts(st[si], compile_classes(c, t, ax[si]), op_range=rng)
+                add_parts(st[si], compile_classes(c, t, ax[si], tensor_cores=tc if si in (0, 3) else False),
+                          op_range=rng)
         self.stages = [Stage(st[si], dev, "sigma%d" % (si + 1), tabs[si]) for si in range(4)]
         # algorithmic bytes per stage (FP64): every operand block read once, output written once
         for si in range(4):

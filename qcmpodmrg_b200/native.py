@@ -49,6 +49,7 @@ _SIGS = {
     "qc_bgemm_tf32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
     "qc_gather_f64": (c_int, [c_vp, c_vp, c_vp, c_ll, c_vp]),
     "qc_reduce_ops_f64": (c_int, [c_vp, c_int, c_ll, c_vp, c_vp]),
+    "qc_tc_status": (c_int, []),
     "qc_sigma_f64_noalloc": (c_int, [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                                      c_vp, c_vp, c_int, c_ll, c_ll, c_ll, c_ll, c_vp]),
     "qc_reduce_ops_f32": (c_int, [c_vp, c_int, c_ll, c_vp, c_vp]),
