@@ -150,11 +150,13 @@ def run_ours(args):
     barrier(dist)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")
     ev0.record()
     energies = []
     for _ in range(args.steps):
         energies.append(step())
     ev1.record()
+    torch.cuda.nvtx.range_pop()
     barrier(dist)
     ck = clocks.stop()
     LOG.enabled = False
