@@ -134,6 +134,27 @@ int qc_bgemm_tf32(const void *tasks_dev, long long ntasks, int opspan, const voi
  * (synchronous: reads a device flag), negative on a CUDA error. */
 int qc_tc_status(void);
 
+/* Fiber-group contraction for the two MPO-site contractions of HVecQt
+ * (the .W_i and .W_{i+1} tensordots, source/mpo_dmrg_kernelQt.py:301-306; a
+ * specialisation of tensordotCAL, source/tools/qtensor.py:623-660, for an
+ * operand-2 block that is a small MPO-bond x MPO-bond matrix).
+ *
+ * For every task (qc_ftask, 32 B): fibers f0 .. min(f0+32, F) of one fiber group,
+ * operators op_b .. op_e (grid.y, at most opspan).  Input blocks fin[in_b..in_e)
+ * (qc_fin, 32 B: offset, rows, storage order [rows][F] or [F][rows], first row in
+ * the staged tile) are staged once; each output block fout[out_b..out_e)
+ * (qc_fout, 32 B: offset, ncols, pair range) is written as
+ *   C[c_base + c_off + f*ncols + c] = alpha * sum_pairs sum_r in[srow+r][f] * W[b_base + w_off + r*ncols + c]
+ * with pairs fpair[pair_b..pair_e) (qc_fpair, 16 B).  max_rows >= the staged rows
+ * of every task (shared memory max_rows*32*sizeof(T), at most 200 KiB).
+ * Null A/W/C with absolute element addresses in ops is allowed. */
+int qc_fiber_f64(const void *tasks_dev, long long ntasks, int opspan, const void *fin_dev,
+                 const void *fout_dev, const void *fpair_dev, const void *ops_dev, int max_rows,
+                 const double *A, const double *W, double *C, void *stream);
+int qc_fiber_f32(const void *tasks_dev, long long ntasks, int opspan, const void *fin_dev,
+                 const void *fout_dev, const void *fpair_dev, const void *ops_dev, int max_rows,
+                 const float *A, const float *W, float *C, void *stream);
+
 /* dst[i] = src[idx[i]] (FP64), i < n.  Used for diag[prjmap] (kernelQt.py:122). */
 int qc_gather_f64(const double *src, const long long *idx, double *dst, long long n, void *stream);
 /* dst[idx[i]] = src[i] (FP64) after zeroing dst[0..ndst). */
@@ -148,6 +169,26 @@ int qc_reduce_ops_f32(const float *part, int nops, long long n, float *out, void
 /* Precision conversions used by the mixed-precision path. */
 int qc_convert_f64_to_f32(const double *src, float *dst, long long n, void *stream);
 int qc_convert_f32_to_f64(const float *src, double *dst, long long n, void *stream);
+
+/* ---------------------------------------------- learned Davidson preconditioner
+ * No counterpart in the reference; it plugs in where pdvdson applies its
+ * diagonal preconditioner (source/tools/pdvdson.py:275-278).  A 3-layer MLP
+ * (F inputs <= 32, width 256, 2 outputs) with BF16 weights [out][in] and FP32
+ * biases, activations and accumulation.  All pointers are device pointers. */
+/* Y[B,2] = MLP(X[B,F]); H1, H2 [B,256] receive the hidden activations. */
+int qc_mlp_forward(int B, int F, const float *X, const void *W1, const float *b1, const void *W2,
+                   const float *b2, const void *W3, const float *b3, float *H1, float *H2, float *Y,
+                   void *stream);
+/* Accumulates (+=) the FP32 gradients of every weight and bias for dL/dY[B,2]. */
+int qc_mlp_backward(int B, int F, const float *X, const void *W2, const void *W3, const float *H1,
+                    const float *H2, const float *dY, float *dW1, float *db1, float *dW2, float *db2,
+                    float *dW3, float *db3, void *stream);
+/* One Adam step on FP32 master weights w (n values); refreshes the BF16 copy wbf16 if non-NULL. */
+int qc_adam_step(int n, float *w, void *wbf16, const float *g, float *m, float *v, float lr, float beta1,
+                 float beta2, float eps, int step, float grad_scale, void *stream);
+/* c[i] = r[i] * exp(Y[2b]) / (|d[i] - e| + exp(Y[2b+1])), b = blk[i]  (FP64 vectors). */
+int qc_precond_apply(long long n, const double *r, const double *d, double e, const int *blk,
+                     const float *Y, double *c, void *stream);
 
 /* Sigma without any device allocation.  This entry point has no counterpart in
  * the reference; it exists for host codes that own the GPU memory budget and

@@ -1,0 +1,106 @@
+// Fiber-group kernel for the two W contractions of sigma (the .W_i and .W_{i+1}
+// stages of HVecQt, source/mpo_dmrg_kernelQt.py:301-306).
+//
+// In those contractions every output block (fiber index f = (l, r), column index
+// c from the MPO bond and a physical index) is a sum over a handful of input
+// blocks times small W blocks (MPO-sector x MPO-sector).  The generic grouped
+// GEMM reads each input block once per output block that uses it; here one CTA
+// owns a tile of FT fibers of one group, stages every input row of the group for
+// those fibers in shared memory once (coalesced along the storage order of each
+// block), then writes every output block of the group for those fibers.  HBM
+// traffic is the algorithmic one: inputs read once, outputs written once.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include "qc_types.h"
+
+namespace {
+
+constexpr int FT = 32;          // fibers per tile
+constexpr int FT_THREADS = 128;
+
+template <typename T>
+__global__ void __launch_bounds__(FT_THREADS)
+k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, const qc_fout *__restrict__ fout,
+        const qc_fpair *__restrict__ fpair, const qc_op *__restrict__ ops, const T *__restrict__ A,
+        const T *__restrict__ W, T *__restrict__ C) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *As = reinterpret_cast<T *>(smem_raw);
+  const qc_ftask t = tasks[blockIdx.x];
+  const int op = t.op_b + (int)blockIdx.y;
+  if (op >= t.op_e) return;
+  const qc_op o = ops[op];
+  const int tid = threadIdx.x;
+  const int nf = min(FT, t.F - t.f0);
+  const T *Ab = A + o.a_base;
+  for (int i = t.in_b; i < t.in_e; ++i) {
+    const qc_fin b = fin[i];
+    const T *src = Ab + b.a_off;
+    const int n = b.rows * FT;
+    if (!b.fiber_major) {             // [rows][F]: consecutive threads -> consecutive fibers
+      for (int idx = tid; idx < n; idx += FT_THREADS) {
+        const int r = idx / FT, f = idx % FT;
+        As[(b.srow + r) * FT + f] = (f < nf) ? src[(long long)r * t.F + t.f0 + f] : T(0);
+      }
+    } else {                          // [F][rows]: consecutive threads -> consecutive rows
+      for (int idx = tid; idx < n; idx += FT_THREADS) {
+        const int f = idx / b.rows, r = idx % b.rows;
+        As[(b.srow + r) * FT + f] = (f < nf) ? src[(long long)(t.f0 + f) * b.rows + r] : T(0);
+      }
+    }
+  }
+  __syncthreads();
+  const T alpha = T(o.alpha);
+  const T *Wb = W + o.b_base;
+  T *Cb = C + o.c_base;
+  for (int j = t.out_b; j < t.out_e; ++j) {
+    const qc_fout ob = fout[j];
+    const int nc = ob.ncols;
+    const int ne = nf * nc;
+    for (int e = tid; e < ne; e += FT_THREADS) {
+      const int f = e / nc, c = e % nc;
+      T acc = T(0);
+      for (int p = ob.pair_b; p < ob.pair_e; ++p) {
+        const qc_fpair pr = fpair[p];
+        const T *w = Wb + pr.w_off + c;
+        const T *a = As + pr.srow * FT + f;
+        for (int r = 0; r < pr.rows; ++r) acc = fma(a[r * FT], w[(long long)r * nc], acc);
+      }
+      Cb[ob.c_off + (long long)(t.f0 + f) * nc + c] = alpha * acc;
+    }
+  }
+}
+
+template <typename T>
+int launch_fiber(const void *tasks, long long ntasks, int opspan, const void *fin, const void *fout,
+                 const void *fpair, const void *ops, int max_rows, const T *A, const T *W, T *C,
+                 cudaStream_t s) {
+  if (ntasks <= 0) return QC_OK;
+  if (ntasks > 0x7fffffffLL || opspan < 1 || opspan > 65535 || max_rows < 1) return QC_ERR_ARG;
+  const size_t smem = (size_t)max_rows * FT * sizeof(T);
+  if (smem > 200 * 1024) return QC_ERR_ARG;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_fiber<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 grid((unsigned)ntasks, (unsigned)opspan);
+  k_fiber<T><<<grid, FT_THREADS, smem, s>>>((const qc_ftask *)tasks, (const qc_fin *)fin, (const qc_fout *)fout,
+                                            (const qc_fpair *)fpair, (const qc_op *)ops, A, W, C);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "[qcgpu] qc_fiber: %s\n", cudaGetErrorString(e));
+    return QC_ERR_CUDA;
+  }
+  return QC_OK;
+}
+
+}  // namespace
+
+extern "C" int qc_fiber_f64(const void *tasks, long long ntasks, int opspan, const void *fin, const void *fout,
+                            const void *fpair, const void *ops, int max_rows, const double *A, const double *W,
+                            double *C, void *stream) {
+  return launch_fiber<double>(tasks, ntasks, opspan, fin, fout, fpair, ops, max_rows, A, W, C, (cudaStream_t)stream);
+}
+
+extern "C" int qc_fiber_f32(const void *tasks, long long ntasks, int opspan, const void *fin, const void *fout,
+                            const void *fpair, const void *ops, int max_rows, const float *A, const float *W,
+                            float *C, void *stream) {
+  return launch_fiber<float>(tasks, ntasks, opspan, fin, fout, fpair, ops, max_rows, A, W, C, (cudaStream_t)stream);
+}

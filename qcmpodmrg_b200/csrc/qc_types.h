@@ -42,3 +42,38 @@ static_assert(sizeof(qc_op) == 32, "qc_op is 32 bytes");
 #define QC_ERR_CUDA -3
 #define QC_ERR_LAYOUT -4
 #define QC_ERR_HALFINT -5
+
+// ---- fiber-group work items (the W contractions of sigma) -------------------
+// A fiber group is a set of output blocks that share their "fiber" index
+// f = (l, r) and read the same input blocks; one task = one tile of fibers.
+struct alignas(16) qc_ftask {
+  int f0, F;           // first fiber of the tile, fibers in the group
+  int in_b, in_e;      // input blocks [in_b, in_e) of qc_fin
+  int out_b, out_e;    // output blocks [out_b, out_e) of qc_fout
+  int op_b, op_e;      // operators (grid.y indexes this range)
+};
+static_assert(sizeof(qc_ftask) == 32, "qc_ftask is 32 bytes");
+
+struct alignas(16) qc_fin {
+  long long a_off;     // input block offset (relative to the operator's A base)
+  int rows;            // extent of the contracted index
+  int fiber_major;     // 0: block stored [rows][F]; 1: stored [F][rows]
+  int srow;            // first shared-memory row
+  int pad;
+};
+static_assert(sizeof(qc_fin) == 32, "qc_fin is 32 bytes");
+
+struct alignas(16) qc_fout {
+  long long c_off;     // output block offset (relative to the operator's C base); (f, c) at c_off + f*ncols + c
+  int ncols;
+  int pair_b, pair_e;  // contributions [pair_b, pair_e) of qc_fpair
+  int pad;
+};
+static_assert(sizeof(qc_fout) == 32, "qc_fout is 32 bytes");
+
+struct alignas(16) qc_fpair {
+  long long w_off;     // W block offset (relative to the operator's B base); (a, c) at w_off + a*ncols + c
+  int srow;            // shared-memory rows of the input block
+  int rows;
+};
+static_assert(sizeof(qc_fpair) == 16, "qc_fpair is 16 bytes");

@@ -52,6 +52,20 @@ class DavidsonResult(object):
 def davidson(hvec, diag, neig=1, v0=None, crit_e=1.e-8, crit_vec=1.e-8, maxcycle=20, crit_indp=1.e-12,
              lshift=1.e-4, nfac=10, precond=None, record=None):
     """Lowest ``neig`` eigenpairs of the operator ``hvec`` (device FP64 vectors)."""
+    gen = davidson_steps(diag, neig, v0, crit_e, crit_vec, maxcycle, crit_indp, lshift, nfac, precond, record)
+    try:
+        x = next(gen)
+        while True:
+            x = gen.send(hvec(x))
+    except StopIteration as stop:
+        return stop.value
+
+
+def davidson_steps(diag, neig=1, v0=None, crit_e=1.e-8, crit_vec=1.e-8, maxcycle=20, crit_indp=1.e-12,
+                   lshift=1.e-4, nfac=10, precond=None, record=None):
+    """The same solver as a generator: yields every vector to multiply, receives H x,
+    and returns the DavidsonResult -- so many independent solves can share one
+    batched matrix-vector launch per step."""
     ndim = diag.numel()
     if neig > ndim:
         raise ValueError("neig > ndim")
@@ -62,7 +76,10 @@ def davidson(hvec, diag, neig=1, v0=None, crit_e=1.e-8, crit_vec=1.e-8, maxcycle
         if n + 1 != neig:
             raise RuntimeError("insufficient orthonormal start basis")
         vbas[1:] = v2
-    wbas = torch.stack([hvec(v) for v in vbas])
+    ws_ = []
+    for v in vbas:
+        ws_.append((yield v))
+    wbas = torch.stack(ws_)
     nmvp = neig
     eigs = torch.full((neig,), 1.e3, dtype=torch.float64, device=diag.device)
     rnorms = []
@@ -95,16 +112,19 @@ def davidson(hvec, diag, neig=1, v0=None, crit_e=1.e-8, crit_vec=1.e-8, maxcycle
         for i in range(neig):
             if rconv[i]:
                 continue
+            if record is not None:      # raw residual, before preconditioning
+                record(rbas[i], diag, eigs[i], xbas[i])
             if precond is None:
                 rbas[i] = rbas[i] / ((diag - eigs[i]).abs() + lshift)
             else:
                 rbas[i] = precond(rbas[i], diag, eigs[i], xbas[i])
-            if record is not None:
-                record(rbas[i], diag, eigs[i], xbas[i])
         nindp, vbas2 = _ortho(vbas, rbas[rindx, :], crit_indp)
         if nindp == 0:
             raise RuntimeError("Davidson: unable to generate a new direction")
-        wbas2 = torch.stack([hvec(v) for v in vbas2])
+        ws_ = []
+        for v in vbas2:
+            ws_.append((yield v))
+        wbas2 = torch.stack(ws_)
         nmvp += nindp
         vbas = torch.cat([vbas, vbas2])
         wbas = torch.cat([wbas, wbas2])

@@ -82,6 +82,7 @@ class DMRG(object):
         # host_api: drive the dot through the reference-facing functions with host
         # (NumPy) vectors, as the reference's pdvdson does (used for end-to-end timing)
         self.host_api = False
+        self.recorder = None      # callback(residual, diag, e, x) fed by Davidson (preconditioner training)
         self.h2d_bytes = 0
         self.d2h_bytes = 0
 
@@ -139,12 +140,22 @@ class DMRG(object):
         v0 = None
         if self.psi0 is not None:
             v0 = self.psi0[0:1].reshape(1, -1)[:, prj].contiguous()
+        learned = hasattr(self.preconditioner, "set_layout")
+        if learned:
+            self.preconditioner.set_layout(lay)
+            self.recorder = self.preconditioner.record
         t0 = time.time()
-        res = davidson(hv, diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec, precond=self.preconditioner)
+        if self.precision == "f64":
+            res = davidson(hv, diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec, precond=self.preconditioner,
+                           record=self.recorder)
+        else:
+            res = self._mixed_davidson(sig, hv, diag, v0, crit_e)
         torch.cuda.synchronize(dev)
         self.stats["hvec_s"] += time.time() - t0
         self.stats["nmvp"] += res.nmvp
         self.stats["sigma_flops"] += res.nmvp * sig.flops
+        if learned:
+            self.preconditioner.end_dot(res.vecs[0])
         civec = torch.zeros((1, dims[3]), dtype=torch.float64, device=dev)
         civec[:, prj] = res.vecs
         t0 = time.time()
@@ -152,6 +163,97 @@ class DMRG(object):
         torch.cuda.synchronize(dev)
         self.stats["decim_s"] += time.time() - t0
         return res, out, dims, sig
+
+    # ---- split dot step (used by the batched multi-instance driver)
+    def dot_begin(self, isite, crit_e):
+        """Plans, diagonal and a Davidson generator for the dot; returns a context."""
+        from .davidson import davidson_steps
+        lay, idl, sig, dg = self.dot_operators(isite)
+        prj = torch.from_numpy(lay.prjmap(idl)).to(self.device)
+        diag = dg()
+        v0 = None
+        if self.psi0 is not None:
+            v0 = self.psi0[0:1].reshape(1, -1)[:, prj].contiguous()
+        gen = davidson_steps(diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec)
+        return {"isite": isite, "lay": lay, "prj": prj, "sig": sig, "gen": gen, "diag": diag}
+
+    def dot_end(self, ctx, res, status, dmax, actlst, elst, dlst):
+        isite = ctx["isite"]
+        dev = self.device
+        ldim, rdim = len(self.qnuml[isite]), len(self.qnumr[isite + 2])
+        dims = (ldim, 16, rdim, ldim * 16 * rdim)
+        self.stats["nmvp"] += res.nmvp
+        self.stats["sigma_flops"] += res.nmvp * ctx["sig"].flops
+        civec = torch.zeros((1, dims[3]), dtype=torch.float64, device=dev)
+        civec[:, ctx["prj"]] = res.vecs
+        dwts, qred, site, srotR, civecs = self.decimate(civec, isite, status, dims, dmax)
+        elst.append(float(res.eigs[0]))
+        dlst.append(float(dwts))
+        self._update(isite, status, qred, site)
+        self.guess(isite, status, actlst, civecs, srotR)
+        return qred, srotR
+
+    def _update(self, isite, status, qred, site):
+        dev = self.device
+        if status == "L":
+            self.qnuml[isite + 1] = qred
+            st = SiteTensor(site, [self.qnuml[isite], QPHYS, qred], L_STATUS, dev)
+            self.lmps[isite] = st
+            rn = Renormalizer(self.ws, isite, "L", st.layout, self.lenv[isite - 1], self.mpo[isite], self.opers)
+            self.lenv[isite] = rn(st.values)
+        else:
+            j = isite + 1
+            self.qnumr[j] = qred
+            st = SiteTensor(site, [qred, QPHYS, self.qnumr[j + 1]], R_STATUS, dev)
+            self.rmps[j] = st
+            rn = Renormalizer(self.ws, j, "R", st.layout, self.renv[j + 1], self.mpo[j], self.opers)
+            self.renv[j] = rn(st.values)
+        self.stats["renorm_flops"] += rn.flops
+
+    def boundary(self, status, qred, srotR):
+        K = self.nsite
+        dev = self.device
+        smat = srotR[0] / torch.linalg.norm(srotR[0])
+        qk = self.qkey.reshape(1, 2).copy()
+        if status == "L":
+            self.lmps[K - 1] = SiteTensor(smat, [qred, QPHYS, qk], L_STATUS, dev)
+            self.qnuml[K] = qk
+        else:
+            self.rmps[0] = SiteTensor(smat, [qk, QPHYS, qred], R_STATUS, dev)
+            self.qnumr[0] = qk
+
+    def _mixed_davidson(self, sig, hv, diag, v0, crit_e):
+        """Davidson with low-precision sigma, then FP64 refinement.
+
+        Phase 1 iterates with the FP32/TF32 sigma until the energy change is below
+        crit_e or the residual below the precision's floor.  Phase 2 applies the
+        FP64 sigma to the final vector: its Rayleigh quotient has an error of second
+        order in the vector's error, and its FP64 residual decides whether FP64
+        Davidson iterations continue from that vector (reference criteria).
+        """
+        floor = 2e-4 if self.precision == "tf32" else 2e-6
+        r1 = davidson(hv, diag, 1, v0, crit_e=crit_e, crit_vec=max(self.crit_vec, floor),
+                      precond=self.preconditioner, record=self.recorder)
+        x = r1.vecs[0] / torch.linalg.norm(r1.vecs[0])
+        y = sig(x, precision="f64")
+        e64 = float(torch.dot(x, y))
+        rn = float(torch.linalg.norm(y - e64 * x))
+        self.stats["nmvp_f64"] = self.stats.get("nmvp_f64", 0) + 1
+        self.stats["nmvp_low"] = self.stats.get("nmvp_low", 0) + r1.nmvp
+        if rn <= self.crit_vec or abs(e64 - float(r1.eigs[0])) <= crit_e:
+            r1.eigs = numpy.array([e64])
+            r1.vecs = x.reshape(1, -1)
+            r1.nmvp += 1
+            return r1
+
+        def hv64(v):
+            return sig(v, precision="f64")
+
+        r2 = davidson(hv64, diag, 1, x.reshape(1, -1), crit_e=crit_e, crit_vec=self.crit_vec,
+                      precond=self.preconditioner)
+        self.stats["nmvp_f64"] += r2.nmvp
+        r2.nmvp += r1.nmvp + 1
+        return r2
 
     def _solve_dot_host(self, isite, status, dmax, crit_e):
         """The same dot, through mpo_dmrg_kernel.HDiag/HVec with host buffers."""

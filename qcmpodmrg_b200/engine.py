@@ -253,6 +253,178 @@ def add_parts(dst, parts, op_range=None, contrib_range=None):
         dst.setdefault(cfg, []).append((tk, ct, fl * mult))
 
 
+# ---------------------------------------------------------------- fiber-group stages
+FTASK_DT = numpy.dtype([("f0", "<i4"), ("F", "<i4"), ("in_b", "<i4"), ("in_e", "<i4"), ("out_b", "<i4"),
+                        ("out_e", "<i4"), ("op_b", "<i4"), ("op_e", "<i4")])
+FIN_DT = numpy.dtype([("a_off", "<i8"), ("rows", "<i4"), ("fiber_major", "<i4"), ("srow", "<i4"), ("pad", "<i4"),
+                      ("pad2", "<i8")])
+FOUT_DT = numpy.dtype([("c_off", "<i8"), ("ncols", "<i4"), ("pair_b", "<i4"), ("pair_e", "<i4"), ("pad", "<i4"),
+                       ("pad2", "<i8")])
+FPAIR_DT = numpy.dtype([("w_off", "<i8"), ("srow", "<i4"), ("rows", "<i4")])
+assert FTASK_DT.itemsize == 32 and FIN_DT.itemsize == 32 and FOUT_DT.itemsize == 32 and FPAIR_DT.itemsize == 16
+FIBER_TILE = 32
+FIBER_MAX_ROWS = 256
+
+
+def compile_fiber(c, triples, rows_axis, fiber_major):
+    """Fiber-group work items of a W contraction (template for one operator).
+
+    The first three output axes form the fiber group (their block dims multiply
+    to the fiber count F), the last two the column block.  Returns None when a
+    group needs more than FIBER_MAX_ROWS staged rows.
+    """
+    if len(triples) == 0:
+        return (numpy.zeros(0, FTASK_DT), numpy.zeros(0, FIN_DT), numpy.zeros(0, FOUT_DT),
+                numpy.zeros(0, FPAIR_DT), 1, 0.0)
+    out, l1, l2 = c.out, c.l1, c.l2
+    ob, i1, i2 = triples[:, 0], triples[:, 1], triples[:, 2]
+    ns = out.nsyms.astype(numpy.int64)
+    gkey = ob // (ns[3] * ns[4])
+    dO = out.block_dims(ob)
+    F = dO[:, 0] * dO[:, 1] * dO[:, 2]
+    ncols = dO[:, 3] * dO[:, 4]
+    rows = l1.block_dims(i1)[:, rows_axis]
+    bounds = numpy.flatnonzero(numpy.r_[True, gkey[1:] != gkey[:-1], True])
+    tasks, fins, fouts, pairs = [], [], [], []
+    nin = nout = npair = 0
+    max_rows = 1
+    flops = 0.0
+    for gi in range(len(bounds) - 1):
+        a, b = bounds[gi], bounds[gi + 1]
+        u1, first1, inv1 = numpy.unique(i1[a:b], return_index=True, return_inverse=True)
+        r1 = rows[a:b][first1]
+        srow = numpy.concatenate([[0], numpy.cumsum(r1)[:-1]])
+        R = int(r1.sum())
+        if R > FIBER_MAX_ROWS:
+            return None
+        max_rows = max(max_rows, R)
+        fi = numpy.zeros(len(u1), FIN_DT)
+        fi["a_off"] = l1.ioff[u1]
+        fi["rows"] = r1
+        fi["fiber_major"] = fiber_major
+        fi["srow"] = srow
+        uo, firsto = numpy.unique(ob[a:b], return_index=True)
+        # triples of a group are ordered by output block: pair ranges are contiguous
+        ends = numpy.r_[firsto[1:], b - a]
+        fo = numpy.zeros(len(uo), FOUT_DT)
+        fo["c_off"] = out.ioff[uo]
+        fo["ncols"] = ncols[a:b][firsto]
+        fo["pair_b"] = npair + firsto
+        fo["pair_e"] = npair + ends
+        fp = numpy.zeros(b - a, FPAIR_DT)
+        fp["w_off"] = l2.ioff[i2[a:b]]
+        fp["srow"] = srow[inv1.ravel()]
+        fp["rows"] = rows[a:b]
+        Fg = int(F[a])
+        nt = (Fg + FIBER_TILE - 1) // FIBER_TILE
+        tk = numpy.zeros(nt, FTASK_DT)
+        tk["f0"] = numpy.arange(nt) * FIBER_TILE
+        tk["F"] = Fg
+        tk["in_b"], tk["in_e"] = nin, nin + len(u1)
+        tk["out_b"], tk["out_e"] = nout, nout + len(uo)
+        tasks.append(tk)
+        fins.append(fi)
+        fouts.append(fo)
+        pairs.append(fp)
+        nin += len(u1)
+        nout += len(uo)
+        npair += b - a
+        flops += 2.0 * float((F[a:b] * ncols[a:b] * rows[a:b]).sum())
+    return (numpy.concatenate(tasks), numpy.concatenate(fins), numpy.concatenate(fouts), numpy.concatenate(pairs),
+            max_rows, flops)
+
+
+class FiberStage(object):
+    """Fiber-group work items of several symmetry classes, resident on the device."""
+
+    def __init__(self, parts, device, name, ops):
+        """parts: list of (tasks, fin, fout, fpair, max_rows, flops, op_range)."""
+        tks, fis, fos, fps = [], [], [], []
+        nin = nout = npair = 0
+        self.max_rows = 1
+        self.flops = 0.0
+        for (tk, fi, fo, fp, mr, fl, rng) in parts:
+            tk = tk.copy()
+            fo = fo.copy()
+            tk["in_b"] += nin
+            tk["in_e"] += nin
+            tk["out_b"] += nout
+            tk["out_e"] += nout
+            tk["op_b"], tk["op_e"] = rng
+            fo["pair_b"] += npair
+            fo["pair_e"] += npair
+            tks.append(tk)
+            fis.append(fi)
+            fos.append(fo)
+            fps.append(fp)
+            nin += len(fi)
+            nout += len(fo)
+            npair += len(fp)
+            self.max_rows = max(self.max_rows, mr)
+            self.flops += fl * (rng[1] - rng[0])
+        cat = lambda xs, dt: numpy.concatenate(xs) if xs else numpy.zeros(0, dt)
+        self.h_tasks, self.h_fin = cat(tks, FTASK_DT), cat(fis, FIN_DT)
+        self.h_fout, self.h_fpair = cat(fos, FOUT_DT), cat(fps, FPAIR_DT)
+        self.host_ops = ops
+        up = lambda a: torch.from_numpy(a.view(numpy.uint8).copy()).to(device)
+        self.d = [up(self.h_tasks), up(self.h_fin), up(self.h_fout), up(self.h_fpair), up(ops)]
+        self.ntasks = len(self.h_tasks)
+        self.span = int(max(1, (self.h_tasks["op_e"] - self.h_tasks["op_b"]).max())) if self.ntasks else 1
+        self.name = name
+        self.bytes = 0.0
+
+    def run(self, A, B, C, kind="f64", stream=None):
+        if self.ntasks == 0:
+            return
+        lib = native.lib()
+        s = stream if stream is not None else torch.cuda.current_stream(C.device).cuda_stream
+        fn = lib.qc_fiber_f64 if kind == "f64" else lib.qc_fiber_f32
+        if LOG.enabled:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+        check(fn(self.d[0].data_ptr(), self.ntasks, self.span, self.d[1].data_ptr(), self.d[2].data_ptr(),
+                 self.d[3].data_ptr(), self.d[4].data_ptr(), self.max_rows, A.data_ptr(), B.data_ptr(),
+                 C.data_ptr(), s), "qc_fiber_" + kind)
+        LOG.launches += 1
+        if LOG.enabled:
+            e1.record()
+            LOG.records.append((self.name, e0, e1, self.flops, self.bytes * (A.element_size() / 8.0)))
+
+
+class CompositeStage(object):
+    """Sub-stages (fiber-group and generic) that together perform one contraction."""
+
+    def __init__(self, subs, name):
+        self.subs = [x for x in subs if x is not None]
+        self.name = name
+        self.flops = sum(x.flops for x in self.subs)
+        self._bytes = 0.0
+
+    @property
+    def bytes(self):
+        return self._bytes
+
+    @bytes.setter
+    def bytes(self, v):
+        self._bytes = v
+        tot = sum(x.flops for x in self.subs) or 1.0
+        for x in self.subs:
+            x.bytes = v * x.flops / tot
+
+    @property
+    def ntasks(self):
+        return sum(x.ntasks for x in self.subs)
+
+    @property
+    def host_ops(self):
+        return self.subs[0].host_ops
+
+    def run(self, A, B, C, kind="f64", stream=None):
+        for x in self.subs:
+            x.run(A, B, C, kind, stream)
+
+
 def op_table(a_base, b_base, c_base, alpha):
     n = max(numpy.size(x) for x in (a_base, b_base, c_base, alpha))
     t = numpy.zeros(n, dtype=OP_DT)

@@ -18,7 +18,8 @@ import torch
 
 from . import native
 from .native import check
-from .engine import (Stage, compile_classes, add_parts, live_blocks, prune, op_table, TASK_DT, CONTRIB_DT, LOG)
+from .engine import (Stage, compile_classes, add_parts, live_blocks, prune, op_table, TASK_DT, CONTRIB_DT, LOG,
+                     compile_fiber, FiberStage, CompositeStage)
 from .mpo import case
 from .qtensor import Contraction, flip_right, flip_horizontal
 
@@ -122,7 +123,7 @@ class SigmaOperator(object):
     """sigma = sum_p w_p R_p W_p[i+1] W_p[i] L_p psi for the dot (isite, isite+1)."""
 
     def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts, precision="f64",
-                 tensor_cores=None):
+                 tensor_cores=None, use_fiber=True):
         self.ws, self.psi, self.precision = ws, psi_layout, precision
         # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 mode
         tc = (precision == "tf32") if tensor_cores is None else tensor_cores
@@ -169,14 +170,30 @@ class SigmaOperator(object):
                 op_table(bases[1][order], Wj.offsets[order], bases[2][order], 1.0),
                 op_table(bases[2][order], R.offsets[order], slot, hp[order])]
         st = [{}, {}, {}, {}]
+        fib = [[], [], [], []]
         pos = 0
+        # W contractions: fiber-group kernel (inputs staged once per fiber tile) where
+        # every group fits in shared memory, generic grouped GEMM otherwise
+        fiber_spec = {1: (0, 0), 2: (3, 1)}      # stage -> (rows axis of operand 1, fiber-major storage)
         for key, (ops, *cs, Rl) in sorted(plans.items()):
             rng = (pos, pos + len(ops))
             pos += len(ops)
             for si, (c, t) in enumerate(cs):
+                if use_fiber and si in fiber_spec:
+                    fp = compile_fiber(c, t, *fiber_spec[si])
+                    if fp is not None:
+                        fib[si].append(fp + (rng,))
+                        continue
                 add_parts(st[si], compile_classes(c, t, ax[si], tensor_cores=tc if si in (0, 3) else False),
                           op_range=rng)
-        self.stages = [Stage(st[si], dev, "sigma%d" % (si + 1), tabs[si]) for si in range(4)]
+        self.stages = []
+        for si in range(4):
+            g = Stage(st[si], dev, "sigma%d" % (si + 1), tabs[si]) if st[si] else None
+            f = FiberStage(fib[si], dev, "sigma%d" % (si + 1), tabs[si]) if fib[si] else None
+            if f is None:
+                self.stages.append(g if g is not None else Stage({}, dev, "sigma%d" % (si + 1), tabs[si]))
+            else:
+                self.stages.append(CompositeStage([f, g], "sigma%d" % (si + 1)))
         # algorithmic bytes per stage (FP64): every operand block read once, output written once
         for si in range(4):
             tot_b = 0
@@ -199,12 +216,16 @@ class SigmaOperator(object):
     def scratch_bytes(self):
         return 8 * sum(self.tot)
 
-    def __call__(self, x, y=None):
-        """x: device tensor (ndim0,) float64 -> y = H x (float64)."""
+    def __call__(self, x, y=None, precision=None):
+        """x: device tensor (ndim0,) float64 -> y = H x (float64).
+
+        precision overrides the operator's precision for this call ("f64" runs the
+        same plan, tensor-core tiles included, on the FP64 engine)."""
         ws = self.ws
+        prec = precision or self.precision
         if y is None:
             y = torch.empty(self.ndim0, dtype=torch.float64, device=ws.device)
-        if self.precision == "f64":
+        if prec == "f64":
             T1 = ws.get("t1", self.tot[0], torch.float64)
             T2 = ws.get("t2", self.tot[1], torch.float64)
             T3 = ws.get("t3", self.tot[2], torch.float64)
@@ -216,7 +237,7 @@ class SigmaOperator(object):
             P[:self.nops * self.ndim0].zero_()
             s[3].run(T3, self.R.values, P, "f64")
             return reduce_ops(P, self.nops, self.ndim0, y)
-        kind = "tf32" if self.precision == "tf32" else "f32"
+        kind = "tf32" if prec == "tf32" else "f32"
         T1 = ws.get("t1", self.tot[0], torch.float32)
         T2 = ws.get("t2", self.tot[1], torch.float32)
         T3 = ws.get("t3", self.tot[2], torch.float32)

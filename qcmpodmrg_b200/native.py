@@ -50,6 +50,13 @@ _SIGS = {
     "qc_gather_f64": (c_int, [c_vp, c_vp, c_vp, c_ll, c_vp]),
     "qc_reduce_ops_f64": (c_int, [c_vp, c_int, c_ll, c_vp, c_vp]),
     "qc_tc_status": (c_int, []),
+    "qc_fiber_f64": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_vp]),
+    "qc_fiber_f32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_vp]),
+    "qc_mlp_forward": (c_int, [c_int, c_int] + [c_vp] * 10 + [c_vp]),
+    "qc_mlp_backward": (c_int, [c_int, c_int] + [c_vp] * 12 + [c_vp]),
+    "qc_adam_step": (c_int, [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                             ctypes.c_float, c_int, ctypes.c_float, c_vp]),
+    "qc_precond_apply": (c_int, [c_ll, c_vp, c_vp, c_dbl, c_vp, c_vp, c_vp, c_vp]),
     "qc_sigma_f64_noalloc": (c_int, [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                                      c_vp, c_vp, c_int, c_ll, c_ll, c_ll, c_ll, c_vp]),
     "qc_reduce_ops_f32": (c_int, [c_vp, c_int, c_ll, c_vp, c_vp]),

@@ -28,6 +28,17 @@ def patch_stage_run(monkeypatch):
         C.copy_(torch.from_numpy(c).to(C.dtype))
 
     monkeypatch.setattr(engine.Stage, "run", run)
+
+    def frun(self, A, B, C, kind="f64", stream=None):
+        if self.ntasks == 0:
+            return
+        a = A.detach().cpu().numpy().astype(numpy.float64)
+        w = B.detach().cpu().numpy().astype(numpy.float64)
+        c = C.detach().cpu().numpy().astype(numpy.float64)
+        _run_fiber(self, a, w, c)
+        C.copy_(torch.from_numpy(c).to(C.dtype))
+
+    monkeypatch.setattr(engine.FiberStage, "run", frun)
     from qcmpodmrg_b200 import kernels
 
     def gather(src, idx, out):
@@ -47,6 +58,32 @@ def patch_stage_run(monkeypatch):
 
     monkeypatch.setattr(kernels, "reduce_ops", reduce_ops)
     monkeypatch.setattr(kernels, "convert", convert)
+
+
+def _run_fiber(st, A, W, C):
+    """Reference semantics of k_fiber: out[f, c] = alpha * sum_pairs sum_r in[r, f] * W[r, c]."""
+    FT = 32
+    for t in st.h_tasks:
+        nf = min(FT, t["F"] - t["f0"])
+        for op in range(t["op_b"], t["op_e"]):
+            o = st.host_ops[op]
+            rows = {}
+            for fi in st.h_fin[t["in_b"]:t["in_e"]]:
+                base = o["a_base"] + fi["a_off"]
+                r = numpy.arange(fi["rows"])[:, None]
+                f = t["f0"] + numpy.arange(nf)[None, :]
+                idx = base + (f * fi["rows"] + r if fi["fiber_major"] else r * t["F"] + f)
+                rows[int(fi["srow"])] = A[idx]
+            for fo in st.h_fout[t["out_b"]:t["out_e"]]:
+                acc = numpy.zeros((nf, fo["ncols"]))
+                for p in st.h_fpair[fo["pair_b"]:fo["pair_e"]]:
+                    blk = rows[int(p["srow"])]
+                    wi = o["b_base"] + p["w_off"] + numpy.arange(p["rows"])[:, None] * fo["ncols"] + \
+                        numpy.arange(fo["ncols"])[None, :]
+                    acc += blk.T @ W[wi]
+                ci = o["c_base"] + fo["c_off"] + (t["f0"] + numpy.arange(nf))[:, None] * fo["ncols"] + \
+                    numpy.arange(fo["ncols"])[None, :]
+                C[ci] = o["alpha"] * acc
 
 
 def _run_tiled(tasks, contribs, ops, summed, A, B, C, tm, tn):

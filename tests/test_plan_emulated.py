@@ -6,6 +6,7 @@ import torch
 
 from helpers import load, record_operators, record_renormalizer
 from emulate import patch_stage_run
+from qcmpodmrg_b200.engine import CompositeStage, Stage
 
 
 @pytest.mark.parametrize("tag", ["K4", "K5", "K6"])
@@ -13,6 +14,7 @@ def test_sigma_diag_renorm_emulated(tag, monkeypatch):
     patch_stage_run(monkeypatch)
     for r in load("kernels_%s.npz" % tag)["records"]:
         sig, dg, ws = record_operators(r, "cpu")
+        assert any(isinstance(s, CompositeStage) for s in sig.stages), "fiber-group stages expected"
         x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))
         y = sig(x).numpy()
         ref = numpy.asarray(r["hvec_y"])
@@ -25,3 +27,15 @@ def test_sigma_diag_renorm_emulated(tag, monkeypatch):
             got = out.op_values(i).numpy()
             assert len(got) == len(b["value"])
             assert numpy.abs(got - b["value"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("tag", ["K5", "K6"])
+def test_sigma_generic_only_emulated(tag, monkeypatch):
+    """The grouped-GEMM work items alone (fiber-group stages disabled) give the same sigma."""
+    patch_stage_run(monkeypatch)
+    for r in load("kernels_%s.npz" % tag)["records"]:
+        sig, dg, ws = record_operators(r, "cpu", use_fiber=False)
+        assert all(isinstance(s, Stage) for s in sig.stages)
+        x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))
+        ref = numpy.asarray(r["hvec_y"])
+        assert numpy.abs(sig(x).numpy() - ref).max() <= 1e-12 * max(1.0, numpy.abs(ref).max())
