@@ -57,8 +57,8 @@ class BatchedSigma(object):
         self.offs = offs
         groups = {}
         fibers = {}
-        ops_all = [[], [], [], []]
-        nops_acc = [0, 0, 0, 0]
+        ops_all = [[], [], [], [], []]
+        nops_acc = [0, 0, 0, 0, 0]
         for i, s in enumerate(items):
             L = s.L.values if kind == "f64" else s.L.f32()
             R = s.R.values if kind == "f64" else s.R.f32()
@@ -70,7 +70,11 @@ class BatchedSigma(object):
             P = self.T[3][int(offs[i, 3]):]
             x = self.X[int(self.xoff[i]):]
             abc = [(L, x, T1), (T1, Wi, T2), (T2, Wj, T3), (T3, R, P)]
-            for si, st in enumerate(s.stages):
+            stages = list(s.stages)
+            if s.fused is not None:         # slot 4: fused W stage, T1 -> T3
+                abc.append((T1, s.Wij if kind == "f64" else s.wij32(), T3))
+                stages.append(s.fused)
+            for si, st in enumerate(stages):
                 ops = _abs_ops(st.host_ops, *abc[si])
                 base = nops_acc[si]
                 nops_acc[si] += len(ops)
@@ -85,7 +89,8 @@ class BatchedSigma(object):
                         tk["op_b"] += base
                         tk["op_e"] += base
                         groups.setdefault((si, cfg), []).append((tk, ct))
-        self.d_ops = [torch.from_numpy(numpy.concatenate(o).view(numpy.uint8).copy()).to(device) for o in ops_all]
+        self.d_ops = [torch.from_numpy(numpy.concatenate(o).view(numpy.uint8).copy()).to(device) if o else None
+                      for o in ops_all]
         self.launches = []
         for (si, cfg), parts in sorted(groups.items()):
             nc = 0
@@ -139,7 +144,7 @@ class BatchedSigma(object):
         s = torch.cuda.current_stream(self.device).cuda_stream
         self.T[3].zero_()
         ffn = lib.qc_fiber_f64 if self.kind == "f64" else lib.qc_fiber_f32
-        for stage in range(4):       # the four contractions in order
+        for stage in (0, 1, 2, 4, 3):       # contractions in dependency order (4: fused W stage)
             for (si, nt, span, mr, dt, dfi, dfo, dfp) in self.fiber_launches:
                 if si != stage:
                     continue

@@ -277,13 +277,18 @@ def compile_fiber(c, triples, rows_axis, fiber_major):
         return (numpy.zeros(0, FTASK_DT), numpy.zeros(0, FIN_DT), numpy.zeros(0, FOUT_DT),
                 numpy.zeros(0, FPAIR_DT), 1, 0.0)
     out, l1, l2 = c.out, c.l1, c.l2
-    ob, i1, i2 = triples[:, 0], triples[:, 1], triples[:, 2]
+    if out.rank != 5:
+        return None
+    srt = numpy.argsort(triples[:, 0], kind="stable")      # pairs of one output block contiguous
+    ob, i1, i2 = triples[srt, 0], triples[srt, 1], triples[srt, 2]
+    rows = l1.block_dims(i1)[:, rows_axis]
+    if not numpy.array_equal(rows, numpy.prod(l1.block_dims(i1)[:, list(c.axes[0])], axis=1)):
+        return None                  # contracted extent is not a single axis
     ns = out.nsyms.astype(numpy.int64)
     gkey = ob // (ns[3] * ns[4])
     dO = out.block_dims(ob)
     F = dO[:, 0] * dO[:, 1] * dO[:, 2]
     ncols = dO[:, 3] * dO[:, 4]
-    rows = l1.block_dims(i1)[:, rows_axis]
     bounds = numpy.flatnonzero(numpy.r_[True, gkey[1:] != gkey[:-1], True])
     tasks, fins, fouts, pairs = [], [], [], []
     nin = nout = npair = 0

@@ -119,11 +119,21 @@ def _ncols(c, triples):
     return numpy.prod(c.out.block_dims(ob)[:, ne1:], axis=1)
 
 
+def pair_flops(c, t):
+    """2*M*N*K summed over the block pairs of one contraction (one operator)."""
+    if len(t) == 0:
+        return 0.0
+    ne1 = c.l1.rank - len(c.axes[0])
+    d = c.out.block_dims(t[:, 0]).astype(numpy.float64)
+    k = c.l1.block_dims(t[:, 1])[:, c.axes[0]].astype(numpy.float64)
+    return 2.0 * float((d.prod(axis=1) * k.prod(axis=1)).sum())
+
+
 class SigmaOperator(object):
     """sigma = sum_p w_p R_p W_p[i+1] W_p[i] L_p psi for the dot (isite, isite+1)."""
 
     def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts, precision="f64",
-                 tensor_cores=None, use_fiber=True):
+                 tensor_cores=None, use_fiber=True, fuse_w=True):
         self.ws, self.psi, self.precision = ws, psi_layout, precision
         # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 mode
         tc = (precision == "tf32") if tensor_cores is None else tensor_cores
@@ -134,6 +144,8 @@ class SigmaOperator(object):
         ax = (([2], [0]), ([0, 2], [0, 3]), ([1, 3], [3, 0]), ([1, 3], [2, 0]))
         bases = [numpy.zeros(nops, dtype=numpy.int64) for _ in range(3)]
         tot = [0, 0, 0]
+        wbase = numpy.zeros(nops, dtype=numpy.int64)
+        wtot = 0
         plans = {}
         for key, ops in sorted(groups.items()):
             i0 = ops[0]
@@ -149,15 +161,33 @@ class SigmaOperator(object):
             t2 = prune(c2.triples, live1=live_blocks(c1.out, t1))
             c3 = Contraction(c2.out, W2, ax[2])
             t3 = prune(c3.triples, live1=live_blocks(c2.out, t2))
+            # .W_i and .W_{i+1} fused: T3 = T1 . (W_i W_{i+1}) with the two-site MPO
+            # block Wij[a, n1', n1, c, n2', n2] = sum_b W_i[a, b, n1', n1] W_{i+1}[b, c, n2', n2]
+            # made once per dot, so T2 is never written (fiber-group kernel only)
+            fused = None
+            if use_fiber and fuse_w:
+                cW = Contraction(W1, W2, ([1], [0]))
+                cF = Contraction(c1.out, cW.out, ([0, 2, 3], [0, 2, 5]))
+                if cF.out is c3.out:
+                    tF = prune(cF.triples, live1=live_blocks(c1.out, t1), live2=live_blocks(cW.out, cW.triples))
+                    fp = compile_fiber(cF, tF, 0, 0)
+                    if fp is not None:
+                        fused = (cW, cF, tF, fp)
             c4 = Contraction(c3.out, Rl, ax[3])
-            t4 = prune(c4.triples, live1=live_blocks(c3.out, t3))
+            t4 = prune(c4.triples, live1=live_blocks(c3.out, fused[2] if fused else t3))
             if c4.out is not psi_layout:
                 raise ValueError("sigma output layout differs from the wavefunction template")
-            plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3), (c4, t4), Rl)
+            plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3), (c4, t4), Rl, fused)
             for s, c in enumerate((c1, c2, c3)):
+                if s == 1 and fused is not None:
+                    continue            # no T2 for fused classes
                 for i in ops:
                     bases[s][i] = tot[s]
                     tot[s] += c.out.size
+            if fused is not None:
+                for i in ops:
+                    wbase[i] = wtot
+                    wtot += fused[0].out.size
         self.tot = tot
         self.nops = nops
         hp = numpy.asarray(hpwts, dtype=numpy.float64)
@@ -171,14 +201,21 @@ class SigmaOperator(object):
                 op_table(bases[2][order], R.offsets[order], slot, hp[order])]
         st = [{}, {}, {}, {}]
         fib = [[], [], [], []]
+        fuse_parts, wij_parts = [], {}
         pos = 0
         # W contractions: fiber-group kernel (inputs staged once per fiber tile) where
         # every group fits in shared memory, generic grouped GEMM otherwise
         fiber_spec = {1: (0, 0), 2: (3, 1)}      # stage -> (rows axis of operand 1, fiber-major storage)
-        for key, (ops, *cs, Rl) in sorted(plans.items()):
+        for key, (ops, *cs, Rl, fused) in sorted(plans.items()):
             rng = (pos, pos + len(ops))
             pos += len(ops)
+            if fused is not None:
+                cW, cF, tF, fp = fused
+                fuse_parts.append(fp + (rng,))
+                add_parts(wij_parts, compile_classes(cW, cW.triples, ([1], [0])), op_range=rng)
             for si, (c, t) in enumerate(cs):
+                if fused is not None and si in (1, 2):
+                    continue
                 if use_fiber and si in fiber_spec:
                     fp = compile_fiber(c, t, *fiber_spec[si])
                     if fp is not None:
@@ -194,24 +231,54 @@ class SigmaOperator(object):
                 self.stages.append(g if g is not None else Stage({}, dev, "sigma%d" % (si + 1), tabs[si]))
             else:
                 self.stages.append(CompositeStage([f, g], "sigma%d" % (si + 1)))
+        # fused W stage (T1 -> T3) and the per-dot two-site MPO blocks it reads
+        self.fused = None
+        self.wtot = wtot
+        if fuse_parts:
+            ftab = op_table(bases[0][order], wbase[order], bases[2][order], 1.0)
+            self.fused = FiberStage(fuse_parts, dev, "sigma23", ftab)
+            wst = Stage(wij_parts, dev, "wij", op_table(Wi.offsets[order], Wj.offsets[order], wbase[order], 1.0))
+            self.Wij = torch.zeros(max(wtot, 1), dtype=torch.float64, device=dev)
+            wst.run(Wi.values, Wj.values, self.Wij, "f64")
+            self._Wij32 = None
         # algorithmic bytes per stage (FP64): every operand block read once, output written once
+        def stage_bytes(c, t, nop, shared2):
+            if len(t) == 0:
+                return 0
+            u1 = numpy.unique(t[:, 1])
+            u2 = numpy.unique(t[:, 2])
+            uo = numpy.unique(t[:, 0])
+            b1 = c.l1.ndim[u1].sum() * nop
+            b2 = c.l2.ndim[u2].sum() * (1 if shared2 else nop)
+            bo = c.out.ndim[uo].sum() * nop
+            return 8 * (b1 + b2 + bo)
+
+        fb = 0
         for si in range(4):
             tot_b = 0
-            for key, (ops, *cs, Rl) in sorted(plans.items()):
-                c, t = cs[si]
-                if len(t) == 0:
+            for key, (ops, *cs, Rl, fused) in sorted(plans.items()):
+                if fused is not None and si in (1, 2):
                     continue
-                u1 = numpy.unique(t[:, 1])
-                u2 = numpy.unique(t[:, 2])
-                uo = numpy.unique(t[:, 0])
-                shared2 = (si == 0)     # psi is read by every operator
-                b1 = c.l1.ndim[u1].sum() * len(ops)
-                b2 = c.l2.ndim[u2].sum() * (1 if shared2 else len(ops))
-                bo = c.out.ndim[uo].sum() * len(ops)
-                tot_b += 8 * (b1 + b2 + bo)
+                c, t = cs[si]
+                tot_b += stage_bytes(c, t, len(ops), si == 0)      # psi is read by every operator
             self.stages[si].bytes = float(tot_b)
-        self.flops = sum(s.flops for s in self.stages)
+        for key, (ops, *cs, Rl, fused) in sorted(plans.items()):
+            if fused is not None:
+                fb += stage_bytes(fused[1], fused[2], len(ops), False)
+        if self.fused is not None:
+            self.fused.bytes = float(fb)
+        # FLOPs of the reference's four-contraction chain (tensordotCAL pair GEMMs),
+        # whatever the fusion used here
+        self.flops = 0.0
+        for key, (ops, *cs, Rl, fused) in sorted(plans.items()):
+            for (c, t) in cs:
+                self.flops += pair_flops(c, t) * len(ops)
         self.ndim0 = psi_layout.size
+
+    def wij32(self):
+        if self._Wij32 is None:
+            self._Wij32 = self.Wij.to(torch.float32)
+        return self._Wij32
 
     def scratch_bytes(self):
         return 8 * sum(self.tot)
@@ -234,6 +301,8 @@ class SigmaOperator(object):
             s[0].run(self.L.values, x, T1, "f64")
             s[1].run(T1, self.Wi.values, T2, "f64")
             s[2].run(T2, self.Wj.values, T3, "f64")
+            if self.fused is not None:
+                self.fused.run(T1, self.Wij, T3, "f64")
             P[:self.nops * self.ndim0].zero_()
             s[3].run(T3, self.R.values, P, "f64")
             return reduce_ops(P, self.nops, self.ndim0, y)
@@ -249,6 +318,8 @@ class SigmaOperator(object):
         s[0].run(self.L.f32(), x32, T1, kind)
         s[1].run(T1, self.Wi.f32(), T2, "f32")
         s[2].run(T2, self.Wj.f32(), T3, "f32")
+        if self.fused is not None:
+            self.fused.run(T1, self.wij32(), T3, "f32")
         P[:self.nops * self.ndim0].zero_()
         s[3].run(T3, self.R.f32(), P, kind)
         reduce_ops(P, self.nops, self.ndim0, y32)
@@ -443,6 +514,8 @@ class Renormalizer(object):
             ax = (([2], [1]), ([1, 2], [2, 1]), ([1, 3], [1, 2]))
         bases = [numpy.zeros(nops, dtype=numpy.int64) for _ in range(3)]
         tot = [0, 0, 0]
+        wbase = numpy.zeros(nops, dtype=numpy.int64)
+        wtot = 0
         plans = {}
         out_layouts = [None] * nops
         for key, ops in sorted(groups.items()):

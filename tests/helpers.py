@@ -25,7 +25,7 @@ def tensorset(dicts, device):
                                                       for d in dicts], device=device)
 
 
-def record_operators(r, device, precision="f64", use_fiber=True):
+def record_operators(r, device, precision="f64", use_fiber=True, fuse_w=True):
     """SigmaOperator / DiagOperator for a recorded reference dot."""
     from qcmpodmrg_b200.kernels import SigmaOperator, DiagOperator, Workspace
     import torch
@@ -37,7 +37,8 @@ def record_operators(r, device, precision="f64", use_fiber=True):
     opers = [int(x) for x in numpy.atleast_1d(r["opers"])]
     hp = numpy.atleast_1d(r["hpwts"]).astype(numpy.float64)
     qkey = numpy.asarray(r["qkey"], dtype=numpy.float64)
-    sig = SigmaOperator(ws, isite, psi, L, R, Wi, Wj, qkey, opers, hp, precision, use_fiber=use_fiber)
+    sig = SigmaOperator(ws, isite, psi, L, R, Wi, Wj, qkey, opers, hp, precision, use_fiber=use_fiber,
+                        fuse_w=fuse_w)
     dg = DiagOperator(ws, isite, psi, L, R, Wi, Wj, qkey, opers, hp)
     return sig, dg, ws
 

@@ -18,20 +18,20 @@ TOL_F32 = 2e-5       # relative 2-norm: FP32 operands and accumulation
 def test_fiber_sigma_f64_matches_reference_and_generic(tag, cuda):
     gen = torch.Generator(device="cpu").manual_seed(3)
     for r in load("kernels_%s.npz" % tag)["records"]:
-        sig, _, _ = record_operators(r, cuda)
-        subs = [x for s in sig.stages if isinstance(s, CompositeStage) for x in s.subs]
-        assert any(isinstance(x, FiberStage) for x in subs)
         ref_sig, _, _ = record_operators(r, cuda, use_fiber=False)
-        x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64)).to(cuda)
-        y = sig(x).cpu().numpy()
-        ref = numpy.asarray(r["hvec_y"])
-        scale = max(1.0, numpy.abs(ref).max())
-        assert numpy.abs(y - ref).max() <= TOL_F64 * scale
-        assert numpy.array_equal(y, sig(x).cpu().numpy()), "bitwise reproducible"
-        xr = torch.randn(sig.ndim0, dtype=torch.float64, generator=gen).to(cuda)
-        a = sig(xr).cpu().numpy()
+        xr = torch.randn(ref_sig.ndim0, dtype=torch.float64, generator=gen).to(cuda)
         b = ref_sig(xr).cpu().numpy()
-        assert numpy.abs(a - b).max() <= TOL_F64 * max(1.0, numpy.abs(b).max())
+        for fuse in (True, False):
+            sig, _, _ = record_operators(r, cuda, fuse_w=fuse)
+            subs = [x for s in sig.stages if isinstance(s, CompositeStage) for x in s.subs]
+            assert sig.fused is not None or any(isinstance(x, FiberStage) for x in subs)
+            x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64)).to(cuda)
+            y = sig(x).cpu().numpy()
+            ref = numpy.asarray(r["hvec_y"])
+            assert numpy.abs(y - ref).max() <= TOL_F64 * max(1.0, numpy.abs(ref).max())
+            assert numpy.array_equal(y, sig(x).cpu().numpy()), "bitwise reproducible"
+            a = sig(xr).cpu().numpy()
+            assert numpy.abs(a - b).max() <= TOL_F64 * max(1.0, numpy.abs(b).max())
 
 
 @pytest.mark.parametrize("tag", ["K5", "K6"])
