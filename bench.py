@@ -166,7 +166,7 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     ms_per_step = ms / args.steps
-    stats = {k: d.stats[k] - s0[k] for k in d.stats}
+    stats = {k: d.stats[k] - s0[k] for k in d.stats if not isinstance(d.stats[k], dict)}
     # per-stage device time from the launch log
     per = {}
     for (name, e0, e1, fl, by) in LOG.records:
@@ -177,12 +177,13 @@ def run_ours(args):
         a[2] += fl
         a[3] += by
     sig_ms = sum(v[1] for k, v in per.items() if k.startswith("sigma"))
-    sig_fl = sum(v[2] for k, v in per.items() if k.startswith("sigma"))
+    sig_fl = stats["sigma_flops"]     # the reference chain's algorithmic FLOPs, whatever the fusion
     top = max(per.items(), key=lambda kv: kv[1][1])
     pk, src = peaks()
     n_l, t_l, f_l, b_l = top[1]
     gbs = b_l / (t_l / 1e3) / 1e9
-    roof = {"kernel": "qc_bgemm (%s)" % top[0], "bound": "hbm", "achieved": round(gbs, 1),
+    kname = "k_fiber" if top[0] == "sigma23" else "k_bgemm"
+    roof = {"kernel": "%s (%s)" % (kname, top[0]), "bound": "hbm", "achieved": round(gbs, 1),
             "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(gbs / pk["hbm_gbs"], 4),
             "peak_source": src, "traffic": None, "launches": n_l,
             "achieved_tflops": round(f_l / (t_l / 1e3) / 1e12, 3)}
@@ -203,6 +204,9 @@ def run_ours(args):
         "matvecs_per_step": stats["nmvp"] / args.steps,
         "stage_ms_per_step": {k: round(v[1] / args.steps, 1) for k, v in sorted(per.items())},
         "roofline": roof, "clocks": ck, "gpu_launches": LOG.launches,
+        "w_contraction_paths": d.stats.get("w_paths"),
+        "phase_s_per_step": {k: round(stats[k] / args.steps, 2) for k in ("plan_s", "hvec_s", "hdiag_s", "renorm_s",
+                                                                         "decim_s") if k in stats},
     }
     if args.e2e:
         line["e2e"] = e2e_leg(d, args)

@@ -71,6 +71,8 @@ class DMRG(object):
         self.thresh = -1.e-14
         self.ifguess = True
         self.ws = Workspace(self.device)
+        self.plan_cache = {}          # oldest first
+        self.plan_cache_size = 2 * self.nsite
         t0 = time.time()
         mpo = build_mpo(ham)
         self.mpo = {i: TensorSet(l, v, device=self.device) for i, (l, v) in mpo.items()}
@@ -111,8 +113,28 @@ class DMRG(object):
         idl = [c[2] for c in cls]
         L, R = self.lenv[isite - 1], self.renv[isite + 2]
         Wi, Wj = self.mpo[isite], self.mpo[isite + 1]
+        # compiled plans depend only on block layouts (interned by content): a dot whose
+        # wavefunction and environment sectors are unchanged reuses them
+        key = (isite, id(lay), tuple(id(x) for x in L.layouts), tuple(id(x) for x in R.layouts))
+        for (_, s_, d_) in self.plan_cache.values():     # cached plans keep no environment alive
+            s_.release()
+            d_.release()
+        hit = self.plan_cache.get(key)
+        if hit is not None and hit[0] is lay:
+            sig, dg = hit[1], hit[2]
+            sig.rebind(L, R)
+            dg.rebind(L, R)
+            self.stats["plan_hits"] = self.stats.get("plan_hits", 0) + 1
+            return lay, idl, sig, dg
         sig = SigmaOperator(self.ws, isite, lay, L, R, Wi, Wj, self.qkey, self.opers, self.hpwts, self.precision)
+        wp = self.stats.setdefault("w_paths", {})
+        for k, v in sig.w_paths.items():
+            wp[k] = wp.get(k, 0) + v
         dg = DiagOperator(self.ws, isite, lay, L, R, Wi, Wj, self.qkey, self.opers, self.hpwts)
+        self.plan_cache[key] = (lay, sig, dg)
+        while len(self.plan_cache) > self.plan_cache_size:
+            self.plan_cache.pop(next(iter(self.plan_cache)))
+        self.stats["plan_misses"] = self.stats.get("plan_misses", 0) + 1
         return lay, idl, sig, dg
 
     def solve_dot(self, isite, status, dmax, crit_e):

@@ -138,6 +138,7 @@ class SigmaOperator(object):
         # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 mode
         tc = (precision == "tf32") if tensor_cores is None else tensor_cores
         self.L, self.R, self.Wi, self.Wj = L, R, Wi, Wj
+        self._lay_ids = ([id(x) for x in L.layouts], [id(x) for x in R.layouts])
         dev = ws.device
         groups = _groups(opers, isite, 2)
         nops = len(opers)
@@ -202,6 +203,8 @@ class SigmaOperator(object):
         st = [{}, {}, {}, {}]
         fib = [[], [], [], []]
         fuse_parts, wij_parts = [], {}
+        # how the W contractions of each symmetry class run: fused / fiber / grouped GEMM
+        self.w_paths = {"fused": 0, "fiber": 0, "generic": 0}
         pos = 0
         # W contractions: fiber-group kernel (inputs staged once per fiber tile) where
         # every group fits in shared memory, generic grouped GEMM otherwise
@@ -212,6 +215,7 @@ class SigmaOperator(object):
             if fused is not None:
                 cW, cF, tF, fp = fused
                 fuse_parts.append(fp + (rng,))
+                self.w_paths["fused"] += 1
                 add_parts(wij_parts, compile_classes(cW, cW.triples, ([1], [0])), op_range=rng)
             for si, (c, t) in enumerate(cs):
                 if fused is not None and si in (1, 2):
@@ -220,7 +224,10 @@ class SigmaOperator(object):
                     fp = compile_fiber(c, t, *fiber_spec[si])
                     if fp is not None:
                         fib[si].append(fp + (rng,))
+                        self.w_paths["fiber"] += 1
                         continue
+                if si in fiber_spec:
+                    self.w_paths["generic"] += 1
                 add_parts(st[si], compile_classes(c, t, ax[si], tensor_cores=tc if si in (0, 3) else False),
                           op_range=rng)
         self.stages = []
@@ -274,6 +281,16 @@ class SigmaOperator(object):
             for (c, t) in cs:
                 self.flops += pair_flops(c, t) * len(ops)
         self.ndim0 = psi_layout.size
+
+    def rebind(self, L, R):
+        """Use new environment values with the same block layouts (cached plan)."""
+        if [id(x) for x in L.layouts] != self._lay_ids[0] or [id(x) for x in R.layouts] != self._lay_ids[1]:
+            raise ValueError("rebind: environment layouts differ from the compiled plan")
+        self.L, self.R = L, R
+
+    def release(self):
+        """Drop the references to the environment values (the plan stays valid)."""
+        self.L = self.R = None
 
     def wij32(self):
         if self._Wij32 is None:
@@ -476,6 +493,15 @@ class DiagOperator(object):
         self.nT = nops * 16 * Ac * ldim
         self.nD = 16 * ldim * rdim
         self.flops = self.sX.flops + self.sT.flops + self.sD.flops
+
+    def rebind(self, L, R):
+        """Use new environment values with the same block layouts (cached plan)."""
+        sub = {"ld": L, "rd": R}
+        self.maps = [(src, dst, n, name, sub[name] if name in sub else tset)
+                     for (src, dst, n, name, tset) in self.maps]
+
+    def release(self):
+        self.rebind(None, None)
 
     def __call__(self):
         ws = self.ws

@@ -21,3 +21,5 @@ def test_sweeps_emulated(tag, monkeypatch):
     out = d.run(fx["init_mps"], int(fx["D"]), int(fx["nsweeps"]))
     assert numpy.abs(out["eav"] - fx["eav"]).max() <= 1e-8
     assert numpy.abs(out["dwt"] - fx["dwt"]).max() <= 1e-10
+    # later sweeps revisit dots with unchanged sectors: their compiled plans are reused
+    assert d.stats.get("plan_hits", 0) > 0
