@@ -143,11 +143,23 @@ int qc_tc_status(void);
  * operators op_b .. op_e (grid.y, at most opspan).  Input blocks fin[in_b..in_e)
  * (qc_fin, 32 B: offset, rows, storage order [rows][F] or [F][rows], first row in
  * the staged tile) are staged once; each output block fout[out_b..out_e)
- * (qc_fout, 32 B: offset, ncols, pair range) is written as
- *   C[c_base + c_off + f*ncols + c] = alpha * sum_pairs sum_r in[srow+r][f] * W[b_base + w_off + r*ncols + c]
+ * (qc_fout, 32 B: offset, fiber strides fhs/flo, ncols, pair range) is written as
+ *   C[c_base + c_off + (f/flo)*fhs + (f%flo)*ncols + c]
+ *       = alpha * sum_pairs sum_r in[srow+r][f] * W[b_base + w_off + r*ncols + c]
+ * (an empty pair range writes zeros)
  * with pairs fpair[pair_b..pair_e) (qc_fpair, 16 B).  max_rows >= the staged rows
  * of every task (shared memory max_rows*32*sizeof(T), at most 200 KiB).
  * Null A/W/C with absolute element addresses in ops is allowed. */
+/* Per-dot operand repack: for every descriptor (qc_bperm, 64 B) and operator
+ * o in [op_b, op_e) (grid.y, at most opspan), copies the block stored row-major
+ * [d0][d1][d2] at src + ops[o].a_base + src_off to
+ * dst + ops[o].c_base + dst_off + i0*s0 + i1*s1 + i2*s2, converting to FP32 when
+ * dst_f32 != 0.  Used to lay environments out as the contiguous GEMM panels of
+ * the sigma contractions (a permutation of the blocks of the reference's packed
+ * qtensor.value, source/tools/qtensor.py:272-346). */
+int qc_block_permute(const void *descs_dev, long long ndescs, int opspan, const void *ops_dev,
+                     const double *src, void *dst, int dst_f32, void *stream);
+
 int qc_fiber_f64(const void *tasks_dev, long long ntasks, int opspan, const void *fin_dev,
                  const void *fout_dev, const void *fpair_dev, const void *ops_dev, int max_rows,
                  const double *A, const double *W, double *C, void *stream);

@@ -65,8 +65,30 @@ k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, cons
         const T *a = As + pr.srow * FT + f;
         for (int r = 0; r < pr.rows; ++r) acc = fma(a[r * FT], w[(long long)r * nc], acc);
       }
-      Cb[ob.c_off + (long long)(t.f0 + f) * nc + c] = alpha * acc;
+      const int fg = t.f0 + f;
+      Cb[ob.c_off + (long long)(fg / ob.flo) * ob.fhs + (long long)(fg % ob.flo) * nc + c] = alpha * acc;
     }
+  }
+}
+
+// dst[dst_off + i0*s0 + i1*s1 + i2*s2] = src[src_off + (i0*d1 + i1)*d2 + i2] for every
+// block (blockIdx.x, grid-stride over its elements) and operator (blockIdx.y).
+template <typename TD>
+__global__ void __launch_bounds__(256)
+k_block_permute(const qc_bperm *__restrict__ descs, const qc_op *__restrict__ ops, const double *__restrict__ src,
+                TD *__restrict__ dst) {
+  const qc_bperm d = descs[blockIdx.x];
+  const int op = d.op_b + (int)blockIdx.y;
+  if (op >= d.op_e) return;
+  const qc_op o = ops[op];
+  const double *s = src + o.a_base + d.src_off;
+  TD *t = dst + o.c_base + d.dst_off;
+  const long long n = (long long)d.d0 * d.d1 * d.d2;
+  const int d12 = d.d1 * d.d2;
+  for (long long e = threadIdx.x; e < n; e += blockDim.x) {
+    const int i0 = (int)(e / d12), rem = (int)(e % d12);
+    const int i1 = rem / d.d2, i2 = rem % d.d2;
+    t[(long long)i0 * d.s0 + (long long)i1 * d.s1 + (long long)i2 * d.s2] = (TD)s[e];
   }
 }
 
@@ -92,6 +114,24 @@ int launch_fiber(const void *tasks, long long ntasks, int opspan, const void *fi
 }
 
 }  // namespace
+
+extern "C" int qc_block_permute(const void *descs, long long ndescs, int opspan, const void *ops, const double *src,
+                                void *dst, int dst_f32, void *stream) {
+  if (ndescs <= 0) return QC_OK;
+  if (ndescs > 0x7fffffffLL || opspan < 1 || opspan > 65535) return QC_ERR_ARG;
+  dim3 grid((unsigned)ndescs, (unsigned)opspan);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dst_f32)
+    k_block_permute<float><<<grid, 256, 0, s>>>((const qc_bperm *)descs, (const qc_op *)ops, src, (float *)dst);
+  else
+    k_block_permute<double><<<grid, 256, 0, s>>>((const qc_bperm *)descs, (const qc_op *)ops, src, (double *)dst);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "[qcgpu] qc_block_permute: %s\n", cudaGetErrorString(e));
+    return QC_ERR_CUDA;
+  }
+  return QC_OK;
+}
 
 extern "C" int qc_fiber_f64(const void *tasks, long long ntasks, int opspan, const void *fin, const void *fout,
                             const void *fpair, const void *ops, int max_rows, const double *A, const double *W,

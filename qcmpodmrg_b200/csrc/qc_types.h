@@ -64,10 +64,11 @@ struct alignas(16) qc_fin {
 static_assert(sizeof(qc_fin) == 32, "qc_fin is 32 bytes");
 
 struct alignas(16) qc_fout {
-  long long c_off;     // output block offset (relative to the operator's C base); (f, c) at c_off + f*ncols + c
+  long long c_off;     // output block offset (relative to the operator's C base)
+  long long fhs;       // (f, c) at c_off + (f / flo)*fhs + (f % flo)*ncols + c
   int ncols;
-  int pair_b, pair_e;  // contributions [pair_b, pair_e) of qc_fpair
-  int pad;
+  int pair_b, pair_e;  // contributions [pair_b, pair_e) of qc_fpair (empty: the block is zeroed)
+  int flo;             // >= F for a block stored [F][ncols]
 };
 static_assert(sizeof(qc_fout) == 32, "qc_fout is 32 bytes");
 
@@ -77,3 +78,17 @@ struct alignas(16) qc_fpair {
   int rows;
 };
 static_assert(sizeof(qc_fpair) == 16, "qc_fpair is 16 bytes");
+
+// ---- block permute-copy (per-dot operand repacks) ---------------------------
+// Copies one rank-3 block stored row-major [d0][d1][d2] at src_off to
+// dst_off + i0*s0 + i1*s1 + i2*s2 (offsets relative to the operator's A / C base
+// of the operator table; grid.y indexes the operators [op_b, op_e)).
+struct alignas(16) qc_bperm {
+  long long src_off, dst_off;
+  int d0, d1, d2;
+  int s0, s1, s2;
+  int op_b, op_e;
+  int pad0, pad1, pad2, pad3;
+};
+static_assert(sizeof(qc_bperm) == 64, "qc_bperm is 64 bytes");
+

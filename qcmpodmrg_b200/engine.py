@@ -258,8 +258,12 @@ FTASK_DT = numpy.dtype([("f0", "<i4"), ("F", "<i4"), ("in_b", "<i4"), ("in_e", "
                         ("out_e", "<i4"), ("op_b", "<i4"), ("op_e", "<i4")])
 FIN_DT = numpy.dtype([("a_off", "<i8"), ("rows", "<i4"), ("fiber_major", "<i4"), ("srow", "<i4"), ("pad", "<i4"),
                       ("pad2", "<i8")])
-FOUT_DT = numpy.dtype([("c_off", "<i8"), ("ncols", "<i4"), ("pair_b", "<i4"), ("pair_e", "<i4"), ("pad", "<i4"),
-                       ("pad2", "<i8")])
+FOUT_DT = numpy.dtype([("c_off", "<i8"), ("fhs", "<i8"), ("ncols", "<i4"), ("pair_b", "<i4"), ("pair_e", "<i4"),
+                       ("flo", "<i4")])
+BPERM_DT = numpy.dtype([("src_off", "<i8"), ("dst_off", "<i8"), ("d0", "<i4"), ("d1", "<i4"), ("d2", "<i4"),
+                        ("s0", "<i4"), ("s1", "<i4"), ("s2", "<i4"), ("op_b", "<i4"), ("op_e", "<i4"),
+                        ("pad", "<i4", (4,))])
+assert BPERM_DT.itemsize == 64
 FPAIR_DT = numpy.dtype([("w_off", "<i8"), ("srow", "<i4"), ("rows", "<i4")])
 assert FTASK_DT.itemsize == 32 and FIN_DT.itemsize == 32 and FOUT_DT.itemsize == 32 and FPAIR_DT.itemsize == 16
 FIBER_TILE = 32
@@ -314,6 +318,8 @@ def compile_fiber(c, triples, rows_axis, fiber_major):
         fo = numpy.zeros(len(uo), FOUT_DT)
         fo["c_off"] = out.ioff[uo]
         fo["ncols"] = ncols[a:b][firsto]
+        fo["flo"] = int(F[a])
+        fo["fhs"] = 0
         fo["pair_b"] = npair + firsto
         fo["pair_e"] = npair + ends
         fp = numpy.zeros(b - a, FPAIR_DT)

@@ -133,7 +133,7 @@ class SigmaOperator(object):
     """sigma = sum_p w_p R_p W_p[i+1] W_p[i] L_p psi for the dot (isite, isite+1)."""
 
     def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts, precision="f64",
-                 tensor_cores=None, use_fiber=True, fuse_w=True):
+                 tensor_cores=None, use_fiber=False, fuse_w=True):
         self.ws, self.psi, self.precision = ws, psi_layout, precision
         # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 mode
         tc = (precision == "tf32") if tensor_cores is None else tensor_cores

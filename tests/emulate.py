@@ -81,8 +81,9 @@ def _run_fiber(st, A, W, C):
                     wi = o["b_base"] + p["w_off"] + numpy.arange(p["rows"])[:, None] * fo["ncols"] + \
                         numpy.arange(fo["ncols"])[None, :]
                     acc += blk.T @ W[wi]
-                ci = o["c_base"] + fo["c_off"] + (t["f0"] + numpy.arange(nf))[:, None] * fo["ncols"] + \
-                    numpy.arange(fo["ncols"])[None, :]
+                fg = t["f0"] + numpy.arange(nf)
+                ci = o["c_base"] + fo["c_off"] + ((fg // fo["flo"]) * fo["fhs"] + (fg % fo["flo"]) * fo["ncols"])[:, None] \
+                    + numpy.arange(fo["ncols"])[None, :]
                 C[ci] = o["alpha"] * acc
 
 

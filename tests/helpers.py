@@ -25,7 +25,7 @@ def tensorset(dicts, device):
                                                       for d in dicts], device=device)
 
 
-def record_operators(r, device, precision="f64", use_fiber=True, fuse_w=True):
+def record_operators(r, device, precision="f64", use_fiber=False, fuse_w=True):
     """SigmaOperator / DiagOperator for a recorded reference dot."""
     from qcmpodmrg_b200.kernels import SigmaOperator, DiagOperator, Workspace
     import torch

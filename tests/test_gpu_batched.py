@@ -12,7 +12,7 @@ def _instances(cuda, kind_prec="f64"):
     from qcmpodmrg_b200.synthetic import product_mps
     from qcmpodmrg_b200.dmrg import DMRG
     out = []
-    for (K, seed) in ((6, 1001), (7, 1002), (8, 1003)):
+    for (K, seed) in ((6, 1001), (8, 1002), (8, 1003)):
         ham = make_hamiltonian(K, K, seed, 3.0)
         d = DMRG(ham, device=cuda, precision=kind_prec)
         d.load_mps(product_mps(ham))

@@ -22,7 +22,7 @@ def test_fiber_sigma_f64_matches_reference_and_generic(tag, cuda):
         xr = torch.randn(ref_sig.ndim0, dtype=torch.float64, generator=gen).to(cuda)
         b = ref_sig(xr).cpu().numpy()
         for fuse in (True, False):
-            sig, _, _ = record_operators(r, cuda, fuse_w=fuse)
+            sig, _, _ = record_operators(r, cuda, use_fiber=True, fuse_w=fuse)
             subs = [x for s in sig.stages if isinstance(s, CompositeStage) for x in s.subs]
             assert sig.fused is not None or any(isinstance(x, FiberStage) for x in subs)
             x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64)).to(cuda)
@@ -37,7 +37,7 @@ def test_fiber_sigma_f64_matches_reference_and_generic(tag, cuda):
 @pytest.mark.parametrize("tag", ["K5", "K6"])
 def test_fiber_sigma_f32(tag, cuda):
     for r in load("kernels_%s.npz" % tag)["records"]:
-        sig, _, _ = record_operators(r, cuda, precision="f32")
+        sig, _, _ = record_operators(r, cuda, precision="f32", use_fiber=True)
         x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64)).to(cuda)
         y = sig(x).cpu().numpy()
         ref = numpy.asarray(r["hvec_y"])

@@ -27,7 +27,7 @@ pytestmark = pytest.mark.gpu
 
 
 C1_TOL_E = 3e-3       # unconverged run: sweep-energy spread between valid trajectories
-C1_TOL_FINAL = 2e-4   # last of the six sweeps
+C1_TOL_FINAL = 5e-4   # last of the six sweeps (observed 1e-4 .. 3e-4 across summation orders)
 C1_EXACT_DOTS = 7     # dots of the first sweep before the first truncating decimation
 
 

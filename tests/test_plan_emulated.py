@@ -14,8 +14,6 @@ def test_sigma_diag_renorm_emulated(tag, monkeypatch):
     patch_stage_run(monkeypatch)
     for r in load("kernels_%s.npz" % tag)["records"]:
         sig, dg, ws = record_operators(r, "cpu")
-        assert sig.fused is not None or any(isinstance(s, CompositeStage) for s in sig.stages), \
-            "fiber-group stages expected"
         x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))
         y = sig(x).numpy()
         ref = numpy.asarray(r["hvec_y"])
@@ -31,12 +29,12 @@ def test_sigma_diag_renorm_emulated(tag, monkeypatch):
 
 
 @pytest.mark.parametrize("tag", ["K5", "K6"])
-def test_sigma_generic_only_emulated(tag, monkeypatch):
-    """The grouped-GEMM work items alone (fiber-group stages disabled) give the same sigma."""
+def test_sigma_fiber_fused_emulated(tag, monkeypatch):
+    """Fiber-group kernel with the two MPO-site contractions fused (two-site W blocks)."""
     patch_stage_run(monkeypatch)
     for r in load("kernels_%s.npz" % tag)["records"]:
-        sig, dg, ws = record_operators(r, "cpu", use_fiber=False)
-        assert all(isinstance(s, Stage) for s in sig.stages)
+        sig, dg, ws = record_operators(r, "cpu", use_fiber=True)
+        assert sig.fused is not None
         x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))
         ref = numpy.asarray(r["hvec_y"])
         assert numpy.abs(sig(x).numpy() - ref).max() <= 1e-12 * max(1.0, numpy.abs(ref).max())
@@ -47,7 +45,8 @@ def test_sigma_fiber_unfused_emulated(tag, monkeypatch):
     """Fiber-group kernel for .W_i and .W_{i+1} as two separate stages (no two-site W)."""
     patch_stage_run(monkeypatch)
     for r in load("kernels_%s.npz" % tag)["records"]:
-        sig, dg, ws = record_operators(r, "cpu", fuse_w=False)
+        sig, dg, ws = record_operators(r, "cpu", use_fiber=True, fuse_w=False)
+        assert any(isinstance(s, CompositeStage) for s in sig.stages)
         assert sig.fused is None
         x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))
         ref = numpy.asarray(r["hvec_y"])
