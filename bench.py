@@ -125,7 +125,7 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32"}[args.precision]
     ham = make_hamiltonian(args.sites, args.sites, SEED + rank * 0, DECAY)
-    d = DMRG(ham, device=dev, precision=prec)
+    d = DMRG(ham, device=dev, precision=prec, w_path=args.w_path)
     d.load_mps(product_mps(ham))
     for D in RAMP:
         if D < args.dmax:
@@ -193,9 +193,11 @@ def run_ours(args):
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": {"f64": "f64", "f32": "f32 (sigma), f64 (Davidson, decimation)",
                   "tf32": "tf32 (sigma), f64 (Davidson, decimation)"}[prec],
-        "data": "synthetic: seeded integrals (K=24, N=24, decay 3, seed 1), product-state start, D ramp 50/100/200",
-        "config": {"workload": "two-site Qt DMRG sweep, K=24 N=24 Sz=0 D=500, 48 operators H_p", "K": args.sites,
-                   "N": args.sites, "D": args.dmax, "precision": args.precision,
+        "data": "synthetic: seeded integrals (K=%d, N=%d, decay 3, seed 1), product-state start, D ramp %s"
+                % (args.sites, args.sites, "/".join(str(x) for x in RAMP if x < args.dmax)),
+        "config": {"workload": "two-site Qt DMRG sweep, K=%d N=%d Sz=0 D=%d, %d operators H_p"
+                               % (args.sites, args.sites, args.dmax, 2 * args.sites), "K": args.sites,
+                   "N": args.sites, "D": args.dmax, "precision": args.precision, "w_path": args.w_path,
                    "l2": "inputs larger than L2: environments and sigma scratch are tens of GB per sweep",
                    "parallelism": "replicas" if world > 1 else "1 GPU"},
         "energy": energies[-1][0], "dwt": energies[-1][1],
@@ -289,6 +291,8 @@ def main():
     ap.add_argument("--dmax", type=int, default=DMAX)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--w-path", default="generic", choices=["generic", "fiber", "fused"],
+                    help="kernels of the two MPO-site contractions of sigma")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -15,9 +15,15 @@
 
 namespace {
 
-constexpr int FT = 32;          // fibers per tile
-constexpr int FT_THREADS = 128;
+constexpr int FT = 32;          // fibers per tile (one warp lane per fiber)
+constexpr int FT_THREADS = 256;
+constexpr int CB = 8;           // output columns per warp work item (register accumulators)
 
+// One CTA = one tile of FT fibers of one fiber group, for one operator (grid.y).
+// Phase 1 stages every input row of the group for those fibers in shared memory.
+// Phase 2: each warp takes (output block, 8-column block) items; lane = fiber,
+// 8 accumulators per lane, W elements are warp-uniform (broadcast) loads, so
+// every W value read serves 32 fibers and every staged input value 8 columns.
 template <typename T>
 __global__ void __launch_bounds__(FT_THREADS)
 k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, const qc_fout *__restrict__ fout,
@@ -52,21 +58,62 @@ k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, cons
   const T alpha = T(o.alpha);
   const T *Wb = W + o.b_base;
   T *Cb = C + o.c_base;
-  for (int j = t.out_b; j < t.out_e; ++j) {
+  const int lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = FT_THREADS / 32;
+  const int fg = t.f0 + lane;
+  // items: (output block j, column block cb), enumerated block by block
+  int j = t.out_b, cb = 0, skip = warp;
+  while (j < t.out_e) {
+    const int nc = fout[j].ncols;
+    const int ncb = (nc + CB - 1) / CB;
+    if (skip < ncb - cb) { cb += skip; break; }
+    skip -= ncb - cb;
+    cb = 0;
+    ++j;
+  }
+  while (j < t.out_e) {
     const qc_fout ob = fout[j];
     const int nc = ob.ncols;
-    const int ne = nf * nc;
-    for (int e = tid; e < ne; e += FT_THREADS) {
-      const int f = e / nc, c = e % nc;
-      T acc = T(0);
-      for (int p = ob.pair_b; p < ob.pair_e; ++p) {
-        const qc_fpair pr = fpair[p];
-        const T *w = Wb + pr.w_off + c;
-        const T *a = As + pr.srow * FT + f;
-        for (int r = 0; r < pr.rows; ++r) acc = fma(a[r * FT], w[(long long)r * nc], acc);
+    const int c0 = cb * CB;
+    const int nb = min(CB, nc - c0);
+    T acc[CB];
+#pragma unroll
+    for (int i = 0; i < CB; ++i) acc[i] = T(0);
+    for (int p = ob.pair_b; p < ob.pair_e; ++p) {
+      const qc_fpair pr = fpair[p];
+      const T *w = Wb + pr.w_off + c0;
+      const T *a = As + pr.srow * FT + lane;
+      if (nb == CB) {
+        for (int r = 0; r < pr.rows; ++r) {
+          const T av = a[r * FT];
+          const T *wr = w + (long long)r * nc;
+#pragma unroll
+          for (int i = 0; i < CB; ++i) acc[i] = fma(av, __ldg(wr + i), acc[i]);
+        }
+      } else {
+        for (int r = 0; r < pr.rows; ++r) {
+          const T av = a[r * FT];
+          const T *wr = w + (long long)r * nc;
+#pragma unroll
+          for (int i = 0; i < CB; ++i)
+            if (i < nb) acc[i] = fma(av, __ldg(wr + i), acc[i]);
+        }
       }
-      const int fg = t.f0 + f;
-      Cb[ob.c_off + (long long)(fg / ob.flo) * ob.fhs + (long long)(fg % ob.flo) * nc + c] = alpha * acc;
+    }
+    if (lane < nf) {
+      T *dst = Cb + ob.c_off + (long long)(fg / ob.flo) * ob.fhs + (long long)(fg % ob.flo) * nc + c0;
+#pragma unroll
+      for (int i = 0; i < CB; ++i)
+        if (i < nb) dst[i] = alpha * acc[i];
+    }
+    // advance NW items
+    int adv = NW;
+    while (j < t.out_e && adv > 0) {
+      const int ncb = (fout[j].ncols + CB - 1) / CB;
+      if (cb + adv < ncb) { cb += adv; adv = 0; break; }
+      adv -= ncb - cb;
+      cb = 0;
+      ++j;
     }
   }
 }

@@ -57,7 +57,7 @@ def boundary_set(nops, device):
 class DMRG(object):
     """Two-site MPO-DMRG with every hot-path contraction on the GPU."""
 
-    def __init__(self, ham, device="cuda", precision="f64", preconditioner=None):
+    def __init__(self, ham, device="cuda", precision="f64", preconditioner=None, w_path="generic"):
         self.ham = ham
         self.device = torch.device(device)
         self.nsite = ham.nsite
@@ -67,6 +67,10 @@ class DMRG(object):
         self.qkey = numpy.array([float(ham.nelec), 0.0])
         self.precision = precision
         self.preconditioner = preconditioner
+        # kernels of the two MPO-site contractions of sigma: "generic" grouped GEMM,
+        # "fiber" (fiber-group kernel per contraction) or "fused" (two-site W blocks)
+        self.sigma_opts = {"generic": {"use_fiber": False}, "fiber": {"use_fiber": True, "fuse_w": False},
+                           "fused": {"use_fiber": True, "fuse_w": True}}[w_path]
         self.crit_vec = 1.e-8
         self.thresh = -1.e-14
         self.ifguess = True
@@ -126,7 +130,8 @@ class DMRG(object):
             dg.rebind(L, R)
             self.stats["plan_hits"] = self.stats.get("plan_hits", 0) + 1
             return lay, idl, sig, dg
-        sig = SigmaOperator(self.ws, isite, lay, L, R, Wi, Wj, self.qkey, self.opers, self.hpwts, self.precision)
+        sig = SigmaOperator(self.ws, isite, lay, L, R, Wi, Wj, self.qkey, self.opers, self.hpwts, self.precision,
+                            **self.sigma_opts)
         wp = self.stats.setdefault("w_paths", {})
         for k, v in sig.w_paths.items():
             wp[k] = wp.get(k, 0) + v

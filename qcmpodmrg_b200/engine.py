@@ -270,79 +270,102 @@ FIBER_TILE = 32
 FIBER_MAX_ROWS = 256
 
 
-def compile_fiber(c, triples, rows_axis, fiber_major):
+def compile_fiber(c, triples, rows_axis, fiber_major, extra_out=None, in_off=None, out_off=None, out_fhs=None,
+                  out_flo=None):
     """Fiber-group work items of a W contraction (template for one operator).
 
     The first three output axes form the fiber group (their block dims multiply
     to the fiber count F), the last two the column block.  Returns None when a
-    group needs more than FIBER_MAX_ROWS staged rows.
+    group needs more than FIBER_MAX_ROWS staged rows.  Optional overrides:
+    in_off / out_off (block offsets by flat block index, instead of the packed
+    layouts' ioff), out_fhs / out_flo (two-level fiber strides of output blocks),
+    extra_out (output blocks without pairs, written as zeros).
     """
-    if len(triples) == 0:
-        return (numpy.zeros(0, FTASK_DT), numpy.zeros(0, FIN_DT), numpy.zeros(0, FOUT_DT),
-                numpy.zeros(0, FPAIR_DT), 1, 0.0)
+    empty = (numpy.zeros(0, FTASK_DT), numpy.zeros(0, FIN_DT), numpy.zeros(0, FOUT_DT), numpy.zeros(0, FPAIR_DT), 1,
+             0.0)
     out, l1, l2 = c.out, c.l1, c.l2
     if out.rank != 5:
         return None
-    srt = numpy.argsort(triples[:, 0], kind="stable")      # pairs of one output block contiguous
-    ob, i1, i2 = triples[srt, 0], triples[srt, 1], triples[srt, 2]
-    rows = l1.block_dims(i1)[:, rows_axis]
-    if not numpy.array_equal(rows, numpy.prod(l1.block_dims(i1)[:, list(c.axes[0])], axis=1)):
+    tri = numpy.asarray(triples, dtype=numpy.int64).reshape(-1, 3)
+    if extra_out is not None and len(extra_out):
+        have = numpy.zeros(out.nblks, dtype=bool)
+        have[tri[:, 0]] = True
+        extra = numpy.unique(numpy.asarray(extra_out, dtype=numpy.int64))
+        extra = extra[~have[extra]]
+    else:
+        extra = numpy.zeros(0, dtype=numpy.int64)
+    if len(tri) == 0 and len(extra) == 0:
+        return empty
+    srt = numpy.argsort(tri[:, 0], kind="stable")      # pairs of one output block contiguous
+    ob, i1, i2 = tri[srt, 0], tri[srt, 1], tri[srt, 2]
+    d1 = l1.block_dims(i1) if len(i1) else numpy.zeros((0, l1.rank), dtype=numpy.int64)
+    rows = d1[:, rows_axis]
+    if not numpy.array_equal(rows, numpy.prod(d1[:, list(c.axes[0])], axis=1)):
         return None                  # contracted extent is not a single axis
     ns = out.nsyms.astype(numpy.int64)
-    gkey = ob // (ns[3] * ns[4])
-    dO = out.block_dims(ob)
-    F = dO[:, 0] * dO[:, 1] * dO[:, 2]
-    ncols = dO[:, 3] * dO[:, 4]
-    bounds = numpy.flatnonzero(numpy.r_[True, gkey[1:] != gkey[:-1], True])
-    tasks, fins, fouts, pairs = [], [], [], []
-    nin = nout = npair = 0
-    max_rows = 1
-    flops = 0.0
-    for gi in range(len(bounds) - 1):
-        a, b = bounds[gi], bounds[gi + 1]
-        u1, first1, inv1 = numpy.unique(i1[a:b], return_index=True, return_inverse=True)
-        r1 = rows[a:b][first1]
-        srow = numpy.concatenate([[0], numpy.cumsum(r1)[:-1]])
-        R = int(r1.sum())
-        if R > FIBER_MAX_ROWS:
-            return None
-        max_rows = max(max_rows, R)
-        fi = numpy.zeros(len(u1), FIN_DT)
-        fi["a_off"] = l1.ioff[u1]
-        fi["rows"] = r1
-        fi["fiber_major"] = fiber_major
-        fi["srow"] = srow
-        uo, firsto = numpy.unique(ob[a:b], return_index=True)
-        # triples of a group are ordered by output block: pair ranges are contiguous
-        ends = numpy.r_[firsto[1:], b - a]
-        fo = numpy.zeros(len(uo), FOUT_DT)
-        fo["c_off"] = out.ioff[uo]
-        fo["ncols"] = ncols[a:b][firsto]
-        fo["flo"] = int(F[a])
-        fo["fhs"] = 0
-        fo["pair_b"] = npair + firsto
-        fo["pair_e"] = npair + ends
-        fp = numpy.zeros(b - a, FPAIR_DT)
-        fp["w_off"] = l2.ioff[i2[a:b]]
-        fp["srow"] = srow[inv1.ravel()]
-        fp["rows"] = rows[a:b]
-        Fg = int(F[a])
-        nt = (Fg + FIBER_TILE - 1) // FIBER_TILE
-        tk = numpy.zeros(nt, FTASK_DT)
-        tk["f0"] = numpy.arange(nt) * FIBER_TILE
-        tk["F"] = Fg
-        tk["in_b"], tk["in_e"] = nin, nin + len(u1)
-        tk["out_b"], tk["out_e"] = nout, nout + len(uo)
-        tasks.append(tk)
-        fins.append(fi)
-        fouts.append(fo)
-        pairs.append(fp)
-        nin += len(u1)
-        nout += len(uo)
-        npair += b - a
-        flops += 2.0 * float((F[a:b] * ncols[a:b] * rows[a:b]).sum())
-    return (numpy.concatenate(tasks), numpy.concatenate(fins), numpy.concatenate(fouts), numpy.concatenate(pairs),
-            max_rows, flops)
+    # output blocks (with pairs, plus zero-filled extras), sorted by block index
+    uo, firsto = numpy.unique(ob, return_index=True)
+    ends = numpy.r_[firsto[1:], len(ob)] if len(ob) else numpy.zeros(0, dtype=numpy.int64)
+    allo = numpy.concatenate([uo, extra])
+    pb = numpy.concatenate([firsto, numpy.zeros(len(extra), dtype=numpy.int64)])
+    pe = numpy.concatenate([ends, numpy.zeros(len(extra), dtype=numpy.int64)])
+    oo = numpy.argsort(allo, kind="stable")
+    allo, pb, pe = allo[oo], pb[oo], pe[oo]
+    dO = out.block_dims(allo)
+    Fo = dO[:, 0] * dO[:, 1] * dO[:, 2]
+    gko = allo // (ns[3] * ns[4])
+    gstart = numpy.flatnonzero(numpy.r_[True, gko[1:] != gko[:-1]])
+    ng = len(gstart)
+    gid_o = numpy.cumsum(numpy.r_[False, gko[1:] != gko[:-1]]) if len(gko) else gko
+    gout_b = gstart
+    gout_e = numpy.r_[gstart[1:], len(allo)]
+    gF = Fo[gstart]
+    # staged input blocks: unique (group, input block) in (group, block) order
+    gk_pair = ob // (ns[3] * ns[4])
+    gid_pair = numpy.searchsorted(gko[gstart], gk_pair)
+    key = gid_pair * int(l1.nblks) + i1
+    uk, first_k, inv_k = numpy.unique(key, return_index=True, return_inverse=True)
+    inv_k = inv_k.ravel()
+    u_gid = uk // int(l1.nblks)
+    u_blk = uk % int(l1.nblks)
+    u_rows = rows[first_k]
+    cs = numpy.cumsum(u_rows) - u_rows
+    gin_b = numpy.searchsorted(u_gid, numpy.arange(ng), side="left")
+    gin_e = numpy.searchsorted(u_gid, numpy.arange(ng), side="right")
+    grow0 = numpy.where(gin_b < len(cs), cs[numpy.minimum(gin_b, max(len(cs) - 1, 0))], 0) if len(cs) else \
+        numpy.zeros(ng, dtype=numpy.int64)
+    u_srow = cs - grow0[u_gid] if len(cs) else cs
+    R = numpy.zeros(ng, dtype=numpy.int64)
+    if len(u_rows):
+        numpy.add.at(R, u_gid, u_rows)
+    if len(R) and R.max() > FIBER_MAX_ROWS:
+        return None
+    fins = numpy.zeros(len(uk), FIN_DT)
+    fins["a_off"] = (l1.ioff if in_off is None else in_off)[u_blk]
+    fins["rows"] = u_rows
+    fins["fiber_major"] = fiber_major
+    fins["srow"] = u_srow
+    fouts = numpy.zeros(len(allo), FOUT_DT)
+    fouts["c_off"] = (out.ioff if out_off is None else out_off)[allo]
+    fouts["ncols"] = dO[:, 3] * dO[:, 4]
+    fouts["flo"] = Fo if out_flo is None else out_flo[allo]
+    fouts["fhs"] = 0 if out_fhs is None else out_fhs[allo]
+    fouts["pair_b"] = pb
+    fouts["pair_e"] = pe
+    pairs = numpy.zeros(len(ob), FPAIR_DT)
+    pairs["w_off"] = l2.ioff[i2]
+    pairs["srow"] = u_srow[inv_k] if len(inv_k) else 0
+    pairs["rows"] = rows
+    nt = (gF + FIBER_TILE - 1) // FIBER_TILE
+    gt = numpy.repeat(numpy.arange(ng), nt)
+    tasks = numpy.zeros(len(gt), FTASK_DT)
+    tasks["f0"] = (numpy.arange(len(gt)) - numpy.repeat(numpy.cumsum(nt) - nt, nt)) * FIBER_TILE
+    tasks["F"] = gF[gt]
+    tasks["in_b"], tasks["in_e"] = gin_b[gt], gin_e[gt]
+    tasks["out_b"], tasks["out_e"] = gout_b[gt], gout_e[gt]
+    dO_p = out.block_dims(ob) if len(ob) else numpy.zeros((0, 5), dtype=numpy.int64)
+    flops = 2.0 * float((dO_p[:, 0] * dO_p[:, 1] * dO_p[:, 2] * dO_p[:, 3] * dO_p[:, 4] * rows).sum())
+    return tasks, fins, fouts, pairs, int(max(1, R.max() if len(R) else 1)), flops
 
 
 class FiberStage(object):
