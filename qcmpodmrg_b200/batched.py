@@ -60,7 +60,7 @@ class BatchedSigma(object):
         ops_all = [[], [], [], [], []]
         nops_acc = [0, 0, 0, 0, 0]
         for i, s in enumerate(items):
-            L = s.L.values if kind == "f64" else s.L.f32()
+            L = s.a1("f64" if kind == "f64" else "f32")      # L panels of the L.psi contraction
             R = s.R.values if kind == "f64" else s.R.f32()
             Wi = s.Wi.values if kind == "f64" else s.Wi.f32()
             Wj = s.Wj.values if kind == "f64" else s.Wj.f32()

@@ -178,9 +178,9 @@ template <typename T, bool S>
 int launch_mode(const qc_task *tk, long long ntasks, int opspan, const qc_contrib *cb, const qc_op *ops,
                 const T *A, const T *B, T *C, int cfg, cudaStream_t s) {
   dim3 grid((unsigned)ntasks, S ? 1u : (unsigned)opspan);
+  // K-tile 8 where two FP64 buffers of 16 would exceed 48 KB of static shared memory
+  constexpr int KW = (sizeof(T) == 8) ? 8 : 16;
   switch (cfg) {
-    // K-tile 8 where two FP64 buffers of 16 would exceed 48 KB of static shared memory
-    constexpr int KW = (sizeof(T) == 8) ? 8 : 16;
     case 0: k_bgemm<T, 64, 64, 16, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
     case 1: k_bgemm<T, 128, 32, 16, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
     case 2: k_bgemm<T, 256, 16, KW, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;

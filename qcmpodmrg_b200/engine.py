@@ -43,7 +43,7 @@ def tile_class_tc(M, N, K):
     return numpy.where((numpy.asarray(M) > 64) & (numpy.asarray(N) > 24) & (numpy.asarray(K) >= 16), TC_CFG, base)
 
 
-def compile_classes(c, triples, axes, tensor_cores=False):
+def compile_classes(c, triples, axes, tensor_cores=False, off1=None):
     """Compile one contraction's pair list, binned by output-block shape into tile classes.
 
     Returns {tile_cfg: (tasks, contribs, flops)} for a single operator (template).
@@ -72,20 +72,129 @@ def compile_classes(c, triples, axes, tensor_cores=False):
         cls = tile_class(M, N)
     for k in numpy.unique(cls):
         sel = triples[cls == k]
-        out[int(k)] = compile_template(c.l1, c.l2, c.out, axes, sel, int(k))
+        out[int(k)] = compile_template(c.l1, c.l2, c.out, axes, sel, int(k), off1=off1)
     return out
 
 
-def compile_template(l1, l2, lo, axes, triples, tile_cfg):
+def panel_sigma1(Ll, psi, t1, nblks_out):
+    """Panel form of the L.psi contraction (HVecQt top1, kernelQt.py:301).
+
+    Every T1 block (a, l, n1, n2, r) is the product of exactly one L block
+    (a, l, l') and one psi block (l', n1, n2, r).  For a fixed contracted sector l'
+    the L blocks (a, l, l') are stacked into one panel [M_l' x D_l'] (a per-dot
+    block permutation of L), so each psi block j gives one GEMM
+    T1panel_j [M_l' x N_j] = Lpanel_l' . psi_j with a long M extent.  T1 blocks
+    keep their row-major storage inside the panel rows.
+
+    Returns None if the pair list is not the full product per sector, else a
+    dict with the L permutation (src/dst offsets of L blocks), the T1 block
+    offsets (by flat T1 block index, for the consumers of T1), the T1 size and
+    the per-panel GEMM descriptions.
+    """
+    if len(t1) == 0:
+        return None
+    ob, iL, ip = t1[:, 0], t1[:, 1], t1[:, 2]
+    if len(numpy.unique(ob)) != len(ob):
+        return None
+    uL = numpy.unique(iL)
+    dL = Ll.block_dims(uL)
+    lkL = Ll.block_sectors(uL)[2]
+    oL = numpy.lexsort((uL, lkL))
+    uL, dL, lkL = uL[oL], dL[oL], lkL[oL]
+    Mb = dL[:, 0] * dL[:, 1]
+    Dk = dL[:, 2]
+    nsec = int(Ll.nsyms[2])
+    M_lk = numpy.bincount(lkL, weights=Mb, minlength=nsec).astype(numpy.int64)
+    cnt_lk = numpy.bincount(lkL, minlength=nsec)
+    start = numpy.searchsorted(lkL, numpy.arange(nsec))
+    cs = numpy.cumsum(Mb) - Mb
+    rowoff = cs - cs[numpy.minimum(start[lkL], len(cs) - 1)]
+    Dk_sec = numpy.zeros(nsec, dtype=numpy.int64)
+    Dk_sec[lkL] = Dk
+    pan_size = M_lk * Dk_sec
+    pan_off = numpy.cumsum(pan_size) - pan_size
+    lperm_src = Ll.ioff[uL]
+    lperm_dst = pan_off[lkL] + rowoff * Dk
+    lperm_n = Mb * Dk
+    # psi blocks: every one pairs with all L blocks of its sector
+    up = numpy.unique(ip)
+    lkp = psi.block_sectors(up)[0]
+    npair_expect = int(cnt_lk[lkp].sum())
+    if npair_expect != len(t1):
+        return None
+    dp = psi.block_dims(up)
+    Nj = numpy.prod(dp[:, 1:], axis=1)
+    Mj = M_lk[lkp]
+    Kj = Dk_sec[lkp]
+    if numpy.any(Kj != dp[:, 0]):
+        return None
+    psz = Mj * Nj
+    t1pan = numpy.cumsum(psz) - psz
+    # T1 block offsets
+    posL = numpy.empty(int(Ll.nblks), dtype=numpy.int64)
+    posL[uL] = numpy.arange(len(uL))
+    posP = numpy.empty(int(psi.nblks), dtype=numpy.int64)
+    posP[up] = numpy.arange(len(up))
+    t1off = numpy.zeros(int(nblks_out), dtype=numpy.int64)
+    t1off[ob] = t1pan[posP[ip]] + rowoff[posL[iL]] * Nj[posP[ip]]
+    return {"lperm": (lperm_src, lperm_dst, lperm_n), "t1off": t1off, "t1size": int(psz.sum()),
+            "gemm": (pan_off[lkp], psi.ioff[up], t1pan, Mj, Nj, Kj)}
+
+
+def compile_panels(gemm, tensor_cores=False):
+    """Work items {tile_cfg: (tasks, contribs, flops)} of dense panel GEMMs
+    C_j[M_j x N_j] = A_j[M_j x K_j] . B_j[K_j x N_j], all operands row-major."""
+    a_off, b_off, c_off, M, N, K = (numpy.asarray(x, dtype=numpy.int64) for x in gemm)
+    if tensor_cores:
+        cls = tile_class_tc(M, N, K)
+    else:
+        cls = tile_class(M, N)
+    out = {}
+    for k in numpy.unique(cls):
+        sel = numpy.flatnonzero(cls == k)
+        tm, tn = TILES[int(k)]
+        nm = (M[sel] + tm - 1) // tm
+        nn = (N[sel] + tn - 1) // tn
+        nt = nm * nn
+        pid = numpy.repeat(numpy.arange(len(sel)), nt)
+        loc = numpy.arange(int(nt.sum())) - numpy.repeat(numpy.cumsum(nt) - nt, nt)
+        g = sel[pid]
+        tasks = numpy.zeros(len(g), TASK_DT)
+        tasks["c_off"] = c_off[g]
+        tasks["M"], tasks["N"] = M[g], N[g]
+        tasks["m0"] = (loc // nn[pid]) * tm
+        tasks["n0"] = (loc % nn[pid]) * tn
+        tasks["mlo"], tasks["nlo"] = M[g], N[g]
+        tasks["c_ml"] = N[g]
+        tasks["c_nl"] = 1
+        tasks["cb"] = pid
+        tasks["ce"] = pid + 1
+        contribs = numpy.zeros(len(sel), CONTRIB_DT)
+        contribs["a_off"], contribs["b_off"] = a_off[sel], b_off[sel]
+        contribs["alpha"] = 1.0
+        contribs["K"] = contribs["klo"] = K[sel]
+        contribs["a_ml"] = K[sel]
+        contribs["a_kl"] = 1
+        contribs["b_kl"] = N[sel]
+        contribs["b_nl"] = 1
+        contribs["op_b"], contribs["op_e"] = 0, 1
+        out[int(k)] = (tasks, contribs, 2.0 * float((M[sel] * N[sel] * K[sel]).sum()))
+    return out
+
+
+def compile_template(l1, l2, lo, axes, triples, tile_cfg, off1=None):
     """Work items of one contraction for a single operator with zero base offsets.
 
     The operator loop is added afterwards through op ranges into an operator table.
+    off1 replaces the packed block offsets of operand 1 (a permuted storage order).
     """
-    return compile_pairs(l1, l2, lo, axes, triples, [0], [0], [0], [1.0], 0, tile_cfg)
+    return compile_pairs(l1, l2, lo, axes, triples, [0], [0], [0], [1.0], 0, tile_cfg, off1=off1)
 
 
-def compile_pairs(l1, l2, lo, axes, triples, base1, base2, baseo, alpha, group_ops, tile_cfg):
+def compile_pairs(l1, l2, lo, axes, triples, base1, base2, baseo, alpha, group_ops, tile_cfg, off1=None):
     """Native plan compiler wrapper -> (tasks, contribs, flops)."""
+    o1 = l1.ioff if off1 is None else numpy.ascontiguousarray(off1, dtype=numpy.int64)
+    assert len(o1) == l1.nblks
     lib = native.lib()
     tm, tn = TILES[tile_cfg]
     ax1 = numpy.array(axes[0], dtype=numpy.int32)
@@ -97,7 +206,7 @@ def compile_pairs(l1, l2, lo, axes, triples, base1, base2, baseo, alpha, group_o
     al = numpy.ascontiguousarray(alpha, dtype=numpy.float64)
     nt = numpy.zeros(1, dtype=numpy.int64)
     fl = numpy.zeros(1, dtype=numpy.float64)
-    head = (l1.rank, ptr(l1.nsyms), ptr(l1.ndims_cat), ptr(l1.ioff), l2.rank, ptr(l2.nsyms), ptr(l2.ndims_cat),
+    head = (l1.rank, ptr(l1.nsyms), ptr(l1.ndims_cat), ptr(o1), l2.rank, ptr(l2.nsyms), ptr(l2.ndims_cat),
             ptr(l2.ioff), lo.rank, ptr(lo.nsyms), ptr(lo.ndims_cat), ptr(lo.ioff), len(axes[0]), ptr(ax1), ptr(ax2), len(tri), ptr(tri), len(b1), ptr(b1), ptr(b2), ptr(bo),
             ptr(al), int(group_ops), tm, tn)
     nc = check(lib.qc_compile_pairs(*(head + (None, 0, None, 0, ptr(nt), ptr(fl)))), "qc_compile_pairs")

@@ -19,7 +19,7 @@ import torch
 from . import native
 from .native import check
 from .engine import (Stage, compile_classes, add_parts, live_blocks, prune, op_table, TASK_DT, CONTRIB_DT, LOG,
-                     compile_fiber, FiberStage, CompositeStage)
+                     compile_fiber, FiberStage, CompositeStage, panel_sigma1, compile_panels, BPERM_DT)
 from .mpo import case
 from .qtensor import Contraction, flip_right, flip_horizontal
 
@@ -72,6 +72,15 @@ class TensorSet(object):
 
 def _stream(device):
     return torch.cuda.current_stream(device).cuda_stream
+
+
+def block_permute(descs, ndescs, opspan, ops, src, dst):
+    """Per-dot block permutation of an FP64 tensor set into dst (FP64 or FP32), qc_block_permute."""
+    check(native.lib().qc_block_permute(descs.data_ptr(), ndescs, opspan, ops.data_ptr(), src.data_ptr(),
+                                        dst.data_ptr(), int(dst.dtype == torch.float32), _stream(dst.device)),
+          "qc_block_permute")
+    LOG.launches += 1
+    return dst
 
 
 def gather(src, idx, out):
@@ -133,7 +142,7 @@ class SigmaOperator(object):
     """sigma = sum_p w_p R_p W_p[i+1] W_p[i] L_p psi for the dot (isite, isite+1)."""
 
     def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts, precision="f64",
-                 tensor_cores=None, use_fiber=False, fuse_w=True):
+                 tensor_cores=None, use_fiber=False, fuse_w=True, panel1=True):
         self.ws, self.psi, self.precision = ws, psi_layout, precision
         # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 mode
         tc = (precision == "tf32") if tensor_cores is None else tensor_cores
@@ -158,6 +167,9 @@ class SigmaOperator(object):
                     raise ValueError("operators of one symmetry class must share their block structure")
             c1 = Contraction(Ll, psi_layout, ax[0])
             t1 = c1.triples
+            # L.psi as dense panel GEMMs (T1 blocks stored panel by panel)
+            pan = panel_sigma1(Ll, psi_layout, t1, c1.out.nblks) if panel1 else None
+            t1off = pan["t1off"] if pan is not None else None
             c2 = Contraction(c1.out, W1, ax[1])
             t2 = prune(c2.triples, live1=live_blocks(c1.out, t1))
             c3 = Contraction(c2.out, W2, ax[2])
@@ -171,20 +183,21 @@ class SigmaOperator(object):
                 cF = Contraction(c1.out, cW.out, ([0, 2, 3], [0, 2, 5]))
                 if cF.out is c3.out:
                     tF = prune(cF.triples, live1=live_blocks(c1.out, t1), live2=live_blocks(cW.out, cW.triples))
-                    fp = compile_fiber(cF, tF, 0, 0)
+                    fp = compile_fiber(cF, tF, 0, 0, in_off=t1off)
                     if fp is not None:
                         fused = (cW, cF, tF, fp)
             c4 = Contraction(c3.out, Rl, ax[3])
             t4 = prune(c4.triples, live1=live_blocks(c3.out, fused[2] if fused else t3))
             if c4.out is not psi_layout:
                 raise ValueError("sigma output layout differs from the wavefunction template")
-            plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3), (c4, t4), Rl, fused)
+            plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3), (c4, t4), Rl, fused, pan)
             for s, c in enumerate((c1, c2, c3)):
                 if s == 1 and fused is not None:
                     continue            # no T2 for fused classes
+                size = pan["t1size"] if (s == 0 and pan is not None) else c.out.size
                 for i in ops:
                     bases[s][i] = tot[s]
-                    tot[s] += c.out.size
+                    tot[s] += size
             if fused is not None:
                 for i in ops:
                     wbase[i] = wtot
@@ -209,9 +222,24 @@ class SigmaOperator(object):
         # W contractions: fiber-group kernel (inputs staged once per fiber tile) where
         # every group fits in shared memory, generic grouped GEMM otherwise
         fiber_spec = {1: (0, 0), 2: (3, 1)}      # stage -> (rows axis of operand 1, fiber-major storage)
-        for key, (ops, *cs, Rl, fused) in sorted(plans.items()):
+        lperm = []
+        for key, (ops, *cs, Rl, fused, pan) in sorted(plans.items()):
             rng = (pos, pos + len(ops))
             pos += len(ops)
+            t1off = pan["t1off"] if pan is not None else None
+            if panel1:
+                if pan is not None:
+                    src, dst, n = pan["lperm"]
+                else:                   # no panels for this class: L blocks copied in place
+                    Ll = cs[0][0].l1
+                    src = dst = Ll.ioff[Ll.idx_allowed]
+                    n = Ll.ndim[Ll.idx_allowed]
+                d = numpy.zeros(len(src), BPERM_DT)
+                d["src_off"], d["dst_off"] = src, dst
+                d["d0"], d["d1"], d["d2"] = 1, 1, n
+                d["s2"] = 1
+                d["op_b"], d["op_e"] = rng
+                lperm.append(d)
             if fused is not None:
                 cW, cF, tF, fp = fused
                 fuse_parts.append(fp + (rng,))
@@ -220,16 +248,20 @@ class SigmaOperator(object):
             for si, (c, t) in enumerate(cs):
                 if fused is not None and si in (1, 2):
                     continue
+                if si == 0 and pan is not None:
+                    add_parts(st[0], compile_panels(pan["gemm"], tensor_cores=tc), op_range=rng)
+                    continue
+                off1 = t1off if si == 1 else None
                 if use_fiber and si in fiber_spec:
-                    fp = compile_fiber(c, t, *fiber_spec[si])
+                    fp = compile_fiber(c, t, *fiber_spec[si], in_off=off1)
                     if fp is not None:
                         fib[si].append(fp + (rng,))
                         self.w_paths["fiber"] += 1
                         continue
                 if si in fiber_spec:
                     self.w_paths["generic"] += 1
-                add_parts(st[si], compile_classes(c, t, ax[si], tensor_cores=tc if si in (0, 3) else False),
-                          op_range=rng)
+                add_parts(st[si], compile_classes(c, t, ax[si], tensor_cores=tc if si in (0, 3) else False,
+                                                  off1=off1), op_range=rng)
         self.stages = []
         for si in range(4):
             g = Stage(st[si], dev, "sigma%d" % (si + 1), tabs[si]) if st[si] else None
@@ -238,6 +270,15 @@ class SigmaOperator(object):
                 self.stages.append(g if g is not None else Stage({}, dev, "sigma%d" % (si + 1), tabs[si]))
             else:
                 self.stages.append(CompositeStage([f, g], "sigma%d" % (si + 1)))
+        # per-dot L panels (a block permutation of every operator's L), FP64 and FP32
+        self.lperm = None
+        if lperm:
+            self._lperm_h = numpy.concatenate(lperm)
+            self.lperm = torch.from_numpy(self._lperm_h.view(numpy.uint8).copy()).to(dev)
+            self._lperm_ops = op_table(L.offsets[order], 0, L.offsets[order], 1.0)
+            self._lperm_ops_d = torch.from_numpy(self._lperm_ops.view(numpy.uint8).copy()).to(dev)
+            self._lperm_span = int(max(len(v[0]) for v in plans.values()))
+            self._build_lpan()
         # fused W stage (T1 -> T3) and the per-dot two-site MPO blocks it reads
         self.fused = None
         self.wtot = wtot
@@ -263,13 +304,13 @@ class SigmaOperator(object):
         fb = 0
         for si in range(4):
             tot_b = 0
-            for key, (ops, *cs, Rl, fused) in sorted(plans.items()):
+            for key, (ops, *cs, Rl, fused, pan) in sorted(plans.items()):
                 if fused is not None and si in (1, 2):
                     continue
                 c, t = cs[si]
                 tot_b += stage_bytes(c, t, len(ops), si == 0)      # psi is read by every operator
             self.stages[si].bytes = float(tot_b)
-        for key, (ops, *cs, Rl, fused) in sorted(plans.items()):
+        for key, (ops, *cs, Rl, fused, pan) in sorted(plans.items()):
             if fused is not None:
                 fb += stage_bytes(fused[1], fused[2], len(ops), False)
         if self.fused is not None:
@@ -277,7 +318,7 @@ class SigmaOperator(object):
         # FLOPs of the reference's four-contraction chain (tensordotCAL pair GEMMs),
         # whatever the fusion used here
         self.flops = 0.0
-        for key, (ops, *cs, Rl, fused) in sorted(plans.items()):
+        for key, (ops, *cs, Rl, fused, pan) in sorted(plans.items()):
             for (c, t) in cs:
                 self.flops += pair_flops(c, t) * len(ops)
         self.ndim0 = psi_layout.size
@@ -287,10 +328,32 @@ class SigmaOperator(object):
         if [id(x) for x in L.layouts] != self._lay_ids[0] or [id(x) for x in R.layouts] != self._lay_ids[1]:
             raise ValueError("rebind: environment layouts differ from the compiled plan")
         self.L, self.R = L, R
+        if self.lperm is not None:
+            self._build_lpan()
+
+    def _build_lpan(self):
+        self.Lpan = torch.empty(max(self.L.total, 1), dtype=torch.float64, device=self.ws.device)
+        block_permute(self.lperm, len(self._lperm_h), self._lperm_span, self._lperm_ops_d, self.L.values,
+                      self.Lpan)
+        self._Lpan32 = None
+
+    def lpan32(self):
+        if self._Lpan32 is None:
+            self._Lpan32 = torch.empty(max(self.L.total, 1), dtype=torch.float32, device=self.ws.device)
+            block_permute(self.lperm, len(self._lperm_h), self._lperm_span, self._lperm_ops_d, self.L.values,
+                          self._Lpan32)
+        return self._Lpan32
+
+    def a1(self, kind):
+        """First operand of the L.psi contraction (L panels, or L itself without panels)."""
+        if self.lperm is not None:
+            return self.Lpan if kind == "f64" else self.lpan32()
+        return self.L.values if kind == "f64" else self.L.f32()
 
     def release(self):
         """Drop the references to the environment values (the plan stays valid)."""
         self.L = self.R = None
+        self.Lpan = self._Lpan32 = None
 
     def wij32(self):
         if self._Wij32 is None:
@@ -315,7 +378,7 @@ class SigmaOperator(object):
             T3 = ws.get("t3", self.tot[2], torch.float64)
             P = ws.get("part", self.nops * self.ndim0, torch.float64)
             s = self.stages
-            s[0].run(self.L.values, x, T1, "f64")
+            s[0].run(self.a1("f64"), x, T1, "f64")
             s[1].run(T1, self.Wi.values, T2, "f64")
             s[2].run(T2, self.Wj.values, T3, "f64")
             if self.fused is not None:
@@ -332,7 +395,7 @@ class SigmaOperator(object):
         convert(x, x32)
         P = ws.get("part32", self.nops * self.ndim0, torch.float32)
         s = self.stages
-        s[0].run(self.L.f32(), x32, T1, kind)
+        s[0].run(self.a1("f32"), x32, T1, kind)
         s[1].run(T1, self.Wi.f32(), T2, "f32")
         s[2].run(T2, self.Wj.f32(), T3, "f32")
         if self.fused is not None:

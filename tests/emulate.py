@@ -14,7 +14,7 @@ def _idx(i, lo, s_hi, s_lo):
 def patch_stage_run(monkeypatch):
     """Route Stage.run through the interpreter (tile extents follow the stage's tile config)."""
     import torch
-    from qcmpodmrg_b200 import engine
+    from qcmpodmrg_b200 import engine, kernels
 
     def run(self, A, B, C, kind="f64", stream=None):
         if self.ntasks == 0:
@@ -39,6 +39,22 @@ def patch_stage_run(monkeypatch):
         C.copy_(torch.from_numpy(c).to(C.dtype))
 
     monkeypatch.setattr(engine.FiberStage, "run", frun)
+
+    def block_permute(descs, ndescs, opspan, ops, src, dst):
+        d = descs.cpu().numpy().view(engine.BPERM_DT)
+        o = ops.cpu().numpy().view(engine.OP_DT)
+        a = src.detach().cpu().numpy().astype(numpy.float64)
+        c = dst.detach().cpu().numpy().astype(numpy.float64)
+        for x in d:
+            for op in range(x["op_b"], x["op_e"]):
+                blk = a[o[op]["a_base"] + x["src_off"]:][:x["d0"] * x["d1"] * x["d2"]].reshape(x["d0"], x["d1"], x["d2"])
+                i0, i1, i2 = numpy.meshgrid(numpy.arange(x["d0"]), numpy.arange(x["d1"]), numpy.arange(x["d2"]),
+                                            indexing="ij")
+                c[o[op]["c_base"] + x["dst_off"] + i0 * x["s0"] + i1 * x["s1"] + i2 * x["s2"]] = blk
+        dst.copy_(torch.from_numpy(c).to(dst.dtype))
+        return dst
+
+    monkeypatch.setattr(kernels, "block_permute", block_permute)
     from qcmpodmrg_b200 import kernels
 
     def gather(src, idx, out):

@@ -25,7 +25,7 @@ def tensorset(dicts, device):
                                                       for d in dicts], device=device)
 
 
-def record_operators(r, device, precision="f64", use_fiber=False, fuse_w=True):
+def record_operators(r, device, precision="f64", use_fiber=False, fuse_w=True, panel1=True):
     """SigmaOperator / DiagOperator for a recorded reference dot."""
     from qcmpodmrg_b200.kernels import SigmaOperator, DiagOperator, Workspace
     import torch
@@ -38,7 +38,7 @@ def record_operators(r, device, precision="f64", use_fiber=False, fuse_w=True):
     hp = numpy.atleast_1d(r["hpwts"]).astype(numpy.float64)
     qkey = numpy.asarray(r["qkey"], dtype=numpy.float64)
     sig = SigmaOperator(ws, isite, psi, L, R, Wi, Wj, qkey, opers, hp, precision, use_fiber=use_fiber,
-                        fuse_w=fuse_w)
+                        fuse_w=fuse_w, panel1=panel1)
     dg = DiagOperator(ws, isite, psi, L, R, Wi, Wj, qkey, opers, hp)
     return sig, dg, ws
 

@@ -44,7 +44,7 @@ def _call(sig, x, y):
 
 def test_noalloc_sigma_matches_regular_path(cuda):
     r = load("kernels_K6.npz")["records"][0]
-    sig, dg, ws = record_operators(r, cuda, use_fiber=False)     # grouped-GEMM stages only
+    sig, dg, ws = record_operators(r, cuda, use_fiber=False, panel1=False)   # packed-layout stages
     gen = torch.Generator(device="cpu").manual_seed(7)
     for call in range(2):
         x = torch.randn(sig.ndim0, dtype=torch.float64, generator=gen).to(cuda)
@@ -64,7 +64,7 @@ def test_noalloc_sigma_matches_regular_path(cuda):
 
 def test_noalloc_rejects_oversized_dot(cuda):
     r = load("kernels_K4.npz")["records"][0]
-    sig, dg, ws = record_operators(r, cuda, use_fiber=False)     # grouped-GEMM stages only
+    sig, dg, ws = record_operators(r, cuda, use_fiber=False, panel1=False)   # packed-layout stages
     x = torch.zeros(sig.ndim0, dtype=torch.float64, device=cuda)
     y = torch.zeros(sig.ndim0, dtype=torch.float64, device=cuda)
     tot = sig.tot
