@@ -14,7 +14,7 @@ import torch
 
 from . import native
 from .native import check
-from .engine import OP_DT, TASK_DT, CONTRIB_DT, TC_CFG, LOG, FiberStage, CompositeStage
+from .engine import OP_DT, TASK_DT, CONTRIB_DT, TC_CFG, LOG, FiberStage, CompositeStage, PanelStage
 
 
 def _abs_ops(ops, a, b, c):
@@ -57,6 +57,7 @@ class BatchedSigma(object):
         self.offs = offs
         groups = {}
         fibers = {}
+        panels = {}
         ops_all = [[], [], [], [], []]
         nops_acc = [0, 0, 0, 0, 0]
         for i, s in enumerate(items):
@@ -83,6 +84,13 @@ class BatchedSigma(object):
                     if isinstance(sub, FiberStage):
                         if sub.ntasks:
                             fibers.setdefault(si, []).append((sub, base))
+                        continue
+                    if isinstance(sub, PanelStage):
+                        for (cfg, tk, _, _) in sub.groups:
+                            tk = tk.copy()
+                            tk["op_b"] += base
+                            tk["op_e"] += base
+                            panels.setdefault((si, cfg), []).append(tk)
                         continue
                     for (cfg, tk, ct) in sub.host_groups:
                         tk = tk.copy()
@@ -137,6 +145,11 @@ class BatchedSigma(object):
             span = int(max(1, (tk["op_e"] - tk["op_b"]).max()))
             self.fiber_launches.append((si, len(tk), span, mr, up(tk), up(numpy.concatenate(fis)),
                                         up(numpy.concatenate(fos)), up(numpy.concatenate(fps))))
+        self.panel_launches = []
+        for (si, cfg), tks in sorted(panels.items()):
+            tk = numpy.concatenate(tks)
+            span = int(max(1, (tk["op_e"] - tk["op_b"]).max()))
+            self.panel_launches.append((si, cfg, len(tk), span, up(tk)))
         self.graph = None
 
     def _launch_all(self):
@@ -144,7 +157,14 @@ class BatchedSigma(object):
         s = torch.cuda.current_stream(self.device).cuda_stream
         self.T[3].zero_()
         ffn = lib.qc_fiber_f64 if self.kind == "f64" else lib.qc_fiber_f32
+        pfn = lib.qc_pgemm_f64 if self.kind == "f64" else lib.qc_pgemm_f32
         for stage in (0, 1, 2, 4, 3):       # contractions in dependency order (4: fused W stage)
+            for (si, cfg, nt, span, dt) in self.panel_launches:
+                if si != stage:
+                    continue
+                check(pfn(dt.data_ptr(), nt, span, self.d_ops[si].data_ptr(), None, None, None, cfg, s),
+                      "batched qc_pgemm")
+                LOG.launches += 1
             for (si, nt, span, mr, dt, dfi, dfo, dfp) in self.fiber_launches:
                 if si != stage:
                     continue

@@ -29,147 +29,101 @@ namespace {
 //                 of the operator table (same block structure, own base offsets).
 // SUMMED = true:  the task computes one tile; every contribution accumulates the
 //                 products of the operators in [c.op_b, c.op_e) (sum over p).
-//
-// Software pipeline: the operand elements of K-tile s+1 are loaded from global
-// memory into registers while the FMAs of K-tile s run from shared memory
-// (two shared-memory buffers, one barrier per K-tile).
 template <typename T, int TM, int TN, int TK, int RM, int RN, bool SUMMED, int kThreads>
-__global__ void __launch_bounds__(kThreads, (kThreads >= 256 ? 2 : 4))
+__global__ void __launch_bounds__(kThreads)
 k_bgemm(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ contribs,
         const qc_op *__restrict__ ops, const T *__restrict__ A, const T *__restrict__ B, T *__restrict__ C) {
   constexpr int TX = TN / RN;
   constexpr int TY = TM / RM;
   static_assert(TX * TY == kThreads, "thread tile");
-  constexpr int LA = (TM * TK + kThreads - 1) / kThreads;   // A elements per thread per K-tile
-  constexpr int LB = (TK * TN + kThreads - 1) / kThreads;
-  __shared__ T As[2][TK][TM + 1];
-  __shared__ T Bs[2][TK][TN + 1];
+  __shared__ T As[TK][TM + 1];
+  __shared__ T Bs[TK][TN + 1];
   __shared__ int arow[TM];
   __shared__ int bcol[TN];
+  __shared__ int akoff[TK];
+  __shared__ int bkoff[TK];
 
   const qc_task t = tasks[blockIdx.x];
   // per-operator mode: blockIdx.y selects the operator of the task's range
   if (!SUMMED && t.op_b + (int)blockIdx.y >= t.op_e) return;
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
-  const int oi = SUMMED ? 0 : (int)blockIdx.y;
-  T acc[RM][RN];
+  {
+    const int oi = SUMMED ? 0 : (int)blockIdx.y;
+    T acc[RM][RN];
 #pragma unroll
-  for (int i = 0; i < RM; ++i)
+    for (int i = 0; i < RM; ++i)
 #pragma unroll
-    for (int j = 0; j < RN; ++j) acc[i][j] = T(0);
+      for (int j = 0; j < RN; ++j) acc[i][j] = T(0);
 
-  for (int ci = t.cb; ci < t.ce; ++ci) {
-    const qc_contrib c = contribs[ci];
-    __syncthreads();                    // previous contribution done with maps and buffers
-    for (int i = tid; i < TM; i += kThreads) {
-      const int m = t.m0 + i;
-      arow[i] = (m < t.M) ? (m / t.mlo) * c.a_mh + (m % t.mlo) * c.a_ml : -1;
-    }
-    for (int j = tid; j < TN; j += kThreads) {
-      const int n = t.n0 + j;
-      bcol[j] = (n < t.N) ? (n / t.nlo) * c.b_nh + (n % t.nlo) * c.b_nl : -1;
-    }
-    __syncthreads();
-    const bool a_kfast = (c.a_kl == 1);
-    const bool b_nfast = (c.b_nl == 1);
-    const bool k1 = (c.klo >= c.K);     // single-level k map
-    const int opb = SUMMED ? c.op_b : t.op_b + oi;
-    const int ope = SUMMED ? c.op_e : opb + 1;
-    const int nsteps = (c.K + TK - 1) / TK;
-    for (int op = opb; op < ope; ++op) {
-      const qc_op o = ops[op];
-      const T alpha = T(o.alpha * c.alpha);
-      const T *Ab = A + o.a_base + c.a_off;
-      const T *Bb = B + o.b_base + c.b_off;
-      T ra[LA], rb[LB];
-      auto load = [&](int k0) {
-#pragma unroll
-        for (int e = 0; e < LA; ++e) {
-          const int idx = tid + e * kThreads;
-          int i, kk;
-          if (a_kfast) { kk = idx % TK; i = idx / TK; } else { i = idx % TM; kk = idx / TM; }
-          const int k = k0 + kk;
-          T v = T(0);
-          if (idx < TM * TK && k < c.K) {
-            const int ro = arow[i];
-            if (ro >= 0) {
-              const int ko = k1 ? k * c.a_kl : (k / c.klo) * c.a_kh + (k % c.klo) * c.a_kl;
-              v = Ab[ro + ko] * alpha;
-            }
+    for (int ci = t.cb; ci < t.ce; ++ci) {
+      const qc_contrib c = contribs[ci];
+      __syncthreads();
+      for (int i = tid; i < TM; i += kThreads) {
+        const int m = t.m0 + i;
+        arow[i] = (m < t.M) ? (m / t.mlo) * c.a_mh + (m % t.mlo) * c.a_ml : -1;
+      }
+      for (int j = tid; j < TN; j += kThreads) {
+        const int n = t.n0 + j;
+        bcol[j] = (n < t.N) ? (n / t.nlo) * c.b_nh + (n % t.nlo) * c.b_nl : -1;
+      }
+      const bool a_kfast = (c.a_kl == 1);
+      const bool b_nfast = (c.b_nl == 1);
+      const int opb = SUMMED ? c.op_b : t.op_b + oi;
+      const int ope = SUMMED ? c.op_e : opb + 1;
+      for (int op = opb; op < ope; ++op) {
+        const qc_op o = ops[op];
+        const T alpha = T(o.alpha * c.alpha);
+        const T *Ab = A + o.a_base + c.a_off;
+        const T *Bb = B + o.b_base + c.b_off;
+        for (int k0 = 0; k0 < c.K; k0 += TK) {
+          __syncthreads();
+          if (tid < TK) {
+            const int k = k0 + tid;
+            akoff[tid] = (k < c.K) ? (k / c.klo) * c.a_kh + (k % c.klo) * c.a_kl : -1;
+            bkoff[tid] = (k < c.K) ? (k / c.klo) * c.b_kh + (k % c.klo) * c.b_kl : -1;
           }
-          ra[e] = v;
-        }
-#pragma unroll
-        for (int e = 0; e < LB; ++e) {
-          const int idx = tid + e * kThreads;
-          int j, kk;
-          if (b_nfast) { j = idx % TN; kk = idx / TN; } else { kk = idx % TK; j = idx / TK; }
-          const int k = k0 + kk;
-          T v = T(0);
-          if (idx < TK * TN && k < c.K) {
-            const int co = bcol[j];
-            if (co >= 0) {
-              const int ko = k1 ? k * c.b_kl : (k / c.klo) * c.b_kh + (k % c.klo) * c.b_kl;
-              v = Bb[ko + co];
-            }
-          }
-          rb[e] = v;
-        }
-      };
-      auto store = [&](int buf) {
-#pragma unroll
-        for (int e = 0; e < LA; ++e) {
-          const int idx = tid + e * kThreads;
-          if (idx < TM * TK) {
+          __syncthreads();
+          for (int idx = tid; idx < TM * TK; idx += kThreads) {
             int i, kk;
             if (a_kfast) { kk = idx % TK; i = idx / TK; } else { i = idx % TM; kk = idx / TM; }
-            As[buf][kk][i] = ra[e];
+            const int ro = arow[i], ko = akoff[kk];
+            As[kk][i] = (ro >= 0 && ko >= 0) ? Ab[ro + ko] * alpha : T(0);
           }
-        }
-#pragma unroll
-        for (int e = 0; e < LB; ++e) {
-          const int idx = tid + e * kThreads;
-          if (idx < TK * TN) {
+          for (int idx = tid; idx < TK * TN; idx += kThreads) {
             int j, kk;
             if (b_nfast) { j = idx % TN; kk = idx / TN; } else { kk = idx % TK; j = idx / TK; }
-            Bs[buf][kk][j] = rb[e];
+            const int co = bcol[j], ko = bkoff[kk];
+            Bs[kk][j] = (co >= 0 && ko >= 0) ? Bb[ko + co] : T(0);
+          }
+          __syncthreads();
+#pragma unroll
+          for (int kk = 0; kk < TK; ++kk) {
+            T a[RM], b[RN];
+#pragma unroll
+            for (int i = 0; i < RM; ++i) a[i] = As[kk][ty + i * TY];
+#pragma unroll
+            for (int j = 0; j < RN; ++j) b[j] = Bs[kk][tx + j * TX];
+#pragma unroll
+            for (int i = 0; i < RM; ++i)
+#pragma unroll
+              for (int j = 0; j < RN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
           }
         }
-      };
-      load(0);
-      for (int s = 0; s < nsteps; ++s) {
-        const int buf = s & 1;
-        store(buf);
-        __syncthreads();
-        if (s + 1 < nsteps) load((s + 1) * TK);      // in flight during the FMAs below
-#pragma unroll
-        for (int kk = 0; kk < TK; ++kk) {
-          T av[RM], bv[RN];
-#pragma unroll
-          for (int i = 0; i < RM; ++i) av[i] = As[buf][kk][ty + i * TY];
-#pragma unroll
-          for (int j = 0; j < RN; ++j) bv[j] = Bs[buf][kk][tx + j * TX];
-#pragma unroll
-          for (int i = 0; i < RM; ++i)
-#pragma unroll
-            for (int j = 0; j < RN; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
-        }
       }
-      __syncthreads();                  // buffers free before the next operator's first store
     }
-  }
-  T *Cb = C + t.c_off + (SUMMED ? 0 : ops[t.op_b + oi].c_base);
+    T *Cb = C + t.c_off + (SUMMED ? 0 : ops[t.op_b + oi].c_base);
 #pragma unroll
-  for (int i = 0; i < RM; ++i) {
-    const int m = t.m0 + ty + i * TY;
-    if (m >= t.M) continue;
-    const long long rowoff = (long long)(m / t.mlo) * t.c_mh + (long long)(m % t.mlo) * t.c_ml;
+    for (int i = 0; i < RM; ++i) {
+      const int m = t.m0 + ty + i * TY;
+      if (m >= t.M) continue;
+      const long long rowoff = (long long)(m / t.mlo) * t.c_mh + (long long)(m % t.mlo) * t.c_ml;
 #pragma unroll
-    for (int j = 0; j < RN; ++j) {
-      const int n = t.n0 + tx + j * TX;
-      if (n >= t.N) continue;
-      Cb[rowoff + (long long)(n / t.nlo) * t.c_nh + (long long)(n % t.nlo) * t.c_nl] = acc[i][j];
+      for (int j = 0; j < RN; ++j) {
+        const int n = t.n0 + tx + j * TX;
+        if (n >= t.N) continue;
+        Cb[rowoff + (long long)(n / t.nlo) * t.c_nh + (long long)(n % t.nlo) * t.c_nl] = acc[i][j];
+      }
     }
   }
 }
@@ -178,15 +132,13 @@ template <typename T, bool S>
 int launch_mode(const qc_task *tk, long long ntasks, int opspan, const qc_contrib *cb, const qc_op *ops,
                 const T *A, const T *B, T *C, int cfg, cudaStream_t s) {
   dim3 grid((unsigned)ntasks, S ? 1u : (unsigned)opspan);
-  // K-tile 8 where two FP64 buffers of 16 would exceed 48 KB of static shared memory
-  constexpr int KW = (sizeof(T) == 8) ? 8 : 16;
   switch (cfg) {
     case 0: k_bgemm<T, 64, 64, 16, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
     case 1: k_bgemm<T, 128, 32, 16, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
-    case 2: k_bgemm<T, 256, 16, KW, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
+    case 2: k_bgemm<T, 256, 16, 16, 4, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
     case 3: k_bgemm<T, 32, 32, 16, 4, 4, S, 64><<<grid, 64, 0, s>>>(tk, cb, ops, A, B, C); break;
     case 4: k_bgemm<T, 64, 16, 16, 4, 4, S, 64><<<grid, 64, 0, s>>>(tk, cb, ops, A, B, C); break;
-    case 5: k_bgemm<T, 128, 64, KW, 8, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
+    case 5: k_bgemm<T, 128, 64, 16, 8, 4, S, 256><<<grid, 256, 0, s>>>(tk, cb, ops, A, B, C); break;
     default: return QC_ERR_ARG;
   }
   return cuda_fail("qc_bgemm");

@@ -77,19 +77,40 @@ __device__ __forceinline__ int canon(int row, int k, int rows) {
   return (((k >> 2) * (rows >> 3) + (row >> 3)) << 5) + ((row & 7) << 2) + (k & 3);
 }
 
+__device__ __forceinline__ void issue_mma(uint32_t tmem, uint32_t a0, uint32_t b0, bool accumulate) {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+  for (int s = 0; s < TC_K / 8; ++s) {
+    const uint64_t da = umma_desc(a0 + s * 2 * (TC_M / 8) * 128, (TC_M / 8) * 128, 128);
+    const uint64_t db = umma_desc(b0 + s * 2 * (TC_N / 8) * 128, (TC_N / 8) * 128, 128);
+    const uint32_t en = (accumulate || s > 0) ? 1u : 0u;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+        :
+        : "r"(tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(en));
+  }
+}
+
+// Two shared-memory stages: while the tensor core multiplies K-slice s (stage
+// s&1), the threads load K-slice s+1 from global memory into registers; stage
+// s&1 is refilled only after the MMAs that read it (committed to mbar[s&1])
+// have completed.
 __global__ void __launch_bounds__(TC_THREADS)
 k_bgemm_tc(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ contribs,
            const qc_op *__restrict__ ops, const float *__restrict__ A, const float *__restrict__ B,
            float *__restrict__ C, int *__restrict__ err) {
-  __shared__ __align__(1024) float As[TC_M * TC_K];
-  __shared__ __align__(1024) float Bs[TC_N * TC_K];
-  __shared__ __align__(8) uint64_t mbar;
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  float *As = reinterpret_cast<float *>(tc_smem);                 // [2][TC_M * TC_K]
+  float *Bs = As + 2 * TC_M * TC_K;                                 // [2][TC_N * TC_K]
+  __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
   __shared__ int arow[TC_M];
   __shared__ int bcol[TC_N];
-  __shared__ int akoff[TC_K];
-  __shared__ int bkoff[TC_K];
   __shared__ int abort_flag;
+  constexpr int LA = TC_M * TC_K / TC_THREADS;
+  constexpr int LB = TC_N * TC_K / TC_THREADS;
 
   const qc_task t = tasks[blockIdx.x];
   if (t.op_b + (int)blockIdx.y >= t.op_e) return;
@@ -105,15 +126,16 @@ k_bgemm_tc(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ con
   }
   if (tid == 0) {
     abort_flag = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
-  const uint32_t bar = smem_u32(&mbar);
-  uint32_t phase = 0;
+  uint32_t ph[2] = {0u, 0u};           // parity of the next completion of mbar[0], mbar[1] (thread 0)
+  int g = 0;                           // K-slices issued so far (all contributions)
   bool accumulate = false;
 
   for (int ci = t.cb; ci < t.ce && !abort_flag; ++ci) {
@@ -127,66 +149,96 @@ k_bgemm_tc(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ con
       const int n = t.n0 + j;
       bcol[j] = (n < t.N) ? (n / t.nlo) * c.b_nh + (n % t.nlo) * c.b_nl : -1;
     }
+    __syncthreads();
     const float alpha = (float)(o.alpha * c.alpha);
     const float *Ab = A + o.a_base + c.a_off;
     const float *Bb = B + o.b_base + c.b_off;
     const bool a_kfast = (c.a_kl == 1);
     const bool b_nfast = (c.b_nl == 1);
-    for (int k0 = 0; k0 < c.K && !abort_flag; k0 += TC_K) {
-      __syncthreads();
-      if (tid < TC_K) {
-        const int k = k0 + tid;
-        akoff[tid] = (k < c.K) ? (k / c.klo) * c.a_kh + (k % c.klo) * c.a_kl : -1;
-        bkoff[tid] = (k < c.K) ? (k / c.klo) * c.b_kh + (k % c.klo) * c.b_kl : -1;
-      }
-      __syncthreads();
-      for (int idx = tid; idx < TC_M * TC_K; idx += TC_THREADS) {
+    const bool k1 = (c.klo >= c.K);
+    const int nsteps = (c.K + TC_K - 1) / TC_K;
+    float ra[LA], rb[LB];
+    auto load = [&](int k0) {
+#pragma unroll
+      for (int e = 0; e < LA; ++e) {
+        const int idx = tid + e * TC_THREADS;
         int i, kk;
         if (a_kfast) { kk = idx % TC_K; i = idx / TC_K; } else { i = idx % TC_M; kk = idx / TC_M; }
-        const int ro = arow[i], ko = akoff[kk];
-        As[canon(i, kk, TC_M)] = to_tf32((ro >= 0 && ko >= 0) ? Ab[ro + ko] * alpha : 0.f);
+        const int k = k0 + kk, ro = arow[i];
+        float v = 0.f;
+        if (ro >= 0 && k < c.K) {
+          const int ko = k1 ? k * c.a_kl : (k / c.klo) * c.a_kh + (k % c.klo) * c.a_kl;
+          v = Ab[ro + ko] * alpha;
+        }
+        ra[e] = v;
       }
-      for (int idx = tid; idx < TC_N * TC_K; idx += TC_THREADS) {
+#pragma unroll
+      for (int e = 0; e < LB; ++e) {
+        const int idx = tid + e * TC_THREADS;
         int j, kk;
         if (b_nfast) { j = idx % TC_N; kk = idx / TC_N; } else { kk = idx % TC_K; j = idx / TC_K; }
-        const int co = bcol[j], ko = bkoff[kk];
-        Bs[canon(j, kk, TC_N)] = to_tf32((co >= 0 && ko >= 0) ? Bb[ko + co] : 0.f);
+        const int k = k0 + kk, co = bcol[j];
+        float v = 0.f;
+        if (co >= 0 && k < c.K) {
+          const int ko = k1 ? k * c.b_kl : (k / c.klo) * c.b_kh + (k % c.klo) * c.b_kl;
+          v = Bb[ko + co];
+        }
+        rb[e] = v;
+      }
+    };
+    load(0);
+    for (int s = 0; s < nsteps; ++s) {
+      const int buf = g & 1;
+      if (tid == 0 && g >= 2) {          // stage buf last read by the MMAs of slice g-2
+        if (!mbar_wait(smem_u32(&mbar[buf]), ph[buf])) {
+          abort_flag = 1;
+          if (err) atomicExch(err, 1);
+        }
+        ph[buf] ^= 1u;
+      }
+      __syncthreads();
+      if (abort_flag) break;
+      float *as = As + buf * TC_M * TC_K;
+      float *bs = Bs + buf * TC_N * TC_K;
+#pragma unroll
+      for (int e = 0; e < LA; ++e) {
+        const int idx = tid + e * TC_THREADS;
+        int i, kk;
+        if (a_kfast) { kk = idx % TC_K; i = idx / TC_K; } else { i = idx % TC_M; kk = idx / TC_M; }
+        as[canon(i, kk, TC_M)] = to_tf32(ra[e]);
+      }
+#pragma unroll
+      for (int e = 0; e < LB; ++e) {
+        const int idx = tid + e * TC_THREADS;
+        int j, kk;
+        if (b_nfast) { j = idx % TC_N; kk = idx / TC_N; } else { kk = idx % TC_K; j = idx / TC_K; }
+        bs[canon(j, kk, TC_N)] = to_tf32(rb[e]);
       }
       // make the generic-proxy shared-memory stores visible to the tensor core
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
       if (tid == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
-#pragma unroll
-        for (int s = 0; s < TC_K / 8; ++s) {
-          const uint64_t da = umma_desc(a0 + s * 2 * (TC_M / 8) * 128, (TC_M / 8) * 128, 128);
-          const uint64_t db = umma_desc(b0 + s * 2 * (TC_N / 8) * 128, (TC_N / 8) * 128, 128);
-          const uint32_t en = (accumulate || s > 0) ? 1u : 0u;
-          asm volatile(
-              "{\n\t.reg .pred p;\n\t"
-              "setp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
-              :
-              : "r"(tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(en));
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-                     : "memory");
-        // only this thread waits; the barrier below publishes the outcome to the CTA
-        if (!mbar_wait(bar, phase)) {
-          // give the in-flight MMAs one more bounded chance before tensor memory is released
-          mbar_wait(bar, phase);
-          abort_flag = 1;
-          if (err) atomicExch(err, 1);
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        issue_mma(tmem, smem_u32(as), smem_u32(bs), accumulate);
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     ::"r"(smem_u32(&mbar[buf])) : "memory");
       }
       accumulate = true;
-      phase ^= 1u;
-      __syncthreads();
+      ++g;
+      if (s + 1 < nsteps) load((s + 1) * TC_K);   // global loads overlap the MMAs just issued
     }
   }
+  // drain: the last commit covers every MMA issued before it
+  if (tid == 0 && g >= 1) {
+    const int lb = (g - 1) & 1;
+    if (!mbar_wait(smem_u32(&mbar[lb]), ph[lb])) {
+      mbar_wait(smem_u32(&mbar[lb]), ph[lb]);     // one more bounded chance before TMEM is released
+      abort_flag = 1;
+      if (err) atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
   __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!abort_flag) {
     float *Cb = C + o.c_base + t.c_off;
     const int m = t.m0 + warp * 32 + lane;
@@ -223,6 +275,8 @@ k_bgemm_tc(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ con
   }
 }
 
+constexpr size_t TC_DSMEM = (size_t)2 * (TC_M + TC_N) * TC_K * sizeof(float);
+
 int *g_tc_err = nullptr;   // device error flag (allocated once, host-visible through qc_tc_status)
 
 }  // namespace
@@ -237,8 +291,14 @@ extern "C" int qc_bgemm_tf32(const void *tasks, long long ntasks, int opspan, co
     if (cudaMalloc(&g_tc_err, sizeof(int)) != cudaSuccess) return QC_ERR_CUDA;
     cudaMemset(g_tc_err, 0, sizeof(int));
   }
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(k_bgemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_DSMEM) != cudaSuccess)
+      return QC_ERR_CUDA;
+    attr_set = true;
+  }
   dim3 grid((unsigned)ntasks, (unsigned)opspan);
-  k_bgemm_tc<<<grid, TC_THREADS, 0, (cudaStream_t)stream>>>((const qc_task *)tasks, (const qc_contrib *)contribs,
+  k_bgemm_tc<<<grid, TC_THREADS, TC_DSMEM, (cudaStream_t)stream>>>((const qc_task *)tasks, (const qc_contrib *)contribs,
                                                             (const qc_op *)ops, A, B, C, g_tc_err);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -141,45 +141,80 @@ def panel_sigma1(Ll, psi, t1, nblks_out):
             "gemm": (pan_off[lkp], psi.ioff[up], t1pan, Mj, Nj, Kj)}
 
 
-def compile_panels(gemm, tensor_cores=False):
-    """Work items {tile_cfg: (tasks, contribs, flops)} of dense panel GEMMs
-    C_j[M_j x N_j] = A_j[M_j x K_j] . B_j[K_j x N_j], all operands row-major."""
+PTASK_DT = numpy.dtype([("a_off", "<i8"), ("b_off", "<i8"), ("c_off", "<i8"), ("M", "<i4"), ("N", "<i4"),
+                        ("K", "<i4"), ("m0", "<i4"), ("n0", "<i4"), ("op_b", "<i4"), ("op_e", "<i4"),
+                        ("pad", "<i4", (3,))])
+assert PTASK_DT.itemsize == 64
+PANEL_TILES = {0: (128, 64), 1: (128, 32), 2: (128, 16)}
+
+
+def panel_class(N):
+    N = numpy.asarray(N)
+    return numpy.where(N > 32, 0, numpy.where(N > 16, 1, 2))
+
+
+def compile_panels(gemm, op_range):
+    """Work items {cfg: (ptasks, flops)} of dense panel GEMMs
+    C_j[M_j x N_j] = A_j[M_j x K_j] . B_j[K_j x N_j], all operands row-major (qc_pgemm_*)."""
     a_off, b_off, c_off, M, N, K = (numpy.asarray(x, dtype=numpy.int64) for x in gemm)
-    if tensor_cores:
-        cls = tile_class_tc(M, N, K)
-    else:
-        cls = tile_class(M, N)
+    cls = panel_class(N)
     out = {}
     for k in numpy.unique(cls):
         sel = numpy.flatnonzero(cls == k)
-        tm, tn = TILES[int(k)]
+        tm, tn = PANEL_TILES[int(k)]
         nm = (M[sel] + tm - 1) // tm
         nn = (N[sel] + tn - 1) // tn
         nt = nm * nn
         pid = numpy.repeat(numpy.arange(len(sel)), nt)
         loc = numpy.arange(int(nt.sum())) - numpy.repeat(numpy.cumsum(nt) - nt, nt)
         g = sel[pid]
-        tasks = numpy.zeros(len(g), TASK_DT)
-        tasks["c_off"] = c_off[g]
-        tasks["M"], tasks["N"] = M[g], N[g]
+        tasks = numpy.zeros(len(g), PTASK_DT)
+        tasks["a_off"], tasks["b_off"], tasks["c_off"] = a_off[g], b_off[g], c_off[g]
+        tasks["M"], tasks["N"], tasks["K"] = M[g], N[g], K[g]
         tasks["m0"] = (loc // nn[pid]) * tm
         tasks["n0"] = (loc % nn[pid]) * tn
-        tasks["mlo"], tasks["nlo"] = M[g], N[g]
-        tasks["c_ml"] = N[g]
-        tasks["c_nl"] = 1
-        tasks["cb"] = pid
-        tasks["ce"] = pid + 1
-        contribs = numpy.zeros(len(sel), CONTRIB_DT)
-        contribs["a_off"], contribs["b_off"] = a_off[sel], b_off[sel]
-        contribs["alpha"] = 1.0
-        contribs["K"] = contribs["klo"] = K[sel]
-        contribs["a_ml"] = K[sel]
-        contribs["a_kl"] = 1
-        contribs["b_kl"] = N[sel]
-        contribs["b_nl"] = 1
-        contribs["op_b"], contribs["op_e"] = 0, 1
-        out[int(k)] = (tasks, contribs, 2.0 * float((M[sel] * N[sel] * K[sel]).sum()))
+        tasks["op_b"], tasks["op_e"] = op_range
+        nop = op_range[1] - op_range[0]
+        out[int(k)] = (tasks, 2.0 * float((M[sel] * N[sel] * K[sel]).sum()) * nop)
     return out
+
+
+class PanelStage(object):
+    """Dense panel GEMMs of one contraction (qc_pgemm_*), one launch per tile class."""
+
+    def __init__(self, parts, device, name, ops):
+        """parts: {cfg: [(ptasks, flops), ...]}"""
+        self.name = name
+        self.host_ops = ops
+        self.d_ops = torch.from_numpy(ops.view(numpy.uint8).copy()).to(device)
+        self.groups = []
+        self.flops = 0.0
+        self.bytes = 0.0
+        self.ntasks = 0
+        for cfg in sorted(parts):
+            tk = numpy.concatenate([p[0] for p in parts[cfg]])
+            self.flops += sum(p[1] for p in parts[cfg])
+            if not len(tk):
+                continue
+            span = int(max(1, (tk["op_e"] - tk["op_b"]).max()))
+            self.groups.append((cfg, tk, torch.from_numpy(tk.view(numpy.uint8).copy()).to(device), span))
+            self.ntasks += len(tk)
+
+    def run(self, A, B, C, kind="f64", stream=None):
+        lib = native.lib()
+        s = stream if stream is not None else torch.cuda.current_stream(C.device).cuda_stream
+        fn = lib.qc_pgemm_f64 if kind == "f64" else lib.qc_pgemm_f32
+        if LOG.enabled:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+        for (cfg, tk, dt, span) in self.groups:
+            check(fn(dt.data_ptr(), len(tk), span, self.d_ops.data_ptr(), A.data_ptr(), B.data_ptr(), C.data_ptr(),
+                     cfg, s), "qc_pgemm_" + kind)
+            LOG.launches += 1
+        if LOG.enabled:
+            e1.record()
+            LOG.records.append((self.name, e0, e1, self.flops, self.bytes * (A.element_size() / 8.0)))
 
 
 def compile_template(l1, l2, lo, axes, triples, tile_cfg, off1=None):

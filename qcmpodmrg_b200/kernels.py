@@ -19,7 +19,7 @@ import torch
 from . import native
 from .native import check
 from .engine import (Stage, compile_classes, add_parts, live_blocks, prune, op_table, TASK_DT, CONTRIB_DT, LOG,
-                     compile_fiber, FiberStage, CompositeStage, panel_sigma1, compile_panels, BPERM_DT)
+                     compile_fiber, FiberStage, CompositeStage, panel_sigma1, compile_panels, BPERM_DT, PanelStage)
 from .mpo import case
 from .qtensor import Contraction, flip_right, flip_horizontal
 
@@ -223,6 +223,7 @@ class SigmaOperator(object):
         # every group fits in shared memory, generic grouped GEMM otherwise
         fiber_spec = {1: (0, 0), 2: (3, 1)}      # stage -> (rows axis of operand 1, fiber-major storage)
         lperm = []
+        pst = {}                        # panel GEMM parts of the L.psi contraction
         for key, (ops, *cs, Rl, fused, pan) in sorted(plans.items()):
             rng = (pos, pos + len(ops))
             pos += len(ops)
@@ -249,7 +250,8 @@ class SigmaOperator(object):
                 if fused is not None and si in (1, 2):
                     continue
                 if si == 0 and pan is not None:
-                    add_parts(st[0], compile_panels(pan["gemm"], tensor_cores=tc), op_range=rng)
+                    for cfg, part in compile_panels(pan["gemm"], rng).items():
+                        pst.setdefault(cfg, []).append(part)
                     continue
                 off1 = t1off if si == 1 else None
                 if use_fiber and si in fiber_spec:
@@ -266,6 +268,8 @@ class SigmaOperator(object):
         for si in range(4):
             g = Stage(st[si], dev, "sigma%d" % (si + 1), tabs[si]) if st[si] else None
             f = FiberStage(fib[si], dev, "sigma%d" % (si + 1), tabs[si]) if fib[si] else None
+            if si == 0 and pst:
+                f = PanelStage(pst, dev, "sigma1", tabs[0])
             if f is None:
                 self.stages.append(g if g is not None else Stage({}, dev, "sigma%d" % (si + 1), tabs[si]))
             else:

@@ -40,6 +40,26 @@ def patch_stage_run(monkeypatch):
 
     monkeypatch.setattr(engine.FiberStage, "run", frun)
 
+    def prun(self, A, B, C, kind="f64", stream=None):
+        a = A.detach().cpu().numpy().astype(numpy.float64)
+        b = B.detach().cpu().numpy().astype(numpy.float64)
+        c = C.detach().cpu().numpy().astype(numpy.float64)
+        for (cfg, tk, _, _) in self.groups:
+            tm, tn = engine.PANEL_TILES[cfg]
+            for t in tk:
+                for op in range(t["op_b"], t["op_e"]):
+                    o = self.host_ops[op]
+                    M, N, K = int(t["M"]), int(t["N"]), int(t["K"])
+                    Am = a[o["a_base"] + t["a_off"]:][:M * K].reshape(M, K)
+                    Bm = b[o["b_base"] + t["b_off"]:][:K * N].reshape(K, N)
+                    m1, n1 = min(M, t["m0"] + tm), min(N, t["n0"] + tn)
+                    blk = o["alpha"] * (Am[t["m0"]:m1] @ Bm[:, t["n0"]:n1])
+                    cm = c[o["c_base"] + t["c_off"]:][:M * N].reshape(M, N)
+                    cm[t["m0"]:m1, t["n0"]:n1] = blk
+        C.copy_(torch.from_numpy(c).to(C.dtype))
+
+    monkeypatch.setattr(engine.PanelStage, "run", prun)
+
     def block_permute(descs, ndescs, opspan, ops, src, dst):
         d = descs.cpu().numpy().view(engine.BPERM_DT)
         o = ops.cpu().numpy().view(engine.OP_DT)
