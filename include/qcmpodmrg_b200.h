@@ -147,8 +147,9 @@ int qc_tc_status(void);
  *   C[c_base + c_off + (f/flo)*fhs + (f%flo)*ncols + c]
  *       = alpha * sum_pairs sum_r in[srow+r][f] * W[b_base + w_off + r*ncols + c]
  * (an empty pair range writes zeros)
- * with pairs fpair[pair_b..pair_e) (qc_fpair, 16 B).  max_rows >= the staged rows
- * of every task (shared memory max_rows*32*sizeof(T), at most 200 KiB).
+ * with pairs fpair[pair_b..pair_e) (qc_fpair, 16 B).  fiber_tile (32 or 64) is
+ * the number of fibers per task (the tasks' f0 step); max_rows >= the staged rows
+ * of every task (shared memory max_rows*fiber_tile*sizeof(T), at most 200 KiB).
  * Null A/W/C with absolute element addresses in ops is allowed. */
 /* Per-dot operand repack: for every descriptor (qc_bperm, 64 B) and operator
  * o in [op_b, op_e) (grid.y, at most opspan), copies the block stored row-major
@@ -162,10 +163,10 @@ int qc_block_permute(const void *descs_dev, long long ndescs, int opspan, const 
 
 int qc_fiber_f64(const void *tasks_dev, long long ntasks, int opspan, const void *fin_dev,
                  const void *fout_dev, const void *fpair_dev, const void *ops_dev, int max_rows,
-                 const double *A, const double *W, double *C, void *stream);
+                 int fiber_tile, const double *A, const double *W, double *C, void *stream);
 int qc_fiber_f32(const void *tasks_dev, long long ntasks, int opspan, const void *fin_dev,
                  const void *fout_dev, const void *fpair_dev, const void *ops_dev, int max_rows,
-                 const float *A, const float *W, float *C, void *stream);
+                 int fiber_tile, const float *A, const float *W, float *C, void *stream);
 
 /* dst[i] = src[idx[i]] (FP64), i < n.  Used for diag[prjmap] (kernelQt.py:122). */
 int qc_gather_f64(const double *src, const long long *idx, double *dst, long long n, void *stream);

@@ -83,7 +83,7 @@ class BatchedSigma(object):
                 for sub in (st.subs if isinstance(st, CompositeStage) else [st]):
                     if isinstance(sub, FiberStage):
                         if sub.ntasks:
-                            fibers.setdefault(si, []).append((sub, base))
+                            fibers.setdefault((si, sub.tile), []).append((sub, base))
                         continue
                     if isinstance(sub, PanelStage):
                         for (cfg, tk, _, _) in sub.groups:
@@ -118,7 +118,7 @@ class BatchedSigma(object):
         # fiber-group work items of all instances, one launch per W contraction
         up = lambda a: torch.from_numpy(a.view(numpy.uint8).copy()).to(device)
         self.fiber_launches = []
-        for si, parts in sorted(fibers.items()):
+        for (si, tile), parts in sorted(fibers.items()):
             tks, fis, fos, fps = [], [], [], []
             nin = nout = npair = 0
             mr = 1
@@ -143,7 +143,7 @@ class BatchedSigma(object):
                 mr = max(mr, sub.max_rows)
             tk = numpy.concatenate(tks)
             span = int(max(1, (tk["op_e"] - tk["op_b"]).max()))
-            self.fiber_launches.append((si, len(tk), span, mr, up(tk), up(numpy.concatenate(fis)),
+            self.fiber_launches.append((si, len(tk), span, mr, tile, up(tk), up(numpy.concatenate(fis)),
                                         up(numpy.concatenate(fos)), up(numpy.concatenate(fps))))
         self.panel_launches = []
         for (si, cfg), tks in sorted(panels.items()):
@@ -165,11 +165,11 @@ class BatchedSigma(object):
                 check(pfn(dt.data_ptr(), nt, span, self.d_ops[si].data_ptr(), None, None, None, cfg, s),
                       "batched qc_pgemm")
                 LOG.launches += 1
-            for (si, nt, span, mr, dt, dfi, dfo, dfp) in self.fiber_launches:
+            for (si, nt, span, mr, tile, dt, dfi, dfo, dfp) in self.fiber_launches:
                 if si != stage:
                     continue
                 check(ffn(dt.data_ptr(), nt, span, dfi.data_ptr(), dfo.data_ptr(), dfp.data_ptr(),
-                          self.d_ops[si].data_ptr(), mr, None, None, None, s), "batched qc_fiber")
+                          self.d_ops[si].data_ptr(), mr, tile, None, None, None, s), "batched qc_fiber")
                 LOG.launches += 1
             for (si, cfg, nt, span, dt, dc) in self.launches:
                 if si != stage:

@@ -15,20 +15,21 @@
 
 namespace {
 
-constexpr int FT = 32;          // fibers per tile (one warp lane per fiber)
 constexpr int FT_THREADS = 256;
 constexpr int CB = 8;           // output columns per warp work item (register accumulators)
 
-// One CTA = one tile of FT fibers of one fiber group, for one operator (grid.y).
-// Phase 1 stages every input row of the group for those fibers in shared memory.
-// Phase 2: each warp takes (output block, 8-column block) items; lane = fiber,
-// 8 accumulators per lane, W elements are warp-uniform (broadcast) loads, so
-// every W value read serves 32 fibers and every staged input value 8 columns.
-template <typename T>
+// One CTA = one tile of FT = 32*FPL fibers of one fiber group, for one operator
+// (grid.y).  Phase 1 stages every input row of the group for those fibers in
+// shared memory.  Phase 2: each warp takes (output block, 8-column block)
+// items; lane l owns fibers l, l+32, ... (FPL of them) with 8 accumulators each;
+// W elements are warp-uniform (broadcast) loads, so every W value read serves
+// 32*FPL fibers and every staged input value 8 columns.
+template <typename T, int FPL>
 __global__ void __launch_bounds__(FT_THREADS)
 k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, const qc_fout *__restrict__ fout,
         const qc_fpair *__restrict__ fpair, const qc_op *__restrict__ ops, const T *__restrict__ A,
         const T *__restrict__ W, T *__restrict__ C) {
+  constexpr int FT = 32 * FPL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *As = reinterpret_cast<T *>(smem_raw);
   const qc_ftask t = tasks[blockIdx.x];
@@ -60,7 +61,6 @@ k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, cons
   T *Cb = C + o.c_base;
   const int lane = tid & 31, warp = tid >> 5;
   constexpr int NW = FT_THREADS / 32;
-  const int fg = t.f0 + lane;
   // items: (output block j, column block cb), enumerated block by block
   int j = t.out_b, cb = 0, skip = warp;
   while (j < t.out_e) {
@@ -76,35 +76,55 @@ k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, cons
     const int nc = ob.ncols;
     const int c0 = cb * CB;
     const int nb = min(CB, nc - c0);
-    T acc[CB];
+    T acc[FPL][CB];
 #pragma unroll
-    for (int i = 0; i < CB; ++i) acc[i] = T(0);
+    for (int q = 0; q < FPL; ++q)
+#pragma unroll
+      for (int i = 0; i < CB; ++i) acc[q][i] = T(0);
     for (int p = ob.pair_b; p < ob.pair_e; ++p) {
       const qc_fpair pr = fpair[p];
       const T *w = Wb + pr.w_off + c0;
       const T *a = As + pr.srow * FT + lane;
       if (nb == CB) {
+#pragma unroll 2
         for (int r = 0; r < pr.rows; ++r) {
-          const T av = a[r * FT];
+          T av[FPL];
+#pragma unroll
+          for (int q = 0; q < FPL; ++q) av[q] = a[r * FT + 32 * q];
           const T *wr = w + (long long)r * nc;
 #pragma unroll
-          for (int i = 0; i < CB; ++i) acc[i] = fma(av, __ldg(wr + i), acc[i]);
+          for (int i = 0; i < CB; ++i) {
+            const T wv = __ldg(wr + i);
+#pragma unroll
+            for (int q = 0; q < FPL; ++q) acc[q][i] = fma(av[q], wv, acc[q][i]);
+          }
         }
       } else {
         for (int r = 0; r < pr.rows; ++r) {
-          const T av = a[r * FT];
+          T av[FPL];
+#pragma unroll
+          for (int q = 0; q < FPL; ++q) av[q] = a[r * FT + 32 * q];
           const T *wr = w + (long long)r * nc;
 #pragma unroll
           for (int i = 0; i < CB; ++i)
-            if (i < nb) acc[i] = fma(av, __ldg(wr + i), acc[i]);
+            if (i < nb) {
+              const T wv = __ldg(wr + i);
+#pragma unroll
+              for (int q = 0; q < FPL; ++q) acc[q][i] = fma(av[q], wv, acc[q][i]);
+            }
         }
       }
     }
-    if (lane < nf) {
-      T *dst = Cb + ob.c_off + (long long)(fg / ob.flo) * ob.fhs + (long long)(fg % ob.flo) * nc + c0;
 #pragma unroll
-      for (int i = 0; i < CB; ++i)
-        if (i < nb) dst[i] = alpha * acc[i];
+    for (int q = 0; q < FPL; ++q) {
+      const int fl = lane + 32 * q;
+      if (fl < nf) {
+        const int fg = t.f0 + fl;
+        T *dst = Cb + ob.c_off + (long long)(fg / ob.flo) * ob.fhs + (long long)(fg % ob.flo) * nc + c0;
+#pragma unroll
+        for (int i = 0; i < CB; ++i)
+          if (i < nb) dst[i] = alpha * acc[q][i];
+      }
     }
     // advance NW items
     int adv = NW;
@@ -141,17 +161,24 @@ k_block_permute(const qc_bperm *__restrict__ descs, const qc_op *__restrict__ op
 
 template <typename T>
 int launch_fiber(const void *tasks, long long ntasks, int opspan, const void *fin, const void *fout,
-                 const void *fpair, const void *ops, int max_rows, const T *A, const T *W, T *C,
+                 const void *fpair, const void *ops, int max_rows, int fiber_tile, const T *A, const T *W, T *C,
                  cudaStream_t s) {
   if (ntasks <= 0) return QC_OK;
   if (ntasks > 0x7fffffffLL || opspan < 1 || opspan > 65535 || max_rows < 1) return QC_ERR_ARG;
-  const size_t smem = (size_t)max_rows * FT * sizeof(T);
+  if (fiber_tile != 32 && fiber_tile != 64) return QC_ERR_ARG;
+  const size_t smem = (size_t)max_rows * fiber_tile * sizeof(T);
   if (smem > 200 * 1024) return QC_ERR_ARG;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_fiber<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid((unsigned)ntasks, (unsigned)opspan);
-  k_fiber<T><<<grid, FT_THREADS, smem, s>>>((const qc_ftask *)tasks, (const qc_fin *)fin, (const qc_fout *)fout,
-                                            (const qc_fpair *)fpair, (const qc_op *)ops, A, W, C);
+  const qc_ftask *tk = (const qc_ftask *)tasks;
+  if (fiber_tile == 32) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_fiber<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fiber<T, 1><<<grid, FT_THREADS, smem, s>>>(tk, (const qc_fin *)fin, (const qc_fout *)fout,
+                                                 (const qc_fpair *)fpair, (const qc_op *)ops, A, W, C);
+  } else {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_fiber<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fiber<T, 2><<<grid, FT_THREADS, smem, s>>>(tk, (const qc_fin *)fin, (const qc_fout *)fout,
+                                                 (const qc_fpair *)fpair, (const qc_op *)ops, A, W, C);
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     fprintf(stderr, "[qcgpu] qc_fiber: %s\n", cudaGetErrorString(e));
@@ -181,13 +208,15 @@ extern "C" int qc_block_permute(const void *descs, long long ndescs, int opspan,
 }
 
 extern "C" int qc_fiber_f64(const void *tasks, long long ntasks, int opspan, const void *fin, const void *fout,
-                            const void *fpair, const void *ops, int max_rows, const double *A, const double *W,
-                            double *C, void *stream) {
-  return launch_fiber<double>(tasks, ntasks, opspan, fin, fout, fpair, ops, max_rows, A, W, C, (cudaStream_t)stream);
+                            const void *fpair, const void *ops, int max_rows, int fiber_tile, const double *A,
+                            const double *W, double *C, void *stream) {
+  return launch_fiber<double>(tasks, ntasks, opspan, fin, fout, fpair, ops, max_rows, fiber_tile, A, W, C,
+                              (cudaStream_t)stream);
 }
 
 extern "C" int qc_fiber_f32(const void *tasks, long long ntasks, int opspan, const void *fin, const void *fout,
-                            const void *fpair, const void *ops, int max_rows, const float *A, const float *W,
-                            float *C, void *stream) {
-  return launch_fiber<float>(tasks, ntasks, opspan, fin, fout, fpair, ops, max_rows, A, W, C, (cudaStream_t)stream);
+                            const void *fpair, const void *ops, int max_rows, int fiber_tile, const float *A,
+                            const float *W, float *C, void *stream) {
+  return launch_fiber<float>(tasks, ntasks, opspan, fin, fout, fpair, ops, max_rows, fiber_tile, A, W, C,
+                             (cudaStream_t)stream);
 }

@@ -411,6 +411,7 @@ assert BPERM_DT.itemsize == 64
 FPAIR_DT = numpy.dtype([("w_off", "<i8"), ("srow", "<i4"), ("rows", "<i4")])
 assert FTASK_DT.itemsize == 32 and FIN_DT.itemsize == 32 and FOUT_DT.itemsize == 32 and FPAIR_DT.itemsize == 16
 FIBER_TILE = 32
+FIBER_ROWS_WIDE = 128     # staged rows up to which a tile holds 64 fibers (two per lane)
 FIBER_MAX_ROWS = 256
 
 
@@ -426,7 +427,7 @@ def compile_fiber(c, triples, rows_axis, fiber_major, extra_out=None, in_off=Non
     extra_out (output blocks without pairs, written as zeros).
     """
     empty = (numpy.zeros(0, FTASK_DT), numpy.zeros(0, FIN_DT), numpy.zeros(0, FOUT_DT), numpy.zeros(0, FPAIR_DT), 1,
-             0.0)
+             0.0, FIBER_TILE)
     out, l1, l2 = c.out, c.l1, c.l2
     if out.rank != 5:
         return None
@@ -500,28 +501,33 @@ def compile_fiber(c, triples, rows_axis, fiber_major, extra_out=None, in_off=Non
     pairs["w_off"] = l2.ioff[i2]
     pairs["srow"] = u_srow[inv_k] if len(inv_k) else 0
     pairs["rows"] = rows
-    nt = (gF + FIBER_TILE - 1) // FIBER_TILE
+    mr = int(max(1, R.max() if len(R) else 1))
+    tile = 64 if mr <= FIBER_ROWS_WIDE else FIBER_TILE      # two fibers per lane where rows allow
+    nt = (gF + tile - 1) // tile
     gt = numpy.repeat(numpy.arange(ng), nt)
     tasks = numpy.zeros(len(gt), FTASK_DT)
-    tasks["f0"] = (numpy.arange(len(gt)) - numpy.repeat(numpy.cumsum(nt) - nt, nt)) * FIBER_TILE
+    tasks["f0"] = (numpy.arange(len(gt)) - numpy.repeat(numpy.cumsum(nt) - nt, nt)) * tile
     tasks["F"] = gF[gt]
     tasks["in_b"], tasks["in_e"] = gin_b[gt], gin_e[gt]
     tasks["out_b"], tasks["out_e"] = gout_b[gt], gout_e[gt]
     dO_p = out.block_dims(ob) if len(ob) else numpy.zeros((0, 5), dtype=numpy.int64)
     flops = 2.0 * float((dO_p[:, 0] * dO_p[:, 1] * dO_p[:, 2] * dO_p[:, 3] * dO_p[:, 4] * rows).sum())
-    return tasks, fins, fouts, pairs, int(max(1, R.max() if len(R) else 1)), flops
+    return tasks, fins, fouts, pairs, mr, flops, tile
 
 
 class FiberStage(object):
     """Fiber-group work items of several symmetry classes, resident on the device."""
 
     def __init__(self, parts, device, name, ops):
-        """parts: list of (tasks, fin, fout, fpair, max_rows, flops, op_range)."""
+        """parts: list of (tasks, fin, fout, fpair, max_rows, flops, fiber_tile, op_range), one fiber tile."""
         tks, fis, fos, fps = [], [], [], []
         nin = nout = npair = 0
         self.max_rows = 1
         self.flops = 0.0
-        for (tk, fi, fo, fp, mr, fl, rng) in parts:
+        tiles = set(p[6] for p in parts)
+        assert len(tiles) <= 1, "one fiber tile per stage"
+        self.tile = tiles.pop() if tiles else FIBER_TILE
+        for (tk, fi, fo, fp, mr, fl, _, rng) in parts:
             tk = tk.copy()
             fo = fo.copy()
             tk["in_b"] += nin
@@ -562,7 +568,7 @@ class FiberStage(object):
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
         check(fn(self.d[0].data_ptr(), self.ntasks, self.span, self.d[1].data_ptr(), self.d[2].data_ptr(),
-                 self.d[3].data_ptr(), self.d[4].data_ptr(), self.max_rows, A.data_ptr(), B.data_ptr(),
+                 self.d[3].data_ptr(), self.d[4].data_ptr(), self.max_rows, self.tile, A.data_ptr(), B.data_ptr(),
                  C.data_ptr(), s), "qc_fiber_" + kind)
         LOG.launches += 1
         if LOG.enabled:
@@ -627,3 +633,11 @@ def prune(triples, live1=None, live2=None):
     if live2 is not None and len(triples):
         keep &= live2[triples[:, 2]]
     return triples[keep]
+
+
+def fiber_stages(parts, device, name, ops):
+    """FiberStage per fiber tile (parts compiled with 32- and 64-fiber tiles)."""
+    by = {}
+    for p in parts:
+        by.setdefault(p[6], []).append(p)
+    return [FiberStage(v, device, name, ops) for k, v in sorted(by.items())]

@@ -19,7 +19,8 @@ import torch
 from . import native
 from .native import check
 from .engine import (Stage, compile_classes, add_parts, live_blocks, prune, op_table, TASK_DT, CONTRIB_DT, LOG,
-                     compile_fiber, FiberStage, CompositeStage, panel_sigma1, compile_panels, BPERM_DT, PanelStage)
+                     compile_fiber, FiberStage, CompositeStage, panel_sigma1, compile_panels, BPERM_DT, PanelStage,
+                     fiber_stages)
 from .mpo import case
 from .qtensor import Contraction, flip_right, flip_horizontal
 
@@ -267,13 +268,13 @@ class SigmaOperator(object):
         self.stages = []
         for si in range(4):
             g = Stage(st[si], dev, "sigma%d" % (si + 1), tabs[si]) if st[si] else None
-            f = FiberStage(fib[si], dev, "sigma%d" % (si + 1), tabs[si]) if fib[si] else None
+            f = fiber_stages(fib[si], dev, "sigma%d" % (si + 1), tabs[si]) if fib[si] else []
             if si == 0 and pst:
-                f = PanelStage(pst, dev, "sigma1", tabs[0])
-            if f is None:
+                f = [PanelStage(pst, dev, "sigma1", tabs[0])]
+            if not f:
                 self.stages.append(g if g is not None else Stage({}, dev, "sigma%d" % (si + 1), tabs[si]))
             else:
-                self.stages.append(CompositeStage([f, g], "sigma%d" % (si + 1)))
+                self.stages.append(CompositeStage(f + [g], "sigma%d" % (si + 1)))
         # per-dot L panels (a block permutation of every operator's L), FP64 and FP32
         self.lperm = None
         if lperm:
@@ -288,7 +289,7 @@ class SigmaOperator(object):
         self.wtot = wtot
         if fuse_parts:
             ftab = op_table(bases[0][order], wbase[order], bases[2][order], 1.0)
-            self.fused = FiberStage(fuse_parts, dev, "sigma23", ftab)
+            self.fused = CompositeStage(fiber_stages(fuse_parts, dev, "sigma23", ftab), "sigma23")
             wst = Stage(wij_parts, dev, "wij", op_table(Wi.offsets[order], Wj.offsets[order], wbase[order], 1.0))
             self.Wij = torch.zeros(max(wtot, 1), dtype=torch.float64, device=dev)
             wst.run(Wi.values, Wj.values, self.Wij, "f64")

@@ -53,8 +53,8 @@ _SIGS = {
     "qc_pgemm_f64": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_vp]),
     "qc_pgemm_f32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_vp]),
     "qc_block_permute": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
-    "qc_fiber_f64": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_vp]),
-    "qc_fiber_f32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_vp]),
+    "qc_fiber_f64": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
+    "qc_fiber_f32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
     "qc_mlp_forward": (c_int, [c_int, c_int] + [c_vp] * 10 + [c_vp]),
     "qc_mlp_backward": (c_int, [c_int, c_int] + [c_vp] * 12 + [c_vp]),
     "qc_adam_step": (c_int, [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,

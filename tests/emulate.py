@@ -98,7 +98,7 @@ def patch_stage_run(monkeypatch):
 
 def _run_fiber(st, A, W, C):
     """Reference semantics of k_fiber: out[f, c] = alpha * sum_pairs sum_r in[r, f] * W[r, c]."""
-    FT = 32
+    FT = st.tile
     for t in st.h_tasks:
         nf = min(FT, t["F"] - t["f0"])
         for op in range(t["op_b"], t["op_e"]):
