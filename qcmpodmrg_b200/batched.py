@@ -62,7 +62,7 @@ class BatchedSigma(object):
         nops_acc = [0, 0, 0, 0, 0]
         for i, s in enumerate(items):
             L = s.a1("f64" if kind == "f64" else "f32")      # L panels of the L.psi contraction
-            R = s.R.values if kind == "f64" else s.R.f32()
+            R = s.b4("f64" if kind == "f64" else "f32")      # R panels of the .R contraction
             Wi = s.Wi.values if kind == "f64" else s.Wi.f32()
             Wj = s.Wj.values if kind == "f64" else s.Wj.f32()
             T1 = self.T[0][int(offs[i, 0]):]

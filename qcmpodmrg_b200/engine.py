@@ -141,6 +141,74 @@ def panel_sigma1(Ll, psi, t1, nblks_out):
             "gemm": (pan_off[lkp], psi.ioff[up], t1pan, Mj, Nj, Kj)}
 
 
+def panel_sigma4(t3lay, Rl, psi, t4):
+    """Panel form of the .R contraction (HVecQt top4, kernelQt.py:306-316).
+
+    sigma block s = (l, n1', n2', r') receives T3 blocks (l, r, n1', c, n2') times
+    R blocks (c, r', r) over the MPO sectors c (r follows from c and r').  T3
+    blocks of one sigma block are stored as the column slabs of one row-major
+    panel [D_l x K_s] (columns (c, r, c) in the R block order), and the R blocks of
+    one sector r' as one row-major panel [K_r' x D_r'] (a per-dot permutation of
+    R with the (c, r) rows transposed), so each sigma block is one dense GEMM per
+    operator.  Returns None unless every sigma block pairs with all R blocks of
+    its sector r' (the full product the layout allows).
+    """
+    if len(t4) == 0:
+        return None
+    so, i3, iR = t4[:, 0], t4[:, 1], t4[:, 2]
+    if len(numpy.unique(i3)) != len(i3):
+        return None
+    secR = Rl.block_sectors(iR)
+    cR, rbR = secR[0], secR[1]
+    o = numpy.lexsort((cR, so))
+    so, i3, iR, cR, rbR = so[o], i3[o], iR[o], cR[o], rbR[o]
+    dR = Rl.block_dims(iR)                   # (Dc, Drb, Dr)
+    kb = dR[:, 0] * dR[:, 2]                 # K extent of the pair
+    # R panels per r' sector: all R blocks of the sector, ordered by c
+    uR = numpy.unique(iR)
+    sR = Rl.block_sectors(uR)
+    oR = numpy.lexsort((sR[0], sR[1]))
+    uR = uR[oR]
+    cU, rbU = sR[0][oR], sR[1][oR]
+    dU = Rl.block_dims(uR)
+    kU = dU[:, 0] * dU[:, 2]
+    nrb = int(Rl.nsyms[1])
+    Krb = numpy.bincount(rbU, weights=kU, minlength=nrb).astype(numpy.int64)
+    Drb_sec = numpy.zeros(nrb, dtype=numpy.int64)
+    Drb_sec[rbU] = dU[:, 1]
+    start = numpy.searchsorted(rbU, numpy.arange(nrb))
+    ck = numpy.cumsum(kU) - kU
+    koffU = ck - ck[numpy.minimum(start[rbU], len(ck) - 1)]
+    psz = Krb * Drb_sec
+    poff = numpy.cumsum(psz) - psz
+    # every sigma block uses all R blocks of its sector, in the same order
+    us, first = numpy.unique(so, return_index=True)
+    rb_s = rbR[first]
+    cnt = numpy.diff(numpy.r_[first, len(so)])
+    if not numpy.array_equal(cnt, numpy.bincount(rbU, minlength=nrb)[rb_s]):
+        return None
+    posU = numpy.empty(int(Rl.nblks), dtype=numpy.int64)
+    posU[uR] = numpy.arange(len(uR))
+    ckb = numpy.cumsum(kb) - kb
+    if numpy.any(koffU[posU[iR]] != ckb - numpy.repeat(ckb[first], cnt)):
+        return None
+    dS = psi.block_dims(us)
+    Dl = dS[:, 0] * dS[:, 1] * dS[:, 2]
+    Ks = Krb[rb_s]
+    tsz = Dl * Ks
+    t3pan = numpy.cumsum(tsz) - tsz
+    sidx = numpy.repeat(numpy.arange(len(us)), cnt)
+    t3off = numpy.zeros(int(t3lay.nblks), dtype=numpy.int64)
+    t3fhs = numpy.zeros(int(t3lay.nblks), dtype=numpy.int64)
+    t3flo = numpy.ones(int(t3lay.nblks), dtype=numpy.int64)
+    t3off[i3] = t3pan[sidx] + koffU[posU[iR]]
+    t3fhs[i3] = Ks[sidx]
+    t3flo[i3] = dR[:, 2]                     # fibers (l, r): r is the fast fiber index
+    rperm = (Rl.ioff[uR], poff[rbU] + koffU * dU[:, 1], dU)
+    return {"t3off": t3off, "t3fhs": t3fhs, "t3flo": t3flo, "t3size": int(tsz.sum()), "needed": i3,
+            "rperm": rperm, "gemm": (t3pan, poff[rb_s], psi.ioff[us], Dl, Drb_sec[rb_s], Ks)}
+
+
 PTASK_DT = numpy.dtype([("a_off", "<i8"), ("b_off", "<i8"), ("c_off", "<i8"), ("M", "<i4"), ("N", "<i4"),
                         ("K", "<i4"), ("m0", "<i4"), ("n0", "<i4"), ("op_b", "<i4"), ("op_e", "<i4"),
                         ("pad", "<i4", (3,))])
@@ -424,7 +492,8 @@ def compile_fiber(c, triples, rows_axis, fiber_major, extra_out=None, in_off=Non
     group needs more than FIBER_MAX_ROWS staged rows.  Optional overrides:
     in_off / out_off (block offsets by flat block index, instead of the packed
     layouts' ioff), out_fhs / out_flo (two-level fiber strides of output blocks),
-    extra_out (output blocks without pairs, written as zeros).
+    extra_out (output blocks that must be written: those without pairs are
+    written as zeros; with out_off, pairs into any other output block are dropped).
     """
     empty = (numpy.zeros(0, FTASK_DT), numpy.zeros(0, FIN_DT), numpy.zeros(0, FOUT_DT), numpy.zeros(0, FPAIR_DT), 1,
              0.0, FIBER_TILE)
@@ -432,6 +501,11 @@ def compile_fiber(c, triples, rows_axis, fiber_major, extra_out=None, in_off=Non
     if out.rank != 5:
         return None
     tri = numpy.asarray(triples, dtype=numpy.int64).reshape(-1, 3)
+    if out_off is not None and extra_out is not None:
+        # output blocks with a remapped location: only the listed ones exist
+        need = numpy.zeros(out.nblks, dtype=bool)
+        need[numpy.asarray(extra_out, dtype=numpy.int64)] = True
+        tri = tri[need[tri[:, 0]]]
     if extra_out is not None and len(extra_out):
         have = numpy.zeros(out.nblks, dtype=bool)
         have[tri[:, 0]] = True

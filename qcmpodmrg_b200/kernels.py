@@ -20,7 +20,7 @@ from . import native
 from .native import check
 from .engine import (Stage, compile_classes, add_parts, live_blocks, prune, op_table, TASK_DT, CONTRIB_DT, LOG,
                      compile_fiber, FiberStage, CompositeStage, panel_sigma1, compile_panels, BPERM_DT, PanelStage,
-                     fiber_stages)
+                     fiber_stages, panel_sigma4)
 from .mpo import case
 from .qtensor import Contraction, flip_right, flip_horizontal
 
@@ -143,7 +143,7 @@ class SigmaOperator(object):
     """sigma = sum_p w_p R_p W_p[i+1] W_p[i] L_p psi for the dot (isite, isite+1)."""
 
     def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts, precision="f64",
-                 tensor_cores=None, use_fiber=False, fuse_w=True, panel1=True):
+                 tensor_cores=None, use_fiber=False, fuse_w=True, panel1=True, panel4=True):
         self.ws, self.psi, self.precision = ws, psi_layout, precision
         # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 mode
         tc = (precision == "tf32") if tensor_cores is None else tensor_cores
@@ -178,24 +178,36 @@ class SigmaOperator(object):
             # .W_i and .W_{i+1} fused: T3 = T1 . (W_i W_{i+1}) with the two-site MPO
             # block Wij[a, n1', n1, c, n2', n2] = sum_b W_i[a, b, n1', n1] W_{i+1}[b, c, n2', n2]
             # made once per dot, so T2 is never written (fiber-group kernel only)
+            c4 = Contraction(c3.out, Rl, ax[3])
+            # .R as dense panel GEMMs (T3 blocks written into sigma-block panels by the
+            # fiber kernel, R blocks permuted into per-sector panels once per dot)
+            pan4 = panel_sigma4(c3.out, Rl, psi_layout, c4.triples) if (use_fiber and panel4) else None
+            o3 = {} if pan4 is None else {"out_off": pan4["t3off"], "out_fhs": pan4["t3fhs"],
+                                          "out_flo": pan4["t3flo"], "extra_out": pan4["needed"]}
             fused = None
+            fib3 = None
             if use_fiber and fuse_w:
                 cW = Contraction(W1, W2, ([1], [0]))
                 cF = Contraction(c1.out, cW.out, ([0, 2, 3], [0, 2, 5]))
                 if cF.out is c3.out:
                     tF = prune(cF.triples, live1=live_blocks(c1.out, t1), live2=live_blocks(cW.out, cW.triples))
-                    fp = compile_fiber(cF, tF, 0, 0, in_off=t1off)
+                    fp = compile_fiber(cF, tF, 0, 0, in_off=t1off, **o3)
                     if fp is not None:
                         fused = (cW, cF, tF, fp)
-            c4 = Contraction(c3.out, Rl, ax[3])
+            elif use_fiber and pan4 is not None:
+                fib3 = compile_fiber(c3, t3, 3, 1, **o3)
+            if pan4 is not None and fused is None and fib3 is None:
+                pan4 = None                 # T3 comes from the grouped GEMM in the packed layout
             t4 = prune(c4.triples, live1=live_blocks(c3.out, fused[2] if fused else t3))
             if c4.out is not psi_layout:
                 raise ValueError("sigma output layout differs from the wavefunction template")
-            plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3), (c4, t4), Rl, fused, pan)
+            plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3), (c4, t4), Rl, fused, pan, pan4, fib3)
             for s, c in enumerate((c1, c2, c3)):
                 if s == 1 and fused is not None:
                     continue            # no T2 for fused classes
                 size = pan["t1size"] if (s == 0 and pan is not None) else c.out.size
+                if s == 2 and pan4 is not None:
+                    size = pan4["t3size"]
                 for i in ops:
                     bases[s][i] = tot[s]
                     tot[s] += size
@@ -225,7 +237,10 @@ class SigmaOperator(object):
         fiber_spec = {1: (0, 0), 2: (3, 1)}      # stage -> (rows axis of operand 1, fiber-major storage)
         lperm = []
         pst = {}                        # panel GEMM parts of the L.psi contraction
-        for key, (ops, *cs, Rl, fused, pan) in sorted(plans.items()):
+        rperm = []
+        p4st = {}                       # panel GEMM parts of the .R contraction
+        any4 = any(v[8] is not None for v in plans.values())
+        for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
             rng = (pos, pos + len(ops))
             pos += len(ops)
             t1off = pan["t1off"] if pan is not None else None
@@ -242,6 +257,28 @@ class SigmaOperator(object):
                 d["s2"] = 1
                 d["op_b"], d["op_e"] = rng
                 lperm.append(d)
+            if any4:
+                d = numpy.zeros(0, BPERM_DT)
+                if pan4 is not None:
+                    src, dst, dU = pan4["rperm"]
+                    d = numpy.zeros(len(src), BPERM_DT)
+                    d["src_off"], d["dst_off"] = src, dst
+                    d["d0"], d["d1"], d["d2"] = dU[:, 0], dU[:, 1], dU[:, 2]
+                    d["s0"], d["s1"], d["s2"] = dU[:, 1], 1, dU[:, 0] * dU[:, 1]
+                else:                       # R blocks copied in place
+                    src = dst = Rl.ioff[Rl.idx_allowed]
+                    d = numpy.zeros(len(src), BPERM_DT)
+                    d["src_off"], d["dst_off"] = src, dst
+                    d["d0"], d["d1"], d["d2"] = 1, 1, Rl.ndim[Rl.idx_allowed]
+                    d["s2"] = 1
+                d["op_b"], d["op_e"] = rng
+                rperm.append(d)
+            if pan4 is not None:
+                for cfg, part in compile_panels(pan4["gemm"], rng).items():
+                    p4st.setdefault(cfg, []).append(part)
+            if fib3 is not None:
+                fib[2].append(fib3 + (rng,))
+                self.w_paths["fiber"] += 1
             if fused is not None:
                 cW, cF, tF, fp = fused
                 fuse_parts.append(fp + (rng,))
@@ -249,6 +286,8 @@ class SigmaOperator(object):
                 add_parts(wij_parts, compile_classes(cW, cW.triples, ([1], [0])), op_range=rng)
             for si, (c, t) in enumerate(cs):
                 if fused is not None and si in (1, 2):
+                    continue
+                if (si == 2 and fib3 is not None) or (si == 3 and pan4 is not None):
                     continue
                 if si == 0 and pan is not None:
                     for cfg, part in compile_panels(pan["gemm"], rng).items():
@@ -271,6 +310,8 @@ class SigmaOperator(object):
             f = fiber_stages(fib[si], dev, "sigma%d" % (si + 1), tabs[si]) if fib[si] else []
             if si == 0 and pst:
                 f = [PanelStage(pst, dev, "sigma1", tabs[0])]
+            if si == 3 and p4st:
+                f = [PanelStage(p4st, dev, "sigma4", tabs[3])]
             if not f:
                 self.stages.append(g if g is not None else Stage({}, dev, "sigma%d" % (si + 1), tabs[si]))
             else:
@@ -284,6 +325,15 @@ class SigmaOperator(object):
             self._lperm_ops_d = torch.from_numpy(self._lperm_ops.view(numpy.uint8).copy()).to(dev)
             self._lperm_span = int(max(len(v[0]) for v in plans.values()))
             self._build_lpan()
+        # per-dot R panels (every operator's R blocks permuted), FP64 and FP32
+        self.rperm = None
+        if rperm:
+            self._rperm_h = numpy.concatenate(rperm)
+            self.rperm = torch.from_numpy(self._rperm_h.view(numpy.uint8).copy()).to(dev)
+            rops = op_table(R.offsets[order], 0, R.offsets[order], 1.0)
+            self._rperm_ops_d = torch.from_numpy(rops.view(numpy.uint8).copy()).to(dev)
+            self._rperm_span = int(max(len(v[0]) for v in plans.values()))
+            self._build_rpan()
         # fused W stage (T1 -> T3) and the per-dot two-site MPO blocks it reads
         self.fused = None
         self.wtot = wtot
@@ -309,13 +359,13 @@ class SigmaOperator(object):
         fb = 0
         for si in range(4):
             tot_b = 0
-            for key, (ops, *cs, Rl, fused, pan) in sorted(plans.items()):
+            for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
                 if fused is not None and si in (1, 2):
                     continue
                 c, t = cs[si]
                 tot_b += stage_bytes(c, t, len(ops), si == 0)      # psi is read by every operator
             self.stages[si].bytes = float(tot_b)
-        for key, (ops, *cs, Rl, fused, pan) in sorted(plans.items()):
+        for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
             if fused is not None:
                 fb += stage_bytes(fused[1], fused[2], len(ops), False)
         if self.fused is not None:
@@ -323,7 +373,7 @@ class SigmaOperator(object):
         # FLOPs of the reference's four-contraction chain (tensordotCAL pair GEMMs),
         # whatever the fusion used here
         self.flops = 0.0
-        for key, (ops, *cs, Rl, fused, pan) in sorted(plans.items()):
+        for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
             for (c, t) in cs:
                 self.flops += pair_flops(c, t) * len(ops)
         self.ndim0 = psi_layout.size
@@ -335,6 +385,26 @@ class SigmaOperator(object):
         self.L, self.R = L, R
         if self.lperm is not None:
             self._build_lpan()
+        if self.rperm is not None:
+            self._build_rpan()
+
+    def _build_rpan(self):
+        self.Rpan = torch.empty(max(self.R.total, 1), dtype=torch.float64, device=self.ws.device)
+        block_permute(self.rperm, len(self._rperm_h), self._rperm_span, self._rperm_ops_d, self.R.values,
+                      self.Rpan)
+        self._Rpan32 = None
+
+    def b4(self, kind):
+        """Second operand of the .R contraction (R panels, or R itself without panels)."""
+        if self.rperm is not None:
+            if kind == "f64":
+                return self.Rpan
+            if self._Rpan32 is None:
+                self._Rpan32 = torch.empty(max(self.R.total, 1), dtype=torch.float32, device=self.ws.device)
+                block_permute(self.rperm, len(self._rperm_h), self._rperm_span, self._rperm_ops_d,
+                              self.R.values, self._Rpan32)
+            return self._Rpan32
+        return self.R.values if kind == "f64" else self.R.f32()
 
     def _build_lpan(self):
         self.Lpan = torch.empty(max(self.L.total, 1), dtype=torch.float64, device=self.ws.device)
@@ -359,6 +429,7 @@ class SigmaOperator(object):
         """Drop the references to the environment values (the plan stays valid)."""
         self.L = self.R = None
         self.Lpan = self._Lpan32 = None
+        self.Rpan = self._Rpan32 = None
 
     def wij32(self):
         if self._Wij32 is None:
@@ -389,7 +460,7 @@ class SigmaOperator(object):
             if self.fused is not None:
                 self.fused.run(T1, self.Wij, T3, "f64")
             P[:self.nops * self.ndim0].zero_()
-            s[3].run(T3, self.R.values, P, "f64")
+            s[3].run(T3, self.b4("f64"), P, "f64")
             return reduce_ops(P, self.nops, self.ndim0, y)
         kind = "tf32" if prec == "tf32" else "f32"
         T1 = ws.get("t1", self.tot[0], torch.float32)
@@ -406,7 +477,7 @@ class SigmaOperator(object):
         if self.fused is not None:
             self.fused.run(T1, self.wij32(), T3, "f32")
         P[:self.nops * self.ndim0].zero_()
-        s[3].run(T3, self.R.f32(), P, kind)
+        s[3].run(T3, self.b4("f32"), P, kind)
         reduce_ops(P, self.nops, self.ndim0, y32)
         convert(y32, y)
         return y
