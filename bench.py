@@ -204,6 +204,8 @@ def run_ours(args):
         "sigma_tflops": round(sig_fl / (sig_ms / 1e3) / 1e12, 3) if sig_ms else None,
         "sigma_share": round(sig_ms / ms, 3) if ms else None,
         "matvecs_per_step": stats["nmvp"] / args.steps,
+        "matvecs_f64_low_per_step": [stats.get("nmvp_f64", stats["nmvp"] if prec == "f64" else 0) / args.steps,
+                                     stats.get("nmvp_low", 0) / args.steps],
         "stage_ms_per_step": {k: round(v[1] / args.steps, 1) for k, v in sorted(per.items())},
         "roofline": roof, "clocks": ck, "gpu_launches": LOG.launches,
         "w_contraction_paths": d.stats.get("w_paths"),

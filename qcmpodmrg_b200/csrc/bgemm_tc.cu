@@ -97,13 +97,18 @@ __device__ __forceinline__ void issue_mma(uint32_t tmem, uint32_t a0, uint32_t b
 // s&1), the threads load K-slice s+1 from global memory into registers; stage
 // s&1 is refilled only after the MMAs that read it (committed to mbar[s&1])
 // have completed.
+// SPLIT: each FP32 operand x is staged as hi = tf32(x) and lo = tf32(x - hi) and the
+// product accumulates hi*hi + hi*lo + lo*hi (three MMAs per K-step): FP32-level
+// accuracy (relative error ~2^-21) on the tensor cores.
+template <bool SPLIT>
 __global__ void __launch_bounds__(TC_THREADS)
 k_bgemm_tc(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ contribs,
            const qc_op *__restrict__ ops, const float *__restrict__ A, const float *__restrict__ B,
            float *__restrict__ C, int *__restrict__ err) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  float *As = reinterpret_cast<float *>(tc_smem);                 // [2][TC_M * TC_K]
-  float *Bs = As + 2 * TC_M * TC_K;                                 // [2][TC_N * TC_K]
+  constexpr int NP = SPLIT ? 2 : 1;                                 // hi (and lo) planes
+  float *As = reinterpret_cast<float *>(tc_smem);                 // [2][NP][TC_M * TC_K]
+  float *Bs = As + 2 * NP * TC_M * TC_K;                            // [2][NP][TC_N * TC_K]
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
   __shared__ int arow[TC_M];
@@ -198,27 +203,38 @@ k_bgemm_tc(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ con
       }
       __syncthreads();
       if (abort_flag) break;
-      float *as = As + buf * TC_M * TC_K;
-      float *bs = Bs + buf * TC_N * TC_K;
+      float *as = As + buf * NP * TC_M * TC_K;
+      float *bs = Bs + buf * NP * TC_N * TC_K;
 #pragma unroll
       for (int e = 0; e < LA; ++e) {
         const int idx = tid + e * TC_THREADS;
         int i, kk;
         if (a_kfast) { kk = idx % TC_K; i = idx / TC_K; } else { i = idx % TC_M; kk = idx / TC_M; }
-        as[canon(i, kk, TC_M)] = to_tf32(ra[e]);
+        const float hi = to_tf32(ra[e]);
+        as[canon(i, kk, TC_M)] = hi;
+        if (SPLIT) as[TC_M * TC_K + canon(i, kk, TC_M)] = to_tf32(ra[e] - hi);
       }
 #pragma unroll
       for (int e = 0; e < LB; ++e) {
         const int idx = tid + e * TC_THREADS;
         int j, kk;
         if (b_nfast) { j = idx % TC_N; kk = idx / TC_N; } else { kk = idx % TC_K; j = idx / TC_K; }
-        bs[canon(j, kk, TC_N)] = to_tf32(rb[e]);
+        const float hi = to_tf32(rb[e]);
+        bs[canon(j, kk, TC_N)] = hi;
+        if (SPLIT) bs[TC_N * TC_K + canon(j, kk, TC_N)] = to_tf32(rb[e] - hi);
       }
       // make the generic-proxy shared-memory stores visible to the tensor core
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
       if (tid == 0) {
-        issue_mma(tmem, smem_u32(as), smem_u32(bs), accumulate);
+        const uint32_t a_hi = smem_u32(as), b_hi = smem_u32(bs);
+        if (SPLIT) {                     // small terms first, then hi*hi
+          issue_mma(tmem, a_hi, b_hi + TC_N * TC_K * 4, accumulate);
+          issue_mma(tmem, a_hi + TC_M * TC_K * 4, b_hi, true);
+          issue_mma(tmem, a_hi, b_hi, true);
+        } else {
+          issue_mma(tmem, a_hi, b_hi, accumulate);
+        }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                      ::"r"(smem_u32(&mbar[buf])) : "memory");
       }
@@ -275,7 +291,7 @@ k_bgemm_tc(const qc_task *__restrict__ tasks, const qc_contrib *__restrict__ con
   }
 }
 
-constexpr size_t TC_DSMEM = (size_t)2 * (TC_M + TC_N) * TC_K * sizeof(float);
+constexpr size_t tc_dsmem(bool split) { return (size_t)2 * (split ? 2 : 1) * (TC_M + TC_N) * TC_K * sizeof(float); }
 
 int *g_tc_err = nullptr;   // device error flag (allocated once, host-visible through qc_tc_status)
 
@@ -283,8 +299,9 @@ int *g_tc_err = nullptr;   // device error flag (allocated once, host-visible th
 
 static thread_local std::string g_tcerr;
 
-extern "C" int qc_bgemm_tf32(const void *tasks, long long ntasks, int opspan, const void *contribs, const void *ops,
-                             int summed, const float *A, const float *B, float *C, int cfg, void *stream) {
+template <bool SPLIT>
+static int launch_tc(const void *tasks, long long ntasks, int opspan, const void *contribs, const void *ops,
+                     int summed, const float *A, const float *B, float *C, int cfg, cudaStream_t stream) {
   if (ntasks <= 0) return QC_OK;
   if (summed || cfg != 5 || ntasks > 0x7fffffffLL || opspan < 1 || opspan > 65535) return QC_ERR_ARG;
   if (!g_tc_err) {
@@ -293,13 +310,14 @@ extern "C" int qc_bgemm_tf32(const void *tasks, long long ntasks, int opspan, co
   }
   static bool attr_set = false;
   if (!attr_set) {
-    if (cudaFuncSetAttribute(k_bgemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_DSMEM) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_bgemm_tc<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_dsmem(SPLIT)) !=
+        cudaSuccess)
       return QC_ERR_CUDA;
     attr_set = true;
   }
   dim3 grid((unsigned)ntasks, (unsigned)opspan);
-  k_bgemm_tc<<<grid, TC_THREADS, TC_DSMEM, (cudaStream_t)stream>>>((const qc_task *)tasks, (const qc_contrib *)contribs,
-                                                            (const qc_op *)ops, A, B, C, g_tc_err);
+  k_bgemm_tc<SPLIT><<<grid, TC_THREADS, tc_dsmem(SPLIT), stream>>>(
+      (const qc_task *)tasks, (const qc_contrib *)contribs, (const qc_op *)ops, A, B, C, g_tc_err);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     g_tcerr = cudaGetErrorString(e);
@@ -307,6 +325,16 @@ extern "C" int qc_bgemm_tf32(const void *tasks, long long ntasks, int opspan, co
     return QC_ERR_CUDA;
   }
   return QC_OK;
+}
+
+extern "C" int qc_bgemm_tf32(const void *tasks, long long ntasks, int opspan, const void *contribs, const void *ops,
+                             int summed, const float *A, const float *B, float *C, int cfg, void *stream) {
+  return launch_tc<false>(tasks, ntasks, opspan, contribs, ops, summed, A, B, C, cfg, (cudaStream_t)stream);
+}
+
+extern "C" int qc_bgemm_tf32x3(const void *tasks, long long ntasks, int opspan, const void *contribs, const void *ops,
+                               int summed, const float *A, const float *B, float *C, int cfg, void *stream) {
+  return launch_tc<true>(tasks, ntasks, opspan, contribs, ops, summed, A, B, C, cfg, (cudaStream_t)stream);
 }
 
 extern "C" int qc_tc_status(void) {

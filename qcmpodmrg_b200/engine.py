@@ -221,10 +221,46 @@ def panel_class(N):
     return numpy.where(N > 32, 0, numpy.where(N > 16, 1, 2))
 
 
-def compile_panels(gemm, op_range):
+def compile_panels(gemm, op_range, tensor_cores=False):
     """Work items {cfg: (ptasks, flops)} of dense panel GEMMs
-    C_j[M_j x N_j] = A_j[M_j x K_j] . B_j[K_j x N_j], all operands row-major (qc_pgemm_*)."""
+    C_j[M_j x N_j] = A_j[M_j x K_j] . B_j[K_j x N_j], all operands row-major (qc_pgemm_*).
+    With tensor_cores, panels that fill a useful part of a 128 x 64 tile are
+    returned separately as grouped-GEMM work items {TC_CFG: (tasks, contribs, flops)}."""
     a_off, b_off, c_off, M, N, K = (numpy.asarray(x, dtype=numpy.int64) for x in gemm)
+    tcsel = (M >= 64) & (N > 24) & (K >= 8) if tensor_cores else numpy.zeros(len(M), dtype=bool)
+    tc = {}
+    if tcsel.any():
+        sel = numpy.flatnonzero(tcsel)
+        tm, tn = TILES[TC_CFG]
+        nm = (M[sel] + tm - 1) // tm
+        nn = (N[sel] + tn - 1) // tn
+        nt = nm * nn
+        pid = numpy.repeat(numpy.arange(len(sel)), nt)
+        loc = numpy.arange(int(nt.sum())) - numpy.repeat(numpy.cumsum(nt) - nt, nt)
+        g = sel[pid]
+        tasks = numpy.zeros(len(g), TASK_DT)
+        tasks["c_off"] = c_off[g]
+        tasks["M"], tasks["N"] = M[g], N[g]
+        tasks["m0"] = (loc // nn[pid]) * tm
+        tasks["n0"] = (loc % nn[pid]) * tn
+        tasks["mlo"], tasks["nlo"] = M[g], N[g]
+        tasks["c_ml"] = N[g]
+        tasks["c_nl"] = 1
+        tasks["cb"], tasks["ce"] = pid, pid + 1
+        tasks["op_b"], tasks["op_e"] = op_range
+        contribs = numpy.zeros(len(sel), CONTRIB_DT)
+        contribs["a_off"], contribs["b_off"] = a_off[sel], b_off[sel]
+        contribs["alpha"] = 1.0
+        contribs["K"] = contribs["klo"] = K[sel]
+        contribs["a_ml"] = K[sel]
+        contribs["a_kl"] = 1
+        contribs["b_kl"] = N[sel]
+        contribs["b_nl"] = 1
+        contribs["op_b"], contribs["op_e"] = 0, 1
+        nop = op_range[1] - op_range[0]
+        tc[TC_CFG] = (tasks, contribs, 2.0 * float((M[sel] * N[sel] * K[sel]).sum()) * nop)
+        keep = numpy.flatnonzero(~tcsel)
+        a_off, b_off, c_off, M, N, K = (x[keep] for x in (a_off, b_off, c_off, M, N, K))
     cls = panel_class(N)
     out = {}
     for k in numpy.unique(cls):
@@ -244,21 +280,25 @@ def compile_panels(gemm, op_range):
         tasks["op_b"], tasks["op_e"] = op_range
         nop = op_range[1] - op_range[0]
         out[int(k)] = (tasks, 2.0 * float((M[sel] * N[sel] * K[sel]).sum()) * nop)
+    if tensor_cores:
+        return out, tc
     return out
 
 
 class PanelStage(object):
     """Dense panel GEMMs of one contraction (qc_pgemm_*), one launch per tile class."""
 
-    def __init__(self, parts, device, name, ops):
-        """parts: {cfg: [(ptasks, flops), ...]}"""
+    def __init__(self, parts, device, name, ops, tc_parts=None):
+        """parts: {cfg: [(ptasks, flops), ...]}; tc_parts: {TC_CFG: [(tasks, contribs, flops)]} run by the
+        tensor-core grouped GEMM in TF32 modes (by the CUDA-core grouped GEMM otherwise)."""
         self.name = name
+        self.tc = Stage(tc_parts, device, name, ops) if tc_parts else None
         self.host_ops = ops
         self.d_ops = torch.from_numpy(ops.view(numpy.uint8).copy()).to(device)
         self.groups = []
-        self.flops = 0.0
+        self.flops = self.tc.flops if self.tc is not None else 0.0
         self.bytes = 0.0
-        self.ntasks = 0
+        self.ntasks = self.tc.ntasks if self.tc is not None else 0
         for cfg in sorted(parts):
             tk = numpy.concatenate([p[0] for p in parts[cfg]])
             self.flops += sum(p[1] for p in parts[cfg])
@@ -280,6 +320,11 @@ class PanelStage(object):
             check(fn(dt.data_ptr(), len(tk), span, self.d_ops.data_ptr(), A.data_ptr(), B.data_ptr(), C.data_ptr(),
                      cfg, s), "qc_pgemm_" + kind)
             LOG.launches += 1
+        if self.tc is not None:
+            en = LOG.enabled
+            LOG.enabled = False
+            self.tc.run(A, B, C, kind, stream)
+            LOG.enabled = en
         if LOG.enabled:
             e1.record()
             LOG.records.append((self.name, e0, e1, self.flops, self.bytes * (A.element_size() / 8.0)))
@@ -438,13 +483,15 @@ class Stage(object):
     def run(self, A, B, C, kind="f64", stream=None):
         lib = native.lib()
         s = stream if stream is not None else torch.cuda.current_stream(C.device).cuda_stream
-        fn = {"f64": lib.qc_bgemm_f64, "f32": lib.qc_bgemm_f32, "tf32": lib.qc_bgemm_f32}[kind]
+        fn = {"f64": lib.qc_bgemm_f64, "f32": lib.qc_bgemm_f32, "tf32": lib.qc_bgemm_f32,
+              "tf32x3": lib.qc_bgemm_f32}[kind]
+        tcfn = lib.qc_bgemm_tf32x3 if kind == "tf32x3" else lib.qc_bgemm_tf32
         if LOG.enabled:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
         for (cfg, tk, ct, dt, dc, span) in self.groups:
-            f = lib.qc_bgemm_tf32 if (kind == "tf32" and cfg == TC_CFG) else fn
+            f = tcfn if (kind in ("tf32", "tf32x3") and cfg == TC_CFG) else fn
             check(f(dt.data_ptr(), len(tk), span, dc.data_ptr(), self.d_ops.data_ptr(), int(self.summed),
                     A.data_ptr(), B.data_ptr(), C.data_ptr(), cfg, s), "qc_bgemm_" + kind)
             LOG.launches += 1

@@ -145,8 +145,8 @@ class SigmaOperator(object):
     def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts, precision="f64",
                  tensor_cores=None, use_fiber=False, fuse_w=True, panel1=True, panel4=True):
         self.ws, self.psi, self.precision = ws, psi_layout, precision
-        # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 mode
-        tc = (precision == "tf32") if tensor_cores is None else tensor_cores
+        # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 modes
+        tc = (precision in ("tf32", "tf32x3")) if tensor_cores is None else tensor_cores
         self.L, self.R, self.Wi, self.Wj = L, R, Wi, Wj
         self._lay_ids = ([id(x) for x in L.layouts], [id(x) for x in R.layouts])
         dev = ws.device
@@ -236,9 +236,9 @@ class SigmaOperator(object):
         # every group fits in shared memory, generic grouped GEMM otherwise
         fiber_spec = {1: (0, 0), 2: (3, 1)}      # stage -> (rows axis of operand 1, fiber-major storage)
         lperm = []
-        pst = {}                        # panel GEMM parts of the L.psi contraction
+        pst, pst_tc = {}, {}            # panel GEMM parts of the L.psi contraction
         rperm = []
-        p4st = {}                       # panel GEMM parts of the .R contraction
+        p4st, p4st_tc = {}, {}          # panel GEMM parts of the .R contraction
         any4 = any(v[8] is not None for v in plans.values())
         for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
             rng = (pos, pos + len(ops))
@@ -274,7 +274,11 @@ class SigmaOperator(object):
                 d["op_b"], d["op_e"] = rng
                 rperm.append(d)
             if pan4 is not None:
-                for cfg, part in compile_panels(pan4["gemm"], rng).items():
+                parts = compile_panels(pan4["gemm"], rng, tensor_cores=bool(tc))
+                if tc:
+                    parts, tcp = parts
+                    add_parts(p4st_tc, tcp)
+                for cfg, part in parts.items():
                     p4st.setdefault(cfg, []).append(part)
             if fib3 is not None:
                 fib[2].append(fib3 + (rng,))
@@ -290,7 +294,11 @@ class SigmaOperator(object):
                 if (si == 2 and fib3 is not None) or (si == 3 and pan4 is not None):
                     continue
                 if si == 0 and pan is not None:
-                    for cfg, part in compile_panels(pan["gemm"], rng).items():
+                    parts = compile_panels(pan["gemm"], rng, tensor_cores=bool(tc))
+                    if tc:
+                        parts, tcp = parts
+                        add_parts(pst_tc, tcp)
+                    for cfg, part in parts.items():
                         pst.setdefault(cfg, []).append(part)
                     continue
                 off1 = t1off if si == 1 else None
@@ -308,10 +316,10 @@ class SigmaOperator(object):
         for si in range(4):
             g = Stage(st[si], dev, "sigma%d" % (si + 1), tabs[si]) if st[si] else None
             f = fiber_stages(fib[si], dev, "sigma%d" % (si + 1), tabs[si]) if fib[si] else []
-            if si == 0 and pst:
-                f = [PanelStage(pst, dev, "sigma1", tabs[0])]
-            if si == 3 and p4st:
-                f = [PanelStage(p4st, dev, "sigma4", tabs[3])]
+            if si == 0 and (pst or pst_tc):
+                f = [PanelStage(pst, dev, "sigma1", tabs[0], pst_tc)]
+            if si == 3 and (p4st or p4st_tc):
+                f = [PanelStage(p4st, dev, "sigma4", tabs[3], p4st_tc)]
             if not f:
                 self.stages.append(g if g is not None else Stage({}, dev, "sigma%d" % (si + 1), tabs[si]))
             else:
@@ -462,7 +470,7 @@ class SigmaOperator(object):
             P[:self.nops * self.ndim0].zero_()
             s[3].run(T3, self.b4("f64"), P, "f64")
             return reduce_ops(P, self.nops, self.ndim0, y)
-        kind = "tf32" if prec == "tf32" else "f32"
+        kind = prec if prec in ("tf32", "tf32x3") else "f32"
         T1 = ws.get("t1", self.tot[0], torch.float32)
         T2 = ws.get("t2", self.tot[1], torch.float32)
         T3 = ws.get("t3", self.tot[2], torch.float32)

@@ -47,6 +47,7 @@ _SIGS = {
     "qc_bgemm_f64": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
     "qc_bgemm_f32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
     "qc_bgemm_tf32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
+    "qc_bgemm_tf32x3": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
     "qc_gather_f64": (c_int, [c_vp, c_vp, c_vp, c_ll, c_vp]),
     "qc_reduce_ops_f64": (c_int, [c_vp, c_int, c_ll, c_vp, c_vp]),
     "qc_tc_status": (c_int, []),
