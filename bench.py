@@ -123,7 +123,7 @@ def run_ours(args):
     dist, rank, world, local = dist_init()
     dev = torch.device("cuda:%d" % local)
     torch.cuda.set_device(dev)
-    prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32"}[args.precision]
+    prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32", "mixed-tc": "tf32x3"}[args.precision]
     ham = make_hamiltonian(args.sites, args.sites, SEED + rank * 0, DECAY)
     d = DMRG(ham, device=dev, precision=prec, w_path=args.w_path)
     d.load_mps(product_mps(ham))
@@ -192,7 +192,8 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 1),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": {"f64": "f64", "f32": "f32 (sigma), f64 (Davidson, decimation)",
-                  "tf32": "tf32 (sigma), f64 (Davidson, decimation)"}[prec],
+                  "tf32": "tf32 (sigma), f64 (Davidson, decimation)",
+                  "tf32x3": "3xtf32 split on tensor cores + f32 (sigma), f64 (Davidson, decimation)"}[prec],
         "data": "synthetic: seeded integrals (K=%d, N=%d, decay 3, seed 1), product-state start, D ramp %s"
                 % (args.sites, args.sites, "/".join(str(x) for x in RAMP if x < args.dmax)),
         "config": {"workload": "two-site Qt DMRG sweep, K=%d N=%d Sz=0 D=%d, %d operators H_p"
@@ -288,7 +289,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "f64", "tf32"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "f64", "tf32", "mixed-tc"])
     ap.add_argument("--sites", type=int, default=K_SITES)
     ap.add_argument("--dmax", type=int, default=DMAX)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")

@@ -86,6 +86,12 @@ class BatchedSigma(object):
                             fibers.setdefault((si, sub.tile), []).append((sub, base))
                         continue
                     if isinstance(sub, PanelStage):
+                        if sub.tc is not None:      # tensor-core panel tiles: grouped-GEMM work items
+                            for (cfg, tk, ct) in sub.tc.host_groups:
+                                tk = tk.copy()
+                                tk["op_b"] += base
+                                tk["op_e"] += base
+                                groups.setdefault((si, cfg), []).append((tk, ct))
                         for (cfg, tk, _, _) in sub.groups:
                             tk = tk.copy()
                             tk["op_b"] += base

@@ -100,9 +100,25 @@ def test_sigma_tf32_all_blocks_on_tensor_cores(tag, cuda):
         sig = SigmaOperator(ws, int(r["key"][2]), helpers.layout_of(r["qtmp"]), sig.L, sig.R, sig.Wi, sig.Wj,
                             numpy.asarray(r["qkey"], dtype=numpy.float64),
                             [int(x) for x in numpy.atleast_1d(r["opers"])],
-                            numpy.atleast_1d(r["hpwts"]).astype(numpy.float64), "tf32", tensor_cores="all")
+                            numpy.atleast_1d(r["hpwts"]).astype(numpy.float64), "tf32", tensor_cores="all",
+                            panel1=False)
         x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64)).to(cuda)
         y = sig(x).cpu().numpy()
         ref = numpy.asarray(r["hvec_y"])
         assert numpy.linalg.norm(y - ref) <= TOL_TF32 * numpy.linalg.norm(ref)
     assert native.lib().qc_tc_status() == 0
+
+
+TOL_TF32X3 = 2e-5   # split TF32 (hi*hi + hi*lo + lo*hi): FP32-level relative error of sigma
+
+
+@pytest.mark.parametrize("tag", ["K5", "K6"])
+def test_sigma_tf32x3_panels(tag, cuda):
+    """L.psi and .R panel GEMMs on the tensor cores with split operands reach FP32 accuracy."""
+    for r in load("kernels_%s.npz" % tag)["records"]:
+        sig, _, _ = record_operators(r, cuda, precision="tf32x3", use_fiber=True)
+        x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64)).to(cuda)
+        y = sig(x).cpu().numpy()
+        ref = numpy.asarray(r["hvec_y"])
+        assert numpy.linalg.norm(y - ref) <= TOL_TF32X3 * numpy.linalg.norm(ref)
+        assert native.lib().qc_tc_status() == 0

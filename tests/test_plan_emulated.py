@@ -51,3 +51,15 @@ def test_sigma_fiber_unfused_emulated(tag, monkeypatch):
         x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))
         ref = numpy.asarray(r["hvec_y"])
         assert numpy.abs(sig(x).numpy() - ref).max() <= 1e-12 * max(1.0, numpy.abs(ref).max())
+
+
+@pytest.mark.parametrize("tag", ["K5", "K6"])
+def test_sigma_tensor_core_panels_emulated(tag, monkeypatch):
+    """Panel GEMMs routed to the tensor-core tile class (TF32 modes) keep the same work-item semantics."""
+    patch_stage_run(monkeypatch)
+    for r in load("kernels_%s.npz" % tag)["records"]:
+        sig, dg, ws = record_operators(r, "cpu", precision="tf32x3", use_fiber=True)
+        x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))
+        ref = numpy.asarray(r["hvec_y"])
+        y = sig(x, precision="f64").numpy()
+        assert numpy.abs(y - ref).max() <= 1e-12 * max(1.0, numpy.abs(ref).max())
