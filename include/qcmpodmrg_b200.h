@@ -140,15 +140,19 @@ int qc_bgemm_tf32x3(const void *tasks_dev, long long ntasks, int opspan, const v
 
 /* Dense panel GEMM: for every task (qc_ptask, 64 B) and operator o in
  * [op_b, op_e) (grid.y, at most opspan):
- *   C[o.c_base + c_off + m*N + n] = o.alpha * sum_k A[o.a_base + a_off + m*K + k] * B[o.b_base + b_off + k*N + n]
- * for the tile m0 <= m < m0+128, n0 <= n < n0+TN.  Used for the L.psi and .R
+ *   C[o.c_base + row(m) + n] = o.alpha * sum_k A[o.a_base + a_off + m*K + k] * B[o.b_base + b_off + k*N + n]
+ * for the tile m0 <= m < m0+128, n0 <= n < n0+TN, where row(m) = c_off + m*N, or
+ * crow[task.crow + m] (device int64 table, may be null if unused) when task.crow >= 0.
+ * Used for the L.psi and .R
  * contractions of HVecQt (source/mpo_dmrg_kernelQt.py:301, 306-316) once L and R
  * are permuted into per-sector panels (qc_block_permute).  tile_cfg: 0 = 128x64,
  * 1 = 128x32, 2 = 128x16. */
 int qc_pgemm_f64(const void *tasks_dev, long long ntasks, int opspan, const void *ops_dev,
-                 const double *A, const double *B, double *C, int tile_cfg, void *stream);
+                 const long long *crow_dev, const double *A, const double *B, double *C, int tile_cfg,
+                 void *stream);
 int qc_pgemm_f32(const void *tasks_dev, long long ntasks, int opspan, const void *ops_dev,
-                 const float *A, const float *B, float *C, int tile_cfg, void *stream);
+                 const long long *crow_dev, const float *A, const float *B, float *C, int tile_cfg,
+                 void *stream);
 
 /* 0 if no tensor-core launch has reported a timed-out wait, 1 otherwise
  * (synchronous: reads a device flag), negative on a CUDA error. */

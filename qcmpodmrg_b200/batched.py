@@ -96,7 +96,7 @@ class BatchedSigma(object):
                             tk = tk.copy()
                             tk["op_b"] += base
                             tk["op_e"] += base
-                            panels.setdefault((si, cfg), []).append(tk)
+                            panels.setdefault((si, cfg), []).append((tk, sub.h_crow))
                         continue
                     for (cfg, tk, ct) in sub.host_groups:
                         tk = tk.copy()
@@ -152,10 +152,18 @@ class BatchedSigma(object):
             self.fiber_launches.append((si, len(tk), span, mr, tile, up(tk), up(numpy.concatenate(fis)),
                                         up(numpy.concatenate(fos)), up(numpy.concatenate(fps))))
         self.panel_launches = []
-        for (si, cfg), tks in sorted(panels.items()):
+        for (si, cfg), parts in sorted(panels.items()):
+            tks, crows, nrow = [], [], 0
+            for tk, crow in parts:          # row tables concatenated, task indices rebased
+                tk = tk.copy()
+                tk["crow"] = numpy.where(tk["crow"] >= 0, tk["crow"] + nrow, -1)
+                tks.append(tk)
+                crows.append(crow)
+                nrow += len(crow)
             tk = numpy.concatenate(tks)
             span = int(max(1, (tk["op_e"] - tk["op_b"]).max()))
-            self.panel_launches.append((si, cfg, len(tk), span, up(tk)))
+            crow = torch.from_numpy(numpy.concatenate(crows).astype(numpy.int64)).to(device)
+            self.panel_launches.append((si, cfg, len(tk), span, up(tk), crow))
         self.graph = None
 
     def _launch_all(self):
@@ -165,11 +173,11 @@ class BatchedSigma(object):
         ffn = lib.qc_fiber_f64 if self.kind == "f64" else lib.qc_fiber_f32
         pfn = lib.qc_pgemm_f64 if self.kind == "f64" else lib.qc_pgemm_f32
         for stage in (0, 1, 2, 4, 3):       # contractions in dependency order (4: fused W stage)
-            for (si, cfg, nt, span, dt) in self.panel_launches:
+            for (si, cfg, nt, span, dt, crow) in self.panel_launches:
                 if si != stage:
                     continue
-                check(pfn(dt.data_ptr(), nt, span, self.d_ops[si].data_ptr(), None, None, None, cfg, s),
-                      "batched qc_pgemm")
+                check(pfn(dt.data_ptr(), nt, span, self.d_ops[si].data_ptr(), crow.data_ptr(), None, None, None, cfg,
+                          s), "batched qc_pgemm")
                 LOG.launches += 1
             for (si, nt, span, mr, tile, dt, dfi, dfo, dfp) in self.fiber_launches:
                 if si != stage:

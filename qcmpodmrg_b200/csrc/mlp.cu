@@ -173,8 +173,9 @@ __global__ void k_precond_apply(long long n, const double *__restrict__ r, const
                                 const int *__restrict__ blk, const float *__restrict__ Y, double *__restrict__ c) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int b = blk[i];
-    const double alpha = exp((double)Y[2 * b]);
-    const double sigma = exp((double)Y[2 * b + 1]);
+    // log alpha and log sigma are clamped to [-30, 30] (the range the training uses)
+    const double alpha = exp(fmin(fmax((double)Y[2 * b], -30.0), 30.0));
+    const double sigma = exp(fmin(fmax((double)Y[2 * b + 1], -30.0), 30.0));
     c[i] = r[i] * alpha / (fabs(d[i] - e) + sigma);
   }
 }

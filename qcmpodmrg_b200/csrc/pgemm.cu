@@ -17,8 +17,8 @@ namespace {
 
 template <typename T, int TM, int TN, int TK, int RM, int RN, int NT>
 __global__ void __launch_bounds__(NT, 2)
-k_pgemm(const qc_ptask *__restrict__ tasks, const qc_op *__restrict__ ops, const T *__restrict__ A,
-        const T *__restrict__ B, T *__restrict__ C) {
+k_pgemm(const qc_ptask *__restrict__ tasks, const qc_op *__restrict__ ops, const long long *__restrict__ crow,
+        const T *__restrict__ A, const T *__restrict__ B, T *__restrict__ C) {
   constexpr int TX = TN / RN, TY = TM / RM;
   static_assert(TX * TY == NT, "thread tile");
   constexpr int LA = (TM * TK + NT - 1) / NT;       // A elements per thread per K-slice
@@ -93,22 +93,23 @@ k_pgemm(const qc_ptask *__restrict__ tasks, const qc_op *__restrict__ ops, const
         for (int j = 0; j < RN; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
     }
   }
-  T *Cb = C + o.c_base + t.c_off;
+  T *Cb = C + o.c_base;
 #pragma unroll
   for (int i = 0; i < RM; ++i) {
     const int m = t.m0 + ty + i * TY;
     if (m >= M) continue;
+    const long long row = (t.crow >= 0) ? crow[t.crow + m] : t.c_off + (long long)m * N;
 #pragma unroll
     for (int j = 0; j < RN; ++j) {
       const int n = t.n0 + tx + j * TX;
-      if (n < N) Cb[(long long)m * N + n] = alpha * acc[i][j];
+      if (n < N) Cb[row + n] = alpha * acc[i][j];
     }
   }
 }
 
 template <typename T>
-int launch_pgemm(const void *tasks, long long ntasks, int opspan, const void *ops, const T *A, const T *B, T *C,
-                 int cfg, cudaStream_t s) {
+int launch_pgemm(const void *tasks, long long ntasks, int opspan, const void *ops, const long long *crow, const T *A,
+                 const T *B, T *C, int cfg, cudaStream_t s) {
   if (ntasks <= 0) return QC_OK;
   if (ntasks > 0x7fffffffLL || opspan < 1 || opspan > 65535) return QC_ERR_ARG;
   dim3 grid((unsigned)ntasks, (unsigned)opspan);
@@ -116,9 +117,9 @@ int launch_pgemm(const void *tasks, long long ntasks, int opspan, const void *op
   const qc_op *op = (const qc_op *)ops;
   constexpr int KT = (sizeof(T) == 8) ? 8 : 16;
   switch (cfg) {
-    case 0: k_pgemm<T, 128, 64, KT, 8, 4, 256><<<grid, 256, 0, s>>>(tk, op, A, B, C); break;   // N > 32
-    case 1: k_pgemm<T, 128, 32, KT, 8, 2, 256><<<grid, 256, 0, s>>>(tk, op, A, B, C); break;   // 16 < N <= 32
-    case 2: k_pgemm<T, 128, 16, KT, 4, 2, 256><<<grid, 256, 0, s>>>(tk, op, A, B, C); break;   // N <= 16
+    case 0: k_pgemm<T, 128, 64, KT, 8, 4, 256><<<grid, 256, 0, s>>>(tk, op, crow, A, B, C); break;   // N > 32
+    case 1: k_pgemm<T, 128, 32, KT, 8, 2, 256><<<grid, 256, 0, s>>>(tk, op, crow, A, B, C); break;   // 16 < N <= 32
+    case 2: k_pgemm<T, 128, 16, KT, 4, 2, 256><<<grid, 256, 0, s>>>(tk, op, crow, A, B, C); break;   // N <= 16
     default: return QC_ERR_ARG;
   }
   cudaError_t e = cudaGetLastError();
@@ -131,12 +132,12 @@ int launch_pgemm(const void *tasks, long long ntasks, int opspan, const void *op
 
 }  // namespace
 
-extern "C" int qc_pgemm_f64(const void *tasks, long long ntasks, int opspan, const void *ops, const double *A,
-                            const double *B, double *C, int cfg, void *stream) {
-  return launch_pgemm<double>(tasks, ntasks, opspan, ops, A, B, C, cfg, (cudaStream_t)stream);
+extern "C" int qc_pgemm_f64(const void *tasks, long long ntasks, int opspan, const void *ops, const long long *crow,
+                            const double *A, const double *B, double *C, int cfg, void *stream) {
+  return launch_pgemm<double>(tasks, ntasks, opspan, ops, crow, A, B, C, cfg, (cudaStream_t)stream);
 }
 
-extern "C" int qc_pgemm_f32(const void *tasks, long long ntasks, int opspan, const void *ops, const float *A,
-                            const float *B, float *C, int cfg, void *stream) {
-  return launch_pgemm<float>(tasks, ntasks, opspan, ops, A, B, C, cfg, (cudaStream_t)stream);
+extern "C" int qc_pgemm_f32(const void *tasks, long long ntasks, int opspan, const void *ops, const long long *crow,
+                            const float *A, const float *B, float *C, int cfg, void *stream) {
+  return launch_pgemm<float>(tasks, ntasks, opspan, ops, crow, A, B, C, cfg, (cudaStream_t)stream);
 }

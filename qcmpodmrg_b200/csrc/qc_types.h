@@ -94,14 +94,15 @@ static_assert(sizeof(qc_bperm) == 64, "qc_bperm is 64 bytes");
 
 
 // ---- dense panel GEMM work items (qc_pgemm_*) -------------------------------
-// C[c_off + m*N + n] = sum_k A[a_off + m*K + k] * B[b_off + k*N + n] for the
-// output tile rows [m0, m0+TM) x cols [n0, n0+TN); offsets relative to the
-// operator's bases; grid.y indexes the operators [op_b, op_e).
+// C[row(m) + n] = sum_k A[a_off + m*K + k] * B[b_off + k*N + n] for the output
+// tile rows [m0, m0+TM) x cols [n0, n0+TN), with row(m) = c_off + m*N, or
+// crow_table[crow + m] when crow >= 0 (rows scattered to separate blocks);
+// offsets relative to the operator's bases; grid.y indexes the operators [op_b, op_e).
 struct alignas(16) qc_ptask {
   long long a_off, b_off, c_off;
   int M, N, K;
   int m0, n0;
   int op_b, op_e;
-  int pad;
+  int crow;
 };
 static_assert(sizeof(qc_ptask) == 64, "qc_ptask is 64 bytes");

@@ -145,13 +145,15 @@ def panel_sigma4(t3lay, Rl, psi, t4):
     """Panel form of the .R contraction (HVecQt top4, kernelQt.py:306-316).
 
     sigma block s = (l, n1', n2', r') receives T3 blocks (l, r, n1', c, n2') times
-    R blocks (c, r', r) over the MPO sectors c (r follows from c and r').  T3
-    blocks of one sigma block are stored as the column slabs of one row-major
-    panel [D_l x K_s] (columns (c, r, c) in the R block order), and the R blocks of
-    one sector r' as one row-major panel [K_r' x D_r'] (a per-dot permutation of
-    R with the (c, r) rows transposed), so each sigma block is one dense GEMM per
-    operator.  Returns None unless every sigma block pairs with all R blocks of
-    its sector r' (the full product the layout allows).
+    R blocks (c, r', r) over the MPO sectors c (r follows from c and r').  For one
+    sector r' all sigma blocks use the same R blocks, so: the R blocks of r' form
+    one row-major panel [K_r' x D_r'] (a per-dot permutation of R with the (c, r)
+    rows transposed); the T3 blocks of every sigma block of r' are written (by the
+    fiber kernel) as row block x column slab of one row-major panel
+    [M_r' x K_r'] (rows: the sigma blocks stacked, D_l rows each; columns: the
+    (c, r, c) slabs in R-panel order); and one dense GEMM per sector and operator
+    writes its rows straight into the sigma blocks through a row table.  Returns
+    None unless every sigma block pairs with all R blocks of its sector.
     """
     if len(t4) == 0:
         return None
@@ -169,7 +171,7 @@ def panel_sigma4(t3lay, Rl, psi, t4):
     sR = Rl.block_sectors(uR)
     oR = numpy.lexsort((sR[0], sR[1]))
     uR = uR[oR]
-    cU, rbU = sR[0][oR], sR[1][oR]
+    rbU = sR[1][oR]
     dU = Rl.block_dims(uR)
     kU = dU[:, 0] * dU[:, 2]
     nrb = int(Rl.nsyms[1])
@@ -192,26 +194,44 @@ def panel_sigma4(t3lay, Rl, psi, t4):
     ckb = numpy.cumsum(kb) - kb
     if numpy.any(koffU[posU[iR]] != ckb - numpy.repeat(ckb[first], cnt)):
         return None
+    # sigma blocks stacked per r' sector
     dS = psi.block_dims(us)
     Dl = dS[:, 0] * dS[:, 1] * dS[:, 2]
-    Ks = Krb[rb_s]
-    tsz = Dl * Ks
+    if numpy.any(dS[:, 3] != Drb_sec[rb_s]):
+        return None
+    os_ = numpy.lexsort((us, rb_s))
+    us, Dl, rb_s = us[os_], Dl[os_], rb_s[os_]
+    crs = numpy.cumsum(Dl) - Dl
+    sstart = numpy.searchsorted(rb_s, numpy.arange(nrb))
+    rowoff = crs - crs[numpy.minimum(sstart[rb_s], len(crs) - 1)]
+    Mrb = numpy.bincount(rb_s, weights=Dl, minlength=nrb).astype(numpy.int64)
+    used = numpy.flatnonzero(Mrb > 0)
+    tsz = Mrb * Krb
     t3pan = numpy.cumsum(tsz) - tsz
-    sidx = numpy.repeat(numpy.arange(len(us)), cnt)
+    # T3 block -> (panel of its r', row block of its sigma block, column slab of its c)
+    spos_by_blk = dict(zip(us.tolist(), range(len(us))))
+    sidx = numpy.array([spos_by_blk[x] for x in so.tolist()], dtype=numpy.int64)
     t3off = numpy.zeros(int(t3lay.nblks), dtype=numpy.int64)
     t3fhs = numpy.zeros(int(t3lay.nblks), dtype=numpy.int64)
     t3flo = numpy.ones(int(t3lay.nblks), dtype=numpy.int64)
-    t3off[i3] = t3pan[sidx] + koffU[posU[iR]]
-    t3fhs[i3] = Ks[sidx]
+    t3off[i3] = t3pan[rbR] + rowoff[sidx] * Krb[rbR] + koffU[posU[iR]]
+    t3fhs[i3] = Krb[rbR]
     t3flo[i3] = dR[:, 2]                     # fibers (l, r): r is the fast fiber index
+    # row table: panel row -> element offset of that row in its sigma block
+    crow = numpy.concatenate([psi.ioff[us] [k] + numpy.arange(Dl[k]) * Drb_sec[rb_s[k]] for k in range(len(us))]) \
+        if len(us) else numpy.zeros(0, dtype=numpy.int64)
+    crow_base = numpy.zeros(nrb, dtype=numpy.int64)
+    crow_base[used] = (numpy.cumsum(Mrb) - Mrb)[used]
     rperm = (Rl.ioff[uR], poff[rbU] + koffU * dU[:, 1], dU)
+    gemm = (t3pan[used], poff[used], numpy.zeros(len(used), dtype=numpy.int64), Mrb[used], Drb_sec[used],
+            Krb[used], crow_base[used])
     return {"t3off": t3off, "t3fhs": t3fhs, "t3flo": t3flo, "t3size": int(tsz.sum()), "needed": i3,
-            "rperm": rperm, "gemm": (t3pan, poff[rb_s], psi.ioff[us], Dl, Drb_sec[rb_s], Ks)}
+            "rperm": rperm, "gemm": gemm, "crow": crow.astype(numpy.int64)}
 
 
 PTASK_DT = numpy.dtype([("a_off", "<i8"), ("b_off", "<i8"), ("c_off", "<i8"), ("M", "<i4"), ("N", "<i4"),
                         ("K", "<i4"), ("m0", "<i4"), ("n0", "<i4"), ("op_b", "<i4"), ("op_e", "<i4"),
-                        ("pad", "<i4", (3,))])
+                        ("crow", "<i4"), ("pad", "<i4", (2,))])
 assert PTASK_DT.itemsize == 64
 PANEL_TILES = {0: (128, 64), 1: (128, 32), 2: (128, 16)}
 
@@ -226,8 +246,10 @@ def compile_panels(gemm, op_range, tensor_cores=False):
     C_j[M_j x N_j] = A_j[M_j x K_j] . B_j[K_j x N_j], all operands row-major (qc_pgemm_*).
     With tensor_cores, panels that fill a useful part of a 128 x 64 tile are
     returned separately as grouped-GEMM work items {TC_CFG: (tasks, contribs, flops)}."""
-    a_off, b_off, c_off, M, N, K = (numpy.asarray(x, dtype=numpy.int64) for x in gemm)
-    tcsel = (M >= 64) & (N > 24) & (K >= 8) if tensor_cores else numpy.zeros(len(M), dtype=bool)
+    a_off, b_off, c_off, M, N, K = (numpy.asarray(x, dtype=numpy.int64) for x in gemm[:6])
+    crow = numpy.asarray(gemm[6], dtype=numpy.int64) if len(gemm) > 6 else numpy.full(len(M), -1, dtype=numpy.int64)
+    # rows scattered through a row table run on the CUDA-core panel kernel
+    tcsel = (M >= 64) & (N > 24) & (K >= 8) & (crow < 0) if tensor_cores else numpy.zeros(len(M), dtype=bool)
     tc = {}
     if tcsel.any():
         sel = numpy.flatnonzero(tcsel)
@@ -260,7 +282,7 @@ def compile_panels(gemm, op_range, tensor_cores=False):
         nop = op_range[1] - op_range[0]
         tc[TC_CFG] = (tasks, contribs, 2.0 * float((M[sel] * N[sel] * K[sel]).sum()) * nop)
         keep = numpy.flatnonzero(~tcsel)
-        a_off, b_off, c_off, M, N, K = (x[keep] for x in (a_off, b_off, c_off, M, N, K))
+        a_off, b_off, c_off, M, N, K, crow = (x[keep] for x in (a_off, b_off, c_off, M, N, K, crow))
     cls = panel_class(N)
     out = {}
     for k in numpy.unique(cls):
@@ -278,6 +300,7 @@ def compile_panels(gemm, op_range, tensor_cores=False):
         tasks["m0"] = (loc // nn[pid]) * tm
         tasks["n0"] = (loc % nn[pid]) * tn
         tasks["op_b"], tasks["op_e"] = op_range
+        tasks["crow"] = crow[g]
         nop = op_range[1] - op_range[0]
         out[int(k)] = (tasks, 2.0 * float((M[sel] * N[sel] * K[sel]).sum()) * nop)
     if tensor_cores:
@@ -288,10 +311,13 @@ def compile_panels(gemm, op_range, tensor_cores=False):
 class PanelStage(object):
     """Dense panel GEMMs of one contraction (qc_pgemm_*), one launch per tile class."""
 
-    def __init__(self, parts, device, name, ops, tc_parts=None):
+    def __init__(self, parts, device, name, ops, tc_parts=None, crow=None):
         """parts: {cfg: [(ptasks, flops), ...]}; tc_parts: {TC_CFG: [(tasks, contribs, flops)]} run by the
-        tensor-core grouped GEMM in TF32 modes (by the CUDA-core grouped GEMM otherwise)."""
+        tensor-core grouped GEMM in TF32 modes (by the CUDA-core grouped GEMM otherwise); crow: the row
+        table the tasks' crow indices point into."""
         self.name = name
+        self.h_crow = crow if crow is not None and len(crow) else numpy.zeros(1, dtype=numpy.int64)
+        self.d_crow = torch.from_numpy(self.h_crow.astype(numpy.int64)).to(device)
         self.tc = Stage(tc_parts, device, name, ops) if tc_parts else None
         self.host_ops = ops
         self.d_ops = torch.from_numpy(ops.view(numpy.uint8).copy()).to(device)
@@ -317,8 +343,8 @@ class PanelStage(object):
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
         for (cfg, tk, dt, span) in self.groups:
-            check(fn(dt.data_ptr(), len(tk), span, self.d_ops.data_ptr(), A.data_ptr(), B.data_ptr(), C.data_ptr(),
-                     cfg, s), "qc_pgemm_" + kind)
+            check(fn(dt.data_ptr(), len(tk), span, self.d_ops.data_ptr(), self.d_crow.data_ptr(), A.data_ptr(),
+                     B.data_ptr(), C.data_ptr(), cfg, s), "qc_pgemm_" + kind)
             LOG.launches += 1
         if self.tc is not None:
             en = LOG.enabled

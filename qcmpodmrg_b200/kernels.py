@@ -239,6 +239,7 @@ class SigmaOperator(object):
         pst, pst_tc = {}, {}            # panel GEMM parts of the L.psi contraction
         rperm = []
         p4st, p4st_tc = {}, {}          # panel GEMM parts of the .R contraction
+        crow_all, crow_n = [], 0        # their row table (panel row -> sigma element offset)
         any4 = any(v[8] is not None for v in plans.values())
         for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
             rng = (pos, pos + len(ops))
@@ -274,7 +275,11 @@ class SigmaOperator(object):
                 d["op_b"], d["op_e"] = rng
                 rperm.append(d)
             if pan4 is not None:
-                parts = compile_panels(pan4["gemm"], rng, tensor_cores=bool(tc))
+                g4 = pan4["gemm"]
+                g4 = g4[:6] + (g4[6] + crow_n,)          # row-table indices into the stage's table
+                crow_all.append(pan4["crow"])
+                crow_n += len(pan4["crow"])
+                parts = compile_panels(g4, rng, tensor_cores=bool(tc))
                 if tc:
                     parts, tcp = parts
                     add_parts(p4st_tc, tcp)
@@ -319,7 +324,8 @@ class SigmaOperator(object):
             if si == 0 and (pst or pst_tc):
                 f = [PanelStage(pst, dev, "sigma1", tabs[0], pst_tc)]
             if si == 3 and (p4st or p4st_tc):
-                f = [PanelStage(p4st, dev, "sigma4", tabs[3], p4st_tc)]
+                f = [PanelStage(p4st, dev, "sigma4", tabs[3], p4st_tc,
+                                crow=numpy.concatenate(crow_all) if crow_all else None)]
             if not f:
                 self.stages.append(g if g is not None else Stage({}, dev, "sigma%d" % (si + 1), tabs[si]))
             else:

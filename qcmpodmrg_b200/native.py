@@ -51,8 +51,8 @@ _SIGS = {
     "qc_gather_f64": (c_int, [c_vp, c_vp, c_vp, c_ll, c_vp]),
     "qc_reduce_ops_f64": (c_int, [c_vp, c_int, c_ll, c_vp, c_vp]),
     "qc_tc_status": (c_int, []),
-    "qc_pgemm_f64": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_vp]),
-    "qc_pgemm_f32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_vp]),
+    "qc_pgemm_f64": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_vp]),
+    "qc_pgemm_f32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_vp]),
     "qc_block_permute": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_int, c_vp]),
     "qc_fiber_f64": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
     "qc_fiber_f32": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),

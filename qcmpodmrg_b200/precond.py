@@ -27,6 +27,7 @@ from .native import check
 NFEAT = 8
 HIDDEN = 256
 NOUT = 2
+YCLAMP = 30.0     # range of the network outputs log(alpha), log(sigma) used by the correction
 
 
 def _stream(dev):
@@ -127,8 +128,11 @@ def correction(r, d, e, blk, Y):
 def loss_and_grad(r, d, e, blk, nblk, Y, t):
     """1 - cos(c, t) and dL/dY (per block) for c = correction(r, d, e, blk, Y)."""
     blk64 = blk.long()
-    alpha = torch.exp(Y[:, 0].double())[blk64]
-    sigma = torch.exp(Y[:, 1].double())[blk64]
+    Yd = Y.double()
+    inside = ((Yd > -YCLAMP) & (Yd < YCLAMP)).double()          # clamp(Y): zero gradient outside
+    Yd = Yd.clamp(-YCLAMP, YCLAMP)
+    alpha = torch.exp(Yd[:, 0])[blk64]
+    sigma = torch.exp(Yd[:, 1])[blk64]
     den = (d - e).abs() + sigma
     c = r * alpha / den
     nc = torch.linalg.norm(c) + 1e-300
@@ -137,7 +141,7 @@ def loss_and_grad(r, d, e, blk, nblk, Y, t):
     dc = -(t / (nc * nt) - cos * c / (nc * nc))
     g_la = torch.zeros(nblk, dtype=torch.float64, device=r.device).index_add_(0, blk64, dc * c)
     g_ls = torch.zeros(nblk, dtype=torch.float64, device=r.device).index_add_(0, blk64, -dc * c * sigma / den)
-    return float(1.0 - cos), torch.stack([g_la, g_ls], dim=1).float().contiguous()
+    return float(1.0 - cos), (torch.stack([g_la, g_ls], dim=1) * inside).float().contiguous()
 
 
 class LearnedPreconditioner(object):
@@ -195,6 +199,8 @@ class LearnedPreconditioner(object):
                 X = features(r, d, e, blk, nblk, it)
                 Y, H1, H2 = self.net.forward(X)
                 L, dY = loss_and_grad(r, d, e, blk, nblk, Y, t)
+                if not (math.isfinite(L) and bool(torch.isfinite(dY).all())):
+                    continue                 # a pair the current network cannot score: no step
                 g = self.net.backward(X, H1, H2, dY)
                 self.net.adam(g, lr=lr)
                 tot += L

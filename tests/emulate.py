@@ -54,8 +54,13 @@ def patch_stage_run(monkeypatch):
                     Bm = b[o["b_base"] + t["b_off"]:][:K * N].reshape(K, N)
                     m1, n1 = min(M, t["m0"] + tm), min(N, t["n0"] + tn)
                     blk = o["alpha"] * (Am[t["m0"]:m1] @ Bm[:, t["n0"]:n1])
-                    cm = c[o["c_base"] + t["c_off"]:][:M * N].reshape(M, N)
-                    cm[t["m0"]:m1, t["n0"]:n1] = blk
+                    if t["crow"] >= 0:         # rows scattered through the row table
+                        rows = self.h_crow[t["crow"] + numpy.arange(t["m0"], m1)]
+                        idx = o["c_base"] + rows[:, None] + numpy.arange(t["n0"], n1)[None, :]
+                        c[idx] = blk
+                    else:
+                        cm = c[o["c_base"] + t["c_off"]:][:M * N].reshape(M, N)
+                        cm[t["m0"]:m1, t["n0"]:n1] = blk
         C.copy_(torch.from_numpy(c).to(C.dtype))
 
     monkeypatch.setattr(engine.PanelStage, "run", prun)
