@@ -529,6 +529,78 @@ def _dense_tasks(M, N, K, a_off, a_m, a_k, b_off, b_k, b_n, c_off, c_m, alpha, g
     return t, contribs[numpy.array(order, dtype=numpy.int64)], 2.0 * M * N * K * ncontr
 
 
+_DIAG_CACHE = {}
+
+
+def _cached(key, lay, build):
+    hit = _DIAG_CACHE.get(key)
+    if hit is not None and hit[0] is lay:
+        return hit[1]
+    if len(_DIAG_CACHE) > 4096:
+        _DIAG_CACHE.clear()
+    val = build()
+    _DIAG_CACHE[key] = (lay, val)
+    return val
+
+
+def _ragged(n):
+    """Block id and in-block position of every element of blocks with n elements each."""
+    n = numpy.asarray(n, dtype=numpy.int64)
+    b = numpy.repeat(numpy.arange(len(n)), n)
+    e = numpy.arange(int(n.sum()), dtype=numpy.int64) - numpy.repeat(numpy.cumsum(n) - n, n)
+    return b, e
+
+
+def _env_diag_map(lay, ncol):
+    """Environment E[a, l, l'] -> its diagonal E[a, l, l] as a dense [A x ncol] matrix (src, dst)."""
+    def build():
+        idx = lay.idx_allowed
+        sa, s1, s2 = numpy.unravel_index(idx, tuple(lay.nsyms))
+        keep = s1 == s2
+        idx, sa, s1 = idx[keep], sa[keep], s1[keep]
+        d = lay.block_dims(idx) if len(idx) else numpy.zeros((0, 3), dtype=numpy.int64)
+        da, dl = d[:, 0], d[:, 1]
+        b, e = _ragged(da * dl)
+        w, u = e // dl[b], e % dl[b]
+        src = lay.ioff[idx][b] + w * dl[b] * dl[b] + u * dl[b] + u
+        dst = (lay.secoff[0][sa][b] + w) * ncol + lay.secoff[1][s1][b] + u
+        return src.astype(numpy.int64), dst.astype(numpy.int64)
+    return _cached(("e", id(lay), ncol), lay, build)
+
+
+def _w_diag_map(lay, n2):
+    """MPO site operator W[a, b, n, n'] -> its physical diagonal as a dense [A x n2 x 4] array (src, dst)."""
+    def build():
+        idx = lay.idx_allowed
+        sa, sb, n, n_ = numpy.unravel_index(idx, tuple(lay.nsyms))
+        keep = n == n_
+        idx, sa, sb, n = idx[keep], sa[keep], sb[keep], n[keep]
+        d = lay.block_dims(idx) if len(idx) else numpy.zeros((0, 4), dtype=numpy.int64)
+        da, db = d[:, 0], d[:, 1]
+        b, e = _ragged(da * db)
+        w, v = e // db[b], e % db[b]
+        src = lay.ioff[idx][b] + w * db[b] + v
+        dst = ((lay.secoff[0][sa][b] + w) * n2 + lay.secoff[1][sb][b] + v) * 4 + n[b]
+        return src.astype(numpy.int64), dst.astype(numpy.int64)
+    return _cached(("w", id(lay), n2), lay, build)
+
+
+def _psi_diag_gather(ql, ldim, rdim):
+    """Packed wavefunction position -> index of the dense [16, ldim, rdim] diagonal."""
+    def build():
+        idx = ql.idx_allowed
+        sl, n, m, sr = numpy.unravel_index(idx, tuple(ql.nsyms))
+        d = ql.block_dims(idx)
+        dl, dr = d[:, 0], d[:, 3]
+        b, e = _ragged(dl * dr)
+        u, v = e // dr[b], e % dr[b]
+        gat = numpy.empty(ql.size, dtype=numpy.int64)
+        gat[ql.ioff[idx][b] + e] = ((n[b] * 4 + m[b]) * ldim * rdim + (ql.secoff[0][sl][b] + u) * rdim
+                                    + ql.secoff[3][sr][b] + v)
+        return gat
+    return _cached(("p", id(ql), ldim, rdim), ql, build)
+
+
 class DiagOperator(object):
     """Davidson diagonal in the packed wavefunction layout (HDiagQt, two-site)."""
 
@@ -543,68 +615,30 @@ class DiagOperator(object):
         Ab = int(Wi.layouts[0].shape[1])
         Ac = int(R.layouts[0].shape[0])
         self.dims = (A, Ab, Ac, ldim, rdim)
-        # ---- index maps for the diagonal elements (host, once per dot) ----
+        # ---- index maps for the diagonal elements (host; cached per interned layout) ----
         Lsrc, Ldst = [], []
         Rsrc, Rdst = [], []
         Wsrc1, Wdst1, Wsrc2, Wdst2 = [], [], [], []
-        cache = {}
-
-        def env_diag(lay, off, opi, nrow, ncol, into_s, into_d):
-            key = ("e", id(lay))
-            if key not in cache:
-                s, d = [], []
-                for idx in lay.idx_allowed:
-                    sa, s1, s2 = numpy.unravel_index(idx, tuple(lay.nsyms))
-                    if s1 != s2:
-                        continue
-                    da, dl, _ = lay.block_dims(idx)[0]
-                    w, u = numpy.meshgrid(numpy.arange(da), numpy.arange(dl), indexing="ij")
-                    s.append(lay.ioff[idx] + w * dl * dl + u * dl + u)
-                    d.append((lay.secoff[0][sa] + w) * ncol + lay.secoff[1][s1] + u)
-                cache[key] = (numpy.concatenate([x.ravel() for x in s]) if s else numpy.zeros(0, numpy.int64),
-                              numpy.concatenate([x.ravel() for x in d]) if d else numpy.zeros(0, numpy.int64))
-            s, d = cache[key]
-            into_s.append(s + off)
-            into_d.append(d + opi * nrow * ncol)
-
-        def w_diag(lay, off, opi, n1, n2, into_s, into_d):
-            key = ("w", id(lay))
-            if key not in cache:
-                s, d = [], []
-                for idx in lay.idx_allowed:
-                    sa, sb, n, n_ = numpy.unravel_index(idx, tuple(lay.nsyms))
-                    if n != n_:
-                        continue
-                    da, db = lay.block_dims(idx)[0][:2]
-                    w, v = numpy.meshgrid(numpy.arange(da), numpy.arange(db), indexing="ij")
-                    s.append(lay.ioff[idx] + w * db + v)
-                    d.append(((lay.secoff[0][sa] + w) * n2 + lay.secoff[1][sb] + v) * 4 + n)
-                cache[key] = (numpy.concatenate([x.ravel() for x in s]) if s else numpy.zeros(0, numpy.int64),
-                              numpy.concatenate([x.ravel() for x in d]) if d else numpy.zeros(0, numpy.int64))
-            s, d = cache[key]
-            into_s.append(s + off)
-            into_d.append(d + opi * n1 * n2 * 4)
-
         for i in range(nops):
-            env_diag(L.layouts[i], L.offsets[i], i, A, ldim, Lsrc, Ldst)
-            env_diag(R.layouts[i], R.offsets[i], i, Ac, rdim, Rsrc, Rdst)
-            w_diag(Wi.layouts[i], Wi.offsets[i], i, A, Ab, Wsrc1, Wdst1)
-            w_diag(Wj.layouts[i], Wj.offsets[i], i, Ab, Ac, Wsrc2, Wdst2)
+            s_, d_ = _env_diag_map(L.layouts[i], ldim)
+            Lsrc.append(s_ + L.offsets[i])
+            Ldst.append(d_ + i * A * ldim)
+            s_, d_ = _env_diag_map(R.layouts[i], rdim)
+            Rsrc.append(s_ + R.offsets[i])
+            Rdst.append(d_ + i * Ac * rdim)
+            s_, d_ = _w_diag_map(Wi.layouts[i], Ab)
+            Wsrc1.append(s_ + Wi.offsets[i])
+            Wdst1.append(d_ + i * A * Ab * 4)
+            s_, d_ = _w_diag_map(Wj.layouts[i], Ac)
+            Wsrc2.append(s_ + Wj.offsets[i])
+            Wdst2.append(d_ + i * Ab * Ac * 4)
         cat = lambda x: torch.from_numpy(numpy.concatenate(x).astype(numpy.int64)).to(dev)
         self.maps = [(cat(Lsrc), cat(Ldst), nops * A * ldim, "ld", L),
                      (cat(Rsrc), cat(Rdst), nops * Ac * rdim, "rd", R),
                      (cat(Wsrc1), cat(Wdst1), nops * A * Ab * 4, "w1", Wi),
                      (cat(Wsrc2), cat(Wdst2), nops * Ab * Ac * 4, "w2", Wj)]
         # ---- packed output gather: psi block (sl, n, m, sr), element (u, v) ----
-        gat = numpy.empty(ql.size, dtype=numpy.int64)
-        for idx in ql.idx_allowed:
-            sl, n, m, sr = numpy.unravel_index(idx, tuple(ql.nsyms))
-            bd = ql.block_dims(idx)[0]
-            dl, dr = bd[0], bd[3]
-            u, v = numpy.meshgrid(numpy.arange(dl), numpy.arange(dr), indexing="ij")
-            o = int(ql.ioff[idx])
-            gat[o:o + dl * dr] = ((n * 4 + m) * ldim * rdim + (ql.secoff[0][sl] + u) * rdim
-                                  + ql.secoff[3][sr] + v).ravel()
+        gat = _psi_diag_gather(ql, ldim, rdim)
         self.gather = torch.from_numpy(gat).to(dev)
         self.ndim0 = ql.size
         # ---- three dense GEMM stages ----
