@@ -208,6 +208,8 @@ def run_ours(args):
         "matvecs_f64_low_per_step": [stats.get("nmvp_f64", stats["nmvp"] if prec == "f64" else 0) / args.steps,
                                      stats.get("nmvp_low", 0) / args.steps],
         "stage_ms_per_step": {k: round(v[1] / args.steps, 1) for k, v in sorted(per.items())},
+        "stage_gbs": {k: round(v[3] / (v[1] / 1e3) / 1e9, 1) for k, v in sorted(per.items()) if v[1] > 0},
+        "stage_tflops": {k: round(v[2] / (v[1] / 1e3) / 1e12, 2) for k, v in sorted(per.items()) if v[1] > 0},
         "roofline": roof, "clocks": ck, "gpu_launches": LOG.launches,
         "w_contraction_paths": d.stats.get("w_paths"),
         "phase_s_per_step": {k: round(stats[k] / args.steps, 2) for k in ("plan_s", "hvec_s", "hdiag_s", "renorm_s",
