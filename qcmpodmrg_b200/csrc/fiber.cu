@@ -61,6 +61,8 @@ k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, cons
   T *Cb = C + o.c_base;
   const int lane = tid & 31, warp = tid >> 5;
   constexpr int NW = FT_THREADS / 32;
+  __shared__ __align__(16) T wslot[NW][32 * CB];     // per-warp staged W rows
+  T *wsl = wslot[warp];
   // items: (output block j, column block cb), enumerated block by block
   int j = t.out_b, cb = 0, skip = warp;
   while (j < t.out_e) {
@@ -85,33 +87,30 @@ k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, cons
       const qc_fpair pr = fpair[p];
       const T *w = Wb + pr.w_off + c0;
       const T *a = As + pr.srow * FT + lane;
-      if (nb == CB) {
-#pragma unroll 2
-        for (int r = 0; r < pr.rows; ++r) {
-          T av[FPL];
+      // the W rows of this pair, 32 at a time: lane l stages row r0+l (8 columns,
+      // zero beyond the block) in this warp's shared slot; the FMAs then read them
+      // as broadcasts, so no global load sits inside the multiply loop
+      for (int r0 = 0; r0 < pr.rows; r0 += 32) {
+        const int nr = min(32, pr.rows - r0);
+        __syncwarp();
+        if (lane < nr) {
+          const T *wr = w + (long long)(r0 + lane) * nc;
 #pragma unroll
-          for (int q = 0; q < FPL; ++q) av[q] = a[r * FT + 32 * q];
-          const T *wr = w + (long long)r * nc;
-#pragma unroll
-          for (int i = 0; i < CB; ++i) {
-            const T wv = __ldg(wr + i);
-#pragma unroll
-            for (int q = 0; q < FPL; ++q) acc[q][i] = fma(av[q], wv, acc[q][i]);
-          }
+          for (int i = 0; i < CB; ++i) wsl[lane * CB + i] = (i < nb) ? __ldg(wr + i) : T(0);
         }
-      } else {
-        for (int r = 0; r < pr.rows; ++r) {
+        __syncwarp();
+#pragma unroll 2
+        for (int r = 0; r < nr; ++r) {
           T av[FPL];
 #pragma unroll
-          for (int q = 0; q < FPL; ++q) av[q] = a[r * FT + 32 * q];
-          const T *wr = w + (long long)r * nc;
+          for (int q = 0; q < FPL; ++q) av[q] = a[(r0 + r) * FT + 32 * q];
+          T wv[CB];
+#pragma unroll
+          for (int i = 0; i < CB; ++i) wv[i] = wsl[r * CB + i];
 #pragma unroll
           for (int i = 0; i < CB; ++i)
-            if (i < nb) {
-              const T wv = __ldg(wr + i);
 #pragma unroll
-              for (int q = 0; q < FPL; ++q) acc[q][i] = fma(av[q], wv, acc[q][i]);
-            }
+            for (int q = 0; q < FPL; ++q) acc[q][i] = fma(av[q], wv[i], acc[q][i]);
         }
       }
     }
@@ -170,12 +169,25 @@ int launch_fiber(const void *tasks, long long ntasks, int opspan, const void *fi
   if (smem > 200 * 1024) return QC_ERR_ARG;
   dim3 grid((unsigned)ntasks, (unsigned)opspan);
   const qc_ftask *tk = (const qc_ftask *)tasks;
+  // the kernels also hold 8-16 KB of static shared memory (per-warp W rows): allow the
+  // full dynamic range once per instantiation
+  static bool attr_set[2] = {false, false};
+  const int v = (fiber_tile == 32) ? 0 : 1;
+  if (!attr_set[v]) {
+    cudaError_t ea = (v == 0) ? cudaFuncSetAttribute(k_fiber<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     200 * 1024)
+                              : cudaFuncSetAttribute(k_fiber<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     200 * 1024);
+    if (ea != cudaSuccess) {
+      fprintf(stderr, "[qcgpu] qc_fiber: %s\n", cudaGetErrorString(ea));
+      return QC_ERR_CUDA;
+    }
+    attr_set[v] = true;
+  }
   if (fiber_tile == 32) {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_fiber<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_fiber<T, 1><<<grid, FT_THREADS, smem, s>>>(tk, (const qc_fin *)fin, (const qc_fout *)fout,
                                                  (const qc_fpair *)fpair, (const qc_op *)ops, A, W, C);
   } else {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_fiber<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_fiber<T, 2><<<grid, FT_THREADS, smem, s>>>(tk, (const qc_fin *)fin, (const qc_fout *)fout,
                                                  (const qc_fpair *)fpair, (const qc_op *)ops, A, W, C);
   }
