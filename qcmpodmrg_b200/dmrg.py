@@ -119,13 +119,16 @@ class DMRG(object):
         Wi, Wj = self.mpo[isite], self.mpo[isite + 1]
         # compiled plans depend only on block layouts (interned by content): a dot whose
         # wavefunction and environment sectors are unchanged reuses them
+        # the key is built from object ids; a hit is confirmed by identity against the layout
+        # objects the entry holds (so no id can be recycled by a new layout while cached)
         key = (isite, id(lay), tuple(id(x) for x in L.layouts), tuple(id(x) for x in R.layouts))
-        for (_, s_, d_) in self.plan_cache.values():     # cached plans keep no environment alive
+        for (_, _, _, s_, d_) in self.plan_cache.values():     # cached plans keep no environment alive
             s_.release()
             d_.release()
         hit = self.plan_cache.get(key)
-        if hit is not None and hit[0] is lay:
-            sig, dg = hit[1], hit[2]
+        if (hit is not None and hit[0] is lay and all(a is b for a, b in zip(hit[1], L.layouts))
+                and all(a is b for a, b in zip(hit[2], R.layouts))):
+            sig, dg = hit[3], hit[4]
             sig.rebind(L, R)
             dg.rebind(L, R)
             self.stats["plan_hits"] = self.stats.get("plan_hits", 0) + 1
@@ -136,7 +139,7 @@ class DMRG(object):
         for k, v in sig.w_paths.items():
             wp[k] = wp.get(k, 0) + v
         dg = DiagOperator(self.ws, isite, lay, L, R, Wi, Wj, self.qkey, self.opers, self.hpwts)
-        self.plan_cache[key] = (lay, sig, dg)
+        self.plan_cache[key] = (lay, tuple(L.layouts), tuple(R.layouts), sig, dg)
         while len(self.plan_cache) > self.plan_cache_size:
             self.plan_cache.pop(next(iter(self.plan_cache)))
         self.stats["plan_misses"] = self.stats.get("plan_misses", 0) + 1

@@ -148,7 +148,7 @@ class SigmaOperator(object):
         # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 modes
         tc = (precision in ("tf32", "tf32x3")) if tensor_cores is None else tensor_cores
         self.L, self.R, self.Wi, self.Wj = L, R, Wi, Wj
-        self._lay_ids = ([id(x) for x in L.layouts], [id(x) for x in R.layouts])
+        self._lays = (list(L.layouts), list(R.layouts))      # held: identity is the plan's key
         dev = ws.device
         groups = _groups(opers, isite, 2)
         nops = len(opers)
@@ -394,7 +394,9 @@ class SigmaOperator(object):
 
     def rebind(self, L, R):
         """Use new environment values with the same block layouts (cached plan)."""
-        if [id(x) for x in L.layouts] != self._lay_ids[0] or [id(x) for x in R.layouts] != self._lay_ids[1]:
+        if (len(L.layouts) != len(self._lays[0]) or len(R.layouts) != len(self._lays[1])
+                or any(a is not b for a, b in zip(L.layouts, self._lays[0]))
+                or any(a is not b for a, b in zip(R.layouts, self._lays[1]))):
             raise ValueError("rebind: environment layouts differ from the compiled plan")
         self.L, self.R = L, R
         if self.lperm is not None:

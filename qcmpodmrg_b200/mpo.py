@@ -143,10 +143,12 @@ def site_operator(p, nsite_spin, isite, int1e, int2e):
     phys = classification(QPHYS, collect=False)
     lay = Layout(W_STATUS, [cl[0], cr[0], phys[0], phys[0]], [cl[1], cr[1], phys[1], phys[1]])
     key = (id(lay), tuple(len(x) for x in cl[2]), tuple(len(x) for x in cr[2]))
-    prj = _PRJ.get(key)
-    if prj is None:
+    hit = _PRJ.get(key)
+    if hit is not None and hit[0] is lay:
+        prj = hit[1]
+    else:
         prj = lay.prjmap([cl[2], cr[2], phys[2], phys[2]])
-        _PRJ[key] = prj
+        _PRJ[key] = (lay, prj)          # the layout is held, so its id cannot be recycled
     return lay, dense.ravel()[prj].copy()
 
 

@@ -30,12 +30,12 @@ def _check(info):
 
 def _ops(dmrg, isite):
     """Sigma/diagonal operators of the dot, cached on the DMRG object while the dot is active."""
-    key = (isite, id(dmrg.lenv[isite - 1]), id(dmrg.renv[isite + 2]))
+    L, R = dmrg.lenv[isite - 1], dmrg.renv[isite + 2]
     cache = getattr(dmrg, "_dot_cache", None)
-    if cache is None or cache[0] != key:
+    if cache is None or cache[0] != isite or cache[1] is not L or cache[2] is not R:
         lay, idl, sig, dg = dmrg.dot_operators(isite)
-        dmrg._dot_cache = (key, lay, idl, sig, dg)
-    return dmrg._dot_cache[1:]
+        dmrg._dot_cache = (isite, L, R, lay, idl, sig, dg)      # environments held: compared by identity
+    return dmrg._dot_cache[3:]
 
 
 def _to_dev(v, dev):

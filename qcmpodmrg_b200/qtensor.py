@@ -9,12 +9,16 @@ buffers); a ``Layout`` is immutable and cached by its defining data.
 Quantum numbers are multiples of 1/2 and are handed to the native code as
 exact int32 values of 2q, so every block map is built in integer arithmetic.
 """
+import weakref
+
 import numpy
 
 from . import native
 from .native import ptr, check
 
-_CACHE = {}
+# layouts are interned by content while alive: equal layouts are the same object, and
+# no entry outlives its layout (a weak map never hands out a recycled object)
+_CACHE = weakref.WeakValueDictionary()
 
 
 def qint(q):
@@ -60,8 +64,6 @@ class Layout(object):
             return obj
         obj = super(Layout, cls).__new__(cls)
         obj._init(status, qs, nd)
-        if len(_CACHE) > 20000:
-            _CACHE.clear()
         _CACHE[key] = obj
         return obj
 

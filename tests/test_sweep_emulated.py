@@ -23,3 +23,27 @@ def test_sweeps_emulated(tag, monkeypatch):
     assert numpy.abs(out["dwt"] - fx["dwt"]).max() <= 1e-10
     # later sweeps revisit dots with unchanged sectors: their compiled plans are reused
     assert d.stats.get("plan_hits", 0) > 0
+
+
+def test_plan_cache_requires_identical_layouts(monkeypatch):
+    """A cached plan is reused only for the very layout objects it was compiled for:
+    an entry whose key matches but whose layouts are other objects (a recycled id)
+    is rebuilt, not reused."""
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    from qcmpodmrg_b200.dmrg import DMRG
+    fx = load("sweep_K4.npz")
+    ham = make_hamiltonian(int(fx["K"]), int(fx["N"]), int(fx["seed"]), None if fx["decay"] < 0 else fx["decay"])
+    d = DMRG(ham, device="cpu")
+    d.load_mps(fx["init_mps"])
+    d.sweep("R", int(fx["D"]), 1e-8)
+    lay, idl, sig, dg = d.dot_operators(1)
+    key = next(k for k in d.plan_cache if k[0] == 1)
+    entry = d.plan_cache[key]
+    fake_L = tuple(object() for _ in entry[1])          # same key, other objects
+    d.plan_cache[key] = (entry[0], fake_L) + entry[2:]
+    misses = d.stats.get("plan_misses", 0)
+    lay2, idl2, sig2, dg2 = d.dot_operators(1)
+    assert sig2 is not sig and d.stats["plan_misses"] == misses + 1
+    lay3, idl3, sig3, dg3 = d.dot_operators(1)           # the rebuilt entry is reused
+    assert sig3 is sig2
