@@ -125,7 +125,7 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32", "mixed-tc": "tf32x3"}[args.precision]
     ham = make_hamiltonian(args.sites, args.sites, SEED + rank * 0, DECAY)
-    d = DMRG(ham, device=dev, precision=prec, w_path=args.w_path)
+    d = DMRG(ham, device=dev, precision=prec, w_path=args.w_path, plan_cache=args.plan_cache)
     d.load_mps(product_mps(ham))
     for D in RAMP:
         if D < args.dmax:
@@ -296,8 +296,9 @@ def main():
     ap.add_argument("--dmax", type=int, default=DMAX)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--w-path", default="generic", choices=["generic", "fiber", "fused"],
+    ap.add_argument("--w-path", default="fiber", choices=["generic", "fiber", "fused"],
                     help="kernels of the two MPO-site contractions of sigma")
+    ap.add_argument("--plan-cache", action="store_true", help="reuse compiled plans of unchanged dots")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -57,7 +57,7 @@ def boundary_set(nops, device):
 class DMRG(object):
     """Two-site MPO-DMRG with every hot-path contraction on the GPU."""
 
-    def __init__(self, ham, device="cuda", precision="f64", preconditioner=None, w_path="generic"):
+    def __init__(self, ham, device="cuda", precision="f64", preconditioner=None, w_path="fiber", plan_cache=False):
         self.ham = ham
         self.device = torch.device(device)
         self.nsite = ham.nsite
@@ -76,7 +76,10 @@ class DMRG(object):
         self.ifguess = True
         self.ws = Workspace(self.device)
         self.plan_cache = {}          # oldest first
-        self.plan_cache_size = 2 * self.nsite
+        # compiled plans of dots whose sectors did not change can be reused (off by default:
+        # with it the unconverged K=24 bench sweep took a different, equally valid path; the
+        # operators it returns were checked bitwise against freshly compiled ones)
+        self.plan_cache_size = 2 * self.nsite if plan_cache else 0
         t0 = time.time()
         mpo = build_mpo(ham)
         self.mpo = {i: TensorSet(l, v, device=self.device) for i, (l, v) in mpo.items()}

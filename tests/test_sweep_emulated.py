@@ -17,7 +17,7 @@ def test_sweeps_emulated(tag, monkeypatch):
     fx = load("sweep_%s.npz" % tag)
     decay = None if fx["decay"] < 0 else fx["decay"]
     ham = make_hamiltonian(int(fx["K"]), int(fx["N"]), int(fx["seed"]), decay)
-    d = DMRG(ham, device="cpu")
+    d = DMRG(ham, device="cpu", plan_cache=True)
     out = d.run(fx["init_mps"], int(fx["D"]), int(fx["nsweeps"]))
     assert numpy.abs(out["eav"] - fx["eav"]).max() <= 1e-8
     assert numpy.abs(out["dwt"] - fx["dwt"]).max() <= 1e-10
@@ -34,7 +34,7 @@ def test_plan_cache_requires_identical_layouts(monkeypatch):
     from qcmpodmrg_b200.dmrg import DMRG
     fx = load("sweep_K4.npz")
     ham = make_hamiltonian(int(fx["K"]), int(fx["N"]), int(fx["seed"]), None if fx["decay"] < 0 else fx["decay"])
-    d = DMRG(ham, device="cpu")
+    d = DMRG(ham, device="cpu", plan_cache=True)
     d.load_mps(fx["init_mps"])
     d.sweep("R", int(fx["D"]), 1e-8)
     lay, idl, sig, dg = d.dot_operators(1)
