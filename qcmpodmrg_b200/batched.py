@@ -240,7 +240,9 @@ class BatchedDMRG(object):
         self.captures = 0
 
     def sweep(self, status, dmax, crit_e):
+        """One sweep of every instance; dmax is one bond dimension or one per instance."""
         n = len(self.inst)
+        dmaxs = list(dmax) if isinstance(dmax, (list, tuple)) else [dmax] * n
         acts = []
         for d in self.inst:
             K = d.nsite
@@ -279,7 +281,7 @@ class BatchedDMRG(object):
                     pend[i] = ctx[i]["gen"].send(ys[k])
                 except StopIteration as stop:
                     res = stop.value
-                    last[i] = self.inst[i].dot_end(ctx[i], res, status, dmax, acts[i], elst[i], dlst[i])
+                    last[i] = self.inst[i].dot_end(ctx[i], res, status, dmaxs[i], acts[i], elst[i], dlst[i])
                     ctx[i] = None
                     pos[i] += 1
         out = []
