@@ -182,7 +182,10 @@ def run_ours(args):
     pk, src = peaks()
     n_l, t_l, f_l, b_l = top[1]
     gbs = b_l / (t_l / 1e3) / 1e9
-    kname = "k_fiber" if top[0] == "sigma23" else "k_bgemm"
+    panel = args.w_path in ("fiber", "fused")
+    kname = {"sigma1": "k_pgemm", "sigma2": "k_fiber" if panel else "k_bgemm",
+             "sigma3": "k_fiber" if panel else "k_bgemm", "sigma23": "k_fiber",
+             "sigma4": "k_pgemm" if panel else "k_bgemm"}.get(top[0], "k_bgemm")
     roof = {"kernel": "%s (%s)" % (kname, top[0]), "bound": "hbm", "achieved": round(gbs, 1),
             "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(gbs / pk["hbm_gbs"], 4),
             "peak_source": src, "traffic": None, "launches": n_l,

@@ -35,6 +35,9 @@ def dpt(q1, q2):
     return (q1[:, None, :] + q2[None, :, :]).reshape(-1, q1.shape[1])
 
 
+ACCEPT_DE = 1e-6      # Eh: FP64 vs low-precision Ritz value agreement that accepts a mixed solve
+
+
 class SiteTensor(object):
     """A site tensor in packed layout on the device (plus its dense form)."""
 
@@ -261,9 +264,11 @@ class DMRG(object):
         Phase 1 iterates with the FP32/TF32 sigma until the energy change is below
         crit_e or the residual below the precision's floor.  Phase 2 applies the
         FP64 sigma to the final vector: its Rayleigh quotient has an error of second
-        order in the vector's error, and its FP64 residual decides whether FP64
-        Davidson iterations (reference criteria) continue from that vector: only
-        when that residual is above 1e-4.
+        order in the vector's error.  The vector is accepted when its FP64 residual is
+        at most 1e-4, or when phase 1 converged by the reference's criteria and the FP64
+        Rayleigh quotient agrees with the low-precision Ritz value within ACCEPT_DE (the
+        low-precision sigma then did not bias the solve); otherwise FP64 Davidson
+        iterations (reference criteria) continue from that vector.
         """
         # residual floor of the low-precision sigma (relative sigma error ~1e-7 FP32,
         # ~1e-3 TF32), and the FP64 residual accepted without FP64 iterations: the
@@ -278,7 +283,8 @@ class DMRG(object):
         rn = float(torch.linalg.norm(y - e64 * x))
         self.stats["nmvp_f64"] = self.stats.get("nmvp_f64", 0) + 1
         self.stats["nmvp_low"] = self.stats.get("nmvp_low", 0) + r1.nmvp
-        if rn <= max(self.crit_vec, accept):
+        converged = r1.niter < 19             # phase 1 met its criteria (not the iteration cap)
+        if rn <= max(self.crit_vec, accept) or (converged and abs(e64 - float(r1.eigs[0])) <= ACCEPT_DE):
             r1.eigs = numpy.array([e64])
             r1.vecs = x.reshape(1, -1)
             r1.nmvp += 1
