@@ -9,6 +9,7 @@ buffers); a ``Layout`` is immutable and cached by its defining data.
 Quantum numbers are multiples of 1/2 and are handed to the native code as
 exact int32 values of 2q, so every block map is built in integer arithmetic.
 """
+import collections
 import weakref
 
 import numpy
@@ -17,8 +18,18 @@ from . import native
 from .native import ptr, check
 
 # layouts are interned by content while alive: equal layouts are the same object, and
-# no entry outlives its layout (a weak map never hands out a recycled object)
+# no entry outlives its layout (a weak map never hands out a recycled object); the most
+# recently used ones are also held strongly so that dots with the same sectors share them
 _CACHE = weakref.WeakValueDictionary()
+_RECENT = collections.OrderedDict()
+_RECENT_MAX = 8192
+
+
+def _hold(key, obj):
+    _RECENT[key] = obj
+    _RECENT.move_to_end(key)
+    while len(_RECENT) > _RECENT_MAX:
+        _RECENT.popitem(last=False)
 
 
 def qint(q):
@@ -61,10 +72,12 @@ class Layout(object):
                tuple(n.tobytes() for n in nd))
         obj = _CACHE.get(key)
         if obj is not None:
+            _hold(key, obj)
             return obj
         obj = super(Layout, cls).__new__(cls)
         obj._init(status, qs, nd)
         _CACHE[key] = obj
+        _hold(key, obj)
         return obj
 
     def _init(self, status, qsyms, ndims):
