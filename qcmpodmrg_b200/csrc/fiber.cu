@@ -43,12 +43,15 @@ k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, cons
     const qc_fin b = fin[i];
     const T *src = Ab + b.a_off;
     const int n = b.rows * FT;
+    // unrolled so that several independent loads are in flight per thread
     if (!b.fiber_major) {             // [rows][F]: consecutive threads -> consecutive fibers
+#pragma unroll 4
       for (int idx = tid; idx < n; idx += FT_THREADS) {
         const int r = idx / FT, f = idx % FT;
         As[(b.srow + r) * FT + f] = (f < nf) ? src[(long long)r * t.F + t.f0 + f] : T(0);
       }
     } else {                          // [F][rows]: consecutive threads -> consecutive rows
+#pragma unroll 4
       for (int idx = tid; idx < n; idx += FT_THREADS) {
         const int f = idx / b.rows, r = idx % b.rows;
         As[(b.srow + r) * FT + f] = (f < nf) ? src[(long long)(t.f0 + f) * b.rows + r] : T(0);

@@ -432,7 +432,8 @@ class DMRG(object):
                 self.rmps[j] = st
                 rn = Renormalizer(self.ws, j, "R", st.layout, self.renv[j + 1], self.mpo[j], self.opers)
                 self.renv[j] = rn(st.values)
-            torch.cuda.synchronize(dev)
+            # no synchronisation here: the next dot's plans are compiled on the host while
+            # the renormalisation runs (renorm_s is host time: plan + launches)
             self.stats["renorm_s"] += time.time() - t0
             self.stats["renorm_flops"] += rn.flops
             self.guess(isite, status, actlst, civecs, srotR)
