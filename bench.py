@@ -289,7 +289,7 @@ def run_reference(args):
 
 
 def run_batched(args):
-    """Independent instances (BASELINE config 3 shape, scaled to --instances) swept in lockstep:
+    """Independent instances (K in [8, 14], D in [64, 128], --instances of them) swept in lockstep:
     one launch per sigma contraction for all instances per Davidson step, replayed from CUDA
     graphs, against the same instances swept one after another.  Prints one JSON line."""
     import torch
