@@ -8,8 +8,10 @@ step = one full two-site sweep (right-to-left then left-to-right) at D=500:
 per dot the sigma/diagonal plans, Davidson (FP64 Rayleigh-Ritz), RDM
 decimation and renormalisation of every operator's environment.
 
-  python bench.py [--steps K] [--warmup W] [--precision mixed|f64] [--gpus N]
+  python bench.py [--steps K] [--warmup W] [--precision mixed|f64|mixed-tc|tf32] [--gpus N]
+                  [--w-path fiber|generic|fused] [--plan-cache] [--sites K] [--dmax D]
   python bench.py --impl reference      # the reference algorithm (oracle port) on the host CPU
+  python bench.py --workload batched    # lockstep independent instances vs one after another
 
 Prints one JSON line.  value = seconds per sweep (lower is better).
 """
