@@ -371,7 +371,7 @@ class SigmaOperator(object):
             return 8 * (b1 + b2 + bo)
 
         fb = 0
-        for si in range(4):
+        for si in range(4 if LOG.enabled else 0):       # only the launch log reads the byte counts
             tot_b = 0
             for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
                 if fused is not None and si in (1, 2):
@@ -380,7 +380,7 @@ class SigmaOperator(object):
                 tot_b += stage_bytes(c, t, len(ops), si == 0)      # psi is read by every operator
             self.stages[si].bytes = float(tot_b)
         for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
-            if fused is not None:
+            if fused is not None and LOG.enabled:
                 fb += stage_bytes(fused[1], fused[2], len(ops), False)
         if self.fused is not None:
             self.fused.bytes = float(fb)
@@ -499,13 +499,15 @@ class SigmaOperator(object):
         return y
 
 
-def _dense_tasks(M, N, K, a_off, a_m, a_k, b_off, b_k, b_n, c_off, c_m, alpha, groups, tile_cfg):
-    """Work items for dense GEMMs C_g = sum_{j in group g} alpha_j A_j B_j.
+def _dense_tasks(M, N, K, a_off, a_m, a_k, b_off, b_k, b_n, c_off, c_m, alpha, per_group, tile_cfg):
+    """Work items for dense GEMMs C_g = sum_{j in group g} alpha_j A_j B_j (vectorised).
 
-    a_off/b_off/alpha are per contribution; groups is a list of (c_off, [contribution ids]).
+    a_off / b_off / alpha are per contribution, grouped consecutively: group g owns
+    contributions [g*per_group, (g+1)*per_group) and writes at c_off[g].
     """
     from .engine import TILES
     tm, tn = TILES[tile_cfg]
+    a_off = numpy.asarray(a_off, dtype=numpy.int64)
     ncontr = len(a_off)
     contribs = numpy.zeros(ncontr, dtype=CONTRIB_DT)
     contribs["a_off"] = a_off
@@ -519,16 +521,53 @@ def _dense_tasks(M, N, K, a_off, a_m, a_k, b_off, b_k, b_n, c_off, c_m, alpha, g
     contribs["b_nl"] = b_n
     contribs["op_b"] = 0
     contribs["op_e"] = 1
-    tasks = []
-    order = []
-    for (co, ids) in groups:
-        cb = len(order)
-        order.extend(ids)
-        for m0 in range(0, M, tm):
-            for n0 in range(0, N, tn):
-                tasks.append((co, M, N, m0, n0, M, N, 0, c_m, 0, 1, cb, len(order), 0, 1))
-    t = numpy.array(tasks, dtype=TASK_DT)
-    return t, contribs[numpy.array(order, dtype=numpy.int64)], 2.0 * M * N * K * ncontr
+    c_off = numpy.asarray(c_off, dtype=numpy.int64)
+    ng = len(c_off)
+    m0 = numpy.arange(0, M, tm)
+    n0 = numpy.arange(0, N, tn)
+    nt = len(m0) * len(n0)
+    t = numpy.zeros(ng * nt, dtype=TASK_DT)
+    g = numpy.repeat(numpy.arange(ng), nt)
+    t["c_off"] = c_off[g]
+    t["M"], t["N"], t["mlo"], t["nlo"] = M, N, M, N
+    t["m0"] = numpy.tile(numpy.repeat(m0, len(n0)), ng)
+    t["n0"] = numpy.tile(numpy.tile(n0, len(m0)), ng)
+    t["c_ml"], t["c_nl"] = c_m, 1
+    t["cb"] = g * per_group
+    t["ce"] = g * per_group + per_group
+    t["op_b"], t["op_e"] = 0, 1
+    return t, contribs, 2.0 * M * N * K * ncontr
+
+
+_DENSE_STAGES = {}
+
+
+def _diag_stages(dev, nops, A, Ab, Ac, ldim, rdim, hp):
+    """The three dense stages of the diagonal; they depend only on the dimensions (and the
+    operator weights), so dots of equal shape share one set of device work lists."""
+    key = (str(dev), nops, A, Ab, Ac, ldim, rdim, hp.tobytes())
+    hit = _DENSE_STAGES.get(key)
+    if hit is not None:
+        return hit
+    p = numpy.repeat(numpy.arange(nops), 16)
+    nm = numpy.tile(numpy.arange(16), nops)
+    n, m = nm // 4, nm % 4
+    # X[p, n, m, a, c] = sum_b W1[p, a, b, n] W2[p, b, c, m]
+    sX = _dense_tasks(A, Ac, Ab, p * A * Ab * 4 + n, Ab * 4, 4, p * Ab * Ac * 4 + m, Ac * 4, 4,
+                      (p * 16 + nm) * A * Ac, Ac, 1.0, 1, 0)
+    # T[p, nm, c, l] = sum_a X[p, nm, a, c] Ld[p, a, l]
+    sT = _dense_tasks(Ac, ldim, A, (p * 16 + nm) * A * Ac, 1, Ac, p * A * ldim, ldim, 1,
+                      (p * 16 + nm) * Ac * ldim, ldim, 1.0, 1, 0)
+    # D[nm, l, r] = sum_p w_p sum_c T[p, nm, c, l] Rd[p, c, r]   (contributions ordered nm-major)
+    nm2 = numpy.repeat(numpy.arange(16), nops)
+    p2 = numpy.tile(numpy.arange(nops), 16)
+    sD = _dense_tasks(ldim, rdim, Ac, (p2 * 16 + nm2) * Ac * ldim, 1, ldim, p2 * Ac * rdim, rdim, 1,
+                      numpy.arange(16) * ldim * rdim, rdim, hp[p2], nops, 0)
+    out = (Stage({0: [sX]}, dev, "diagX"), Stage({0: [sT]}, dev, "diagT"), Stage({0: [sD]}, dev, "diagD"))
+    if len(_DENSE_STAGES) > 256:
+        _DENSE_STAGES.clear()
+    _DENSE_STAGES[key] = out
+    return out
 
 
 _DIAG_CACHE = {}
@@ -643,41 +682,9 @@ class DiagOperator(object):
         gat = _psi_diag_gather(ql, ldim, rdim)
         self.gather = torch.from_numpy(gat).to(dev)
         self.ndim0 = ql.size
-        # ---- three dense GEMM stages ----
+        # ---- three dense GEMM stages (shared by dots of equal dimensions) ----
         hp = numpy.asarray(hpwts, dtype=numpy.float64)
-        # X[p, n, m, a, c] = sum_b W1[p, a, b, n] W2[p, b, c, m]
-        a_off, b_off, al, grp = [], [], [], []
-        for p in range(nops):
-            for n in range(4):
-                for m in range(4):
-                    grp.append((((p * 16 + n * 4 + m) * A * Ac), [len(a_off)]))
-                    a_off.append(p * A * Ab * 4 + n)
-                    b_off.append(p * Ab * Ac * 4 + m)
-                    al.append(1.0)
-        sX = _dense_tasks(A, Ac, Ab, a_off, Ab * 4, 4, b_off, Ac * 4, 4, None, Ac, al, grp, 0)
-        # T[p, nm, c, l] = sum_a X[p, nm, a, c] Ld[p, a, l]
-        a_off, b_off, al, grp = [], [], [], []
-        for p in range(nops):
-            for nm in range(16):
-                grp.append(((p * 16 + nm) * Ac * ldim, [len(a_off)]))
-                a_off.append((p * 16 + nm) * A * Ac)
-                b_off.append(p * A * ldim)
-                al.append(1.0)
-        sT = _dense_tasks(Ac, ldim, A, a_off, 1, Ac, b_off, ldim, 1, None, ldim, al, grp, 0)
-        # D[nm, l, r] = sum_p w_p sum_c T[p, nm, c, l] Rd[p, c, r]
-        a_off, b_off, al, grp = [], [], [], []
-        for nm in range(16):
-            ids = []
-            for p in range(nops):
-                ids.append(len(a_off))
-                a_off.append((p * 16 + nm) * Ac * ldim)
-                b_off.append(p * Ac * rdim)
-                al.append(hp[p])
-            grp.append((nm * ldim * rdim, ids))
-        sD = _dense_tasks(ldim, rdim, Ac, a_off, 1, ldim, b_off, rdim, 1, None, rdim, al, grp, 0)
-        self.sX = Stage({0: [sX]}, dev, "diagX")
-        self.sT = Stage({0: [sT]}, dev, "diagT")
-        self.sD = Stage({0: [sD]}, dev, "diagD")
+        self.sX, self.sT, self.sD = _diag_stages(dev, nops, A, Ab, Ac, ldim, rdim, hp)
         self.nX = nops * 16 * A * Ac
         self.nT = nops * 16 * Ac * ldim
         self.nD = 16 * ldim * rdim
