@@ -148,14 +148,14 @@ class OracleDMRG(object):
                 q = QTensor([False, False, True])
                 q.from_dense(site, [self.qnuml[isite], QPHYS, qred])
                 self.lmps[isite] = q
-                self.lenv[isite] = RenormOracle(self.opers, isite, "L")(q, self.lenv[isite - 1], self.mpo[isite])
+                self.renormalize(isite, "L", q)
             else:
                 j = isite + 1
                 self.qnumr[j] = qred
                 q = QTensor([True, False, False])
                 q.from_dense(site, [qred, QPHYS, self.qnumr[j + 1]])
                 self.rmps[j] = q
-                self.renv[j] = RenormOracle(self.opers, j, "R")(q, self.renv[j + 1], self.mpo[j])
+                self.renormalize(j, "R", q)
             self.timings["renorm"] += time.time() - t0
             self.guess(isite, status, actlst, civecs, srotR)
             self.log.append({"status": status, "isite": isite, "e": float(eig[0]), "dwt": float(dwts),
@@ -176,6 +176,13 @@ class OracleDMRG(object):
         eav_i = int(numpy.argmin(elst))
         self.nmvp_total += nmvp
         return nmvp, elst[eav_i], dlst[eav_i], elst, dlst
+
+    def renormalize(self, isite, status, q):
+        """renorm (mpo_dmrg_kernel.py:347-377): new environments of site isite."""
+        if status == "L":
+            self.lenv[isite] = RenormOracle(self.opers, isite, "L")(q, self.lenv[isite - 1], self.mpo[isite])
+        else:
+            self.renv[isite] = RenormOracle(self.opers, isite, "R")(q, self.renv[isite + 1], self.mpo[isite])
 
     def guess(self, isite, status, actlst, civecs, srotR):
         if not self.ifguess:

@@ -129,3 +129,80 @@ def davidson_steps(diag, neig=1, v0=None, crit_e=1.e-8, crit_vec=1.e-8, maxcycle
         vbas = torch.cat([vbas, vbas2])
         wbas = torch.cat([wbas, wbas2])
     return DavidsonResult(eigs.cpu().numpy(), vr @ vbas, nmvp, maxcycle, rnorms)
+
+
+def _gen_ortho(vbas, crit_indp):
+    """First row normalised, the others orthonormalised against it and each other
+    (pgdvdson.genOrthoBas, source/tools/pgdvdson.py:362-374)."""
+    v0 = vbas[0:1] / torch.linalg.norm(vbas[0])
+    if vbas.shape[0] == 1:
+        return v0
+    n, v2 = _ortho(v0, vbas[1:], crit_indp)
+    return torch.cat([v0, v2]) if n else v0
+
+
+def _eigh_general(h, s):
+    """Generalised symmetric eigenproblem h x = e s x with s positive definite, by the
+    Cholesky reduction s = C C^T: eigenvectors normalised to x^T s x = 1 (as LAPACK sygvd)."""
+    c, info = torch.linalg.cholesky_ex(s)
+    if int(info) != 0:
+        raise RuntimeError("generalised Davidson: the subspace metric is not positive definite")
+    a = torch.linalg.solve_triangular(c, h, upper=False)
+    a = torch.linalg.solve_triangular(c, a.T, upper=False)
+    a = 0.5 * (a + a.T)
+    e, y = torch.linalg.eigh(a)
+    x = torch.linalg.solve_triangular(c.T, y, upper=True)
+    return e, x
+
+
+def gdavidson(hvec, svec, diag, neig=1, v0=None, crit_e=1.e-8, crit_vec=1.e-8, maxcycle=20, crit_indp=1.e-12,
+              lshift=1.e-4, nfac=10):
+    """Lowest ``neig`` solutions of H x = e S x (pgdvdson.eigenSolver.solve_iter,
+    source/tools/pgdvdson.py:90-330): the subspace problem is generalised, residuals are
+    H x - e S x, the restart keeps span{x, x_old - x} orthonormalised by genOrthoBas, the
+    preconditioner is iop=4 and the start vectors carry no noise.  The returned vectors
+    are S-normalised.  Both products are called one vector at a time (HSVecs, :63-75)."""
+    ndim = diag.numel()
+    if neig > ndim:
+        raise ValueError("neig > ndim")
+    vbas = gen_v0(diag, neig) if v0 is None else v0.reshape(neig, ndim).to(torch.float64).clone()
+    vbas = _gen_ortho(vbas, crit_indp)
+    wbas = torch.stack([hvec(v) for v in vbas])
+    sbas = torch.stack([svec(v) for v in vbas])
+    nmvp = vbas.shape[0]
+    eigs = torch.full((neig,), 1.e3, dtype=torch.float64, device=diag.device)
+    rnorms = []
+    for niter in range(1, maxcycle):
+        h = vbas @ wbas.T
+        s = vbas @ sbas.T
+        e, u = _eigh_general(0.5 * (h + h.T), 0.5 * (s + s.T))
+        vr = u[:, :neig].T.contiguous()
+        teig = e[:neig]
+        econv = (teig - eigs).abs() <= crit_e
+        eigs = teig.clone()
+        rbas = vr @ wbas - eigs[:, None] * (vr @ sbas)
+        rn_h = torch.linalg.norm(rbas, dim=1).cpu().tolist()
+        ec_h = econv.cpu().tolist()
+        rnorms.append(rn_h)
+        rconv = [x <= crit_vec for x in rn_h]
+        rindx = [i for i in range(neig) if not rconv[i] and not ec_h[i]]
+        if len(rindx) == 0 or niter == maxcycle - 1:
+            return DavidsonResult(eigs.cpu().numpy(), vr @ vbas, nmvp, niter, rnorms)
+        nsub = vbas.shape[0]
+        if nsub > nfac * neig:
+            pr = torch.eye(nsub, dtype=torch.float64, device=diag.device)[:neig, :] - vr
+            vr = _gen_ortho(torch.cat([vr, pr[rindx, :]]), crit_indp)
+            vbas, wbas, sbas = vr @ vbas, vr @ wbas, vr @ sbas
+        for i in range(neig):
+            if not rconv[i]:
+                rbas[i] = rbas[i] / ((diag - eigs[i]).abs() + lshift)
+        nindp, vbas2 = _ortho(vbas, rbas[rindx, :], crit_indp)
+        if nindp == 0:
+            raise RuntimeError("generalised Davidson: unable to generate a new direction")
+        wbas2 = torch.stack([hvec(v) for v in vbas2])
+        sbas2 = torch.stack([svec(v) for v in vbas2])
+        nmvp += nindp
+        vbas = torch.cat([vbas, vbas2])
+        wbas = torch.cat([wbas, wbas2])
+        sbas = torch.cat([sbas, sbas2])
+    return DavidsonResult(eigs.cpu().numpy(), vr @ vbas, nmvp, maxcycle, rnorms)

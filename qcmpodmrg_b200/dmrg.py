@@ -60,14 +60,12 @@ def boundary_set(nops, device):
 class DMRG(object):
     """Two-site MPO-DMRG with every hot-path contraction on the GPU."""
 
+    ifs2proj = False          # spin projection: qcmpodmrg_b200.spin.SPDMRG
+
     def __init__(self, ham, device="cuda", precision="f64", preconditioner=None, w_path="fiber", plan_cache=False):
         self.ham = ham
         self.device = torch.device(device)
         self.nsite = ham.nsite
-        self.nops = ham.sbas
-        self.opers = list(range(ham.sbas))
-        self.hpwts = numpy.ones(self.nops)
-        self.qkey = numpy.array([float(ham.nelec), 0.0])
         self.precision = precision
         self.preconditioner = preconditioner
         # kernels of the two MPO-site contractions of sigma: "generic" grouped GEMM,
@@ -84,8 +82,7 @@ class DMRG(object):
         # operators it returns were checked bitwise against freshly compiled ones)
         self.plan_cache_size = 2 * self.nsite if plan_cache else 0
         t0 = time.time()
-        mpo = build_mpo(ham)
-        self.mpo = {i: TensorSet(l, v, device=self.device) for i, (l, v) in mpo.items()}
+        self._setup_operators(ham)
         self.t_mpo = time.time() - t0
         self.log = []
         self.stats = {"hvec_s": 0.0, "hdiag_s": 0.0, "renorm_s": 0.0, "decim_s": 0.0, "plan_s": 0.0,
@@ -99,6 +96,15 @@ class DMRG(object):
         self.d2h_bytes = 0
 
     # ------------------------------------------------------------- set-up
+    def _setup_operators(self, ham):
+        """H = sum_p H_p, one operator per spin orbital (mpo_dmrg_class.partition, one rank)."""
+        self.nops = ham.sbas
+        self.opers = list(range(ham.sbas))
+        self.hpwts = numpy.ones(self.nops)
+        self.qkey = numpy.array([float(ham.nelec), 0.0])
+        mpo = build_mpo(ham)
+        self.mpo = {i: TensorSet(l, v, device=self.device) for i, (l, v) in mpo.items()}
+
     def load_mps(self, init):
         K = self.nsite
         dev = self.device
@@ -235,16 +241,24 @@ class DMRG(object):
             self.qnuml[isite + 1] = qred
             st = SiteTensor(site, [self.qnuml[isite], QPHYS, qred], L_STATUS, dev)
             self.lmps[isite] = st
-            rn = Renormalizer(self.ws, isite, "L", st.layout, self.lenv[isite - 1], self.mpo[isite], self.opers)
-            self.lenv[isite] = rn(st.values)
+            self.stats["renorm_flops"] += self.renormalize(isite, "L", st)
         else:
             j = isite + 1
             self.qnumr[j] = qred
             st = SiteTensor(site, [qred, QPHYS, self.qnumr[j + 1]], R_STATUS, dev)
             self.rmps[j] = st
+            self.stats["renorm_flops"] += self.renormalize(j, "R", st)
+
+    def renormalize(self, j, status, st):
+        """New environments of site j from its site tensor (renorm, mpo_dmrg_kernel.py:347-377);
+        returns the FLOPs launched."""
+        if status == "L":
+            rn = Renormalizer(self.ws, j, "L", st.layout, self.lenv[j - 1], self.mpo[j], self.opers)
+            self.lenv[j] = rn(st.values)
+        else:
             rn = Renormalizer(self.ws, j, "R", st.layout, self.renv[j + 1], self.mpo[j], self.opers)
             self.renv[j] = rn(st.values)
-        self.stats["renorm_flops"] += rn.flops
+        return rn.flops
 
     def boundary(self, status, qred, srotR):
         K = self.nsite
@@ -423,19 +437,17 @@ class DMRG(object):
                 self.qnuml[isite + 1] = qred
                 st = SiteTensor(site, [self.qnuml[isite], QPHYS, qred], L_STATUS, dev)
                 self.lmps[isite] = st
-                rn = Renormalizer(self.ws, isite, "L", st.layout, self.lenv[isite - 1], self.mpo[isite], self.opers)
-                self.lenv[isite] = rn(st.values)
+                rflops = self.renormalize(isite, "L", st)
             else:
                 j = isite + 1
                 self.qnumr[j] = qred
                 st = SiteTensor(site, [qred, QPHYS, self.qnumr[j + 1]], R_STATUS, dev)
                 self.rmps[j] = st
-                rn = Renormalizer(self.ws, j, "R", st.layout, self.renv[j + 1], self.mpo[j], self.opers)
-                self.renv[j] = rn(st.values)
+                rflops = self.renormalize(j, "R", st)
             # no synchronisation here: the next dot's plans are compiled on the host while
             # the renormalisation runs (renorm_s is host time: plan + launches)
             self.stats["renorm_s"] += time.time() - t0
-            self.stats["renorm_flops"] += rn.flops
+            self.stats["renorm_flops"] += rflops
             self.guess(isite, status, actlst, civecs, srotR)
             self.log.append({"status": status, "isite": isite, "e": elst[-1], "dwt": dlst[-1],
                              "nmvp": int(res.nmvp), "bond": int(len(qred)), "ndim0": int(sig.ndim0),

@@ -92,6 +92,14 @@ def gather(src, idx, out):
     return out
 
 
+def scatter(src, idx, out):
+    """out = 0; out[idx[i]] = src[i] on the device (qc_scatter_f64)."""
+    check(native.lib().qc_scatter_f64(src.data_ptr(), idx.data_ptr(), out.data_ptr(), idx.numel(), out.numel(),
+                                      _stream(out.device)), "qc_scatter_f64")
+    LOG.launches += 1
+    return out
+
+
 def convert(src, out):
     """FP64 <-> FP32 conversion on the device."""
     lib = native.lib()

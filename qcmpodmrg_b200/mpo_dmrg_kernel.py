@@ -5,8 +5,15 @@ mpo_dmrg_dot.ci_solver, dotutil.genHDiag and mpo_dmrg_opt.sweep call:
 
   HDiag(info, ndim0, prjmap)                       source/mpo_dmrg_kernel.py:41-51
   HVec(vec0, info, ndim0, prjmap)                  source/mpo_dmrg_kernel.py:117-136
+  SDiag(info, ndim0, prjmap)                       source/mpo_dmrg_kernel.py:183-190
+  SVec(vec0, info, ndim0, prjmap)                  source/mpo_dmrg_kernel.py:226-231
   renorm(dmrg, isite, ncsite, flst, flstN, site, status)   :347-377
   pRDM(cimat, info)                                :278-282 (noise-free part)
+
+With a spin-projected ``dmrg`` (qcmpodmrg_b200.spin.SPDMRG, the reference's
+ifs2proj) HVec/HDiag are the projected Hamiltonian's, SVec/SDiag the projector's
+(zero without projection, as in the reference), and renorm also renormalises the
+projector's environments (renormQt_S00), stored in ``flstN[0][1]``.
 
 ``info = [dmrg, isite, ncsite, flst, status, ifsym]`` as in mpo_dmrg_dot.py:31.
 Here ``dmrg`` is a qcmpodmrg_b200.dmrg.DMRG (device-resident environments);
@@ -18,7 +25,6 @@ the two-site Qt path exists (ncsite == 2, ifQt); anything else raises.
 import numpy
 import torch
 
-from .kernels import Renormalizer
 
 
 def _check(info):
@@ -61,24 +67,55 @@ def HDiag(info, ndim0, prjmap):
     return dg().cpu().numpy()
 
 
+def _sops(dmrg, isite):
+    """Projector operators of a spin-projected dot, cached like _ops."""
+    PL, PR = dmrg.plenv[isite - 1], dmrg.prenv[isite + 2]
+    cache = getattr(dmrg, "_sdot_cache", None)
+    if cache is None or cache[0] != isite or cache[1] is not PL or cache[2] is not PR:
+        sv, sd = dmrg.dot_projector(isite)
+        dmrg._sdot_cache = (isite, PL, PR, sv, sd)
+    return dmrg._sdot_cache[3:]
+
+
+def SVec(vec0, info, ndim0, prjmap):
+    """S vec0 = P vec0 with the spin projector in the packed layout (SVecQt); zero
+    without spin projection."""
+    dmrg, isite = _check(info)
+    if not getattr(dmrg, "ifs2proj", False):
+        z = numpy.zeros(ndim0)
+        return torch.from_numpy(z).to(vec0.device) if torch.is_tensor(vec0) else z
+    sv, sd = _sops(dmrg, isite)
+    if ndim0 != sv.ndim0:
+        raise ValueError("ndim0 does not match the dot's wavefunction template")
+    y = sv(_to_dev(vec0, dmrg.device))
+    return y if torch.is_tensor(vec0) else y.cpu().numpy()
+
+
+def SDiag(info, ndim0, prjmap):
+    """Diagonal of the spin projector in the packed layout (SDiagQt); zero without projection."""
+    dmrg, isite = _check(info)
+    if not getattr(dmrg, "ifs2proj", False):
+        return numpy.zeros(ndim0)
+    sv, sd = _sops(dmrg, isite)
+    return sd().cpu().numpy()
+
+
 def renorm(dmrg, isite, ncsite, flst, flstN, site, status):
-    """New environments of every operator; stored in flstN[0][0] and in dmrg's env table.
+    """New environments of every operator; stored in flstN[0][0] and in dmrg's env table
+    (with spin projection also the projector's, renormQt_S00, in flstN[0][1]).
 
     ``site`` is a qcmpodmrg_b200.dmrg.SiteTensor (packed values on the device).
     """
     if ncsite != 2:
         raise NotImplementedError("only the two-site dot is implemented")
-    if status == "L":
-        rn = Renormalizer(dmrg.ws, isite, "L", site.layout, dmrg.lenv[isite - 1], dmrg.mpo[isite], dmrg.opers)
-        new = rn(site.values)
-        dmrg.lenv[isite] = new
-    else:
-        j = isite + ncsite - 1
-        rn = Renormalizer(dmrg.ws, j, "R", site.layout, dmrg.renv[j + 1], dmrg.mpo[j], dmrg.opers)
-        new = rn(site.values)
-        dmrg.renv[j] = new
+    j = isite if status == "L" else isite + ncsite - 1
+    dmrg.renormalize(j, status, site)
+    sp = getattr(dmrg, "ifs2proj", False)
+    new = dmrg.lenv[j] if status == "L" else dmrg.renv[j]
     if flstN is not None:
         flstN[0][0] = new
+        if sp:
+            flstN[0][1] = dmrg.plenv[j] if status == "L" else dmrg.prenv[j]
     return 0
 
 

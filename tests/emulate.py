@@ -93,6 +93,13 @@ def patch_stage_run(monkeypatch):
 
     monkeypatch.setattr(kernels, "gather", gather)
 
+    def scatter(src, idx, out):
+        out.zero_()
+        out[idx] = src[:idx.numel()]
+        return out
+
+    monkeypatch.setattr(kernels, "scatter", scatter)
+
     def reduce_ops(part, nops, n, out):
         out[:n].copy_(part[:nops * n].reshape(nops, n).sum(0).to(out.dtype))
         return out

@@ -80,8 +80,12 @@ class Recorder(object):
 
 
 def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.0,
-                  tol=1.e-7, maxslc=1, record_envs=True, workdir=None):
-    """Run the reference flow; return (result dict, recorder)."""
+                  tol=1.e-7, maxslc=1, record_envs=True, workdir=None, npts=None, sval=0.0, sz=0.0):
+    """Run the reference flow; return (result dict, recorder).
+
+    npts: spin projection (SP-MPS) with ``npts`` quadrature points for <S^2> = sval(sval+1),
+    Sz = sz, set as examples/examples_spmpsQt/main_spmps.py does (ifs2proj, s2quad).
+    """
     mpo_dmrg_class, mpo_dmrg_schedule, mpo_dmrg_kernel, qtensor_api, qtensor, class_molinfo = _ref()
     from qcmpodmrg.source import mpo_dmrg_io
     ham = make_hamiltonian(K, N, seed, decay)
@@ -89,7 +93,8 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
     cwd = os.getcwd()
     os.chdir(wd)
     rec = Recorder(targets)
-    orig = (mpo_dmrg_kernel.HVec, mpo_dmrg_kernel.HDiag, mpo_dmrg_kernel.renorm)
+    orig = (mpo_dmrg_kernel.HVec, mpo_dmrg_kernel.HDiag, mpo_dmrg_kernel.renorm,
+            mpo_dmrg_kernel.SVec, mpo_dmrg_kernel.SDiag)
     try:
         write_mole(os.path.join(wd, "mole.h5"), ham)
         mol = class_molinfo()
@@ -135,6 +140,10 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
         dmrg2.ifdvdnz = False
         sc2 = mpo_dmrg_schedule.schedule()
         sc2.fixed(ncsite=2, maxM=D, maxiter=nsweeps, tol=tol, noise=noise)
+        if npts is not None:
+            dmrg2.ifs2proj = True
+            dmrg2.npts = npts
+            dmrg2.s2quad(sval, sz)
         mol.build()
         dmrg2.path = mol.path
         dmrg2.partition()
@@ -166,6 +175,36 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
                     r["mpo_j"] = _load_mpo(qtensor, d.fhop, isite + 1, d.nops)
                 r["hpwts"] = numpy.array(d.hpwts)
                 r["opers"] = numpy.array([o[0] for o in d.opers])
+                if npts is not None:
+                    r["opers_ipt"] = numpy.array([o[1] for o in d.opers])
+                    r["qpts"] = numpy.array(d.qpts, dtype=numpy.float64)
+                    r["qwts"] = numpy.array(d.qwts, dtype=numpy.float64)
+            return out
+
+        def svec_hook(vec0, info, ndim0, prjmap):
+            out = orig[3](vec0, info, ndim0, prjmap)
+            d, isite, ncsite, flst, status, ifsym = info
+            k = (d.isweep, status, isite)
+            r = rec.records.setdefault(k, {})
+            if k in rec.targets and "svec_x" not in r:
+                r["svec_x"] = numpy.array(vec0)
+                r["svec_y"] = numpy.array(out)
+                # the two-site sweep never calls SDiag (only PT does): record it on the same dot
+                r["sdiag"] = numpy.array(orig[4](info, ndim0, prjmap))
+                if record_envs:
+                    fLp, fRp = flst[0][2:4]
+                    r["penvL"] = [qt_to_dict(_load_qt(qtensor, fLp, "opers%d" % i)) for i in range(d.npts)]
+                    r["penvR"] = [qt_to_dict(_load_qt(qtensor, fRp, "opers%d" % i)) for i in range(d.npts)]
+                    r["pop"] = [qt_to_dict(_load_qt(qtensor, d.fpop, "op%d" % i)) for i in range(d.npts)]
+            return out
+
+        def sdiag_hook(info, ndim0, prjmap):
+            out = orig[4](info, ndim0, prjmap)
+            d, isite, ncsite, flst, status, ifsym = info
+            k = (d.isweep, status, isite)
+            r = rec.records.setdefault(k, {})
+            if k in rec.targets and "sdiag" not in r:
+                r["sdiag"] = numpy.array(out)
             return out
 
         def hdiag_hook(info, ndim0, prjmap):
@@ -185,11 +224,16 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
                 r["renorm_site"] = qt_to_dict(site)
                 if record_envs:
                     r["renorm_out"] = _load_envs(qtensor, flstN[0][0], d.nops)
+                    if npts is not None:
+                        r["renorm_pout"] = [qt_to_dict(_load_qt(qtensor, flstN[0][1], "opers%d" % i))
+                                            for i in range(d.npts)]
             return out
 
         mpo_dmrg_kernel.HVec = hvec_hook
         mpo_dmrg_kernel.HDiag = hdiag_hook
         mpo_dmrg_kernel.renorm = renorm_hook
+        mpo_dmrg_kernel.SVec = svec_hook
+        mpo_dmrg_kernel.SDiag = sdiag_hook
         dmrg2.default(sc2, flmps1)
         result = {
             "K": K, "N": N, "D": D, "seed": seed, "decay": decay, "nsweeps": nsweeps,
@@ -199,7 +243,8 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
             "init_mps": init_mps,
         }
     finally:
-        mpo_dmrg_kernel.HVec, mpo_dmrg_kernel.HDiag, mpo_dmrg_kernel.renorm = orig
+        (mpo_dmrg_kernel.HVec, mpo_dmrg_kernel.HDiag, mpo_dmrg_kernel.renorm,
+         mpo_dmrg_kernel.SVec, mpo_dmrg_kernel.SDiag) = orig
         os.chdir(cwd)
     return result, rec
 
@@ -212,6 +257,12 @@ def _load_envs(qtensor, f, nops):
         assert q.nslc == 1, "fixtures assume maxslc=1"
         out.append(qt_to_dict(q.dic[0]))
     return out
+
+
+def _load_qt(qtensor, f, name):
+    q = qtensor.qtensor()
+    q.load(f, name)
+    return q
 
 
 def _load_mpo(qtensor, fhop, isite, nops):

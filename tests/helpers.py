@@ -57,3 +57,55 @@ def record_renormalizer(r, device):
         E, W, j = tensorset(r["envR"], device), tensorset(r["mpo_j"], device), isite + 1
     rn = Renormalizer(ws, j, status, site, E, W, opers)
     return rn, numpy.asarray(r["renorm_site"]["value"], dtype=numpy.float64)
+
+
+def record_sp_operators(r, device, use_fiber=True, fuse_w=False):
+    """Projected H and S operators (+ diagonals) of a recorded spin-projected reference dot."""
+    from qcmpodmrg_b200.kernels import SigmaOperator, DiagOperator, Workspace
+    from qcmpodmrg_b200.spin import ProjectedOperator, reduce_layout, reduce_map
+    import torch
+    ws = Workspace(torch.device(device))
+    isite = int(r["key"][2])
+    lay = layout_of(r["qtmp"])
+    lay_n = reduce_layout(lay)
+    red = reduce_map(lay, lay_n)
+    qkey = numpy.asarray(r["qkey"], dtype=numpy.float64)
+    opers = [int(x) for x in numpy.atleast_1d(r["opers"])]
+    hp = numpy.atleast_1d(r["hpwts"]).astype(numpy.float64)
+    L, R = tensorset(r["envL"], device), tensorset(r["envR"], device)
+    Wi, Wj = tensorset(r["mpo_i"], device), tensorset(r["mpo_j"], device)
+    PL, PR, P = tensorset(r["penvL"], device), tensorset(r["penvR"], device), tensorset(r["pop"], device)
+    qw = numpy.atleast_1d(r["qwts"]).astype(numpy.float64)
+    popers = [0] * len(qw)
+    opts = {"use_fiber": use_fiber, "fuse_w": fuse_w}
+    sig = ProjectedOperator(ws, SigmaOperator(ws, isite, lay_n, L, R, Wi, Wj, qkey[:1], opers, hp, **opts), red)
+    sv = ProjectedOperator(ws, SigmaOperator(ws, isite, lay_n, PL, PR, P, P, qkey[:1], popers, qw, **opts), red)
+    dg = DiagOperator(ws, isite, lay, L, R, Wi, Wj, qkey, opers, hp)
+    sd = DiagOperator(ws, isite, lay, PL, PR, P, P, qkey, popers, qw)
+    return sig, sv, dg, sd, ws
+
+
+def record_sp_renormalizers(r, device):
+    """Renormalizers of the H and projector environments for a recorded SP dot, and the
+    N-reduced site values they take."""
+    from qcmpodmrg_b200.kernels import Renormalizer, Workspace
+    from qcmpodmrg_b200.spin import reduce_layout, reduce_map
+    import torch
+    ws = Workspace(torch.device(device))
+    isite = int(r["key"][2])
+    status = "L" if int(r["key"][1]) == 0 else "R"
+    site = layout_of(r["renorm_site"])
+    site_n = reduce_layout(site)
+    vals = numpy.zeros(site_n.size)
+    vals[reduce_map(site, site_n)] = numpy.asarray(r["renorm_site"]["value"], dtype=numpy.float64)
+    opers = [int(x) for x in numpy.atleast_1d(r["opers"])]
+    P = tensorset(r["pop"], device)
+    popers = [0] * len(r["pop"])
+    if status == "L":
+        E, PE, W, j = tensorset(r["envL"], device), tensorset(r["penvL"], device), tensorset(r["mpo_i"], device), isite
+    else:
+        E, PE, W, j = (tensorset(r["envR"], device), tensorset(r["penvR"], device), tensorset(r["mpo_j"], device),
+                       isite + 1)
+    rn = Renormalizer(ws, j, status, site_n, E, W, opers)
+    rp = Renormalizer(ws, j, status, site_n, PE, P, popers)
+    return rn, rp, vals

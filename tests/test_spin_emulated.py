@@ -1,0 +1,131 @@
+"""Spin projection on the product's plans, with the kernels interpreted on the CPU:
+the projected H / S operators, their diagonals, both renormalisations and a sweep
+reproduce the reference's outputs (tests/golden/*SP_K*.npz)."""
+import numpy
+import pytest
+import torch
+
+from helpers import load, record_sp_operators, record_sp_renormalizers
+from emulate import patch_stage_run
+from qcmpodmrg_b200.hamiltonian import make_hamiltonian
+
+
+@pytest.mark.parametrize("tag", ["SP_K4", "SP_K5"])
+@pytest.mark.parametrize("w_path", ["generic", "fiber"])
+def test_sp_operators_emulated(tag, w_path, monkeypatch):
+    patch_stage_run(monkeypatch)
+    for r in load("kernels_%s.npz" % tag)["records"]:
+        sig, sv, dg, sd, ws = record_sp_operators(r, "cpu", use_fiber=(w_path == "fiber"))
+        y = sig(torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))).numpy()
+        assert numpy.abs(y - r["hvec_y"]).max() <= 1e-12 * max(1.0, numpy.abs(r["hvec_y"]).max())
+        s = sv(torch.from_numpy(numpy.asarray(r["svec_x"], dtype=numpy.float64))).numpy()
+        assert numpy.abs(s - r["svec_y"]).max() <= 1e-13
+        assert numpy.abs(dg().numpy() - r["hdiag"]).max() <= 1e-12
+        assert numpy.abs(sd().numpy() - r["sdiag"]).max() <= 1e-13
+
+
+@pytest.mark.parametrize("tag", ["SP_K4", "SP_K5"])
+def test_sp_renormalizers_emulated(tag, monkeypatch):
+    patch_stage_run(monkeypatch)
+    for r in load("kernels_%s.npz" % tag)["records"]:
+        rn, rp, vals = record_sp_renormalizers(r, "cpu")
+        site = torch.from_numpy(vals)
+        for op, ref in ((rn, r["renorm_out"]), (rp, r["renorm_pout"])):
+            out = op(site)
+            for i, b in enumerate(ref):
+                assert out.layouts[i].size == len(b["value"])
+                assert numpy.abs(out.op_values(i).numpy() - b["value"]).max() <= 1e-12
+
+
+def test_gdavidson_device_matches_oracle():
+    from oracle.spin import gdavidson as ogd
+    from qcmpodmrg_b200.davidson import gdavidson
+    rng = numpy.random.default_rng(1)
+    n = 90
+    h = rng.uniform(-1, 1, (n, n))
+    h = numpy.diag(numpy.arange(n) * 0.5) + h + h.T
+    s = rng.uniform(0, 1, (n, n))
+    s = numpy.diag(rng.uniform(0.8, 1.0, n)) + 0.05 * (s + s.T)
+    ht, st = torch.from_numpy(h), torch.from_numpy(s)
+    r = gdavidson(lambda x: ht @ x, lambda x: st @ x, torch.from_numpy(numpy.diag(h).copy()), 1, crit_e=1e-12,
+                  crit_vec=1e-9, maxcycle=60)
+    e, v, nm = ogd(lambda x: h @ x, lambda x: s @ x, numpy.diag(h).copy(), 1, crit_e=1e-12, crit_vec=1e-9,
+                   maxcycle=60)
+    assert abs(r.eigs[0] - e[0]) < 1e-11 and r.nmvp == nm
+    x = r.vecs[0].numpy()
+    assert abs(x @ s @ x - 1.0) < 1e-12
+
+
+def test_sp_sweep_emulated(monkeypatch):
+    """One R+L sweep of the spin-projected K=4 run: every dot's energy as the reference's."""
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    from qcmpodmrg_b200.spin import SPDMRG
+    sw = load("sweep_SP_K4.npz")
+    ham = make_hamiltonian(int(sw["K"]), int(sw["N"]), int(sw["seed"]), None)
+    d = SPDMRG(ham, int(sw["npts"]), device="cpu")
+    out = d.run(sw["init_mps"], int(sw["D"]), 1)
+    n = len(out["esweeps"])
+    assert n == 2 * (int(sw["K"]) - 1)
+    assert numpy.abs(out["esweeps"] - sw["esweeps"][:n]).max() <= 1e-8
+    assert abs(out["eav"][0] - sw["eav"][0]) <= 1e-8
+    assert out["nmvp"][0] == sw["nmvp"][0]
+
+
+def test_sp_dropin_matches_oracle_on_same_dot(monkeypatch):
+    """mpo_dmrg_kernel.HVec/SVec/HDiag/SDiag/renorm on a spin-projected DMRG equal the oracle
+    computing the same dot from the same MPS (environments built independently)."""
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    _dropin_vs_oracle("cpu")
+
+
+def _dropin_vs_oracle(device):
+    from oracle import spin as ospin
+    from oracle.blocks import QTensor, classification
+    from oracle.mpo import QPHYS
+    from oracle.kernels import hdiag
+    from qcmpodmrg_b200 import mpo_dmrg_kernel as MK
+    from qcmpodmrg_b200.spin import SPDMRG
+    sw = load("sweep_SP_K5.npz")
+    ham = make_hamiltonian(int(sw["K"]), int(sw["N"]), int(sw["seed"]), sw["decay"])
+    npts = int(sw["npts"])
+    d = SPDMRG(ham, npts, device=device)
+    d.load_mps(sw["init_mps"])
+    o = ospin.SPOracleDMRG(ham, npts)
+    o.load_mps(sw["init_mps"])
+    K = int(sw["K"])
+    isite = K - 2                     # first dot of the R sweep: L environments from the MPS
+    qtmp = QTensor([False, False, False, True])
+    cls = [classification(q) for q in (o.qnuml[isite], QPHYS, QPHYS, o.qkey - o.qnumr[isite + 2])]
+    qtmp.from_qsyms(4, [c[0] for c in cls], [c[1] for c in cls])
+    prjmap = qtmp.prjmap([c[2] for c in cls])
+    ndim0 = qtmp.size_allowed
+    x = numpy.random.default_rng(5).standard_normal(ndim0)
+    info = [d, isite, 2, [[d.lenv[isite - 1], d.renv[isite + 2]]], "R", True]
+    L, R = o.lenv[isite - 1], o.renv[isite + 2]
+    Wi, Wj = o.mpo[isite], o.mpo[isite + 1]
+    PL, PR = o.plenv[isite - 1], o.prenv[isite + 2]
+    yh = ospin.sigma_sp(qtmp, o.qkey, L, R, Wi, Wj, o.opers, o.hpwts, isite)(x)
+    ys = ospin.svec(qtmp, o.qkey, PL, PR, o.pops, o.qwts, isite)(x)
+    assert numpy.abs(MK.HVec(x, info, ndim0, prjmap) - yh).max() <= 1e-12 * max(1.0, numpy.abs(yh).max())
+    assert numpy.abs(MK.SVec(x, info, ndim0, prjmap) - ys).max() <= 1e-13
+    ldim, rdim = len(o.qnuml[isite]), len(o.qnumr[isite + 2])
+    dims = (ldim, 16, rdim, ldim * 16 * rdim)
+    assert numpy.abs(MK.HDiag(info, ndim0, prjmap) - hdiag(prjmap, dims, L, R, Wi, Wj, o.hpwts)).max() <= 1e-12
+    sd = ospin.sdiag(prjmap, dims, PL, PR, o.pops, o.qwts)
+    assert numpy.abs(MK.SDiag(info, ndim0, prjmap) - sd).max() <= 1e-13
+    # the reference's own consistency check (checkDiagQt, kernelQt.py:129-150): the
+    # effective operators are symmetric and their diagonals are HDiag / SDiag
+    if ndim0 <= 64:
+        eye = numpy.identity(ndim0)
+        for vec, dia in ((MK.HVec, MK.HDiag), (MK.SVec, MK.SDiag)):
+            m = numpy.array([vec(e, info, ndim0, prjmap) for e in eye]).T
+            assert numpy.abs(m - m.T).max() <= 1e-12
+            assert numpy.abs(numpy.diag(m) - dia(info, ndim0, prjmap)).max() <= 1e-12
+    # renorm of the L environments of site 0 from the MPS: H and projector sets
+    flstN = [[None, None]]
+    MK.renorm(d, 0, 2, None, flstN, d.lmps[0], "L")
+    for E, ref in ((flstN[0][0], o.lenv[0]), (flstN[0][1], o.plenv[0])):
+        for i, q in enumerate(ref):
+            assert numpy.abs(E.op_values(i).cpu().numpy() - q.value).max() <= 1e-12

@@ -7,7 +7,7 @@ import numpy
 import pytest
 import torch
 
-from helpers import load, record_operators
+from helpers import load, record_operators, record_sp_operators
 from emulate import patch_stage_run
 from qcmpodmrg_b200.engine import CompositeStage, FiberStage, PanelStage, PANEL_TILES
 
@@ -60,27 +60,44 @@ def _panel_writes(ps):
     return numpy.concatenate(out) if out else numpy.zeros(0, dtype=numpy.int64)
 
 
+def _check_sigma_writes(sig):
+    ndst = {"sigma1": sig.tot[0], "sigma2": sig.tot[1], "sigma3": sig.tot[2], "sigma23": sig.tot[2],
+            "sigma4": sig.nops * sig.ndim0}
+    stages = list(sig.stages) + ([sig.fused] if sig.fused is not None else [])
+    for st in stages:
+        for sub in _subs(st):
+            if isinstance(sub, FiberStage) and sub.ntasks:
+                w = _fiber_writes(sub)
+                assert w.min() >= 0 and w.max() < ndst[sub.name], sub.name
+                assert len(numpy.unique(w)) == len(w), "overlapping writes in " + sub.name
+                src = {"sigma2": sig.tot[0], "sigma3": sig.tot[1], "sigma23": sig.tot[0]}[sub.name]
+                assert _fiber_reads(sub) < src, sub.name
+            if isinstance(sub, PanelStage) and sub.groups:
+                w = _panel_writes(sub)
+                assert w.min() >= 0 and w.max() < ndst[sub.name], sub.name
+                assert len(numpy.unique(w)) == len(w), "overlapping writes in " + sub.name
+
+
 @pytest.mark.parametrize("tag", ["K4", "K5", "K6"])
 @pytest.mark.parametrize("fuse", [False, True])
 def test_fiber_and_panel_writes_in_bounds_and_disjoint(tag, fuse, monkeypatch):
     patch_stage_run(monkeypatch)
     for r in load("kernels_%s.npz" % tag)["records"]:
         sig, _, _ = record_operators(r, "cpu", use_fiber=True, fuse_w=fuse)
-        ndst = {"sigma1": sig.tot[0], "sigma2": sig.tot[1], "sigma3": sig.tot[2], "sigma23": sig.tot[2],
-                "sigma4": sig.nops * sig.ndim0}
-        stages = list(sig.stages) + ([sig.fused] if sig.fused is not None else [])
-        for st in stages:
-            for sub in _subs(st):
-                if isinstance(sub, FiberStage) and sub.ntasks:
-                    w = _fiber_writes(sub)
-                    assert w.min() >= 0 and w.max() < ndst[sub.name], sub.name
-                    assert len(numpy.unique(w)) == len(w), "overlapping writes in " + sub.name
-                    src = {"sigma2": sig.tot[0], "sigma3": sig.tot[1], "sigma23": sig.tot[0]}[sub.name]
-                    assert _fiber_reads(sub) < src, sub.name
-                if isinstance(sub, PanelStage) and sub.groups:
-                    w = _panel_writes(sub)
-                    assert w.min() >= 0 and w.max() < ndst[sub.name], sub.name
-                    assert len(numpy.unique(w)) == len(w), "overlapping writes in " + sub.name
+        _check_sigma_writes(sig)
+
+
+@pytest.mark.parametrize("tag", ["SP_K4", "SP_K5"])
+def test_spin_projected_plans_write_in_bounds_and_disjoint(tag, monkeypatch):
+    """The same invariants for the N-symmetry plans of the projected H and S operators,
+    and the reduction map stays inside the reduced vector."""
+    patch_stage_run(monkeypatch)
+    for r in load("kernels_%s.npz" % tag)["records"]:
+        sig, sv, _, _, _ = record_sp_operators(r, "cpu", use_fiber=True)
+        for op in (sig, sv):
+            _check_sigma_writes(op.inner)
+            red = op.red.numpy()
+            assert red.min() >= 0 and red.max() < op.nn and len(numpy.unique(red)) == len(red)
 
 
 @pytest.mark.parametrize("tag", ["K5", "K6"])
