@@ -192,9 +192,14 @@ int qc_fiber_f32(const void *tasks_dev, long long ntasks, int opspan, const void
                  const void *fout_dev, const void *fpair_dev, const void *ops_dev, int max_rows,
                  int fiber_tile, const float *A, const float *W, float *C, void *stream);
 
-/* dst[i] = src[idx[i]] (FP64), i < n.  Used for diag[prjmap] (kernelQt.py:122). */
+/* dst[i] = src[idx[i]] (FP64), i < n.  Used for diag[prjmap] (kernelQt.py:122) and, with
+ * spin projection, for projectionNMs of the N-symmetry sigma back to the (N, Sz) layout
+ * (qtensor.py:546-560, called at kernelQt.py:310 and :445). */
 int qc_gather_f64(const double *src, const long long *idx, double *dst, long long n, void *stream);
-/* dst[idx[i]] = src[i] (FP64) after zeroing dst[0..ndst). */
+/* dst[idx[i]] = src[i] (FP64) after zeroing dst[0..ndst).  With spin projection this is
+ * reduceQsymsToN of the wavefunction and of site tensors (qtensor.py:528-543, called at
+ * kernelQt.py:160, :382, :638 and :775): the same elements, zero in the blocks that only
+ * N symmetry allows. */
 int qc_scatter_f64(const double *src, const long long *idx, double *dst, long long n,
                    long long ndst, void *stream);
 

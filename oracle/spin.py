@@ -150,7 +150,7 @@ class ProjectedSigma(SigmaOracle):
     """sigma = P_(N,Sz) sum_x w_x R_x W_x[i+1] W_x[i] L_x (psi reduced to N).
 
     HVecQt with ifs2proj (the R environment flipped with qkey[:1], kernelQt.py:297-298,
-    the result projected back with projectionNMs, :308-310) and, with the projector's
+    the result projected back with projectionNMs, :309-311) and, with the projector's
     environments and R(theta) operators, SVecQt (kernelQt.py:373-450).
     """
 
