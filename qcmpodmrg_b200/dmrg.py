@@ -19,7 +19,7 @@ import time
 import numpy
 import torch
 
-from .kernels import SigmaOperator, DiagOperator, Renormalizer, TensorSet, Workspace
+from .kernels import SigmaOperator, DiagOperator, Renormalizer, TensorSet, Workspace, NoiseRDM
 from .mpo import QPHYS, build_mpo
 from .qtensor import Layout, classification
 from .davidson import davidson
@@ -33,6 +33,22 @@ def dpt(q1, q2):
     q1 = numpy.asarray(q1, dtype=numpy.float64)
     q2 = numpy.asarray(q2, dtype=numpy.float64)
     return (q1[:, None, :] + q2[None, :, :]).reshape(-1, q1.shape[1])
+
+
+def noise_psi_layout(ql, qr, qkey, status):
+    """The wavefunction as the rank-3 tensor pRDMQt contracts (setupQtmpPRDM,
+    source/mpo_dmrg_dotutil.py:543-569): [l, n1, (n2 r)] for 'L', [(l n1), n2, r] for
+    'R', merged indices classified by their quantum numbers.  Returns the layout, its
+    sector -> dense-position lists, and those of the dense density matrix's indices."""
+    if status == "L":
+        qn = [ql, QPHYS, qkey - dpt(QPHYS, qr)]
+    else:
+        qn = [dpt(ql, QPHYS), QPHYS, qkey - qr]
+    cls = [classification(q) for q in qn]
+    lay = Layout([False, False, True], [c[0] for c in cls], [c[1] for c in cls])
+    idl = [c[2] for c in cls]
+    dense_idl = [idl[0], idl[1], idl[0], idl[1]] if status == "L" else [idl[1], idl[2], idl[1], idl[2]]
+    return lay, idl, dense_idl
 
 
 ACCEPT_DE = 1e-6      # Eh: FP64 vs low-precision Ritz value agreement that accepts a mixed solve
@@ -74,6 +90,7 @@ class DMRG(object):
                            "fused": {"use_fiber": True, "fuse_w": True}}[w_path]
         self.crit_vec = 1.e-8
         self.thresh = -1.e-14
+        self.noise = 0.0          # weight of the pRDM noise term in the decimation (schedule noise)
         self.ifguess = True
         self.ws = Workspace(self.device)
         self.plan_cache = {}          # oldest first
@@ -351,16 +368,50 @@ class DMRG(object):
         self.stats["decim_s"] += time.time() - t0
         return res, out, dims, sig
 
+    def prdm(self, civecs, isite, status, dims):
+        """Density matrix of the half of the dot being kept, sum_i C_i C_i^T, plus
+        noise * the pRDM noise term of every state when noise >= 1e-10 (pRDMQt,
+        source/mpo_dmrg_kernelQt.py:453-626; decimation, mpo_dmrg_dotutil.py:294-330)."""
+        ldim, cdim, rdim, ndim = dims
+        neig = civecs.shape[0]
+        c = civecs.reshape(neig, ldim * 4, 4 * rdim)
+        nz = self.noise_operator(isite, status) if self.noise >= 1.e-10 else None
+        rdm = None
+        for i in range(neig):
+            m = c[i] @ c[i].T if status == "L" else c[i].T @ c[i]
+            rdm = m if rdm is None else rdm + m
+            if nz is not None:
+                op, lay, prj = nz
+                rdm = rdm + self.noise * op(self._noise_values(lay, civecs[i].reshape(-1)[prj]))
+        return rdm
+
+    def noise_operator(self, isite, status):
+        """NoiseRDM for the dot, the rank-3 wavefunction layout and its dense->packed map."""
+        lay, idl, dense_idl = noise_psi_layout(self.qnuml[isite], self.qnumr[isite + 2], self.qkey, status)
+        if status == "L":
+            E, W, j = self.lenv[isite - 1], self.mpo[isite], isite
+        else:
+            E, W, j = self.renv[isite + 2], self.mpo[isite + 1], isite + 1
+        lay_op, qkey = self._noise_layout(lay)
+        op = NoiseRDM(self.ws, j, status, lay_op, E, W, self.opers, qkey, dense_idl)
+        self.stats["prdm_flops"] = self.stats.get("prdm_flops", 0.0) + op.flops
+        return op, lay, torch.from_numpy(lay.prjmap(idl)).to(self.device)
+
+    def _noise_layout(self, lay):
+        return lay, self.qkey
+
+    def _noise_values(self, lay, vals):
+        return vals
+
     def decimate(self, civecs, isite, status, dims, dmax):
         ldim, cdim, rdim, ndim = dims
         neig = civecs.shape[0]
         lcdim, crdim = ldim * 4, 4 * rdim
         c = civecs.reshape(neig, lcdim, crdim)
+        rdm = self.prdm(civecs, isite, status, dims)
         if status == "L":
-            rdm = sum(c[i] @ c[i].T for i in range(neig))
             classes = dpt(self.qnuml[isite], QPHYS)
         else:
-            rdm = sum(c[i].T @ c[i] for i in range(neig))
             classes = dpt(QPHYS, self.qnumr[isite + 2])
         tr = float(torch.trace(rdm))
         if abs(tr) < 1.e-12:
@@ -477,8 +528,9 @@ class DMRG(object):
             self.psi0 = torch.stack([torch.tensordot(srotR[i], t, dims=([2], [0])).reshape(-1)
                                      for i in range(srotR.shape[0])])
 
-    def run(self, init_mps, dmax, nsweeps, tol=1.e-7, callback=None):
-        """schedule.fixed(ncsite=2, maxM=dmax, tol=tol, noise=0): sweeps R then L until |dE| < tol."""
+    def run(self, init_mps, dmax, nsweeps, tol=1.e-7, callback=None, noise=0.0):
+        """schedule.fixed(ncsite=2, maxM=dmax, tol=tol, noise=noise): sweeps R then L until |dE| < tol."""
+        self.noise = float(noise)
         self.load_mps(init_mps)
         eav, dwt, esweeps, nmvps = [], [], [], []
         eold = 1.e3

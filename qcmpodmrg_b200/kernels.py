@@ -22,7 +22,7 @@ from .engine import (Stage, compile_classes, add_parts, live_blocks, prune, op_t
                      compile_fiber, FiberStage, CompositeStage, panel_sigma1, compile_panels, BPERM_DT, PanelStage,
                      fiber_stages, panel_sigma4)
 from .mpo import case
-from .qtensor import Contraction, flip_right, flip_horizontal
+from .qtensor import Contraction, Layout, flip_right, flip_horizontal
 
 
 class Workspace(object):
@@ -797,3 +797,119 @@ class Renormalizer(object):
         s[1].run(self.W.values, T1, T2, "f64")
         s[2].run(T2, site_values, out, "f64")
         return TensorSet(self.out_layouts, out, self.out_offsets)
+
+
+class NoiseRDM(object):
+    """Noise term of the decimation's density matrix (pRDMQt with noise > 0).
+
+    status 'L' (source/mpo_dmrg_kernelQt.py:488-531): with psi as [l, n1, X]
+    (X = (n2, r) merged), T2_p[l, X, b, n1'] = sum W_p[a, b, n1', n1] L_p[a, l, l'] psi[l', n1, X]
+    and rho[l n1', l' n1''] = sum_p sum_{X, b} T2_p T2_p.
+    status 'R' (:568-611): with psi as [Y, n2, r] (Y = (l, n1) merged) and R_p flipped,
+    T2_p[a, n2', Y, r'] and rho[n2' r', n2'' r''] = sum_p sum_{a, Y} T2_p T2_p.
+    Three grouped-GEMM launches over all operators (per-operator Gram blocks), one
+    fixed-order sum over operators, and a scatter into the dense matrix the
+    decimation uses.  ``psi_layout`` is the rank-3 wavefunction layout (N-reduced
+    with spin projection, with qkey[:1] then).
+    """
+
+    def __init__(self, ws, isite, status, psi_layout, E, W, opers, qkey, dense_idl):
+        self.ws, self.status = ws, status
+        dev = ws.device
+        groups = _groups(opers, isite, 1)
+        nops = len(opers)
+        if status == "L":
+            ax = (([2], [0]), ([0, 2], [0, 3]), ([1, 2], [1, 2]))
+        else:
+            ax = (([2], [2]), ([1, 3], [2, 1]), ([0, 2], [0, 2]))
+        bases = [numpy.zeros(nops, dtype=numpy.int64) for _ in range(2)]
+        tot = [0, 0]
+        plans = {}
+        out = None
+        for key, ops in sorted(groups.items()):
+            i0 = ops[0]
+            El, Wl = E.layouts[i0], W.layouts[i0]
+            for i in ops:
+                if E.layouts[i] is not El or W.layouts[i] is not Wl:
+                    raise ValueError("operators of one symmetry class must share their block structure")
+            if status == "L":
+                c1 = Contraction(El, psi_layout, ax[0])
+                t1 = c1.triples
+                c2 = Contraction(c1.out, Wl, ax[1])
+                t2 = prune(c2.triples, live1=live_blocks(c1.out, t1))
+            else:
+                Rl = _flip_right_ket(El, qkey)
+                c1 = Contraction(psi_layout, Rl, ax[0])
+                t1 = c1.triples
+                c2 = Contraction(Wl, c1.out, ax[1])
+                t2 = prune(c2.triples, live2=live_blocks(c1.out, t1))
+            c3 = Contraction(c2.out, c2.out, ax[2])
+            live2 = live_blocks(c2.out, t2)
+            t3 = prune(c3.triples, live1=live2, live2=live2)
+            if out is None:
+                out = c3.out
+            elif c3.out is not out:
+                raise ValueError("noise RDM blocks differ between operator classes")
+            plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3))
+            for s, c in enumerate((c1, c2)):
+                for i in ops:
+                    bases[s][i] = tot[s]
+                    tot[s] += c.out.size
+        self.out_layout = out
+        self.tot = tot
+        self.nops = nops
+        self.size = out.size if out is not None else 0
+        order = numpy.concatenate([numpy.array(plans[k][0]) for k in sorted(plans)])
+        slot = numpy.arange(nops, dtype=numpy.int64) * self.size
+        if status == "L":
+            t0 = op_table(E.offsets[order], 0, bases[0][order], 1.0)
+            t1_ = op_table(bases[0][order], W.offsets[order], bases[1][order], 1.0)
+        else:
+            t0 = op_table(0, E.offsets[order], bases[0][order], 1.0)
+            t1_ = op_table(W.offsets[order], bases[0][order], bases[1][order], 1.0)
+        tabs = [t0, t1_, op_table(bases[1][order], bases[1][order], slot, 1.0)]
+        st = [{}, {}, {}]
+        pos = 0
+        for key, (ops, *cs) in sorted(plans.items()):
+            rng = (pos, pos + len(ops))
+            pos += len(ops)
+            for si, (c, t) in enumerate(cs):
+                add_parts(st[si], compile_classes(c, t, ax[si]), op_range=rng)
+        self.stages = [Stage(st[si], dev, "prdm%d" % (si + 1), tabs[si]) for si in range(3)]
+        self.flops = sum(s.flops for s in self.stages)
+        self.E, self.W = E, W
+        n = int(numpy.prod(out.shape)) if out is not None else 0
+        self.dense_shape = tuple(int(x) for x in out.shape) if out is not None else (0,)
+        self.prj = torch.from_numpy(out.prjmap(dense_idl)).to(dev) if out is not None else None
+        self.ndense = n
+
+    def __call__(self, psi_values):
+        """psi_values: packed rank-3 wavefunction (device FP64) -> dense noise RDM (d x d)."""
+        ws = self.ws
+        T1 = ws.get("n1", self.tot[0], torch.float64)
+        T2 = ws.get("n2", self.tot[1], torch.float64)
+        P = ws.get("npart", self.nops * self.size, torch.float64)
+        s = self.stages
+        if self.status == "L":
+            s[0].run(self.E.values, psi_values, T1, "f64")
+            s[1].run(T1, self.W.values, T2, "f64")
+        else:
+            s[0].run(psi_values, self.E.values, T1, "f64")
+            s[1].run(self.W.values, T1, T2, "f64")
+        P[:self.nops * self.size].zero_()
+        s[2].run(T2, T2, P, "f64")
+        vals = torch.empty(max(self.size, 1), dtype=torch.float64, device=ws.device)[:self.size]
+        reduce_ops(P, self.nops, self.size, vals)
+        dense = torch.empty(self.ndense, dtype=torch.float64, device=ws.device)
+        scatter(vals, self.prj, dense)
+        d = self.dense_shape
+        return dense.reshape(d[0] * d[1], d[2] * d[3])
+
+
+def _flip_right_ket(lay, qkey):
+    """R environment as pRDMQt 'R' contracts it with the wavefunction's right index
+    (kernelQt.py:592-598): qsyms [-q0, -(qkey - q1), qkey - q2], index 1 flipped in/out."""
+    st = lay.status.copy()
+    st[1] = not st[1]
+    qkey = numpy.asarray(qkey, dtype=numpy.float64)
+    return Layout(st, [-lay.qsyms[0], -(qkey - lay.qsyms[1]), qkey - lay.qsyms[2]], lay.ndims)

@@ -8,7 +8,7 @@ mpo_dmrg_dot.ci_solver, dotutil.genHDiag and mpo_dmrg_opt.sweep call:
   SDiag(info, ndim0, prjmap)                       source/mpo_dmrg_kernel.py:183-190
   SVec(vec0, info, ndim0, prjmap)                  source/mpo_dmrg_kernel.py:226-231
   renorm(dmrg, isite, ncsite, flst, flstN, site, status)   :347-377
-  pRDM(cimat, info)                                :278-282 (noise-free part)
+  pRDM(cimat, info)                                :278-282 (with the noise term, pRDMQt)
 
 With a spin-projected ``dmrg`` (qcmpodmrg_b200.spin.SPDMRG, the reference's
 ifs2proj) HVec/HDiag are the projected Hamiltonian's, SVec/SDiag the projector's
@@ -120,14 +120,16 @@ def renorm(dmrg, isite, ncsite, flst, flstN, site, status):
 
 
 def pRDM(cimat, info):
-    """Reduced density matrix of the superblock, sum_i C_i C_i^+ (noise = 0)."""
+    """Density matrix of the kept half of the dot, sum_i C_i C_i^+, plus dmrg.noise times
+    the noise term sum_p (L_p C W_p)(L_p C W_p)^+ when dmrg.noise >= 1e-10 (pRDMQt)."""
     dmrg, isite, ncsite, flst, status, ifsym = info
+    if ncsite != 2:
+        raise NotImplementedError("only the two-site dot is implemented")
     c = _to_dev(cimat, dmrg.device)
     neig = c.shape[0]
     if status == "L":      # cimat [neig, ldim, dim, crdim] (dotutil.py:276-281)
-        m = c.reshape(neig, c.shape[1] * c.shape[2], -1)
-        rdm = sum(m[i] @ m[i].T for i in range(neig))
+        ldim, rdim = c.shape[1], c.shape[3] // 4
     else:                  # cimat [neig, lcdim, dim, rdim] (dotutil.py:282-288)
-        m = c.reshape(neig, c.shape[1], -1)
-        rdm = sum(m[i].T @ m[i] for i in range(neig))
+        ldim, rdim = c.shape[1] // 4, c.shape[3]
+    rdm = dmrg.prdm(c.reshape(neig, -1), isite, status, (ldim, 16, rdim, ldim * 16 * rdim))
     return rdm.cpu().numpy()

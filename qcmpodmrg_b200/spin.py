@@ -255,6 +255,17 @@ class SPDMRG(DMRG):
             self.prenv[j] = rp(vals)
         return rn.flops + rp.flops
 
+    def _noise_layout(self, lay):
+        """pRDMQt contracts the N-reduced wavefunction (kernelQt.py:493, :572)."""
+        lay_n = reduce_layout(lay)
+        self._noise_red = (lay, lay_n, torch.from_numpy(reduce_map(lay, lay_n)).to(self.device))
+        return lay_n, self.qkey[:1]
+
+    def _noise_values(self, lay, vals):
+        lay0, lay_n, red = self._noise_red
+        out = torch.empty(lay_n.size, dtype=torch.float64, device=self.device)
+        return K.scatter(vals.contiguous(), red, out)
+
     def _psi_layout(self, isite):
         ql, qr = self.qnuml[isite], self.qnumr[isite + 2]
         cls = [classification(q) for q in (ql, QPHYS, QPHYS, self.qkey - qr)]

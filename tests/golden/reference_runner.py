@@ -94,7 +94,7 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
     os.chdir(wd)
     rec = Recorder(targets)
     orig = (mpo_dmrg_kernel.HVec, mpo_dmrg_kernel.HDiag, mpo_dmrg_kernel.renorm,
-            mpo_dmrg_kernel.SVec, mpo_dmrg_kernel.SDiag)
+            mpo_dmrg_kernel.SVec, mpo_dmrg_kernel.SDiag, mpo_dmrg_kernel.pRDM)
     try:
         write_mole(os.path.join(wd, "mole.h5"), ham)
         mol = class_molinfo()
@@ -234,6 +234,19 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
         mpo_dmrg_kernel.renorm = renorm_hook
         mpo_dmrg_kernel.SVec = svec_hook
         mpo_dmrg_kernel.SDiag = sdiag_hook
+
+        def prdm_hook(cimat, info):
+            out = orig[5](cimat, info)
+            d, isite, ncsite, flst, status, ifsym = info
+            k = (d.isweep, status, isite)
+            r = rec.records.setdefault(k, {})
+            if k in rec.targets and "prdm_out" not in r:
+                r["prdm_cimat"] = numpy.array(cimat)
+                r["prdm_out"] = numpy.array(out)
+                r["noise"] = float(d.noise)
+            return out
+
+        mpo_dmrg_kernel.pRDM = prdm_hook
         dmrg2.default(sc2, flmps1)
         result = {
             "K": K, "N": N, "D": D, "seed": seed, "decay": decay, "nsweeps": nsweeps,
@@ -244,7 +257,7 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
         }
     finally:
         (mpo_dmrg_kernel.HVec, mpo_dmrg_kernel.HDiag, mpo_dmrg_kernel.renorm,
-         mpo_dmrg_kernel.SVec, mpo_dmrg_kernel.SDiag) = orig
+         mpo_dmrg_kernel.SVec, mpo_dmrg_kernel.SDiag, mpo_dmrg_kernel.pRDM) = orig
         os.chdir(cwd)
     return result, rec
 

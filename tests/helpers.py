@@ -109,3 +109,49 @@ def record_sp_renormalizers(r, device):
     rn = Renormalizer(ws, j, status, site_n, E, W, opers)
     rp = Renormalizer(ws, j, status, site_n, PE, P, popers)
     return rn, rp, vals
+
+
+def _dense_qnums(qsyms, env, index):
+    """Dense per-state quantum numbers of an environment index from the sector list
+    ``qsyms`` (same sector order) and the environment's recorded positions (idlst)."""
+    nd = numpy.asarray(env["ndims%d" % index], dtype=numpy.int64)
+    pos = numpy.asarray(env["idlst%d" % index], dtype=numpy.int64)
+    q = numpy.asarray(qsyms, dtype=numpy.float64).reshape(len(nd), -1)
+    out = numpy.zeros((int(nd.sum()), q.shape[1]))
+    out[pos] = numpy.repeat(q, nd, axis=0)
+    return out
+
+
+def record_noise(r, device):
+    """(NoiseRDM, packed rank-3 wavefunction values, C C^T) for a recorded pRDM call;
+    spin-projected records (with a quadrature) get the N-reduced layout."""
+    from qcmpodmrg_b200.kernels import NoiseRDM, Workspace, scatter
+    from qcmpodmrg_b200.dmrg import noise_psi_layout
+    from qcmpodmrg_b200.spin import reduce_layout, reduce_map
+    import torch
+    ws = Workspace(torch.device(device))
+    isite = int(r["key"][2])
+    status = "L" if int(r["key"][1]) == 0 else "R"
+    qkey = numpy.asarray(r["qkey"], dtype=numpy.float64)
+    q = r["qtmp"]
+    ql = _dense_qnums(q["qsyms0"], r["envL"][0], 1)
+    qr = qkey - _dense_qnums(q["qsyms3"], r["envR"][0], 1)
+    lay, idl, dense_idl = noise_psi_layout(ql, qr, qkey, status)
+    c = numpy.asarray(r["prdm_cimat"], dtype=numpy.float64)
+    vals = torch.from_numpy(c[0].reshape(-1)[lay.prjmap(idl)].copy()).to(device)
+    sp = "qwts" in r
+    if sp:
+        lay_n = reduce_layout(lay)
+        out = torch.empty(lay_n.size, dtype=torch.float64, device=device)
+        vals = scatter(vals, torch.from_numpy(reduce_map(lay, lay_n)).to(device), out)
+        lay, qkey = lay_n, qkey[:1]
+    opers = [int(x) for x in numpy.atleast_1d(r["opers"])]
+    if status == "L":
+        E, W, j = tensorset(r["envL"], device), tensorset(r["mpo_i"], device), isite
+        m = c.reshape(c.shape[0], c.shape[1] * c.shape[2], -1)
+        cc = sum(m[i] @ m[i].T for i in range(len(m)))
+    else:
+        E, W, j = tensorset(r["envR"], device), tensorset(r["mpo_j"], device), isite + 1
+        m = c.reshape(c.shape[0], c.shape[1], -1)
+        cc = sum(m[i].T @ m[i] for i in range(len(m)))
+    return NoiseRDM(ws, j, status, lay, E, W, opers, qkey, dense_idl), vals, cc
