@@ -12,6 +12,7 @@ decimation and renormalisation of every operator's environment.
                   [--w-path fiber|generic|fused] [--plan-cache] [--sites K] [--dmax D]
   python bench.py --impl reference      # the reference algorithm (oracle port) on the host CPU
   python bench.py --workload batched    # lockstep independent instances vs one after another
+  python bench.py --workload sp --sites 12 --dmax 100 --npts 4   # spin-projected (S=0) sweeps, FP64
 
 Prints one JSON line.  value = seconds per sweep (lower is better).
 """
@@ -29,6 +30,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "sweep sec & sigma TFLOP/s @K=24,D=500: mixed+learned vs FP64, |ΔE|≤1e-6 Eh"
+METRIC_SP = "spin-projected sweep sec (S=0 projector, FP64)"
 K_SITES, N_ELEC, DECAY, SEED, DMAX = 24, 24, 3.0, 1, 500
 RAMP = (50, 100, 200)
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
@@ -141,7 +143,13 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32", "mixed-tc": "tf32x3"}[args.precision]
     ham = make_hamiltonian(args.sites, args.sites, SEED + rank * 0, DECAY)
-    d = DMRG(ham, device=dev, precision=prec, w_path=args.w_path, plan_cache=args.plan_cache)
+    sp = args.workload == "sp"
+    if sp:
+        from qcmpodmrg_b200.spin import SPDMRG
+        prec = "f64"                  # the spin-projected path runs in FP64
+        d = SPDMRG(ham, args.npts, 0.0, 0.0, device=dev, w_path=args.w_path)
+    else:
+        d = DMRG(ham, device=dev, precision=prec, w_path=args.w_path, plan_cache=args.plan_cache)
     d.load_mps(product_mps(ham))
     for D in RAMP:
         if D < args.dmax:
@@ -204,7 +212,8 @@ def run_ours(args):
             "achieved_tflops": round(f_l / (t_l / 1e3) / 1e12, 3)}
     # whole job: world replicas each did args.steps sweeps in ms (slowest rank)
     line = {
-        "metric": METRIC, "value": round(ms_per_step / 1e3 / world, 3), "unit": "s/sweep", "n_gpus": world,
+        "metric": METRIC_SP if sp else METRIC, "value": round(ms_per_step / 1e3 / world, 3), "unit": "s/sweep",
+        "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 1),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": {"f64": "f64", "f32": "f32 (sigma), f64 (Davidson, decimation)",
@@ -212,7 +221,11 @@ def run_ours(args):
                   "tf32x3": "3xtf32 split on tensor cores + f32 (sigma), f64 (Davidson, decimation)"}[prec],
         "data": "synthetic: seeded integrals (K=%d, N=%d, decay 3, seed 1), product-state start, D ramp %s"
                 % (args.sites, args.sites, "/".join(str(x) for x in RAMP if x < args.dmax)),
-        "config": {"workload": "two-site Qt DMRG sweep, K=%d N=%d Sz=0 D=%d, %d operators H_p"
+        "config": {"workload": ("spin-projected (S=0, %d Gauss-Legendre points) two-site Qt DMRG sweep, K=%d "
+                                "N=%d Sz=0 D=%d, %d operators H_p R(theta_g) + %d projector terms"
+                                % (args.npts, args.sites, args.sites, args.dmax, 2 * args.sites * args.npts,
+                                   args.npts)) if sp else
+                               "two-site Qt DMRG sweep, K=%d N=%d Sz=0 D=%d, %d operators H_p"
                                % (args.sites, args.sites, args.dmax, 2 * args.sites), "K": args.sites,
                    "N": args.sites, "D": args.dmax, "precision": args.precision, "w_path": args.w_path,
                    "l2": "inputs larger than L2: environments and sigma scratch are tens of GB per sweep",
@@ -232,12 +245,12 @@ def run_ours(args):
         "phase_s_per_step": {k: round(stats[k] / args.steps, 2) for k in ("plan_s", "hvec_s", "hdiag_s", "renorm_s",
                                                                          "decim_s") if k in stats},
     }
-    if args.e2e:
+    if args.e2e and not sp:
         e2e = e2e_leg(d, args)
         e2e["value"] = round(max_over_ranks(dist, e2e["value"], dev) / world, 3)
         line["e2e"] = e2e
     if rank == 0 and args.cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(d, ms_per_step / 1e3)
+        line["cpu_baseline"] = cpu_baseline_sample(d, ms_per_step / 1e3, sp=sp)
     if dist is not None:
         dist.destroy_process_group()
     if rank == 0:
@@ -262,14 +275,13 @@ def e2e_leg(d, args):
             "path": "qcmpodmrg_b200.mpo_dmrg_kernel.HVec/HDiag with host buffers, host Davidson"}
 
 
-def cpu_baseline_sample(d, gpu_sweep_s):
-    """The oracle (NumPy restatement of the reference's HVecQt) timed on this host's cores on
-    one sigma matvec at the mid-chain dot of the same state; scaled to a sweep by algorithmic
-    sigma FLOPs (the same count the GPU reports)."""
-    from oracle.kernels import SigmaOracle
-    from oracle.bench_cpu import oracle_dot
+def cpu_baseline_sample(d, gpu_sweep_s, sp=False):
+    """The oracle (NumPy restatement of the reference's HVecQt; with spin projection its
+    H and S products) timed on this host's cores on one matvec at the mid-chain dot of the
+    same state; scaled to a sweep by algorithmic sigma FLOPs (the same count the GPU reports)."""
+    from oracle.bench_cpu import oracle_dot, oracle_sp_dot
     isite = d.nsite // 2
-    ora, x, flops_dot = oracle_dot(d, isite)
+    ora, x, flops_dot = (oracle_sp_dot if sp else oracle_dot)(d, isite)
     t0 = time.time()
     ora(x)
     t = time.time() - t0
@@ -372,7 +384,9 @@ def main():
     ap.add_argument("--w-path", default="fiber", choices=["generic", "fiber", "fused"],
                     help="kernels of the two MPO-site contractions of sigma")
     ap.add_argument("--plan-cache", action="store_true", help="reuse compiled plans of unchanged dots")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "sp"],
+                    help="sp: spin-projected sweeps (SP-MPS, S=0) with --npts quadrature points")
+    ap.add_argument("--npts", type=int, default=4)
     ap.add_argument("--instances", type=int, default=16)
     args = ap.parse_args()
     if args.workload == "batched":

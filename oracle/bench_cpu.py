@@ -54,6 +54,29 @@ def oracle_dot(d, isite):
     return sig, x, s.flops
 
 
+def oracle_sp_dot(d, isite):
+    """Oracle H and S products (HVecQt with ifs2proj, SVecQt) of a spin-projected dot."""
+    from .spin import sigma_sp, svec
+    L, R = d.lenv[isite - 1], d.renv[isite + 2]
+    PL, PR = d.plenv[isite - 1], d.prenv[isite + 2]
+    Wi, Wj = d.mpo[isite], d.mpo[isite + 1]
+
+    def conv(ts):
+        return [_qt(l.status, l.qsyms, l.ndims, ts.op_values(i).cpu().numpy()) for i, l in enumerate(ts.layouts)]
+
+    ql, qr = d.qnuml[isite], d.qnumr[isite + 2]
+    cls = [classification(q) for q in (ql, QPHYS, QPHYS, d.qkey - qr)]
+    qtmp = QTensor([False, False, False, True]).from_qsyms(4, [c[0] for c in cls], [c[1] for c in cls],
+                                                           allocate=False)
+    hv = sigma_sp(qtmp, d.qkey, conv(L), conv(R), conv(Wi), conv(Wj), list(d.opers), d.hpwts, isite)
+    pops = conv(d.pops)
+    sv = svec(qtmp, d.qkey, conv(PL), conv(PR), pops, d.qwts, isite)
+    lay, idl, s, dg = d.dot_operators(isite)
+    s2, sd = d.dot_projector(isite)
+    x = numpy.random.default_rng(0).standard_normal(qtmp.size_allowed)
+    return (lambda v: (hv(v), sv(v))), x, s.flops + s2.flops
+
+
 _CACHE = {}
 
 
