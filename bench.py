@@ -227,7 +227,8 @@ def run_ours(args):
                                    args.npts)) if sp else
                                "two-site Qt DMRG sweep, K=%d N=%d Sz=0 D=%d, %d operators H_p"
                                % (args.sites, args.sites, args.dmax, 2 * args.sites), "K": args.sites,
-                   "N": args.sites, "D": args.dmax, "precision": args.precision, "w_path": args.w_path,
+                   "N": args.sites, "D": args.dmax, "precision": "f64" if sp else args.precision,
+                   "w_path": args.w_path,
                    "l2": "inputs larger than L2: environments and sigma scratch are tens of GB per sweep",
                    "parallelism": "replicas" if world > 1 else "1 GPU",
                    "value_definition": "slowest rank's seconds for its sweeps / sweeps done by all ranks"},

@@ -151,7 +151,11 @@ class SigmaOperator(object):
     """sigma = sum_p w_p R_p W_p[i+1] W_p[i] L_p psi for the dot (isite, isite+1)."""
 
     def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts, precision="f64",
-                 tensor_cores=None, use_fiber=False, fuse_w=True, panel1=True, panel4=True):
+                 tensor_cores=None, use_fiber=False, fuse_w=True, panel1=True, panel4=True, live=None):
+        """live: optional mask over the wavefunction layout's flat blocks.  Blocks outside it
+        are zero in every input vector and discarded in every output (the blocks that N
+        symmetry adds to an (N, Sz) wavefunction under spin projection): block pairs that
+        read them in the first contraction or write them in the last are not compiled."""
         self.ws, self.psi, self.precision = ws, psi_layout, precision
         # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 modes
         tc = (precision in ("tf32", "tf32x3")) if tensor_cores is None else tensor_cores
@@ -175,7 +179,7 @@ class SigmaOperator(object):
                         or flip_right(R.layouts[i], qkey) is not Rl):
                     raise ValueError("operators of one symmetry class must share their block structure")
             c1 = Contraction(Ll, psi_layout, ax[0])
-            t1 = c1.triples
+            t1 = c1.triples if live is None else prune(c1.triples, live2=live)
             # L.psi as dense panel GEMMs (T1 blocks stored panel by panel)
             pan = panel_sigma1(Ll, psi_layout, t1, c1.out.nblks) if panel1 else None
             t1off = pan["t1off"] if pan is not None else None
@@ -187,9 +191,10 @@ class SigmaOperator(object):
             # block Wij[a, n1', n1, c, n2', n2] = sum_b W_i[a, b, n1', n1] W_{i+1}[b, c, n2', n2]
             # made once per dot, so T2 is never written (fiber-group kernel only)
             c4 = Contraction(c3.out, Rl, ax[3])
+            t4all = c4.triples if live is None else c4.triples[live[c4.triples[:, 0]]]
             # .R as dense panel GEMMs (T3 blocks written into sigma-block panels by the
             # fiber kernel, R blocks permuted into per-sector panels once per dot)
-            pan4 = panel_sigma4(c3.out, Rl, psi_layout, c4.triples) if (use_fiber and panel4) else None
+            pan4 = panel_sigma4(c3.out, Rl, psi_layout, t4all) if (use_fiber and panel4) else None
             o3 = {} if pan4 is None else {"out_off": pan4["t3off"], "out_fhs": pan4["t3fhs"],
                                           "out_flo": pan4["t3flo"], "extra_out": pan4["needed"]}
             fused = None
@@ -206,7 +211,7 @@ class SigmaOperator(object):
                 fib3 = compile_fiber(c3, t3, 3, 1, **o3)
             if pan4 is not None and fused is None and fib3 is None:
                 pan4 = None                 # T3 comes from the grouped GEMM in the packed layout
-            t4 = prune(c4.triples, live1=live_blocks(c3.out, fused[2] if fused else t3))
+            t4 = prune(t4all, live1=live_blocks(c3.out, fused[2] if fused else t3))
             if c4.out is not psi_layout:
                 raise ValueError("sigma output layout differs from the wavefunction template")
             plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3), (c4, t4), Rl, fused, pan, pan4, fib3)

@@ -200,8 +200,10 @@ class SPDMRG(DMRG):
 
     ifs2proj = True
 
-    def __init__(self, ham, npts, sval=0.0, sz=0.0, device="cuda", w_path="fiber", quad="GaussLegendre"):
+    def __init__(self, ham, npts, sval=0.0, sz=0.0, device="cuda", w_path="fiber", quad="GaussLegendre",
+                 prune_zero_blocks=True):
         self.npts, self.sval, self.sz, self.quad = int(npts), float(sval), float(sz), quad
+        self.prune_zero_blocks = prune_zero_blocks
         super(SPDMRG, self).__init__(ham, device=device, precision="f64", w_path=w_path)
 
     def _setup_operators(self, ham):
@@ -272,6 +274,11 @@ class SPDMRG(DMRG):
         lay = Layout(PSI_STATUS, [c[0] for c in cls], [c[1] for c in cls])
         return lay, [c[2] for c in cls]
 
+    def _live(self, lay):
+        """Blocks of the N-reduced wavefunction that can be non-zero: the (N, Sz) ones (the
+        reference also contracts the zero blocks; skipping them changes no result)."""
+        return lay.allowed.astype(bool) if self.prune_zero_blocks else None
+
     def dot_operators(self, isite):
         """H_eff (projected) and its diagonal for the dot; the plan is compiled per dot."""
         lay, idl = self._psi_layout(isite)
@@ -280,7 +287,7 @@ class SPDMRG(DMRG):
         L, R = self.lenv[isite - 1], self.renv[isite + 2]
         Wi, Wj = self.mpo[isite], self.mpo[isite + 1]
         inner = SigmaOperator(self.ws, isite, lay_n, L, R, Wi, Wj, self.qkey[:1], self.opers, self.hpwts,
-                              "f64", **self.sigma_opts)
+                              "f64", live=self._live(lay), **self.sigma_opts)
         sig = ProjectedOperator(self.ws, inner, red)
         dg = DiagOperator(self.ws, isite, lay, L, R, Wi, Wj, self.qkey, self.opers, self.hpwts)
         return lay, idl, sig, dg
@@ -292,7 +299,7 @@ class SPDMRG(DMRG):
         red = reduce_map(lay, lay_n)
         PL, PR = self.plenv[isite - 1], self.prenv[isite + 2]
         inner = SigmaOperator(self.ws, isite, lay_n, PL, PR, self.pops, self.pops, self.qkey[:1], self.popers,
-                              self.qwts, "f64", **self.sigma_opts)
+                              self.qwts, "f64", live=self._live(lay), **self.sigma_opts)
         sv = ProjectedOperator(self.ws, inner, red)
         sd = DiagOperator(self.ws, isite, lay, PL, PR, self.pops, self.pops, self.qkey, self.popers, self.qwts)
         return sv, sd

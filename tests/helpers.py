@@ -59,8 +59,9 @@ def record_renormalizer(r, device):
     return rn, numpy.asarray(r["renorm_site"]["value"], dtype=numpy.float64)
 
 
-def record_sp_operators(r, device, use_fiber=True, fuse_w=False):
-    """Projected H and S operators (+ diagonals) of a recorded spin-projected reference dot."""
+def record_sp_operators(r, device, use_fiber=True, fuse_w=False, prune=True):
+    """Projected H and S operators (+ diagonals) of a recorded spin-projected reference dot
+    (prune: skip the block pairs that read or write the zero blocks of the reduced vector)."""
     from qcmpodmrg_b200.kernels import SigmaOperator, DiagOperator, Workspace
     from qcmpodmrg_b200.spin import ProjectedOperator, reduce_layout, reduce_map
     import torch
@@ -77,7 +78,7 @@ def record_sp_operators(r, device, use_fiber=True, fuse_w=False):
     PL, PR, P = tensorset(r["penvL"], device), tensorset(r["penvR"], device), tensorset(r["pop"], device)
     qw = numpy.atleast_1d(r["qwts"]).astype(numpy.float64)
     popers = [0] * len(qw)
-    opts = {"use_fiber": use_fiber, "fuse_w": fuse_w}
+    opts = {"use_fiber": use_fiber, "fuse_w": fuse_w, "live": lay.allowed.astype(bool) if prune else None}
     sig = ProjectedOperator(ws, SigmaOperator(ws, isite, lay_n, L, R, Wi, Wj, qkey[:1], opers, hp, **opts), red)
     sv = ProjectedOperator(ws, SigmaOperator(ws, isite, lay_n, PL, PR, P, P, qkey[:1], popers, qw, **opts), red)
     dg = DiagOperator(ws, isite, lay, L, R, Wi, Wj, qkey, opers, hp)

@@ -11,17 +11,29 @@ from qcmpodmrg_b200.hamiltonian import make_hamiltonian
 
 
 @pytest.mark.parametrize("tag", ["SP_K4", "SP_K5"])
-@pytest.mark.parametrize("w_path", ["generic", "fiber"])
-def test_sp_operators_emulated(tag, w_path, monkeypatch):
+@pytest.mark.parametrize("w_path,prune", [("generic", True), ("fiber", True), ("fiber", False)])
+def test_sp_operators_emulated(tag, w_path, prune, monkeypatch):
     patch_stage_run(monkeypatch)
     for r in load("kernels_%s.npz" % tag)["records"]:
-        sig, sv, dg, sd, ws = record_sp_operators(r, "cpu", use_fiber=(w_path == "fiber"))
+        sig, sv, dg, sd, ws = record_sp_operators(r, "cpu", use_fiber=(w_path == "fiber"), prune=prune)
         y = sig(torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))).numpy()
         assert numpy.abs(y - r["hvec_y"]).max() <= 1e-12 * max(1.0, numpy.abs(r["hvec_y"]).max())
         s = sv(torch.from_numpy(numpy.asarray(r["svec_x"], dtype=numpy.float64))).numpy()
         assert numpy.abs(s - r["svec_y"]).max() <= 1e-13
         assert numpy.abs(dg().numpy() - r["hdiag"]).max() <= 1e-12
         assert numpy.abs(sd().numpy() - r["sdiag"]).max() <= 1e-13
+
+
+def test_sp_pruning_skips_zero_block_work(monkeypatch):
+    """Skipping the pairs of the zero blocks leaves results unchanged and removes work."""
+    patch_stage_run(monkeypatch)
+    r = load("kernels_SP_K5.npz")["records"][-1]
+    a = record_sp_operators(r, "cpu", prune=True)
+    b = record_sp_operators(r, "cpu", prune=False)
+    x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))
+    for i in (0, 1):
+        assert numpy.abs(a[i](x).numpy() - b[i](x).numpy()).max() <= 1e-13
+        assert a[i].flops < b[i].flops
 
 
 @pytest.mark.parametrize("tag", ["SP_K4", "SP_K5"])

@@ -20,10 +20,10 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("tag", ["SP_K4", "SP_K5"])
-@pytest.mark.parametrize("w_path", ["generic", "fiber"])
-def test_gpu_sp_operators(tag, w_path, cuda):
+@pytest.mark.parametrize("w_path,prune", [("generic", True), ("fiber", True), ("fiber", False)])
+def test_gpu_sp_operators(tag, w_path, prune, cuda):
     for r in load("kernels_%s.npz" % tag)["records"]:
-        sig, sv, dg, sd, ws = record_sp_operators(r, cuda, use_fiber=(w_path == "fiber"))
+        sig, sv, dg, sd, ws = record_sp_operators(r, cuda, use_fiber=(w_path == "fiber"), prune=prune)
         x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64)).to(cuda)
         y = sig(x).cpu().numpy()
         assert numpy.abs(y - r["hvec_y"]).max() <= 1e-12 * max(1.0, numpy.abs(r["hvec_y"]).max())
