@@ -10,8 +10,9 @@ from emulate import patch_stage_run
 from qcmpodmrg_b200.hamiltonian import make_hamiltonian
 
 
-@pytest.mark.parametrize("tag", ["SP_K4", "SP_K5"])
-@pytest.mark.parametrize("w_path,prune", [("generic", True), ("fiber", True), ("fiber", False)])
+@pytest.mark.parametrize("tag,w_path,prune", [("SP_K4", "generic", True), ("SP_K4", "fiber", True),
+                                               ("SP_K4", "fiber", False), ("SP_K5", "generic", True),
+                                               ("SP_K5", "fiber", True)])
 def test_sp_operators_emulated(tag, w_path, prune, monkeypatch):
     patch_stage_run(monkeypatch)
     for r in load("kernels_%s.npz" % tag)["records"]:
@@ -27,7 +28,7 @@ def test_sp_operators_emulated(tag, w_path, prune, monkeypatch):
 def test_sp_pruning_skips_zero_block_work(monkeypatch):
     """Skipping the pairs of the zero blocks leaves results unchanged and removes work."""
     patch_stage_run(monkeypatch)
-    r = load("kernels_SP_K5.npz")["records"][-1]
+    r = load("kernels_SP_K4.npz")["records"][-1]
     a = record_sp_operators(r, "cpu", prune=True)
     b = record_sp_operators(r, "cpu", prune=False)
     x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))

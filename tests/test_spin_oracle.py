@@ -156,9 +156,12 @@ def test_oracle_gdavidson_solves_generalised_problem():
 
 
 def test_sp_oracle_sweep_matches_reference():
-    """K=4, 3 quadrature points, D=16 (no truncation): energies, weights and matvec counts."""
+    """K=4, 3 quadrature points, D=16 (no truncation), first R+L sweep: every dot energy,
+    the averaged energy, weight and matvec count."""
     sw = load("sweep_SP_K4.npz")
-    out = ospin.SPOracleDMRG(_ham(sw), int(sw["npts"])).run(sw["init_mps"], int(sw["D"]), int(sw["nsweeps"]))
-    assert numpy.abs(out["eav"] - sw["eav"]).max() <= 1e-8
-    assert numpy.abs(out["dwt"] - sw["dwt"]).max() <= 1e-10
-    assert numpy.array_equal(out["nmvp"], sw["nmvp"])
+    out = ospin.SPOracleDMRG(_ham(sw), int(sw["npts"])).run(sw["init_mps"], int(sw["D"]), 1)
+    n = len(out["esweeps"])
+    assert n == 2 * (int(sw["K"]) - 1)
+    assert numpy.abs(out["esweeps"] - sw["esweeps"][:n]).max() <= 1e-8
+    assert abs(out["eav"][0] - sw["eav"][0]) <= 1e-8 and abs(out["dwt"][0] - sw["dwt"][0]) <= 1e-10
+    assert out["nmvp"][0] == sw["nmvp"][0]
