@@ -64,6 +64,16 @@ int qc_block_layout(int rank, const int *nsyms, const long long *ndims,
                     const int *allowed, int *iblks, long long *ioff, long long *ndim,
                     long long *size_allowed, long long *nallowed);
 
+/* Davidson-diagonal gather map of a two-site wavefunction layout (rank 4: l, n1, n2, r with
+ * four 1-dim physical sectors): gat[packed position] = index into the dense diagonal
+ * [16][ldim][rdim], every index numbered sector by sector (HDiagQt's diag[prjmap],
+ * source/mpo_dmrg_kernelQt.py:119-122).  blocks: the nblk allowed flat block indices; ndims:
+ * the sector sizes of the four indices back to back; ioff: packed offset of every flat block;
+ * size: the layout's element count (bounds check).  Host function. */
+int qc_psi_diag_gather(long long nblk, const long long *blocks, const int *nsyms,
+                       const long long *ndims, const long long *ioff, long long ldim,
+                       long long rdim, long long size, long long *gat);
+
 /* Block-pair list of a contraction: replaces the pair loop of
  * qtensor.tensordotSYM (source/qtensor/qtensor.py:617-636).  For every
  * allowed output block (out_iblks over the external sectors e1+e2, row-major)

@@ -321,3 +321,37 @@ extern "C" long long qc_compile_pairs(int r1, const int *nsyms1, const long long
   }
   return nc;
 }
+
+// Packed two-site wavefunction position -> index of the dense diagonal [16][ldim][rdim]
+// (HDiagQt's diag[prjmap], source/mpo_dmrg_kernelQt.py:119-122, with every index numbered
+// sector by sector).  The layout is rank 4 (l, n1, n2, r) with one-dimensional physical
+// sectors; block (sl, n, m, sr) of size dl x dr starts at ioff[block].
+extern "C" int qc_psi_diag_gather(long long nblk, const long long *blocks, const int *nsyms,
+                                  const long long *ndims, const long long *ioff, long long ldim,
+                                  long long rdim, long long size, long long *gat) {
+  if (nblk < 0 || !nsyms || !ndims || !ioff || !gat || (nblk > 0 && !blocks))
+    return set_err(QC_ERR_ARG, "qc_psi_diag_gather: bad arguments");
+  const long long n0 = nsyms[0], n1 = nsyms[1], n2 = nsyms[2], n3 = nsyms[3];
+  const long long *d0 = ndims, *d1 = ndims + n0, *d2 = d1 + n1, *d3 = d2 + n2;
+  std::vector<long long> so0(n0 + 1, 0), so3(n3 + 1, 0);
+  for (long long s = 0; s < n0; ++s) so0[s + 1] = so0[s] + d0[s];
+  for (long long s = 0; s < n3; ++s) so3[s + 1] = so3[s] + d3[s];
+  if (so0[n0] != ldim || so3[n3] != rdim || n1 != 4 || n2 != 4)
+    return set_err(QC_ERR_ARG, "qc_psi_diag_gather: layout does not match the dense diagonal");
+  for (long long s = 0; s < 4; ++s)
+    if (d1[s] != 1 || d2[s] != 1) return set_err(QC_ERR_ARG, "qc_psi_diag_gather: physical sectors not 1-dim");
+  for (long long b = 0; b < nblk; ++b) {
+    long long f = blocks[b];
+    const long long sr = f % n3; f /= n3;
+    const long long m = f % n2; f /= n2;
+    const long long n = f % n1; f /= n1;
+    const long long sl = f;
+    if (sl < 0 || sl >= n0) return set_err(QC_ERR_ARG, "qc_psi_diag_gather: block index out of range");
+    const long long dl = d0[sl], dr = d3[sr], o = ioff[blocks[b]];
+    if (o < 0 || o + dl * dr > size) return set_err(QC_ERR_ARG, "qc_psi_diag_gather: block outside the layout");
+    const long long base = (n * 4 + m) * ldim * rdim + so0[sl] * rdim + so3[sr];
+    for (long long u = 0; u < dl; ++u)
+      for (long long v = 0; v < dr; ++v) gat[o + u * dr + v] = base + u * rdim + v;
+  }
+  return QC_OK;
+}

@@ -320,7 +320,7 @@ class PanelStage(object):
         self.d_crow = torch.from_numpy(self.h_crow.astype(numpy.int64)).to(device)
         self.tc = Stage(tc_parts, device, name, ops) if tc_parts else None
         self.host_ops = ops
-        self.d_ops = torch.from_numpy(ops.view(numpy.uint8).copy()).to(device)
+        self.d_ops = upload(ops, device)
         self.groups = []
         self.flops = self.tc.flops if self.tc is not None else 0.0
         self.bytes = 0.0
@@ -331,7 +331,7 @@ class PanelStage(object):
             if not len(tk):
                 continue
             span = int(max(1, (tk["op_e"] - tk["op_b"]).max()))
-            self.groups.append((cfg, tk, torch.from_numpy(tk.view(numpy.uint8).copy()).to(device), span))
+            self.groups.append((cfg, tk, upload(tk, device), span))
             self.ntasks += len(tk)
 
     def run(self, A, B, C, kind="f64", stream=None):
@@ -474,7 +474,7 @@ class Stage(object):
         self.name = name
         self.summed = bool(summed)
         self.host_ops = ops
-        self.d_ops = torch.from_numpy(ops.view(numpy.uint8).copy()).to(device)
+        self.d_ops = upload(ops, device)
         self.groups = []
         self.bytes = 0.0          # algorithmic bytes (operands read once, output written once)
         self.flops = 0.0
@@ -497,8 +497,7 @@ class Stage(object):
             tk = numpy.concatenate(tasks)
             ct = numpy.concatenate(contribs)
             span = 1 if self.summed else int(max(1, (tk["op_e"] - tk["op_b"]).max()))
-            self.groups.append((cfg, tk, ct, torch.from_numpy(tk.view(numpy.uint8).copy()).to(device),
-                                torch.from_numpy(ct.view(numpy.uint8).copy()).to(device), span))
+            self.groups.append((cfg, tk, ct, upload(tk, device), upload(ct, device), span))
             self.ntasks += len(tk)
             self.ncontribs += len(ct)
 
@@ -697,8 +696,7 @@ class FiberStage(object):
         self.h_tasks, self.h_fin = cat(tks, FTASK_DT), cat(fis, FIN_DT)
         self.h_fout, self.h_fpair = cat(fos, FOUT_DT), cat(fps, FPAIR_DT)
         self.host_ops = ops
-        up = lambda a: torch.from_numpy(a.view(numpy.uint8).copy()).to(device)
-        self.d = [up(self.h_tasks), up(self.h_fin), up(self.h_fout), up(self.h_fpair), up(ops)]
+        self.d = [upload(a, device) for a in (self.h_tasks, self.h_fin, self.h_fout, self.h_fpair, ops)]
         self.ntasks = len(self.h_tasks)
         self.span = int(max(1, (self.h_tasks["op_e"] - self.h_tasks["op_b"]).max())) if self.ntasks else 1
         self.name = name
@@ -754,6 +752,14 @@ class CompositeStage(object):
     def run(self, A, B, C, kind="f64", stream=None):
         for x in self.subs:
             x.run(A, B, C, kind, stream)
+
+
+def upload(a, device):
+    """Bytes of a host work list as a device tensor (no intermediate host copy for a GPU; a
+    private copy on the CPU so that the tensor never aliases the host array)."""
+    b = numpy.ascontiguousarray(a).view(numpy.uint8)
+    t = torch.from_numpy(b)
+    return t.clone() if torch.device(device).type == "cpu" else t.to(device)
 
 
 def op_table(a_base, b_base, c_base, alpha):

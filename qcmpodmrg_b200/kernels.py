@@ -20,7 +20,7 @@ from . import native
 from .native import check
 from .engine import (Stage, compile_classes, add_parts, live_blocks, prune, op_table, TASK_DT, CONTRIB_DT, LOG,
                      compile_fiber, FiberStage, CompositeStage, panel_sigma1, compile_panels, BPERM_DT, PanelStage,
-                     fiber_stages, panel_sigma4)
+                     fiber_stages, panel_sigma4, upload)
 from .mpo import case
 from .qtensor import Contraction, Layout, flip_right, flip_horizontal
 
@@ -347,18 +347,18 @@ class SigmaOperator(object):
         self.lperm = None
         if lperm:
             self._lperm_h = numpy.concatenate(lperm)
-            self.lperm = torch.from_numpy(self._lperm_h.view(numpy.uint8).copy()).to(dev)
+            self.lperm = upload(self._lperm_h, dev)
             self._lperm_ops = op_table(L.offsets[order], 0, L.offsets[order], 1.0)
-            self._lperm_ops_d = torch.from_numpy(self._lperm_ops.view(numpy.uint8).copy()).to(dev)
+            self._lperm_ops_d = upload(self._lperm_ops, dev)
             self._lperm_span = int(max(len(v[0]) for v in plans.values()))
             self._build_lpan()
         # per-dot R panels (every operator's R blocks permuted), FP64 and FP32
         self.rperm = None
         if rperm:
             self._rperm_h = numpy.concatenate(rperm)
-            self.rperm = torch.from_numpy(self._rperm_h.view(numpy.uint8).copy()).to(dev)
+            self.rperm = upload(self._rperm_h, dev)
             rops = op_table(R.offsets[order], 0, R.offsets[order], 1.0)
-            self._rperm_ops_d = torch.from_numpy(rops.view(numpy.uint8).copy()).to(dev)
+            self._rperm_ops_d = upload(rops, dev)
             self._rperm_span = int(max(len(v[0]) for v in plans.values()))
             self._build_rpan()
         # fused W stage (T1 -> T3) and the per-dot two-site MPO blocks it reads
@@ -640,18 +640,15 @@ def _w_diag_map(lay, n2):
 
 
 def _psi_diag_gather(ql, ldim, rdim):
-    """Packed wavefunction position -> index of the dense [16, ldim, rdim] diagonal."""
+    """Packed wavefunction position -> index of the dense [16, ldim, rdim] diagonal
+    (qc_psi_diag_gather, host code of the native library)."""
     def build():
-        idx = ql.idx_allowed
-        sl, n, m, sr = numpy.unravel_index(idx, tuple(ql.nsyms))
-        d = ql.block_dims(idx)
-        dl, dr = d[:, 0], d[:, 3]
-        b, e = _ragged(dl * dr)
-        u, v = e // dr[b], e % dr[b]
-        gat = numpy.empty(ql.size, dtype=numpy.int64)
-        gat[ql.ioff[idx][b] + e] = ((n[b] * 4 + m[b]) * ldim * rdim + (ql.secoff[0][sl][b] + u) * rdim
-                                    + ql.secoff[3][sr][b] + v)
-        return gat
+        blocks = numpy.ascontiguousarray(ql.idx_allowed, dtype=numpy.int64)
+        gat = numpy.empty(max(ql.size, 1), dtype=numpy.int64)
+        check(native.lib().qc_psi_diag_gather(len(blocks), native.ptr(blocks), native.ptr(ql.nsyms),
+                                              native.ptr(ql.ndims_cat), native.ptr(ql.ioff), ldim, rdim, ql.size,
+                                              native.ptr(gat)), "qc_psi_diag_gather")
+        return gat[:ql.size]
     return _cached(("p", id(ql), ldim, rdim), ql, build)
 
 

@@ -40,6 +40,7 @@ _SIGS = {
     "qc_sym_allowed": (c_int, [c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
     "qc_sym_allowed_gpu": (c_int, [c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "qc_block_layout": (c_int, [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "qc_psi_diag_gather": (c_int, [c_ll, c_vp, c_vp, c_vp, c_vp, c_ll, c_ll, c_ll, c_vp]),
     "qc_contract_pairs": (c_ll, [c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_vp, c_ll]),
     "qc_compile_pairs": (c_ll, [c_int, c_vp, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp, c_vp, c_vp,
                                 c_int, c_vp, c_vp, c_ll, c_vp, c_int, c_vp, c_vp, c_vp, c_vp, c_int,
