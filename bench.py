@@ -30,7 +30,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "sweep sec & sigma TFLOP/s @K=24,D=500: mixed+learned vs FP64, |ΔE|≤1e-6 Eh"
-METRIC_SP = "spin-projected sweep sec (S=0 projector, FP64)"
+METRIC_SP = "spin-projected sweep sec (S=0 projector)"
 K_SITES, N_ELEC, DECAY, SEED, DMAX = 24, 24, 3.0, 1, 500
 RAMP = (50, 100, 200)
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
@@ -146,8 +146,9 @@ def run_ours(args):
     sp = args.workload == "sp"
     if sp:
         from qcmpodmrg_b200.spin import SPDMRG
-        prec = "f64"                  # the spin-projected path runs in FP64
-        d = SPDMRG(ham, args.npts, 0.0, 0.0, device=dev, w_path=args.w_path)
+        if prec not in ("f64", "f32"):
+            raise SystemExit("--workload sp runs with --precision f64 or mixed")
+        d = SPDMRG(ham, args.npts, 0.0, 0.0, device=dev, w_path=args.w_path, precision=prec)
     else:
         d = DMRG(ham, device=dev, precision=prec, w_path=args.w_path, plan_cache=args.plan_cache)
     d.load_mps(product_mps(ham))
@@ -227,7 +228,7 @@ def run_ours(args):
                                    args.npts)) if sp else
                                "two-site Qt DMRG sweep, K=%d N=%d Sz=0 D=%d, %d operators H_p"
                                % (args.sites, args.sites, args.dmax, 2 * args.sites), "K": args.sites,
-                   "N": args.sites, "D": args.dmax, "precision": "f64" if sp else args.precision,
+                   "N": args.sites, "D": args.dmax, "precision": args.precision,
                    "w_path": args.w_path,
                    "l2": "inputs larger than L2: environments and sigma scratch are tens of GB per sweep",
                    "parallelism": "replicas" if world > 1 else "1 GPU",

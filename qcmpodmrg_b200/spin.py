@@ -201,10 +201,14 @@ class SPDMRG(DMRG):
     ifs2proj = True
 
     def __init__(self, ham, npts, sval=0.0, sz=0.0, device="cuda", w_path="fiber", quad="GaussLegendre",
-                 prune_zero_blocks=True):
+                 prune_zero_blocks=True, precision="f64"):
+        """precision: "f64", or "f32" for FP32 H and S products in the generalised Davidson
+        followed by an FP64 check of the solution (FP64 iterations when it fails)."""
+        if precision not in ("f64", "f32"):
+            raise ValueError("spin projection runs in f64 or f32 (mixed)")
         self.npts, self.sval, self.sz, self.quad = int(npts), float(sval), float(sz), quad
         self.prune_zero_blocks = prune_zero_blocks
-        super(SPDMRG, self).__init__(ham, device=device, precision="f64", w_path=w_path)
+        super(SPDMRG, self).__init__(ham, device=device, precision=precision, w_path=w_path)
 
     def _setup_operators(self, ham):
         self.qpts, self.qwts = s2quad(self.npts, self.sval, self.sz, self.quad)
@@ -268,6 +272,35 @@ class SPDMRG(DMRG):
         out = torch.empty(lay_n.size, dtype=torch.float64, device=self.device)
         return K.scatter(vals.contiguous(), red, out)
 
+    def _mixed_gdavidson(self, sig, sv, diag, v0, crit_e):
+        """Generalised Davidson with FP32 H and S products, then one FP64 pair of products:
+        the FP64 Rayleigh quotient e = x.Hx / x.Sx is accurate to second order in the
+        vector's error.  Accepted when the FP64 residual |Hx - e Sx| (x S-normalised) is at
+        most 1e-4, or when the FP32 solve converged by the reference's criteria and e agrees
+        with its Ritz value within 1e-6 Eh; otherwise FP64 iterations continue from x."""
+        from .dmrg import ACCEPT_DE
+        r1 = gdavidson(sig, sv, diag, 1, v0, crit_e=crit_e, crit_vec=max(self.crit_vec, 1e-5))
+        x = r1.vecs[0]
+        hx, sx = sig(x, precision="f64"), sv(x, precision="f64")
+        xsx = float(torch.dot(x, sx))
+        if xsx <= 0.0:
+            raise RuntimeError("spin projection: the FP32 solution has no weight in the projected space")
+        e64 = float(torch.dot(x, hx)) / xsx
+        rn = float(torch.linalg.norm(hx - e64 * sx)) / xsx ** 0.5
+        self.stats["nmvp_f64"] = self.stats.get("nmvp_f64", 0) + 1
+        self.stats["nmvp_low"] = self.stats.get("nmvp_low", 0) + r1.nmvp
+        converged = r1.niter < 19
+        if rn <= max(self.crit_vec, 1e-4) or (converged and abs(e64 - float(r1.eigs[0])) <= ACCEPT_DE):
+            r1.eigs = numpy.array([e64])
+            r1.vecs = (x / xsx ** 0.5).reshape(1, -1)
+            r1.nmvp += 1
+            return r1
+        r2 = gdavidson(lambda v: sig(v, precision="f64"), lambda v: sv(v, precision="f64"), diag, 1,
+                       x.reshape(1, -1), crit_e=crit_e, crit_vec=self.crit_vec)
+        self.stats["nmvp_f64"] += r2.nmvp
+        r2.nmvp += r1.nmvp + 1
+        return r2
+
     def _psi_layout(self, isite):
         ql, qr = self.qnuml[isite], self.qnumr[isite + 2]
         cls = [classification(q) for q in (ql, QPHYS, QPHYS, self.qkey - qr)]
@@ -287,7 +320,7 @@ class SPDMRG(DMRG):
         L, R = self.lenv[isite - 1], self.renv[isite + 2]
         Wi, Wj = self.mpo[isite], self.mpo[isite + 1]
         inner = SigmaOperator(self.ws, isite, lay_n, L, R, Wi, Wj, self.qkey[:1], self.opers, self.hpwts,
-                              "f64", live=self._live(lay), **self.sigma_opts)
+                              self.precision, live=self._live(lay), **self.sigma_opts)
         sig = ProjectedOperator(self.ws, inner, red)
         dg = DiagOperator(self.ws, isite, lay, L, R, Wi, Wj, self.qkey, self.opers, self.hpwts)
         return lay, idl, sig, dg
@@ -299,7 +332,7 @@ class SPDMRG(DMRG):
         red = reduce_map(lay, lay_n)
         PL, PR = self.plenv[isite - 1], self.prenv[isite + 2]
         inner = SigmaOperator(self.ws, isite, lay_n, PL, PR, self.pops, self.pops, self.qkey[:1], self.popers,
-                              self.qwts, "f64", live=self._live(lay), **self.sigma_opts)
+                              self.qwts, self.precision, live=self._live(lay), **self.sigma_opts)
         sv = ProjectedOperator(self.ws, inner, red)
         sd = DiagOperator(self.ws, isite, lay, PL, PR, self.pops, self.pops, self.qkey, self.popers, self.qwts)
         return sv, sd
@@ -324,7 +357,10 @@ class SPDMRG(DMRG):
         if self.psi0 is not None:
             v0 = self.psi0[0:1].reshape(1, -1)[:, prj].contiguous()
         t0 = time.time()
-        res = gdavidson(sig, sv, diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec)
+        if self.precision == "f64":
+            res = gdavidson(sig, sv, diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec)
+        else:
+            res = self._mixed_gdavidson(sig, sv, diag, v0, crit_e)
         torch.cuda.synchronize(dev)
         self.stats["hvec_s"] += time.time() - t0
         self.stats["nmvp"] += res.nmvp

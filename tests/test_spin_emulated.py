@@ -142,3 +142,17 @@ def _dropin_vs_oracle(device):
     for E, ref in ((flstN[0][0], o.lenv[0]), (flstN[0][1], o.plenv[0])):
         for i, q in enumerate(ref):
             assert numpy.abs(E.op_values(i).cpu().numpy() - q.value).max() <= 1e-12
+
+
+def test_sp_mixed_sweep_emulated(monkeypatch):
+    """FP32 H and S products with the FP64 check: the K=4 spin-projected run reaches the
+    reference's energies within 1e-6 Eh (intermediates rounded to FP32 by the interpreter)."""
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    from qcmpodmrg_b200.spin import SPDMRG
+    sw = load("sweep_SP_K4.npz")
+    ham = make_hamiltonian(int(sw["K"]), int(sw["N"]), int(sw["seed"]), None)
+    d = SPDMRG(ham, int(sw["npts"]), device="cpu", precision="f32")
+    out = d.run(sw["init_mps"], int(sw["D"]), 1)
+    assert abs(out["eav"][0] - sw["eav"][0]) <= 1e-6
+    assert d.stats.get("nmvp_low", 0) > 0 and d.stats.get("nmvp_f64", 0) > 0

@@ -68,3 +68,14 @@ def test_gpu_sp_truncated_sweeps_converge_to_reference(cuda):
     out = SPDMRG(ham, int(sw["npts"]), device=cuda).run(sw["init_mps"], int(sw["D"]), int(sw["nsweeps"]))
     assert abs(out["eav"][-1] - sw["eav"][-1]) <= 1e-6
     assert numpy.abs(out["eav"] - sw["eav"][:len(out["eav"])]).max() <= 1e-5
+
+
+def test_gpu_sp_mixed_precision(cuda):
+    """FP32 H and S products with the FP64 check reach the reference's K=4 energies to 1e-6 Eh."""
+    from qcmpodmrg_b200.spin import SPDMRG
+    sw = load("sweep_SP_K4.npz")
+    ham = make_hamiltonian(int(sw["K"]), int(sw["N"]), int(sw["seed"]), None)
+    d = SPDMRG(ham, int(sw["npts"]), device=cuda, precision="f32")
+    out = d.run(sw["init_mps"], int(sw["D"]), int(sw["nsweeps"]))
+    assert numpy.abs(out["eav"] - sw["eav"][:len(out["eav"])]).max() <= 1e-6
+    assert d.stats.get("nmvp_low", 0) > 0
