@@ -89,6 +89,13 @@ def fci_energy(ham):
     Independent check used by the tests: DMRG with an unrestricted bond
     dimension must reproduce it.
     """
+    h, dets = fci_hamiltonian(ham)
+    return numpy.linalg.eigvalsh(h)[0]
+
+
+def fci_hamiltonian(ham):
+    """H in the (N, Sz=0) determinant basis (sorted spin-orbital tuples; 2i = alpha,
+    2i+1 = beta), symmetrised, and the determinants."""
     from itertools import combinations
     n = ham.sbas
     N = ham.nelec
@@ -148,5 +155,4 @@ def fci_energy(ham):
                         d, sg = apply(dj, [(p, True), (q, True), (s_, False), (r, False)])
                         if d is not None and d in index:
                             H[index[d], j] += sg * val
-    w = numpy.linalg.eigvalsh(0.5 * (H + H.T))
-    return w[0]
+    return 0.5 * (H + H.T), dets

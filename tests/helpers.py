@@ -156,3 +156,30 @@ def record_noise(r, device):
         m = c.reshape(c.shape[0], c.shape[1], -1)
         cc = sum(m[i].T @ m[i] for i in range(len(m)))
     return NoiseRDM(ws, j, status, lay, E, W, opers, qkey, dense_idl), vals, cc
+
+
+def fci_spin_states(ham, nstates=8):
+    """Lowest eigenvalues of H in the (N, Sz=0) determinant space with their <S^2>
+    (S^2 = S+^T S+ there), by exact diagonalisation (small K only): an independent check
+    of spin-projected results."""
+    from itertools import combinations
+    from qcmpodmrg_b200.hamiltonian import fci_hamiltonian
+    n, N = ham.sbas, ham.nelec
+    na = N // 2
+    alpha, beta = [2 * i for i in range(n // 2)], [2 * i + 1 for i in range(n // 2)]
+    h, dets = fci_hamiltonian(ham)
+    up = {d: i for i, d in enumerate(tuple(sorted(a + b)) for a in combinations(alpha, na + 1)
+                                     for b in combinations(beta, N - na - 1))}
+    sp = numpy.zeros((len(up), len(dets)))
+    for j, d in enumerate(dets):
+        for i in range(n // 2):
+            a, b = 2 * i, 2 * i + 1
+            if b in d and a not in d:
+                occ = list(d)
+                sign = (-1) ** occ.index(b)
+                occ.remove(b)
+                sign *= (-1) ** sum(1 for o in occ if o < a)
+                sp[up[tuple(sorted(occ + [a]))], j] += sign
+    w, v = numpy.linalg.eigh(h)
+    s2 = numpy.einsum("ij,ik,kj->j", v, sp.T @ sp, v)
+    return w[:nstates], s2[:nstates]

@@ -156,3 +156,19 @@ def test_sp_mixed_sweep_emulated(monkeypatch):
     out = d.run(sw["init_mps"], int(sw["D"]), 1)
     assert abs(out["eav"][0] - sw["eav"][0]) <= 1e-6
     assert d.stats.get("nmvp_low", 0) > 0 and d.stats.get("nmvp_f64", 0) > 0
+
+
+def test_sp_triplet_reaches_fci_triplet(monkeypatch):
+    """Projection onto S=1 (Sz=0, 3 points, every state kept): the sweep lands on the lowest
+    triplet of exact diagonalisation, not on the singlet ground state."""
+    from helpers import fci_spin_states
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    from qcmpodmrg_b200.spin import SPDMRG
+    sw = load("sweep_SP_K4.npz")
+    ham = make_hamiltonian(4, 4, 1, None)
+    w, s2 = fci_spin_states(ham)
+    e_t = w[numpy.flatnonzero(numpy.abs(s2 - 2.0) < 1e-6)[0]]
+    assert abs(s2[0]) < 1e-6 and e_t > w[0] + 0.1          # the ground state is a singlet
+    out = SPDMRG(ham, 3, sval=1.0, sz=0.0, device="cpu").run(sw["init_mps"], 16, 1)
+    assert abs(out["eav"][0] - e_t) <= 1e-8

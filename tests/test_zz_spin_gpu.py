@@ -79,3 +79,14 @@ def test_gpu_sp_mixed_precision(cuda):
     out = d.run(sw["init_mps"], int(sw["D"]), int(sw["nsweeps"]))
     assert numpy.abs(out["eav"] - sw["eav"][:len(out["eav"])]).max() <= 1e-6
     assert d.stats.get("nmvp_low", 0) > 0
+
+
+def test_gpu_sp_triplet_reaches_fci_triplet(cuda):
+    from helpers import fci_spin_states
+    from qcmpodmrg_b200.spin import SPDMRG
+    sw = load("sweep_SP_K4.npz")
+    ham = make_hamiltonian(4, 4, 1, None)
+    w, s2 = fci_spin_states(ham)
+    e_t = w[numpy.flatnonzero(numpy.abs(s2 - 2.0) < 1e-6)[0]]
+    out = SPDMRG(ham, 3, sval=1.0, sz=0.0, device=cuda).run(sw["init_mps"], 16, 2)
+    assert abs(out["eav"][-1] - e_t) <= 1e-8
