@@ -247,7 +247,7 @@ def run_ours(args):
         "phase_s_per_step": {k: round(stats[k] / args.steps, 2) for k in ("plan_s", "hvec_s", "hdiag_s", "renorm_s",
                                                                          "decim_s") if k in stats},
     }
-    if args.e2e and not sp:
+    if args.e2e:
         e2e = e2e_leg(d, args)
         e2e["value"] = round(max_over_ranks(dist, e2e["value"], dev) / world, 3)
         line["e2e"] = e2e
@@ -274,7 +274,8 @@ def e2e_leg(d, args):
     d.host_api = False
     return {"value": round(dt, 3), "unit": "s/sweep", "h2d_bytes_per_step": int(d.h2d_bytes),
             "d2h_bytes_per_step": int(d.d2h_bytes),
-            "path": "qcmpodmrg_b200.mpo_dmrg_kernel.HVec/HDiag with host buffers, host Davidson"}
+            "path": "qcmpodmrg_b200.mpo_dmrg_kernel.HVec/HDiag%s with host buffers, host Davidson"
+                    % ("/SVec" if getattr(d, "ifs2proj", False) else "")}
 
 
 def cpu_baseline_sample(d, gpu_sweep_s, sp=False):

@@ -337,9 +337,52 @@ class SPDMRG(DMRG):
         sd = DiagOperator(self.ws, isite, lay, PL, PR, self.pops, self.pops, self.qkey, self.popers, self.qwts)
         return sv, sd
 
+    def _solve_dot_host(self, isite, status, dmax, crit_e):
+        """The same dot through mpo_dmrg_kernel.HDiag/HVec/SVec with host (NumPy) vectors
+        and the generalised Davidson on the host, as the reference's pgdvdson calls them."""
+        from . import mpo_dmrg_kernel as MK
+        dev = self.device
+        info = [self, isite, 2, [[self.lenv[isite - 1], self.renv[isite + 2], self.plenv[isite - 1],
+                                  self.prenv[isite + 2]]], status, True]
+        t0 = time.time()
+        lay, idl, sig, dg = MK._ops(self, isite)
+        sv, sd = MK._sops(self, isite)
+        prj_h = lay.prjmap(idl)
+        self.stats["plan_s"] += time.time() - t0
+        ndim0 = lay.size
+        ldim, rdim = len(self.qnuml[isite]), len(self.qnumr[isite + 2])
+        dims = (ldim, 16, rdim, ldim * 16 * rdim)
+        diag = torch.from_numpy(MK.HDiag(info, ndim0, prj_h))
+        self.d2h_bytes += 8 * ndim0
+
+        def host(fn):
+            def apply(x):
+                y = fn(x.numpy(), info, ndim0, prj_h)
+                self.h2d_bytes += 8 * ndim0
+                self.d2h_bytes += 8 * ndim0
+                return torch.from_numpy(y)
+            return apply
+
+        v0 = None
+        if self.psi0 is not None:
+            v0 = self.psi0[0:1].reshape(1, -1)[:, torch.from_numpy(prj_h).to(self.psi0.device)].cpu()
+        t0 = time.time()
+        res = gdavidson(host(MK.HVec), host(MK.SVec), diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec)
+        self.stats["hvec_s"] += time.time() - t0
+        self.stats["nmvp"] += res.nmvp
+        self.stats["sigma_flops"] += res.nmvp * (sig.flops + sv.flops)
+        civec = torch.zeros((1, dims[3]), dtype=torch.float64, device=dev)
+        civec[:, torch.from_numpy(prj_h).to(dev)] = res.vecs.to(dev)
+        self.h2d_bytes += 8 * ndim0
+        t0 = time.time()
+        out = self.decimate(civec, isite, status, dims, dmax)
+        torch.cuda.synchronize(dev)
+        self.stats["decim_s"] += time.time() - t0
+        return res, out, dims, sig
+
     def solve_dot(self, isite, status, dmax, crit_e):
         if self.host_api:
-            raise NotImplementedError("host-buffer dot driver: plain (unprojected) DMRG only")
+            return self._solve_dot_host(isite, status, dmax, crit_e)
         dev = self.device
         t0 = time.time()
         lay, idl, sig, dg = self.dot_operators(isite)

@@ -172,3 +172,19 @@ def test_sp_triplet_reaches_fci_triplet(monkeypatch):
     assert abs(s2[0]) < 1e-6 and e_t > w[0] + 0.1          # the ground state is a singlet
     out = SPDMRG(ham, 3, sval=1.0, sz=0.0, device="cpu").run(sw["init_mps"], 16, 1)
     assert abs(out["eav"][0] - e_t) <= 1e-8
+
+
+def test_sp_host_api_sweep_emulated(monkeypatch):
+    """The spin-projected dot driven through mpo_dmrg_kernel.HVec/SVec/HDiag with host vectors
+    (the reference's calling convention) gives the same first sweep as the device driver."""
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    from qcmpodmrg_b200.spin import SPDMRG
+    sw = load("sweep_SP_K4.npz")
+    ham = make_hamiltonian(int(sw["K"]), int(sw["N"]), int(sw["seed"]), None)
+    d = SPDMRG(ham, int(sw["npts"]), device="cpu")
+    d.host_api = True
+    out = d.run(sw["init_mps"], int(sw["D"]), 1)
+    n = len(out["esweeps"])
+    assert numpy.abs(out["esweeps"] - sw["esweeps"][:n]).max() <= 1e-8
+    assert d.h2d_bytes > 0 and d.d2h_bytes > 0
