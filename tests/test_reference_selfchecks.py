@@ -18,11 +18,10 @@ from emulate import patch_stage_run
 @pytest.mark.parametrize("tag", ["K4", "K5"])
 def test_check_diag_qt(tag, monkeypatch):
     patch_stage_run(monkeypatch)
-    for r in load("kernels_%s.npz" % tag)["records"]:
+    recs = load("kernels_%s.npz" % tag)["records"]
+    for r in [max(recs, key=lambda x: len(x["hvec_x"]))]:      # the largest recorded dot
         sig, dg, ws = record_operators(r, "cpu", use_fiber=True)
         n = sig.ndim0
-        if n > 400:
-            continue
         h = numpy.array([sig(torch.from_numpy(e)).numpy() for e in numpy.identity(n)]).T
         assert numpy.linalg.norm(h - h.T) <= 1e-10
         assert numpy.linalg.norm(numpy.diag(h) - dg().numpy()) <= 1e-10
