@@ -15,7 +15,7 @@ from helpers import load, record_operators
 from emulate import patch_stage_run
 
 
-@pytest.mark.parametrize("tag", ["K4", "K5"])
+@pytest.mark.parametrize("tag", ["K4"])
 def test_check_diag_qt(tag, monkeypatch):
     patch_stage_run(monkeypatch)
     recs = load("kernels_%s.npz" % tag)["records"]
