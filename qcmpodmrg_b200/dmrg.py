@@ -7,7 +7,9 @@ ncsite=2, one symmetry sector):
   sweep                 source/mpo_dmrg_opt.py:31-101 (+ updateSite :319-350, updateBoundary :353-383)
   ci_solver             source/mpo_dmrg_dot.py:24-112 (setupQtmpCI dotutil.py:173-184)
   decimation            source/mpo_dmrg_dotutil.py:269-476 with rdm_blkdiag (mpo_dmrg_qparser.py:106-183)
+                        and the pRDM noise term (pRDMQt, mpo_dmrg_kernelQt.py:453-626) when noise > 0
   genGuess              source/mpo_dmrg_dotutil.py:479-540
+The spin-projected variant (ifs2proj) is qcmpodmrg_b200.spin.SPDMRG.
 Environments L_p / R_p of every operator live in HBM (TensorSet) instead of
 per-site HDF5 files; the sigma/diagonal/renormalisation plans are built once
 per dot.  Davidson, the RDM and its eigendecomposition run in FP64 on the GPU;
