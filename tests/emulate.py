@@ -11,6 +11,12 @@ def _idx(i, lo, s_hi, s_lo):
     return (i // lo) * s_hi + (i % lo) * s_lo
 
 
+def _f64(t):
+    """A device buffer as float64 NumPy (scratch may hold never-written FP32 bit patterns)."""
+    with numpy.errstate(invalid="ignore", over="ignore"):
+        return t.detach().cpu().numpy().astype(numpy.float64)
+
+
 def patch_stage_run(monkeypatch):
     """Route Stage.run through the interpreter (tile extents follow the stage's tile config)."""
     import torch
@@ -19,9 +25,9 @@ def patch_stage_run(monkeypatch):
     def run(self, A, B, C, kind="f64", stream=None):
         if self.ntasks == 0:
             return
-        a = A.detach().cpu().numpy().astype(numpy.float64)
-        b = B.detach().cpu().numpy().astype(numpy.float64)
-        c = C.detach().cpu().numpy().astype(numpy.float64)
+        a = _f64(A)
+        b = _f64(B)
+        c = _f64(C)
         for cfg, tk, ct in self.host_groups:
             tm, tn = engine.TILES[cfg]
             _run_tiled(tk, ct, self.host_ops, self.summed, a, b, c, tm, tn)
@@ -32,18 +38,18 @@ def patch_stage_run(monkeypatch):
     def frun(self, A, B, C, kind="f64", stream=None):
         if self.ntasks == 0:
             return
-        a = A.detach().cpu().numpy().astype(numpy.float64)
-        w = B.detach().cpu().numpy().astype(numpy.float64)
-        c = C.detach().cpu().numpy().astype(numpy.float64)
+        a = _f64(A)
+        w = _f64(B)
+        c = _f64(C)
         _run_fiber(self, a, w, c)
         C.copy_(torch.from_numpy(c).to(C.dtype))
 
     monkeypatch.setattr(engine.FiberStage, "run", frun)
 
     def prun(self, A, B, C, kind="f64", stream=None):
-        a = A.detach().cpu().numpy().astype(numpy.float64)
-        b = B.detach().cpu().numpy().astype(numpy.float64)
-        c = C.detach().cpu().numpy().astype(numpy.float64)
+        a = _f64(A)
+        b = _f64(B)
+        c = _f64(C)
         for (cfg, tk, _, _) in self.groups:
             tm, tn = engine.PANEL_TILES[cfg]
             for t in tk:
@@ -68,8 +74,8 @@ def patch_stage_run(monkeypatch):
     def block_permute(descs, ndescs, opspan, ops, src, dst):
         d = descs.cpu().numpy().view(engine.BPERM_DT)
         o = ops.cpu().numpy().view(engine.OP_DT)
-        a = src.detach().cpu().numpy().astype(numpy.float64)
-        c = dst.detach().cpu().numpy().astype(numpy.float64)
+        a = _f64(src)
+        c = _f64(dst)
         for x in d:
             for op in range(x["op_b"], x["op_e"]):
                 blk = a[o[op]["a_base"] + x["src_off"]:][:x["d0"] * x["d1"] * x["d2"]].reshape(x["d0"], x["d1"], x["d2"])
