@@ -31,7 +31,7 @@ from . import kernels as K
 from .kernels import SigmaOperator, DiagOperator, Renormalizer, TensorSet, _ragged
 from .mpo import QPHYS, W_STATUS, _hfac_spin, _link, _elem_q, _wq
 from .qtensor import Layout, classification
-from .dmrg import DMRG, PSI_STATUS
+from .dmrg import DMRG, PSI_STATUS, L_STATUS, SiteTensor
 from .davidson import gdavidson
 
 QPHYS_N = QPHYS[:, 0:1].copy()
@@ -229,7 +229,6 @@ class SPDMRG(DMRG):
         return lay_n, vals
 
     def load_mps(self, init):
-        from .dmrg import SiteTensor, L_STATUS
         Kn = self.nsite
         dev = self.device
         self.qnuml = [numpy.array(init["qnum%d" % i], dtype=numpy.float64).reshape(-1, 2) for i in range(Kn + 1)]
