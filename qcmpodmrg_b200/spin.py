@@ -109,11 +109,11 @@ def _order_n(q):
     return numpy.argsort(numpy.rint(2 * q[:, 0]).astype(numpy.int64), kind="stable")
 
 
-def sp_site_operator(p, phi, nsite_spin, isite, int1e, int2e):
-    """H_p R(phi) at spatial site isite with N-only quantum numbers: (Layout, packed values)."""
+def _sp_site_block(p, nsite_spin, isite, int1e, int2e):
+    """H_p at spatial site isite with its MPO bond ordered by N (stable), and the N-only
+    layout every H_p R(theta) shares: (dense [A, B, 4, 4] in that order, layout, packing map)."""
     hq, v = int1e[p], int2e[p]
     dense = _link(_hfac_spin(p, nsite_spin, 2 * isite, hq, v), _hfac_spin(p, nsite_spin, 2 * isite + 1, hq, v))
-    dense = numpy.tensordot(dense, exp_isy_phi(phi), axes=([3], [0]))
     ql1, _ = _elem_q(p, 2 * isite)
     _, qr1 = _elem_q(p, 2 * isite + 1)
     ql2, _ = _wq(nsite_spin, 2 * isite, p % 2)
@@ -122,7 +122,14 @@ def sp_site_operator(p, phi, nsite_spin, isite, int1e, int2e):
     il, ir = _order_n(ql), _order_n(qr)
     cl, cr = classification(ql[il]), classification(qr[ir])
     lay = Layout(W_STATUS, [cl[0], cr[0], _PHYS_N[0], _PHYS_N[0]], [cl[1], cr[1], _PHYS_N[1], _PHYS_N[1]])
-    return lay, _packed(lay, [cl[2], cr[2], _PHYS_N[2], _PHYS_N[2]], dense[numpy.ix_(il, ir)])
+    prj = lay.prjmap([cl[2], cr[2], _PHYS_N[2], _PHYS_N[2]])
+    return numpy.ascontiguousarray(dense[numpy.ix_(il, ir)]), lay, prj
+
+
+def sp_site_operator(p, phi, nsite_spin, isite, int1e, int2e):
+    """H_p R(phi) at spatial site isite with N-only quantum numbers: (Layout, packed values)."""
+    dense, lay, prj = _sp_site_block(p, nsite_spin, isite, int1e, int2e)
+    return lay, numpy.tensordot(dense, exp_isy_phi(phi), axes=([3], [0])).ravel()[prj].copy()
 
 
 def sp_opers(sbas, npts):
@@ -131,12 +138,23 @@ def sp_opers(sbas, npts):
 
 
 def build_mpo_sp(ham, qpts, isites=None):
-    """Layouts and values of H_p R(theta_g) for every operator at every spatial site."""
-    ops = sp_opers(ham.sbas, len(qpts))
+    """Layouts and values of H_p R(theta_g) for every operator at every spatial site.
+
+    H_p, its bond order and its layout are built once per (p, site); the rotations of
+    all quadrature points are applied to it in one contraction."""
+    npts = len(qpts)
+    rot = numpy.stack([exp_isy_phi(t) for t in qpts]).transpose(1, 0, 2).reshape(4, 4 * npts)   # [m, (g k)]
     out = {}
     for i in (range(ham.nsite) if isites is None else isites):
-        pairs = [sp_site_operator(p, qpts[g], ham.sbas, i, ham.int1e, ham.int2e) for (p, g) in ops]
-        out[i] = ([a for a, _ in pairs], [b for _, b in pairs])
+        lays, vals = [], []
+        for p in range(ham.sbas):
+            dense, lay, prj = _sp_site_block(p, ham.sbas, i, ham.int1e, ham.int2e)
+            a, b = dense.shape[:2]
+            allg = (dense.reshape(-1, 4) @ rot).reshape(a, b, 4, npts, 4).transpose(3, 0, 1, 2, 4).reshape(npts, -1)
+            for g in range(npts):
+                lays.append(lay)
+                vals.append(allg[g][prj].copy())
+        out[i] = (lays, vals)
     return out
 
 
