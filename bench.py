@@ -322,7 +322,8 @@ def run_reference(args):
 def run_batched(args):
     """Independent instances (K in [8, 14], D in [64, 128], --instances of them) swept in lockstep:
     one launch per sigma contraction for all instances per Davidson step, replayed from CUDA
-    graphs, against the same instances swept one after another.  Prints one JSON line."""
+    graphs (or launched directly with --no-graphs), against the same instances swept one after
+    another.  Prints one JSON line."""
     import torch
     from qcmpodmrg_b200.hamiltonian import make_hamiltonian
     from qcmpodmrg_b200.synthetic import product_mps
@@ -355,7 +356,7 @@ def run_batched(args):
     t_seq = time.time() - t0
     del seq
     bat = make()
-    b = BatchedDMRG(bat, kind="f64", use_graphs=True)
+    b = BatchedDMRG(bat, kind="f64", use_graphs=args.graphs)
     torch.cuda.synchronize()
     t0 = time.time()
     for st in ("R", "L"):
@@ -369,7 +370,7 @@ def run_batched(args):
                                    % len(shapes), "shapes": shapes},
             "sequential_instance_sweeps_per_s": round(len(shapes) / t_seq, 3),
             "batched_s": round(t_bat, 2), "sequential_s": round(t_seq, 2),
-            "graph_captures": b.captures, "lockstep_steps": b.steps}
+            "graphs": args.graphs, "graph_captures": b.captures, "lockstep_steps": b.steps}
     print(json.dumps(line), flush=True)
 
 
@@ -391,6 +392,8 @@ def main():
                     help="sp: spin-projected sweeps (SP-MPS, S=0) with --npts quadrature points")
     ap.add_argument("--npts", type=int, default=4)
     ap.add_argument("--instances", type=int, default=16)
+    ap.add_argument("--no-graphs", dest="graphs", action="store_false",
+                    help="batched workload: plain lockstep launches instead of CUDA-graph replay")
     args = ap.parse_args()
     if args.workload == "batched":
         run_batched(args)
