@@ -117,3 +117,17 @@ def test_sweep_with_noise_emulated(monkeypatch):
     fx = load("sweep_NZ_K5.npz")
     _first_sweep_matches(DMRG(_ham(fx), device="cpu").run(fx["init_mps"], int(fx["D"]), 1,
                                                           noise=float(fx["noise"])), fx)
+
+
+def test_sp_half_sweep_with_noise_emulated(monkeypatch):
+    """Spin projection and the noise term together (the reference's K=5, 3-point run with
+    noise 1e-4): every dot energy of the first right-to-left half sweep and its matvecs."""
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    from qcmpodmrg_b200.spin import SPDMRG
+    fx = load("sweep_NZSP_K5.npz")
+    d = SPDMRG(_ham(fx), int(fx["npts"]), device="cpu")
+    d.noise = float(fx["noise"])
+    d.load_mps(fx["init_mps"])
+    n, e, dw, el, dl = d.sweep("R", int(fx["D"]), 1e-7)
+    assert numpy.abs(numpy.array(el) - fx["esweeps"][:len(el)]).max() <= 1e-8
