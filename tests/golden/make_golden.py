@@ -50,13 +50,14 @@ def qsym_cases(seed=7):
     print("qsym cases:", len(cases), "allowed counts", [int(c["allowed"].sum()) for c in cases])
 
 
-def run_case(tag, K, N, D, nsweeps, seed, decay, targets, record_envs=True, npts=None, noise=0.0):
+def run_case(tag, K, N, D, nsweeps, seed, decay, targets, record_envs=True, npts=None, noise=0.0,
+             quad="GaussLegendre"):
     res, rec = rr.run_reference(K=K, N=N, D=D, nsweeps=nsweeps, seed=seed, decay=decay, targets=targets,
-                                record_envs=record_envs, npts=npts, noise=noise)
+                                record_envs=record_envs, npts=npts, noise=noise, quad=quad)
     sweep = {"K": K, "N": N, "D": D, "seed": seed, "decay": -1.0 if decay is None else float(decay),
              "nsweeps": nsweeps, "eav": res["eav"], "dwt": res["dwt"], "esweeps": res["esweeps"],
              "nmvp": res["nmvp"], "init_mps": {k: v for k, v in res["init_mps"].items() if k != "nsite"},
-             "npts": 0 if npts is None else int(npts), "noise": float(noise)}
+             "npts": 0 if npts is None else int(npts), "noise": float(noise), "quad": quad}
     fixtures.save(os.path.join(HERE, "sweep_%s.npz" % tag), sweep)
     if targets:
         recs = []
@@ -86,6 +87,7 @@ if __name__ == "__main__":
     if a.spin:
         run_case("SP_K4", 4, 4, 16, 2, 1, None, [(0, "R", 1), (0, "L", 1), (1, "L", 2)], npts=3)
         run_case("SP_K5", 5, 4, 12, 3, 2, 2.0, [(0, "R", 2), (1, "L", 1)], npts=4)
+        run_case("SPS_K4", 4, 4, 16, 1, 1, None, [(0, "L", 1)], npts=5, quad="Simpson")
         sys.exit(0)
     if a.config1:
         run_case("C1", 12, 12, 100, 6, 1, None, [], record_envs=False)

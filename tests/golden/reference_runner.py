@@ -80,11 +80,13 @@ class Recorder(object):
 
 
 def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.0,
-                  tol=1.e-7, maxslc=1, record_envs=True, workdir=None, npts=None, sval=0.0, sz=0.0):
+                  tol=1.e-7, maxslc=1, record_envs=True, workdir=None, npts=None, sval=0.0, sz=0.0,
+                  quad="GaussLegendre"):
     """Run the reference flow; return (result dict, recorder).
 
     npts: spin projection (SP-MPS) with ``npts`` quadrature points for <S^2> = sval(sval+1),
-    Sz = sz, set as examples/examples_spmpsQt/main_spmps.py does (ifs2proj, s2quad).
+    Sz = sz, set as examples/examples_spmpsQt/main_spmps.py does (ifs2proj, s2quad); quad
+    selects the reference's quadrature rule (GaussLegendre or Simpson).
     """
     mpo_dmrg_class, mpo_dmrg_schedule, mpo_dmrg_kernel, qtensor_api, qtensor, class_molinfo = _ref()
     from qcmpodmrg.source import mpo_dmrg_io
@@ -143,6 +145,7 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
         if npts is not None:
             dmrg2.ifs2proj = True
             dmrg2.npts = npts
+            dmrg2.quad = quad
             dmrg2.s2quad(sval, sz)
         mol.build()
         dmrg2.path = mol.path

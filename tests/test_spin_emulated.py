@@ -12,7 +12,7 @@ from qcmpodmrg_b200.hamiltonian import make_hamiltonian
 
 @pytest.mark.parametrize("tag,w_path,prune", [("SP_K4", "generic", True), ("SP_K4", "fiber", True),
                                                ("SP_K4", "fiber", False), ("SP_K5", "generic", True),
-                                               ("SP_K5", "fiber", True)])
+                                               ("SP_K5", "fiber", True), ("SPS_K4", "fiber", True)])
 def test_sp_operators_emulated(tag, w_path, prune, monkeypatch):
     patch_stage_run(monkeypatch)
     for r in load("kernels_%s.npz" % tag)["records"]:
@@ -188,3 +188,17 @@ def test_sp_host_api_sweep_emulated(monkeypatch):
     n = len(out["esweeps"])
     assert numpy.abs(out["esweeps"] - sw["esweeps"][:n]).max() <= 1e-8
     assert d.h2d_bytes > 0 and d.d2h_bytes > 0
+
+
+def test_sp_simpson_sweep_emulated(monkeypatch):
+    """Simpson's rule with 5 points (an inexact projector): the first sweep's dot energies
+    equal the reference's, quadrature error included."""
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    from qcmpodmrg_b200.spin import SPDMRG
+    sw = load("sweep_SPS_K4.npz")
+    ham = make_hamiltonian(int(sw["K"]), int(sw["N"]), int(sw["seed"]), None)
+    out = SPDMRG(ham, int(sw["npts"]), device="cpu", quad="Simpson").run(sw["init_mps"], int(sw["D"]), 1)
+    n = len(out["esweeps"])
+    assert numpy.abs(out["esweeps"] - sw["esweeps"][:n]).max() <= 1e-8
+    assert out["nmvp"][0] == sw["nmvp"][0]

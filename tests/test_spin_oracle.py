@@ -9,7 +9,11 @@ from oracle import spin as ospin
 from oracle.kernels import hdiag, RenormOracle
 from qcmpodmrg_b200.hamiltonian import make_hamiltonian
 
-TAGS = ["SP_K4", "SP_K5"]
+TAGS = ["SP_K4", "SP_K5", "SPS_K4"]
+
+
+def _quad(sw):
+    return str(sw["quad"]) if "quad" in sw else "GaussLegendre"
 
 
 def _ham(sw):
@@ -46,7 +50,7 @@ def test_quadrature_matches_reference(tag):
     sw = load("sweep_%s.npz" % tag)
     r = load("kernels_%s.npz" % tag)["records"][0]
     for fn in (ospin.s2quad, spin.s2quad):
-        pts, wts = fn(int(sw["npts"]))
+        pts, wts = fn(int(sw["npts"]), quad=_quad(sw))
         assert numpy.abs(pts - r["qpts"]).max() <= 1e-15
         assert numpy.abs(wts - r["qwts"]).max() <= 1e-15
     # Simpson and S > 0 agree between the two restatements
@@ -72,7 +76,7 @@ def test_sp_operators_match_reference(tag):
     sw = load("sweep_%s.npz" % tag)
     ham = _ham(sw)
     npts = int(sw["npts"])
-    qpts, _ = spin.s2quad(npts)
+    qpts, _ = spin.s2quad(npts, quad=_quad(sw))
     for r in load("kernels_%s.npz" % tag)["records"]:
         isite = int(r["key"][2])
         ops = ospin.sp_opers(ham.sbas, npts)
