@@ -15,7 +15,9 @@ Rewrites applied (syntax only, no algorithmic change):
   * ``d.keys()[0]`` -> ``list(d.keys())[0]``; ``dic.values()`` -> list;
   * integer ``/`` at the three places where Python 2 relied on it
     (mpo_dmrg_dotutil.py:278,286, mpo_dmrg_qphys.py:36);
-  * ``string.join`` in itools/molinfo.py.
+  * ``string.join`` in itools/molinfo.py;
+  * ``size > 0`` tests on possibly-empty MPO-bond slices (``None`` in Python 2 compares
+    below 0: mpo_dmrg_initQt.py:170,253, mpo_dmrg_kernelQt.py:694,762,1059,1148).
 
 The C library ``ctypes/qsym.c`` is compiled from where it lies with the
 reference's own install.sh command into ``baseline/_ref/qcmpodmrg/libs``.
@@ -141,6 +143,8 @@ def convert_file(path, siblings):
     src = src.replace("idlst = dic.values()", "idlst = list(dic.values())")
     src = src.replace("string.join(time.asctime().split(':'))", "' '.join(time.asctime().split(':'))")
     src = src.replace("string.join(dat.split(' ')[1:],'_')", "'_'.join(dat.split(' ')[1:])")
+    # Python 2 orders None below every number: an empty MPO-bond slice (size None) is skipped
+    src = src.replace("if qops.dic[jslc].size > 0:", "if (qops.dic[jslc].size or 0) > 0:")
     base = os.path.basename(path)
     if base == "mpo_dmrg_dotutil.py":
         src = src.replace("cdimc = cdim/dim", "cdimc = cdim//dim")

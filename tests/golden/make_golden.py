@@ -7,6 +7,7 @@ and /root/reference; run where the reference sources are present:
     python tests/golden/make_golden.py --config1  # K=12, N=12, D=100, 6 sweeps (~30 min CPU)
     python tests/golden/make_golden.py --spin     # spin-projected K=4 / K=5 runs (minutes)
     python tests/golden/make_golden.py --noise    # K=5 / K=6 runs with the pRDM noise term
+    python tests/golden/make_golden.py --sliced   # K=5 run with the MPO bond in 3 slices (maxslc=3)
 
 Outputs:
   qsym_cases.npz       symAllowed masks from the reference's own libqsym.so
@@ -51,13 +52,13 @@ def qsym_cases(seed=7):
 
 
 def run_case(tag, K, N, D, nsweeps, seed, decay, targets, record_envs=True, npts=None, noise=0.0,
-             quad="GaussLegendre"):
+             quad="GaussLegendre", maxslc=1):
     res, rec = rr.run_reference(K=K, N=N, D=D, nsweeps=nsweeps, seed=seed, decay=decay, targets=targets,
-                                record_envs=record_envs, npts=npts, noise=noise, quad=quad)
+                                record_envs=record_envs, npts=npts, noise=noise, quad=quad, maxslc=maxslc)
     sweep = {"K": K, "N": N, "D": D, "seed": seed, "decay": -1.0 if decay is None else float(decay),
              "nsweeps": nsweeps, "eav": res["eav"], "dwt": res["dwt"], "esweeps": res["esweeps"],
              "nmvp": res["nmvp"], "init_mps": {k: v for k, v in res["init_mps"].items() if k != "nsite"},
-             "npts": 0 if npts is None else int(npts), "noise": float(noise), "quad": quad}
+             "npts": 0 if npts is None else int(npts), "noise": float(noise), "quad": quad, "maxslc": maxslc}
     fixtures.save(os.path.join(HERE, "sweep_%s.npz" % tag), sweep)
     if targets:
         recs = []
@@ -78,7 +79,11 @@ if __name__ == "__main__":
     ap.add_argument("--config1", action="store_true")
     ap.add_argument("--spin", action="store_true", help="only the spin-projected (SP-MPS) fixtures")
     ap.add_argument("--noise", action="store_true", help="only the fixtures with the pRDM noise term")
+    ap.add_argument("--sliced", action="store_true", help="only the run with the MPO bond cut into slices")
     a = ap.parse_args()
+    if a.sliced:
+        run_case("SL_K5", 5, 4, 12, 3, 2, 2.0, [], record_envs=False, maxslc=3)
+        sys.exit(0)
     if a.noise:
         run_case("NZ_K5", 5, 4, 12, 3, 2, 2.0, [(0, "R", 2), (0, "L", 1), (1, "L", 2)], noise=1e-4)
         run_case("NZ_K6", 6, 6, 14, 3, 3, None, [(0, "R", 3), (1, "L", 2)], noise=1e-3)
