@@ -45,7 +45,8 @@ def test_sweeps_match_reference(tag, cuda):
     assert abs(out["dwt"][n - 1] - fx["dwt"][n - 1]) <= 1e-10
     assert numpy.abs(out["eav"][:n] - fx["eav"][:n]).max() <= 1e-5
     if tag == "K5" and n >= 3 and os.path.exists(os.path.join(GOLDEN, "sweep_SL_K5.npz")):
-        assert abs(out["eav"][2] - load("sweep_SL_K5.npz")["eav"][2]) <= 1e-8     # the maxslc=3 reference run
+        # the maxslc=3 reference run, held like the other sweeps before the last
+        assert abs(out["eav"][2] - load("sweep_SL_K5.npz")["eav"][2]) <= 1e-5
 
 
 def test_sweeps_config1_partial(cuda):
