@@ -8,6 +8,7 @@ and /root/reference; run where the reference sources are present:
     python tests/golden/make_golden.py --spin     # spin-projected K=4 / K=5 runs (minutes)
     python tests/golden/make_golden.py --noise    # K=5 / K=6 runs with the pRDM noise term
     python tests/golden/make_golden.py --sliced   # K=5 run with the MPO bond in 3 slices (maxslc=3)
+    python tests/golden/make_golden.py --filling  # K=5 runs with N=2 and N=8 electrons
 
 Outputs:
   qsym_cases.npz       symAllowed masks from the reference's own libqsym.so
@@ -80,7 +81,12 @@ if __name__ == "__main__":
     ap.add_argument("--spin", action="store_true", help="only the spin-projected (SP-MPS) fixtures")
     ap.add_argument("--noise", action="store_true", help="only the fixtures with the pRDM noise term")
     ap.add_argument("--sliced", action="store_true", help="only the run with the MPO bond cut into slices")
+    ap.add_argument("--filling", action="store_true", help="only the runs away from half filling")
     a = ap.parse_args()
+    if a.filling:
+        run_case("K5N2", 5, 2, 16, 2, 4, None, [(0, "L", 2)])
+        run_case("K5N8", 5, 8, 16, 2, 5, 2.0, [(0, "R", 1)])
+        sys.exit(0)
     if a.sliced:
         run_case("SL_K5", 5, 4, 12, 3, 2, 2.0, [], record_envs=False, maxslc=3)
         sys.exit(0)

@@ -15,7 +15,7 @@ TOL_F64 = 1e-12
 TOL_F32 = 2e-5
 
 
-@pytest.mark.parametrize("tag", ["K4", "K5", "K6"])
+@pytest.mark.parametrize("tag", ["K4", "K5", "K6", "K5N2", "K5N8"])
 def test_sigma_diag_renorm_f64(tag, cuda):
     for r in load("kernels_%s.npz" % tag)["records"]:
         sig, dg, ws = record_operators(r, cuda)

@@ -31,7 +31,7 @@ C1_TOL_FINAL = 5e-4   # last of the six sweeps (observed 1e-4 .. 3e-4 across sum
 C1_EXACT_DOTS = 7     # dots of the first sweep before the first truncating decimation
 
 
-@pytest.mark.parametrize("tag", ["K4", "K5", "K6"])
+@pytest.mark.parametrize("tag", ["K4", "K5", "K6", "K5N2", "K5N8"])
 def test_sweeps_match_reference(tag, cuda):
     if not os.path.exists(os.path.join(GOLDEN, "sweep_%s.npz" % tag)):
         pytest.skip("fixture not generated")

@@ -16,10 +16,10 @@ def test_oracle_symallowed_matches_reference_libqsym():
         assert numpy.array_equal(got, c["allowed"])
 
 
-@pytest.mark.parametrize("tag", ["K4", "K5", "K6"])
+@pytest.mark.parametrize("tag", ["K4", "K5", "K6", "K5N2", "K5N8"])
 def test_oracle_kernels_match_reference(tag):
     fx = load("kernels_%s.npz" % tag)
-    assert len(fx["records"]) >= 2
+    assert len(fx["records"]) >= 1
     for r in fx["records"]:
         qtmp = from_dict(r["qtmp"])
         L = [from_dict(d) for d in r["envL"]]

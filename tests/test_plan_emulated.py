@@ -9,7 +9,7 @@ from emulate import patch_stage_run
 from qcmpodmrg_b200.engine import CompositeStage, Stage
 
 
-@pytest.mark.parametrize("tag", ["K4", "K5", "K6"])
+@pytest.mark.parametrize("tag", ["K4", "K5", "K6", "K5N2", "K5N8"])
 def test_sigma_diag_renorm_emulated(tag, monkeypatch):
     patch_stage_run(monkeypatch)
     for r in load("kernels_%s.npz" % tag)["records"]:

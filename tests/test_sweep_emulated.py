@@ -9,7 +9,7 @@ from emulate import patch_stage_run
 from qcmpodmrg_b200.hamiltonian import make_hamiltonian
 
 
-@pytest.mark.parametrize("tag", ["K4"])
+@pytest.mark.parametrize("tag", ["K4", "K5N2", "K5N8"])
 def test_sweeps_emulated(tag, monkeypatch):
     patch_stage_run(monkeypatch)
     monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
