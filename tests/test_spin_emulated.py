@@ -145,16 +145,18 @@ def _dropin_vs_oracle(device):
 
 
 def test_sp_mixed_sweep_emulated(monkeypatch):
-    """FP32 H and S products with the FP64 check: the K=4 spin-projected run reaches the
-    reference's energies within 1e-6 Eh (intermediates rounded to FP32 by the interpreter)."""
+    """FP32 H and S products with the FP64 check: the K=4 spin-projected first half sweep
+    reaches the reference's energies within 1e-6 Eh (intermediates rounded to FP32 by the
+    interpreter)."""
     patch_stage_run(monkeypatch)
     monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
     from qcmpodmrg_b200.spin import SPDMRG
     sw = load("sweep_SP_K4.npz")
     ham = make_hamiltonian(int(sw["K"]), int(sw["N"]), int(sw["seed"]), None)
     d = SPDMRG(ham, int(sw["npts"]), device="cpu", precision="f32")
-    out = d.run(sw["init_mps"], int(sw["D"]), 1)
-    assert abs(out["eav"][0] - sw["eav"][0]) <= 1e-6
+    d.load_mps(sw["init_mps"])
+    n, e, dw, el, dl = d.sweep("R", int(sw["D"]), 1e-7)       # the first half sweep
+    assert numpy.abs(numpy.array(el) - sw["esweeps"][:len(el)]).max() <= 1e-6
     assert d.stats.get("nmvp_low", 0) > 0 and d.stats.get("nmvp_f64", 0) > 0
 
 
@@ -176,7 +178,7 @@ def test_sp_triplet_reaches_fci_triplet(monkeypatch):
 
 def test_sp_host_api_sweep_emulated(monkeypatch):
     """The spin-projected dot driven through mpo_dmrg_kernel.HVec/SVec/HDiag with host vectors
-    (the reference's calling convention) gives the same first sweep as the device driver."""
+    (the reference's calling convention) gives the reference's first half sweep."""
     patch_stage_run(monkeypatch)
     monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
     from qcmpodmrg_b200.spin import SPDMRG
@@ -184,21 +186,21 @@ def test_sp_host_api_sweep_emulated(monkeypatch):
     ham = make_hamiltonian(int(sw["K"]), int(sw["N"]), int(sw["seed"]), None)
     d = SPDMRG(ham, int(sw["npts"]), device="cpu")
     d.host_api = True
-    out = d.run(sw["init_mps"], int(sw["D"]), 1)
-    n = len(out["esweeps"])
-    assert numpy.abs(out["esweeps"] - sw["esweeps"][:n]).max() <= 1e-8
+    d.load_mps(sw["init_mps"])
+    n, e, dw, el, dl = d.sweep("R", int(sw["D"]), 1e-7)       # the first half sweep
+    assert numpy.abs(numpy.array(el) - sw["esweeps"][:len(el)]).max() <= 1e-8
     assert d.h2d_bytes > 0 and d.d2h_bytes > 0
 
 
 def test_sp_simpson_sweep_emulated(monkeypatch):
-    """Simpson's rule with 5 points (an inexact projector): the first sweep's dot energies
-    equal the reference's, quadrature error included."""
+    """Simpson's rule with 5 points (an inexact projector): the first half sweep's dot
+    energies equal the reference's, quadrature error included."""
     patch_stage_run(monkeypatch)
     monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
     from qcmpodmrg_b200.spin import SPDMRG
     sw = load("sweep_SPS_K4.npz")
     ham = make_hamiltonian(int(sw["K"]), int(sw["N"]), int(sw["seed"]), None)
-    out = SPDMRG(ham, int(sw["npts"]), device="cpu", quad="Simpson").run(sw["init_mps"], int(sw["D"]), 1)
-    n = len(out["esweeps"])
-    assert numpy.abs(out["esweeps"] - sw["esweeps"][:n]).max() <= 1e-8
-    assert out["nmvp"][0] == sw["nmvp"][0]
+    d = SPDMRG(ham, int(sw["npts"]), device="cpu", quad="Simpson")
+    d.load_mps(sw["init_mps"])
+    n, e, dw, el, dl = d.sweep("R", int(sw["D"]), 1e-7)       # the first half sweep
+    assert numpy.abs(numpy.array(el) - sw["esweeps"][:len(el)]).max() <= 1e-8
