@@ -169,3 +169,24 @@ def test_sp_oracle_sweep_matches_reference():
     assert numpy.abs(out["esweeps"] - sw["esweeps"][:n]).max() <= 1e-8
     assert abs(out["eav"][0] - sw["eav"][0]) <= 1e-8 and abs(out["dwt"][0] - sw["dwt"][0]) <= 1e-10
     assert out["nmvp"][0] == sw["nmvp"][0]
+
+
+@pytest.mark.parametrize("sval,npts", [(0.0, 3), (1.0, 4), (2.0, 6), (0.5, 4), (1.5, 5)])
+def test_quadrature_projects_onto_total_spin(sval, npts):
+    """sum_g w_g d^S'_{MM}(theta_g) = delta(S, S') for every S' the Gauss-Legendre rule
+    integrates exactly (the projector's defining property, mpo_dmrg_util.py:35-89)."""
+    from qcmpodmrg_b200.spin import s2quad, smalld
+    m = sval - int(sval)                       # Sz = 0 or 1/2
+    pts, wts = s2quad(npts, sval, m)
+    for sp in numpy.arange(m, npts - 0.5, 1.0):
+        got = sum(w * smalld(sp, m, m, t) for t, w in zip(pts, wts))
+        assert abs(got - (1.0 if abs(sp - sval) < 1e-9 else 0.0)) <= 1e-12
+
+
+def test_smalld_is_orthogonal():
+    """d^j(beta) is a real orthogonal matrix in (m', m) for integer and half-integer j."""
+    from qcmpodmrg_b200.spin import smalld
+    for j in (0.5, 1.0, 1.5, 2.0, 3.0):
+        ms = numpy.arange(-j, j + 0.5, 1.0)
+        d = numpy.array([[smalld(j, a, b, 0.83) for b in ms] for a in ms])
+        assert numpy.abs(d @ d.T - numpy.identity(len(ms))).max() <= 1e-13
