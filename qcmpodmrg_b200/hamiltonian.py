@@ -74,8 +74,11 @@ def to_spin_orbital(h, eri):
 
 
 def make_hamiltonian(K, N, seed, decay=None):
-    """Build the synthetic Hamiltonian of K spatial orbitals and N electrons (Sz=0)."""
-    assert N % 2 == 0 and N <= 2 * K
+    """Build the synthetic Hamiltonian of K spatial orbitals and N electrons; the start
+    occupation fills spin orbitals 0..N-1 (alpha, beta alternating: Sz = 0 for even N,
+    +1/2 for odd N)."""
+    if not 0 <= N <= 2 * K:
+        raise ValueError("need 0 <= N <= 2K")
     h, eri = spatial_integrals(K, seed, decay)
     int1e, int2e = to_spin_orbital(h, eri)
     occun = numpy.zeros(2 * K)
@@ -84,7 +87,8 @@ def make_hamiltonian(K, N, seed, decay=None):
 
 
 def fci_energy(ham):
-    """Exact ground energy in the (N, Sz=0) determinant space (small K only).
+    """Exact ground energy in the determinant space of N electrons with N//2 alpha ones
+    (Sz = 0, or -1/2 for odd N; small K only).
 
     Independent check used by the tests: DMRG with an unrestricted bond
     dimension must reproduce it.
@@ -94,8 +98,9 @@ def fci_energy(ham):
 
 
 def fci_hamiltonian(ham):
-    """H in the (N, Sz=0) determinant basis (sorted spin-orbital tuples; 2i = alpha,
-    2i+1 = beta), symmetrised, and the determinants."""
+    """H in the basis of determinants with N//2 alpha electrons (Sz = 0, or -1/2 for odd
+    N; sorted spin-orbital tuples, 2i = alpha, 2i+1 = beta), symmetrised, and the
+    determinants."""
     from itertools import combinations
     n = ham.sbas
     N = ham.nelec

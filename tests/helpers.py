@@ -159,9 +159,9 @@ def record_noise(r, device):
 
 
 def fci_spin_states(ham, nstates=8):
-    """Lowest eigenvalues of H in the (N, Sz=0) determinant space with their <S^2>
-    (S^2 = S+^T S+ there), by exact diagonalisation (small K only): an independent check
-    of spin-projected results."""
+    """Lowest eigenvalues of H among determinants with N//2 alpha electrons (Sz = 0, or
+    -1/2 for odd N) with <S- S+> (= S(S+1) - Sz^2 - Sz), by exact diagonalisation (small
+    K only): an independent check of spin-projected results."""
     from itertools import combinations
     from qcmpodmrg_b200.hamiltonian import fci_hamiltonian
     n, N = ham.sbas, ham.nelec

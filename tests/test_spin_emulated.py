@@ -204,3 +204,18 @@ def test_sp_simpson_sweep_emulated(monkeypatch):
     d.load_mps(sw["init_mps"])
     n, e, dw, el, dl = d.sweep("R", int(sw["D"]), 1e-7)       # the first half sweep
     assert numpy.abs(numpy.array(el) - sw["esweeps"][:len(el)]).max() <= 1e-8
+
+
+def test_sp_half_integer_spin_reaches_fci_doublet(monkeypatch):
+    """Odd electron number (K=4, N=3) projected onto S=1/2, Sz=1/2 from the occupation-number
+    start: one sweep lands on the lowest doublet of exact diagonalisation."""
+    from helpers import fci_spin_states
+    from qcmpodmrg_b200.synthetic import product_mps
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    from qcmpodmrg_b200.spin import SPDMRG
+    ham = make_hamiltonian(4, 3, 1, None)
+    w, s2 = fci_spin_states(ham)                 # Sz = -1/2 determinants: S(S+1) = s2 - 1/4
+    e_d = w[numpy.flatnonzero(numpy.abs(s2 - 0.25 - 0.75) < 1e-6)[0]]
+    out = SPDMRG(ham, 4, sval=0.5, sz=0.5, device="cpu").run(product_mps(ham), 16, 1)
+    assert abs(out["eav"][0] - e_d) <= 1e-8
