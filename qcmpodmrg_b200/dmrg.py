@@ -80,8 +80,11 @@ class DMRG(object):
 
     ifs2proj = False          # spin projection: qcmpodmrg_b200.spin.SPDMRG
 
-    def __init__(self, ham, device="cuda", precision="f64", preconditioner=None, w_path="fiber", plan_cache=False):
+    def __init__(self, ham, device="cuda", precision="f64", preconditioner=None, w_path="fiber", plan_cache=False,
+                 sz=0.0):
+        """sz: the target Sz of the (N, Sz) sector (the reference's qsectors key [N, Sz])."""
         self.ham = ham
+        self.sz = float(sz)
         self.device = torch.device(device)
         self.nsite = ham.nsite
         self.precision = precision
@@ -120,7 +123,7 @@ class DMRG(object):
         self.nops = ham.sbas
         self.opers = list(range(ham.sbas))
         self.hpwts = numpy.ones(self.nops)
-        self.qkey = numpy.array([float(ham.nelec), 0.0])
+        self.qkey = numpy.array([float(ham.nelec), self.sz])
         mpo = build_mpo(ham)
         self.mpo = {i: TensorSet(l, v, device=self.device) for i, (l, v) in mpo.items()}
 

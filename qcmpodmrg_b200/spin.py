@@ -224,9 +224,9 @@ class SPDMRG(DMRG):
         followed by an FP64 check of the solution (FP64 iterations when it fails)."""
         if precision not in ("f64", "f32"):
             raise ValueError("spin projection runs in f64 or f32 (mixed)")
-        self.npts, self.sval, self.sz, self.quad = int(npts), float(sval), float(sz), quad
+        self.npts, self.sval, self.quad = int(npts), float(sval), quad
         self.prune_zero_blocks = prune_zero_blocks
-        super(SPDMRG, self).__init__(ham, device=device, precision=precision, w_path=w_path)
+        super(SPDMRG, self).__init__(ham, device=device, precision=precision, w_path=w_path, sz=sz)
 
     def _setup_operators(self, ham):
         self.qpts, self.qwts = s2quad(self.npts, self.sval, self.sz, self.quad)

@@ -47,3 +47,16 @@ def test_plan_cache_requires_identical_layouts(monkeypatch):
     assert sig2 is not sig and d.stats["plan_misses"] == misses + 1
     lay3, idl3, sig3, dg3 = d.dot_operators(1)           # the rebuilt entry is reused
     assert sig3 is sig2
+
+
+def test_odd_electron_number_sector(monkeypatch):
+    """N=3 in K=4 orbitals, sector Sz=1/2, from the occupation-number start: the sweeps reach
+    exact diagonalisation's ground energy (the Sz=+1/2 and -1/2 spectra coincide)."""
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    from qcmpodmrg_b200.dmrg import DMRG
+    from qcmpodmrg_b200.hamiltonian import fci_energy
+    from qcmpodmrg_b200.synthetic import product_mps
+    ham = make_hamiltonian(4, 3, 1, None)
+    out = DMRG(ham, device="cpu", sz=0.5).run(product_mps(ham), 16, 2)
+    assert abs(out["eav"][-1] - fci_energy(ham)) <= 1e-8
