@@ -90,3 +90,15 @@ def test_gpu_sp_triplet_reaches_fci_triplet(cuda):
     e_t = w[numpy.flatnonzero(numpy.abs(s2 - 2.0) < 1e-6)[0]]
     out = SPDMRG(ham, 3, sval=1.0, sz=0.0, device=cuda).run(sw["init_mps"], 16, 2)
     assert abs(out["eav"][-1] - e_t) <= 1e-8
+
+
+def test_gpu_sp_half_integer_spin(cuda):
+    """K=4, N=3 projected onto S=1/2, Sz=1/2: the lowest doublet of exact diagonalisation."""
+    from helpers import fci_spin_states
+    from qcmpodmrg_b200.spin import SPDMRG
+    from qcmpodmrg_b200.synthetic import product_mps
+    ham = make_hamiltonian(4, 3, 1, None)
+    w, s2 = fci_spin_states(ham)
+    e_d = w[numpy.flatnonzero(numpy.abs(s2 - 1.0) < 1e-6)[0]]
+    out = SPDMRG(ham, 4, sval=0.5, sz=0.5, device=cuda).run(product_mps(ham), 16, 2)
+    assert abs(out["eav"][-1] - e_d) <= 1e-8
