@@ -63,11 +63,3 @@ def test_sweeps_config1_partial(cuda):
     assert numpy.abs(out["eav"] - fx["eav"]).max() <= C1_TOL_E
     assert abs(out["eav"][-1] - fx["eav"][-1]) <= C1_TOL_FINAL
 
-
-def test_odd_electron_number_sector(cuda):
-    from qcmpodmrg_b200.dmrg import DMRG
-    from qcmpodmrg_b200.hamiltonian import fci_energy
-    from qcmpodmrg_b200.synthetic import product_mps
-    ham = make_hamiltonian(4, 3, 1, None)
-    out = DMRG(ham, device=cuda, sz=0.5).run(product_mps(ham), 16, 2)
-    assert abs(out["eav"][-1] - fci_energy(ham)) <= 1e-8

@@ -102,3 +102,13 @@ def test_gpu_sp_half_integer_spin(cuda):
     e_d = w[numpy.flatnonzero(numpy.abs(s2 - 1.0) < 1e-6)[0]]
     out = SPDMRG(ham, 4, sval=0.5, sz=0.5, device=cuda).run(product_mps(ham), 16, 2)
     assert abs(out["eav"][-1] - e_d) <= 1e-8
+
+
+def test_gpu_odd_electron_number_sector(cuda):
+    """Plain (unprojected) sweeps in the N=3, Sz=1/2 sector reach the exact ground energy."""
+    from qcmpodmrg_b200.dmrg import DMRG
+    from qcmpodmrg_b200.hamiltonian import fci_energy
+    from qcmpodmrg_b200.synthetic import product_mps
+    ham = make_hamiltonian(4, 3, 1, None)
+    out = DMRG(ham, device=cuda, sz=0.5).run(product_mps(ham), 16, 2)
+    assert abs(out["eav"][-1] - fci_energy(ham)) <= 1e-8
