@@ -1,6 +1,7 @@
 """GPU parity of spin projection (SP-MPS): the projected H and S operators, their
 diagonals, both renormalisations, the drop-in functions and whole sweeps against
-the reference's outputs (tests/golden/*SP_K*.npz) and the oracle.
+the reference's outputs (tests/golden/*SP_K*.npz), the oracle and exact
+diagonalisation (S=1, S=1/2); also the plain sweep in an odd-N sector.
 
 Tolerances: operators 1e-12 relative (FP64, summation order differs from NumPy);
 the K=4 run keeps every state (D=16), so its energies are held to 1e-8 and its
