@@ -2,8 +2,10 @@
 
 A CPU (NumPy/SciPy, FP64) restatement of the reference's two-site Qt DMRG hot
 path: block layout and pair lists (blocks.py), the H_p site operators (mpo.py),
-sigma/diagonal/renormalisation (kernels.py), Davidson and RDM decimation
-(solver.py) and the sweep driver (dmrg.py).  Each function cites the reference
+sigma/diagonal/renormalisation and the pRDM noise term (kernels.py), Davidson
+and RDM decimation (solver.py), the sweep driver (dmrg.py) and spin projection
+(spin.py: quadrature, H_p R(theta) operators, SVecQt/SDiagQt/renormQt_S00, the
+generalised Davidson and the projected sweep).  Each function cites the reference
 file:line it follows.  It is pinned against outputs of the reference itself,
 run here through tests/golden/convert_reference.py, stored as fixtures under
 tests/golden/.
