@@ -131,63 +131,83 @@ def max_over_ranks(dist, value, device="cuda"):
     return float(t.item())
 
 
-def run_ours(args):
-    import torch
+def _make_dmrg(args, prec, dev, seed_rank=0):
     from qcmpodmrg_b200.hamiltonian import make_hamiltonian
     from qcmpodmrg_b200.synthetic import product_mps
     from qcmpodmrg_b200.dmrg import DMRG
-    from qcmpodmrg_b200.engine import LOG
-
-    dist, rank, world, local = dist_init()
-    dev = torch.device("cuda:%d" % local)
-    torch.cuda.set_device(dev)
-    prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32", "mixed-tc": "tf32x3"}[args.precision]
-    ham = make_hamiltonian(args.sites, args.sites, SEED + rank * 0, DECAY)
-    sp = args.workload == "sp"
-    if sp:
+    ham = make_hamiltonian(args.sites, args.sites, SEED + seed_rank * 0, DECAY)
+    if args.workload == "sp":
         from qcmpodmrg_b200.spin import SPDMRG
         if prec not in ("f64", "f32"):
             raise SystemExit("--workload sp runs with --precision f64 or mixed")
         d = SPDMRG(ham, args.npts, 0.0, 0.0, device=dev, w_path=args.w_path, precision=prec)
     else:
         d = DMRG(ham, device=dev, precision=prec, w_path=args.w_path, plan_cache=args.plan_cache)
+    if args.precond == "learned" and prec != "f64":
+        from qcmpodmrg_b200.precond import LearnedPreconditioner
+        d.preconditioner = LearnedPreconditioner(dev, train_sweeps=args.precond_train)
     d.load_mps(product_mps(ham))
     for D in RAMP:
         if D < args.dmax:
             d.sweep("R", D, 1e-7)
             d.sweep("L", D, 1e-7)
+    return d
 
-    def step():
-        f0 = d.stats["sigma_flops"]
-        d.sweep("R", args.dmax, 1e-7)
-        n, e, dw, el, dl = d.sweep("L", args.dmax, 1e-7)
-        d.sweep_sigma_flops = d.stats["sigma_flops"] - f0
-        return e, dw
 
-    for _ in range(args.warmup):
-        step()
+def _step(d, args):
+    """One sweep (R then L) at D = dmax; returns (energy, discarded weight, matvecs)."""
+    f0, n0 = d.stats["sigma_flops"], d.stats["nmvp"]
+    d.sweep("R", args.dmax, 1e-7)
+    n, e, dw, el, dl = d.sweep("L", args.dmax, 1e-7)
+    d.sweep_sigma_flops = d.stats["sigma_flops"] - f0
+    if hasattr(d.preconditioner, "end_sweep"):
+        d.preconditioner.end_sweep()
+    return e, dw, d.stats["nmvp"] - n0
+
+
+def _timed_sweeps(d, args, nsteps, dist):
+    """nsteps sweeps bracketed by barrier + synchronize, CUDA events on the launching
+    stream before every sweep and after the last; returns (total ms, per-sweep ms, results)."""
+    import torch
+    barrier(dist)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(nsteps + 1)]
+    res = []
+    evs[0].record()
+    for k in range(nsteps):
+        res.append(_step(d, args))
+        evs[k + 1].record()
+    barrier(dist)
+    per = [evs[k].elapsed_time(evs[k + 1]) for k in range(nsteps)]
+    return evs[0].elapsed_time(evs[-1]), per, res
+
+
+def run_ours(args):
+    import gc
+    import torch
+    from qcmpodmrg_b200.engine import LOG
+
+    dist, rank, world, local = dist_init()
+    dev = torch.device("cuda:%d" % local)
+    torch.cuda.set_device(dev)
+    prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32", "mixed-tc": "tf32x3"}[args.precision]
+    sp = args.workload == "sp"
+    d = _make_dmrg(args, prec, dev, rank)
+    warm = [_step(d, args) for _ in range(args.warmup)]
+    snap = d.snapshot() if args.e2e else None
     # ---- timed region (device events on the launching stream, barrier + sync both sides)
-    s0 = dict(d.stats)
+    s0 = {k: v for k, v in d.stats.items() if not isinstance(v, dict)}
     LOG.reset()
     LOG.enabled = True
     clocks = ClockSampler(local)
     clocks.start()
-    barrier(dist)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("timed")
-    ev0.record()
-    energies = []
-    for _ in range(args.steps):
-        energies.append(step())
-    ev1.record()
+    ms_local, per_sweep, energies = _timed_sweeps(d, args, args.steps, dist)
     torch.cuda.nvtx.range_pop()
-    barrier(dist)
     ck = clocks.stop()
     LOG.enabled = False
-    ms = max_over_ranks(dist, ev0.elapsed_time(ev1), dev)
+    ms = max_over_ranks(dist, ms_local, dev)
     ms_per_step = ms / args.steps
-    stats = {k: d.stats[k] - s0[k] for k in d.stats if not isinstance(d.stats[k], dict)}
+    stats = {k: d.stats[k] - s0[k] for k in s0}
     # per-stage device time from the launch log
     per = {}
     for (name, e0, e1, fl, by) in LOG.records:
@@ -203,13 +223,10 @@ def run_ours(args):
     pk, src = peaks()
     n_l, t_l, f_l, b_l = top[1]
     gbs = b_l / (t_l / 1e3) / 1e9
-    panel = args.w_path in ("fiber", "fused")
-    kname = {"sigma1": "k_pgemm", "sigma2": "k_fiber" if panel else "k_bgemm",
-             "sigma3": "k_fiber" if panel else "k_bgemm", "sigma23": "k_fiber",
-             "sigma4": "k_pgemm" if panel else "k_bgemm"}.get(top[0], "k_bgemm")
+    kname = stage_kernel(top[0], args.w_path, prec)
     roof = {"kernel": "%s (%s)" % (kname, top[0]), "bound": "hbm", "achieved": round(gbs, 1),
             "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(gbs / pk["hbm_gbs"], 4),
-            "peak_source": src, "traffic": None, "launches": n_l,
+            "peak_source": src, "traffic": traffic_per_launch(top[0], b_l / max(n_l, 1)), "launches": n_l,
             "achieved_tflops": round(f_l / (t_l / 1e3) / 1e12, 3)}
     # whole job: world replicas each did args.steps sweeps in ms (slowest rank)
     line = {
@@ -229,13 +246,14 @@ def run_ours(args):
                                "two-site Qt DMRG sweep, K=%d N=%d Sz=0 D=%d, %d operators H_p"
                                % (args.sites, args.sites, args.dmax, 2 * args.sites), "K": args.sites,
                    "N": args.sites, "D": args.dmax, "precision": args.precision,
-                   "w_path": args.w_path,
+                   "w_path": args.w_path, "precond": args.precond,
                    "l2": "inputs larger than L2: environments and sigma scratch are tens of GB per sweep",
                    "parallelism": "replicas" if world > 1 else "1 GPU",
                    "value_definition": "slowest rank's seconds for its sweeps / sweeps done by all ranks"},
         "energy": energies[-1][0], "dwt": energies[-1][1],
+        "sweep_ms": [round(x, 1) for x in per_sweep],
         "sigma_tflops": round(sig_fl / (sig_ms / 1e3) / 1e12, 3) if sig_ms else None,
-        "sigma_share": round(sig_ms / ms, 3) if ms else None,
+        "sigma_share": round(sig_ms / ms_local, 3) if ms_local else None,
         "matvecs_per_step": stats["nmvp"] / args.steps,
         "matvecs_f64_low_per_step": [stats.get("nmvp_f64", stats["nmvp"] if prec == "f64" else 0) / args.steps,
                                      stats.get("nmvp_low", 0) / args.steps],
@@ -247,24 +265,60 @@ def run_ours(args):
         "phase_s_per_step": {k: round(stats[k] / args.steps, 2) for k in ("plan_s", "hvec_s", "hdiag_s", "renorm_s",
                                                                          "decim_s") if k in stats},
     }
+    if "plan_hits" in d.stats or "plan_misses" in d.stats:
+        line["plan_cache"] = {"hits": stats.get("plan_hits", 0), "misses": stats.get("plan_misses", 0)}
     if args.e2e:
-        e2e = e2e_leg(d, args)
+        e2e = e2e_leg(d, args, snap, per_sweep[0], energies[0][2])
         e2e["value"] = round(max_over_ranks(dist, e2e["value"], dev) / world, 3)
         line["e2e"] = e2e
-    if rank == 0 and args.cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(d, ms_per_step / 1e3, sp=sp)
+    del snap
+    if rank == 0:
+        acc = accuracy_leg(d, prec, args.cpu_baseline, sp)
+        if args.cpu_baseline:
+            line["cpu_baseline"] = acc.pop("cpu_baseline")
+        line["accuracy"] = acc
+    if hasattr(d.preconditioner, "summary"):
+        line["precond_stats"] = d.preconditioner.summary()
+    if args.f64_steps > 0 and prec != "f64" and not sp:
+        # the FP64 GPU arm: same workload, same schedule, same sweeps timed
+        del d
+        gc.collect()
+        torch.cuda.empty_cache()
+        line["f64_arm"] = f64_arm(args, dev, dist, rank, [w[0] for w in warm] + [e[0] for e in energies],
+                                  per_sweep)
     if dist is not None:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def e2e_leg(d, args):
-    """One sweep through the reference-facing API (mpo_dmrg_kernel.HVec/HDiag with host NumPy
-    vectors, Davidson on the host as in the reference's pdvdson); copies are in the timed region."""
+def stage_kernel(stage, w_path, prec):
+    panel = w_path in ("fiber", "fused")
+    return {"sigma1": "k_pgemm" if panel else "k_bgemm", "sigma2": "k_fiber" if panel else "k_bgemm",
+            "sigma3": "k_fiber" if panel else "k_bgemm", "sigma23": "k_fiber",
+            "sigma4": "k_pgemm" if panel else "k_bgemm"}.get(stage, "k_bgemm")
+
+
+# DRAM bytes per launch measured by ncu for a stage's kernel, scaled to the launch's
+# algorithmic bytes (profiles/ holds the captures); None where no capture exists
+TRAFFIC_RATIO = {}
+
+
+def traffic_per_launch(stage, algo_bytes):
+    r = TRAFFIC_RATIO.get(stage)
+    return None if r is None else round(r * algo_bytes)
+
+
+def e2e_leg(d, args, snap, device_ms_first, matvecs_first):
+    """The first timed sweep again, from the same state (restored from the snapshot taken
+    before the timed region), through the reference-facing API: mpo_dmrg_kernel.HVec/HDiag
+    with host NumPy vectors and the Davidson on the host, as the reference's pdvdson calls
+    them; host<->device copies are inside the timed region."""
     import torch
+    d.restore(snap)
     d.host_api = True
     d.h2d_bytes = d.d2h_bytes = 0
+    n0 = d.stats["nmvp"]
     torch.cuda.synchronize()
     t0 = time.time()
     d.sweep("R", args.dmax, 1e-7)
@@ -273,26 +327,67 @@ def e2e_leg(d, args):
     dt = time.time() - t0
     d.host_api = False
     return {"value": round(dt, 3), "unit": "s/sweep", "h2d_bytes_per_step": int(d.h2d_bytes),
-            "d2h_bytes_per_step": int(d.d2h_bytes),
-            "path": "qcmpodmrg_b200.mpo_dmrg_kernel.HVec/HDiag%s with host buffers, host Davidson"
-                    % ("/SVec" if getattr(d, "ifs2proj", False) else "")}
+            "d2h_bytes_per_step": int(d.d2h_bytes), "matvecs": int(d.stats["nmvp"] - n0),
+            "same_sweep_device_s": round(device_ms_first / 1e3, 3), "same_sweep_device_matvecs": int(matvecs_first),
+            "path": "qcmpodmrg_b200.mpo_dmrg_kernel.HVec/HDiag%s with host buffers, host Davidson; the first "
+                    "timed sweep re-run from the same state" % ("/SVec" if getattr(d, "ifs2proj", False) else "")}
 
 
-def cpu_baseline_sample(d, gpu_sweep_s, sp=False):
-    """The oracle (NumPy restatement of the reference's HVecQt; with spin projection its
-    H and S products) timed on this host's cores on one matvec at the mid-chain dot of the
-    same state; scaled to a sweep by algorithmic sigma FLOPs (the same count the GPU reports)."""
-    from oracle.bench_cpu import oracle_dot, oracle_sp_dot
+def accuracy_leg(d, prec, with_oracle, sp):
+    """Sigma at the mid-chain dot of the final state, on a seeded vector: the FP64 GPU path
+    and the timed precision against the oracle (the NumPy restatement of HVecQt, timed on
+    this host's cores, which also gives cpu_baseline)."""
+    import torch
     isite = d.nsite // 2
-    ora, x, flops_dot = (oracle_sp_dot if sp else oracle_dot)(d, isite)
-    t0 = time.time()
-    ora(x)
-    t = time.time() - t0
-    rate = flops_dot / t
-    est = d.sweep_sigma_flops / rate
-    return {"value": round(est, 1), "unit": "s/sweep", "cores": os.cpu_count(),
-            "kind": "port", "sample": "one oracle sigma matvec at the mid-chain dot (%.1f s, %.2f GFLOP/s), "
-                                      "scaled to the sweep's sigma FLOPs" % (t, rate / 1e9)}
+    lay, idl, s, dg = d.dot_operators(isite)
+    out = {"dot": isite, "ndim0": int(s.ndim0)}
+    x = numpy.random.default_rng(0).standard_normal(s.ndim0)
+    xd = torch.from_numpy(x).to(d.device)
+    y64 = s(xd, precision="f64").cpu().numpy()
+    ylo = s(xd).cpu().numpy() if prec != "f64" else y64
+    if with_oracle:
+        from oracle.bench_cpu import oracle_dot, oracle_sp_dot
+        ora, xo, flops_dot = (oracle_sp_dot if sp else oracle_dot)(d, isite)
+        t0 = time.time()
+        yo = ora(x)
+        t = time.time() - t0
+        if sp:
+            yo = yo[0]
+        nrm = numpy.linalg.norm(yo)
+        out["sigma_relerr_vs_oracle"] = {"f64": float(numpy.linalg.norm(y64 - yo) / nrm),
+                                         prec: float(numpy.linalg.norm(ylo - yo) / nrm)}
+        rate = flops_dot / t
+        out["cpu_baseline"] = {"value": round(d.sweep_sigma_flops / rate, 1), "unit": "s/sweep",
+                               "cores": os.cpu_count(), "kind": "port",
+                               "sample": "one oracle sigma matvec at the mid-chain dot (%.1f s, %.2f GFLOP/s), "
+                                         "scaled to the last timed sweep's sigma FLOPs" % (t, rate / 1e9)}
+    out["sigma_relerr_vs_f64_gpu"] = float(numpy.linalg.norm(ylo - y64) / numpy.linalg.norm(y64))
+    return out
+
+
+def f64_arm(args, dev, dist, rank, e_mixed, ms_mixed):
+    """The plain FP64 GPU path on the same workload and schedule (ramp, warm-up sweeps),
+    timing the first f64_steps sweeps after the warm-up; compared with the mixed arm's
+    energy after the same number of sweeps and its time for the same sweeps."""
+    import torch
+    n = min(args.f64_steps, args.steps)
+    d = _make_dmrg(args, "f64", dev, rank)
+    for _ in range(args.warmup):
+        _step(d, args)
+    ms, per, res = _timed_sweeps(d, args, n, dist)
+    ms = max_over_ranks(dist, ms, dev)
+    e64 = res[-1][0]
+    em = e_mixed[args.warmup + n - 1]
+    t_mixed = max_over_ranks(dist, sum(ms_mixed[:n]), dev)
+    out = {"sweeps_timed": n, "s_per_sweep": round(ms / n / 1e3, 3), "sweep_ms": [round(x, 1) for x in per],
+           "energy_f64": e64, "energy_mixed_same_sweep": em, "abs_dE_vs_f64": abs(em - e64),
+           "energy_mixed_final": e_mixed[-1], "matvecs_per_sweep": sum(r[2] for r in res) / n,
+           "speedup_vs_f64": round(ms / t_mixed, 3),
+           "definition": "same schedule from the same start: sweeps %d..%d after the warm-up, FP64 GPU time / "
+                         "mixed time for those sweeps; |dE| between the two arms' energies after sweep %d"
+                         % (args.warmup + 1, args.warmup + n, args.warmup + n)}
+    del d
+    return out
 
 
 def run_reference(args):
@@ -388,6 +483,11 @@ def main():
     ap.add_argument("--w-path", default="fiber", choices=["generic", "fiber", "fused"],
                     help="kernels of the two MPO-site contractions of sigma")
     ap.add_argument("--plan-cache", action="store_true", help="reuse compiled plans of unchanged dots")
+    ap.add_argument("--f64-steps", type=int, default=3,
+                    help="sweeps timed on the plain FP64 GPU arm after the same warm-up (0: no FP64 arm)")
+    ap.add_argument("--precond", default="jacobi", choices=["jacobi", "learned"],
+                    help="Davidson preconditioner of the mixed-precision arm")
+    ap.add_argument("--precond-train", type=int, default=2, help="sweeps whose solver pairs train the network")
     ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "sp"],
                     help="sp: spin-projected sweeps (SP-MPS, S=0) with --npts quadrature points")
     ap.add_argument("--npts", type=int, default=4)
@@ -395,6 +495,18 @@ def main():
     ap.add_argument("--no-graphs", dest="graphs", action="store_false",
                     help="batched workload: plain lockstep launches instead of CUDA-graph replay")
     args = ap.parse_args()
+    world = os.environ.get("WORLD_SIZE")
+    if args.gpus > 1 and world is None:
+        # one process per GPU: relaunch under torch.distributed.run (replicas, see dist_init)
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+               "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+        sys.exit(subprocess.call(cmd))
+    if world is not None and int(world) != args.gpus:
+        sys.exit("bench.py: --gpus %d but WORLD_SIZE=%s" % (args.gpus, world))
     if args.workload == "batched":
         run_batched(args)
     elif args.impl == "reference":

@@ -26,6 +26,11 @@ extern "C" {
 #define QC_ERR_LAYOUT -4
 #define QC_ERR_HALFINT -5
 
+/* Kinds of work-item groups in a compiled plan. */
+#define QC_GROUP_BGEMM 1   /* qc_task + qc_contrib (packed-layout grouped GEMM) */
+#define QC_GROUP_PANEL 2   /* qc_ptask (dense panel GEMM) */
+#define QC_GROUP_FIBER 3   /* qc_ftask + qc_fin / qc_fout / qc_fpair (fiber-group kernel) */
+
 /* ---------------------------------------------------------------- libqsym.so */
 
 /* Replaces ctypes/qsym.c:5-22 symAllowed (and symAllowed2..8, :24-480).
@@ -249,9 +254,15 @@ int qc_precond_apply(long long n, const double *r, const double *d, double e, co
  * qc_bgemm_f64 contractions and the operator sum as the regular path, with the
  * intermediates held in a fixed 32 MiB device array inside the library
  * (present on every GPU that loads it, until process exit).
+ * Only plans whose every group is a packed-layout grouped GEMM are accepted
+ * (group_kind[g] == QC_GROUP_BGEMM; in Python SigmaOperator(use_fiber=False,
+ * panel1=False), see SigmaOperator.work_groups).  The default sigma plan, with
+ * dense-panel and fiber-group stages, is refused with QC_ERR_ARG before any
+ * work is queued.  The work lists are trusted as compiled by this library for
+ * the given t1 / t2 / t3.
  *   groups: ngroups work-item groups of the compiled sigma plan, ordered by
  *     stage 0..3 (L.psi, .W_i, .W_{i+1}, .R); for each: stage, device task and
- *     contribution arrays, task count, operator span, tile configuration;
+ *     contribution arrays, task count, operator span, tile configuration, kind;
  *   stage_ops[4]: device operator tables of the four stages;
  *   L, Wi, Wj, R: device environment / site-operator values; x: device input;
  *   y: device output (ndim0 doubles); t1, t2, t3: intermediate sizes (doubles).
@@ -264,7 +275,8 @@ int qc_precond_apply(long long n, const double *r, const double *d, double e, co
 int qc_sigma_f64_noalloc(int ngroups, const int *group_stage, const void *const *group_tasks,
                          const long long *group_ntasks, const int *group_opspan,
                          const void *const *group_contribs, const int *group_cfg,
-                         const void *const *stage_ops, const double *L, const double *Wi,
+                         const int *group_kind, const void *const *stage_ops, const double *L,
+                         const double *Wi,
                          const double *Wj, const double *R, const double *x, double *y, int nops,
                          long long ndim0, long long t1, long long t2, long long t3, void *stream);
 

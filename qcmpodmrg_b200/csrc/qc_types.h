@@ -43,6 +43,11 @@ static_assert(sizeof(qc_op) == 32, "qc_op is 32 bytes");
 #define QC_ERR_LAYOUT -4
 #define QC_ERR_HALFINT -5
 
+// Kinds of work-item groups in a compiled plan (the records a group's task array holds).
+#define QC_GROUP_BGEMM 1   // qc_task + qc_contrib (packed-layout grouped GEMM, k_bgemm)
+#define QC_GROUP_PANEL 2   // qc_ptask (dense panel GEMM, k_pgemm)
+#define QC_GROUP_FIBER 3   // qc_ftask + qc_fin/qc_fout/qc_fpair (fiber-group kernel, k_fiber)
+
 // ---- fiber-group work items (the W contractions of sigma) -------------------
 // A fiber group is a set of output blocks that share their "fiber" index
 // f = (l, r) and read the same input blocks; one task = one tile of fibers.

@@ -11,6 +11,14 @@
 // part of the library image instead: nothing is allocated per call.
 //
 // Limits and sharing rules:
+//  * only plans made entirely of packed-layout grouped-GEMM groups are accepted
+//    (QC_GROUP_BGEMM: qc_task / qc_contrib records, the operands in the packed
+//    block layout; in Python, SigmaOperator(use_fiber=False, panel1=False)).
+//    Each group carries its kind; a plan with dense-panel or fiber-group stages
+//    (the default sigma plan) reads other operands through other records and is
+//    refused with QC_ERR_ARG before any work is queued.  The work lists
+//    themselves are trusted: they must come from this library's plan compiler
+//    for these t1 / t2 / t3 sizes;
 //  * the array holds QC_NOALLOC_SCRATCH_DOUBLES doubles (32 MiB); every GPU that
 //    loads the library holds that much device memory until the process exits;
 //  * one call needs t1 + t2 + t3 + nops * ndim0 doubles (plus 256-byte padding
@@ -70,20 +78,25 @@ static inline long long pad256(long long n) { return (n + 31) & ~31LL; }   // 32
 extern "C" int qc_sigma_f64_noalloc(int ngroups, const int *group_stage, const void *const *group_tasks,
                                     const long long *group_ntasks, const int *group_opspan,
                                     const void *const *group_contribs, const int *group_cfg,
-                                    const void *const *stage_ops, const double *L, const double *Wi,
+                                    const int *group_kind, const void *const *stage_ops, const double *L, const double *Wi,
                                     const double *Wj, const double *R, const double *x, double *y, int nops,
                                     long long ndim0, long long t1, long long t2, long long t3, void *stream) {
   if (ngroups < 0 || !group_stage || !group_tasks || !group_ntasks || !group_opspan || !group_contribs ||
-      !group_cfg || !stage_ops || nops < 1 || ndim0 < 1 || t1 < 0 || t2 < 0 || t3 < 0)
+      !group_cfg || !group_kind || !stage_ops || nops < 1 || ndim0 < 1 || t1 < 0 || t2 < 0 || t3 < 0)
     return noalloc_fail(QC_ERR_ARG, "qc_sigma_f64_noalloc: bad arguments");
   const long long need = pad256(t1) + pad256(t2) + pad256(t3) + pad256((long long)nops * ndim0);
   if (need > QC_NOALLOC_SCRATCH_DOUBLES)
     return noalloc_fail(QC_ERR_CAPACITY, "qc_sigma_f64_noalloc: this dot needs " + std::to_string(need) +
                                              " scratch doubles, the static array holds " +
                                              std::to_string(QC_NOALLOC_SCRATCH_DOUBLES));
-  for (int g = 1; g < ngroups; ++g)
-    if (group_stage[g] < group_stage[g - 1] || group_stage[g] < 0 || group_stage[g] > 3)
+  for (int g = 0; g < ngroups; ++g) {
+    if (group_stage[g] < 0 || group_stage[g] > 3 || (g > 0 && group_stage[g] < group_stage[g - 1]))
       return noalloc_fail(QC_ERR_ARG, "qc_sigma_f64_noalloc: groups must be ordered by stage 0..3");
+    if (group_kind[g] != QC_GROUP_BGEMM)
+      return noalloc_fail(QC_ERR_ARG, "qc_sigma_f64_noalloc: group " + std::to_string(g) + " is of kind " +
+                                          std::to_string(group_kind[g]) +
+                                          "; only packed-layout grouped-GEMM plans (QC_GROUP_BGEMM) are accepted");
+  }
   double *base = nullptr;
   int rc = scratch_base(&base);
   if (rc != QC_OK) return rc;

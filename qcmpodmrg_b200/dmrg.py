@@ -83,6 +83,10 @@ class DMRG(object):
     def __init__(self, ham, device="cuda", precision="f64", preconditioner=None, w_path="fiber", plan_cache=False,
                  sz=0.0):
         """sz: the target Sz of the (N, Sz) sector (the reference's qsectors key [N, Sz])."""
+        n2s = int(round(2 * float(sz)))
+        if abs(2 * float(sz) - n2s) > 1e-9 or (n2s - int(ham.nelec)) % 2 != 0 or abs(float(sz)) > ham.nelec / 2.0:
+            raise ValueError("sz=%g is not an Sz of %d electrons (2*Sz must have the parity of N and "
+                             "|Sz| <= N/2)" % (float(sz), int(ham.nelec)))
         self.ham = ham
         self.sz = float(sz)
         self.device = torch.device(device)
@@ -213,7 +217,7 @@ class DMRG(object):
             res = davidson(hv, diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec, precond=self.preconditioner,
                            record=self.recorder)
         else:
-            res = self._mixed_davidson(sig, hv, diag, v0, crit_e)
+            res = self._mixed_davidson(hv, lambda v: sig(v, precision="f64"), diag, v0, crit_e)
         torch.cuda.synchronize(dev)
         self.stats["hvec_s"] += time.time() - t0
         self.stats["nmvp"] += res.nmvp
@@ -294,8 +298,8 @@ class DMRG(object):
             self.rmps[0] = SiteTensor(smat, [qk, QPHYS, qred], R_STATUS, dev)
             self.qnumr[0] = qk
 
-    def _mixed_davidson(self, sig, hv, diag, v0, crit_e):
-        """Davidson with low-precision sigma, then FP64 refinement.
+    def _mixed_davidson(self, hv, hv64, diag, v0, crit_e):
+        """Davidson with low-precision sigma (hv), then FP64 refinement (hv64).
 
         Phase 1 iterates with the FP32/TF32 sigma until the energy change is below
         crit_e or the residual below the precision's floor.  Phase 2 applies the
@@ -304,7 +308,8 @@ class DMRG(object):
         at most 1e-4, or when phase 1 converged by the reference's criteria and the FP64
         Rayleigh quotient agrees with the low-precision Ritz value within ACCEPT_DE (the
         low-precision sigma then did not bias the solve); otherwise FP64 Davidson
-        iterations (reference criteria) continue from that vector.
+        iterations (reference criteria) continue from that vector.  Vectors are device
+        tensors, or host tensors when hv / hv64 are the host-buffer entry points.
         """
         # residual floor of the low-precision sigma (relative sigma error ~1e-7 FP32,
         # ~1e-3 TF32), and the FP64 residual accepted without FP64 iterations: the
@@ -314,7 +319,7 @@ class DMRG(object):
         r1 = davidson(hv, diag, 1, v0, crit_e=crit_e, crit_vec=max(self.crit_vec, floor),
                       precond=self.preconditioner, record=self.recorder)
         x = r1.vecs[0] / torch.linalg.norm(r1.vecs[0])
-        y = sig(x, precision="f64")
+        y = hv64(x)
         e64 = float(torch.dot(x, y))
         rn = float(torch.linalg.norm(y - e64 * x))
         self.stats["nmvp_f64"] = self.stats.get("nmvp_f64", 0) + 1
@@ -325,10 +330,6 @@ class DMRG(object):
             r1.vecs = x.reshape(1, -1)
             r1.nmvp += 1
             return r1
-
-        def hv64(v):
-            return sig(v, precision="f64")
-
         r2 = davidson(hv64, diag, 1, x.reshape(1, -1), crit_e=crit_e, crit_vec=self.crit_vec,
                       precond=self.preconditioner)
         self.stats["nmvp_f64"] += r2.nmvp
@@ -360,7 +361,22 @@ class DMRG(object):
         if self.psi0 is not None:
             v0 = self.psi0[0:1].reshape(1, -1)[:, torch.from_numpy(prj_h).to(self.psi0.device)].cpu()
         t0 = time.time()
-        res = davidson(hv, diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec)
+        if self.precision == "f64":
+            res = davidson(hv, diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec)
+        else:               # the same mixed-precision solve, FP64 products through the same entry point
+
+            def hv64(x):
+                y = K.HVec(x.numpy(), info, ndim0, prj_h, precision="f64")
+                self.h2d_bytes += 8 * ndim0
+                self.d2h_bytes += 8 * ndim0
+                return torch.from_numpy(y)
+
+            learned = self.preconditioner
+            self.preconditioner = None if hasattr(learned, "set_layout") else learned
+            try:
+                res = self._mixed_davidson(hv, hv64, diag, v0, crit_e)
+            finally:
+                self.preconditioner = learned
         self.stats["hvec_s"] += time.time() - t0
         self.stats["nmvp"] += res.nmvp
         self.stats["sigma_flops"] += res.nmvp * sig.flops
@@ -533,9 +549,26 @@ class DMRG(object):
             self.psi0 = torch.stack([torch.tensordot(srotR[i], t, dims=([2], [0])).reshape(-1)
                                      for i in range(srotR.shape[0])])
 
+    def snapshot(self):
+        """The state between two sweeps (after a left-to-right sweep): left-canonical site
+        tensors, bond quantum numbers and the next dot's start vector (device copies)."""
+        st = {"site%d" % i: self.lmps[i].dense.clone() for i in range(self.nsite)}
+        st.update({"qnum%d" % i: self.qnuml[i].copy() for i in range(self.nsite + 1)})
+        st["psi0"] = None if self.psi0 is None else self.psi0.clone()
+        return st
+
+    def restore(self, st):
+        """Return to a snapshot: environments rebuilt from the site tensors (genHopsQt)."""
+        self.load_mps(st)
+        self.psi0 = None if st["psi0"] is None else st["psi0"].clone()
+
     def run(self, init_mps, dmax, nsweeps, tol=1.e-7, callback=None, noise=0.0):
         """schedule.fixed(ncsite=2, maxM=dmax, tol=tol, noise=noise): sweeps R then L until |dE| < tol."""
         self.noise = float(noise)
+        last = numpy.asarray(init_mps["qnum%d" % self.nsite], dtype=numpy.float64).reshape(-1, 2)
+        if last.shape[0] != 1 or numpy.abs(last[0] - self.qkey).max() > 1e-9:
+            raise ValueError("the start MPS ends in the sector %s, the target sector is %s"
+                             % (last.tolist(), self.qkey.tolist()))
         self.load_mps(init_mps)
         eav, dwt, esweeps, nmvps = [], [], [], []
         eold = 1.e3

@@ -468,6 +468,37 @@ class SigmaOperator(object):
     def scratch_bytes(self):
         return 8 * sum(self.tot)
 
+    def work_groups(self):
+        """The plan's device work-item groups in stage order, as the C-ABI's
+        qc_sigma_f64_noalloc takes them: (stage, kind, tasks, ntasks, opspan, contribs,
+        tile_cfg), kind one of native.GROUP_BGEMM / GROUP_PANEL / GROUP_FIBER.  Groups
+        that read the per-dot panels (the tensor-core tiles of a panel stage included)
+        are GROUP_PANEL; the fused two-site W stage counts as a fiber group of stage 1."""
+        out = []
+
+        def walk(st, si, kind=None):
+            if st is None:
+                return
+            if isinstance(st, CompositeStage):
+                for x in st.subs:
+                    walk(x, si, kind)
+            elif isinstance(st, PanelStage):
+                for (cfg, tk, dt, span) in st.groups:
+                    out.append((si, native.GROUP_PANEL, dt.data_ptr(), len(tk), span, 0, cfg))
+                walk(st.tc, si, native.GROUP_PANEL)
+            elif isinstance(st, FiberStage):
+                if st.ntasks:
+                    out.append((si, native.GROUP_FIBER, st.d[0].data_ptr(), st.ntasks, st.span, 0, 0))
+            else:
+                for (cfg, tk, ct, dt, dc, span) in st.groups:
+                    out.append((si, kind or native.GROUP_BGEMM, dt.data_ptr(), len(tk), span, dc.data_ptr(), cfg))
+
+        for si, st in enumerate(self.stages):
+            walk(st, si)
+            if si == 1:
+                walk(self.fused, 1, native.GROUP_FIBER)
+        return out
+
     def __call__(self, x, y=None, precision=None):
         """x: device tensor (ndim0,) float64 -> y = H x (float64).
 

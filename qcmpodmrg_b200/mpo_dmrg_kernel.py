@@ -50,13 +50,15 @@ def _to_dev(v, dev):
     return torch.from_numpy(numpy.ascontiguousarray(v, dtype=numpy.float64)).to(dev)
 
 
-def HVec(vec0, info, ndim0, prjmap):
-    """sigma = H_eff vec0 in the packed (qtmp) layout."""
+def HVec(vec0, info, ndim0, prjmap, precision=None):
+    """sigma = H_eff vec0 in the packed (qtmp) layout.  ``precision`` (an addition to the
+    reference's signature, optional) overrides the sigma precision of the DMRG object for
+    this call, e.g. "f64" for the FP64 check of a mixed-precision solve."""
     dmrg, isite = _check(info)
     lay, idl, sig, dg = _ops(dmrg, isite)
     if ndim0 != sig.ndim0:
         raise ValueError("ndim0 does not match the dot's wavefunction template")
-    y = sig(_to_dev(vec0, dmrg.device))
+    y = sig(_to_dev(vec0, dmrg.device), precision=precision)
     return y if torch.is_tensor(vec0) else y.cpu().numpy()
 
 

@@ -16,6 +16,7 @@ c_char_p = ctypes.c_char_p
 TASK_BYTES = 64
 CONTRIB_BYTES = 80
 OP_BYTES = 32
+GROUP_BGEMM, GROUP_PANEL, GROUP_FIBER = 1, 2, 3     # work-item group kinds (qc_types.h)
 
 
 class NativeError(RuntimeError):
@@ -63,7 +64,7 @@ _SIGS = {
                              ctypes.c_float, c_int, ctypes.c_float, c_vp]),
     "qc_precond_apply": (c_int, [c_ll, c_vp, c_vp, c_dbl, c_vp, c_vp, c_vp, c_vp]),
     "qc_sigma_f64_noalloc": (c_int, [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
-                                     c_vp, c_vp, c_int, c_ll, c_ll, c_ll, c_ll, c_vp]),
+                                     c_vp, c_vp, c_vp, c_int, c_ll, c_ll, c_ll, c_ll, c_vp]),
     "qc_reduce_ops_f32": (c_int, [c_vp, c_int, c_ll, c_vp, c_vp]),
     "qc_scatter_f64": (c_int, [c_vp, c_vp, c_vp, c_ll, c_ll, c_vp]),
     "qc_convert_f64_to_f32": (c_int, [c_vp, c_vp, c_ll, c_vp]),

@@ -147,10 +147,16 @@ def loss_and_grad(r, d, e, blk, nblk, Y, t):
 class LearnedPreconditioner(object):
     """Davidson preconditioner callable + the training-pair collector."""
 
-    def __init__(self, device, seed=0):
+    def __init__(self, device, seed=0, train_sweeps=0, epochs=30):
+        """train_sweeps > 0: collect (residual, exact correction) pairs during that many
+        sweeps (end_sweep() counts them), then train on the GPU and switch the network on."""
         self.device = torch.device(device)
         self.net = MLP(self.device, seed)
         self.enabled = False         # Jacobi fallback until trained
+        self.train_sweeps = int(train_sweeps)
+        self.epochs = int(epochs)
+        self.sweeps = 0
+        self.train_info = None
         self.blk = None
         self.nblk = 0
         self.it = 0
@@ -159,6 +165,26 @@ class LearnedPreconditioner(object):
         self.max_pairs = 400
         self._dot = []
         self.history = []
+        if self.train_sweeps > 0:
+            self.collect = True
+
+    def end_sweep(self):
+        """Schedule hook: after train_sweeps sweeps of collected pairs, train and enable."""
+        self.sweeps += 1
+        if self.train_sweeps > 0 and self.sweeps == self.train_sweeps:
+            self.collect = False
+            import time as _t
+            t0 = _t.time()
+            jac = self.jacobi_loss()
+            losses = self.train(epochs=self.epochs)
+            self.enabled = True
+            self.train_info = {"pairs": len(self.pairs), "epochs": self.epochs, "train_s": round(_t.time() - t0, 2),
+                               "loss_first": losses[0] if losses else None,
+                               "loss_last": losses[-1] if losses else None, "jacobi_loss": jac}
+            self.pairs = []              # the device copies are not needed any more
+
+    def summary(self):
+        return {"enabled": self.enabled, "trained_after_sweeps": self.train_sweeps, "train": self.train_info}
 
     # -- per dot
     def set_layout(self, layout):

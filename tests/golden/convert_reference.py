@@ -22,7 +22,8 @@ Rewrites applied (syntax only, no algorithmic change):
 The C library ``ctypes/qsym.c`` is compiled from where it lies with the
 reference's own install.sh command into ``baseline/_ref/qcmpodmrg/libs``.
 
-Usage:  python tests/golden/convert_reference.py [--ref /root/reference]
+Usage:  python tests/golden/convert_reference.py [--ref REFERENCE_ROOT]
+        (default: the environment variable QCMPODMRG_REFERENCE)
 """
 import argparse
 import io
@@ -194,7 +195,7 @@ def convert(ref):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("QCMPODMRG_REFERENCE", "/root/reference"))
     a = ap.parse_args()
     n = convert(a.ref)
     print("converted into", OUT_ROOT, "files that failed to convert:", n)

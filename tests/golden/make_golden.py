@@ -1,7 +1,7 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
 Requires the converted reference (python tests/golden/convert_reference.py)
-and /root/reference; run where the reference sources are present:
+and the reference's sources (environment QCMPODMRG_REFERENCE); run where they are present:
 
     python tests/golden/make_golden.py            # small fixtures (seconds)
     python tests/golden/make_golden.py --config1  # K=12, N=12, D=100, 6 sweeps (~30 min CPU)
