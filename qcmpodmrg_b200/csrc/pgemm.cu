@@ -36,6 +36,7 @@ k_pgemm(const qc_ptask *__restrict__ tasks, const qc_op *__restrict__ ops, const
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
   const int M = t.M, N = t.N, K = t.K;
+  const long long lda = t.lda > 0 ? t.lda : K;
 
   T ra[LA], rb[LB];
   auto load = [&](int k0) {
@@ -44,7 +45,7 @@ k_pgemm(const qc_ptask *__restrict__ tasks, const qc_op *__restrict__ ops, const
       const int idx = tid + e * NT;
       const int kk = idx % TK, i = idx / TK;
       const int m = t.m0 + i, k = k0 + kk;
-      ra[e] = (idx < TM * TK && m < M && k < K) ? Ab[(long long)m * K + k] : T(0);
+      ra[e] = (idx < TM * TK && m < M && k < K) ? Ab[(long long)m * lda + k] : T(0);
     }
 #pragma unroll
     for (int e = 0; e < LB; ++e) {       // B: consecutive n of one k row

@@ -99,8 +99,8 @@ static_assert(sizeof(qc_bperm) == 64, "qc_bperm is 64 bytes");
 
 
 // ---- dense panel GEMM work items (qc_pgemm_*) -------------------------------
-// C[row(m) + n] = sum_k A[a_off + m*K + k] * B[b_off + k*N + n] for the output
-// tile rows [m0, m0+TM) x cols [n0, n0+TN), with row(m) = c_off + m*N, or
+// C[row(m) + n] = sum_k A[a_off + m*lda + k] * B[b_off + k*N + n] for the output
+// tile rows [m0, m0+TM) x cols [n0, n0+TN) (lda = K when 0), with row(m) = c_off + m*N, or
 // crow_table[crow + m] when crow >= 0 (rows scattered to separate blocks);
 // offsets relative to the operator's bases; grid.y indexes the operators [op_b, op_e).
 struct alignas(16) qc_ptask {
@@ -109,5 +109,39 @@ struct alignas(16) qc_ptask {
   int m0, n0;
   int op_b, op_e;
   int crow;
+  int lda;             // row stride of A (0: K)
 };
 static_assert(sizeof(qc_ptask) == 64, "qc_ptask is 64 bytes");
+
+// ---- tensor-core panel GEMM work units (qc_tcpanel_*) ------------------------
+// One unit = one 128-row x up-to-BN-column output tile of one operator:
+//   C[row(m), n0 + n] = alpha * sum_k A[m, k] * B[n0 + n, k]    (m < m_valid, n < n_valid)
+// A and B are read by TMA through tensor maps (maps[a_map], maps[b_map]) of this GPU's
+// own buffers: A rows a_c1 .. a_c1+127 of operator slice a_c2, B rows b_c1 .. of slice
+// b_c2, both K-major (k contiguous), nk stages of 32 k.  Epilogue: row m goes to
+// C + ops[op].c_base + crow[c_off + m] + b_c1 (rows scattered through a row table).
+struct alignas(16) qc_tcunit {
+  int a_map, b_map;
+  int a_c1, b_c1;
+  int a_c2, b_c2;
+  int nk;
+  int m_valid;
+  int n_valid;
+  int op;
+  int pad0, pad1;
+  long long c_off;
+  long long pad2;
+};
+static_assert(sizeof(qc_tcunit) == 64, "qc_tcunit is 64 bytes");
+
+// One tensor map to encode on the host (cuTensorMapEncodeTiled, FP32 elements).
+struct alignas(16) qc_tmdesc {
+  long long addr;        // global address, 16-byte aligned
+  int rank;              // 2 .. 5
+  int swizzle;           // CUtensorMapSwizzle value (3 = 128-byte swizzle)
+  long long dims[5];     // elements per dimension (dimension 0 contiguous)
+  long long strides[4];  // byte strides of dimensions 1 .. rank-1 (multiples of 16)
+  int box[5];            // box extent per dimension (box[0] * 4 <= 128 with 128-byte swizzle)
+  int pad;
+};
+static_assert(sizeof(qc_tmdesc) == 112, "qc_tmdesc is 112 bytes");

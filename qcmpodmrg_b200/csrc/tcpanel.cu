@@ -1,0 +1,459 @@
+// Panel GEMM on the 5th-generation tensor cores, fed by TMA: the .R contraction of
+// HVecQt (top4 = top3 . R, source/mpo_dmrg_kernelQt.py:302-306) in FP32-level
+// precision from split TF32 products.
+//
+// For one output sector r' of one operator, sigma rows (the T3 panel [M x K], row
+// stride Kp, written by the fiber kernel) times the R panel of r' (stored transposed,
+// [N x K] with k contiguous, pre-split into TF32 hi and lo planes once per dot) give
+// the sigma rows of that sector; the K extent (sum over MPO sectors c of D_c * D_r)
+// is long, the N extent (D_r') short.
+//
+// Persistent, warp-specialised CTA (6 warps):
+//   warp 0     one thread issues the TMA loads (cp.async.bulk.tensor, 128-byte swizzle)
+//              of every 32-wide K stage into a ring of S shared-memory stages;
+//   warp 1     owns the tensor memory (2 x BN columns: two accumulators) and one thread
+//              issues tcgen05.mma kind::tf32, 12 per stage: a_lo.b_hi + a_hi.b_lo +
+//              a_hi.b_hi for each 8-wide K step, committed to the stage's "empty"
+//              barrier and, after a unit's last stage, to the accumulator's "full" one;
+//   warps 2-5  split each raw FP32 A stage in place into hi = tf32(x) and a lo plane
+//              tf32(x - hi) (A_SPLIT), then read a finished accumulator with
+//              tcgen05.ld (warp w owns TMEM lanes 32*(w%4) ..) and store its rows through
+//              the row table; the other accumulator meanwhile takes the next unit.
+// No cluster, no multicast: every CTA loads its own tiles of this GPU's own memory.
+// Every wait is bounded: on expiry the CTA raises *err, stops issuing work, waits
+// (bounded) for its loads and products in flight and still frees its tensor memory.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include "qc_types.h"
+
+namespace {
+
+constexpr int TP_BM = 128;
+constexpr int TP_BK = 32;                  // 32 FP32 = 128 bytes: one swizzle row
+constexpr int TP_THREADS = 192;
+constexpr long long TP_SPIN = 1LL << 26;   // polls before a wait gives up (~seconds)
+
+__device__ __forceinline__ uint32_t su32(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ bool wait_parity(uint32_t bar, uint32_t parity) {
+  for (long long it = 0; it < TP_SPIN; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (it > 256) __nanosleep(32);
+  }
+  return false;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load3(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                          uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load4(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                          uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+      "[%2];" ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+      : "memory");
+}
+
+// Tensor maps live in global memory (written from the host before the launch).
+__device__ __forceinline__ void tmap_acquire(const CUtensorMap *map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle (layout type 2), 8-row
+// groups 1024 bytes apart (SBO); the leading offset is unused for this layout.
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
+// Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = n.
+__device__ __forceinline__ uint32_t idesc_tf32(int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TP_BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <int BN>
+__host__ __device__ constexpr int stage_bytes() { return 2 * TP_BM * TP_BK * 4 + 2 * BN * TP_BK * 4; }
+
+template <bool A_SPLIT, int BN, int S>
+__global__ void __launch_bounds__(TP_THREADS, 1)
+k_tcpanel(const qc_tcunit *__restrict__ units, int nunits, const CUtensorMap *__restrict__ maps,
+          const qc_op *__restrict__ ops, const long long *__restrict__ crow, float *__restrict__ C,
+          int *__restrict__ err) {
+  static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N");
+  extern __shared__ unsigned char tp_smem_raw[];
+  // stage s: [A0 (raw / hi) | A1 (lo) | B0 (hi) | B1 (lo)], each 1024-byte aligned
+  unsigned char *smem = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(tp_smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  constexpr int A_BYTES = TP_BM * TP_BK * 4;
+  constexpr int B_BYTES = BN * TP_BK * 4;
+  constexpr int ST_BYTES = stage_bytes<BN>();
+  __shared__ __align__(8) uint64_t full[S], empty[S], split[S], accf[2], acce[2], fin;
+  __shared__ uint32_t tmem_base;
+  __shared__ volatile int abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base)),
+                 "r"(2 * BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    for (int s = 0; s < S; ++s) {
+      mbar_init(su32(&full[s]), 1);
+      mbar_init(su32(&empty[s]), 1);
+      mbar_init(su32(&split[s]), 4);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(su32(&accf[b]), 1);
+      mbar_init(su32(&acce[b]), 4);
+    }
+    mbar_init(su32(&fin), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+
+  auto fail = [&]() {
+    abort_flag = 1;
+    if (err) atomicExch(err, 1);
+  };
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      int it = 0;
+      int issued[S];
+      for (int s = 0; s < S; ++s) issued[s] = -1;
+      for (int u = blockIdx.x; u < nunits && !abort_flag; u += gridDim.x) {
+        const qc_tcunit t = units[u];
+        const CUtensorMap *am = maps + t.a_map;
+        const CUtensorMap *bm = maps + t.b_map;
+        tmap_acquire(am);
+        tmap_acquire(bm);
+        for (int k = 0; k < t.nk; ++k, ++it) {
+          const int s = it % S;
+          const uint32_t ph = (uint32_t)((it / S) & 1);
+          if (!wait_parity(su32(&empty[s]), ph ^ 1u)) {
+            fail();
+            break;
+          }
+          unsigned char *st = smem + s * ST_BYTES;
+          mbar_arrive_tx(su32(&full[s]), (A_SPLIT ? A_BYTES : 2 * A_BYTES) + 2 * B_BYTES);
+          if (A_SPLIT)
+            tma_load3(su32(st), am, k * TP_BK, t.a_c1, t.a_c2, su32(&full[s]));
+          else
+            tma_load4(su32(st), am, k * TP_BK, t.a_c1, t.a_c2, 0, su32(&full[s]));
+          tma_load4(su32(st + 2 * A_BYTES), bm, k * TP_BK, t.b_c1, t.b_c2, 0, su32(&full[s]));
+          issued[s] = (int)ph;
+        }
+      }
+      // loads still in flight land before the CTA leaves (bounded)
+      for (int s = 0; s < S; ++s)
+        if (issued[s] >= 0) wait_parity(su32(&full[s]), (uint32_t)issued[s]);
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      int it = 0, uc = 0;
+      bool any = false;
+      for (int u = blockIdx.x; u < nunits && !abort_flag; u += gridDim.x, ++uc) {
+        const qc_tcunit t = units[u];
+        const int buf = uc & 1;
+        if (!wait_parity(su32(&acce[buf]), (uint32_t)(((uc >> 1) & 1) ^ 1))) {
+          fail();
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d = tmem + (uint32_t)(buf * BN);
+        const int nmma = ((t.n_valid + 15) / 16) * 16;
+        const uint32_t idesc = idesc_tf32(nmma > BN ? BN : nmma);
+        bool ok = true;
+        for (int k = 0; k < t.nk; ++k, ++it) {
+          const int s = it % S;
+          const uint32_t ph = (uint32_t)((it / S) & 1);
+          if (!wait_parity(su32(A_SPLIT ? &split[s] : &full[s]), ph)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t st = su32(smem + s * ST_BYTES);
+          const uint32_t a_hi = st, a_lo = st + A_BYTES, b_hi = st + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < TP_BK / 8; ++kk) {
+            const uint32_t off = kk * 32;              // 8 TF32 = 32 bytes along the swizzled row
+            const uint32_t first = (k == 0 && kk == 0) ? 0u : 1u;
+            mma_tf32(d, desc_sw128(a_lo + off), desc_sw128(b_hi + off), idesc, first);
+            mma_tf32(d, desc_sw128(a_hi + off), desc_sw128(b_lo + off), idesc, 1u);
+            mma_tf32(d, desc_sw128(a_hi + off), desc_sw128(b_hi + off), idesc, 1u);
+          }
+          mma_commit(su32(&empty[s]));
+          any = true;
+        }
+        if (!ok) {
+          fail();
+          break;
+        }
+        mma_commit(su32(&accf[buf]));
+      }
+      // every product issued has finished before the tensor memory is released (bounded)
+      if (any) {
+        mma_commit(su32(&fin));
+        if (!wait_parity(su32(&fin), 0u)) fail();
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ split + epilogue (warps 2-5)
+    const int hid = threadIdx.x - 64;          // 0 .. 127
+    const int q = warp & 3;                    // TMEM lane quarter of this warp
+    int it = 0, uc = 0;
+    for (int u = blockIdx.x; u < nunits && !abort_flag; u += gridDim.x, ++uc) {
+      const qc_tcunit t = units[u];
+      if (A_SPLIT) {
+        bool ok = true;
+        for (int k = 0; k < t.nk; ++k, ++it) {
+          const int s = it % S;
+          const uint32_t ph = (uint32_t)((it / S) & 1);
+          if (!wait_parity(su32(&full[s]), ph)) {
+            ok = false;
+            break;
+          }
+          float4 *a0 = reinterpret_cast<float4 *>(smem + s * ST_BYTES);
+          float4 *a1 = reinterpret_cast<float4 *>(smem + s * ST_BYTES + A_BYTES);
+#pragma unroll
+          for (int j = 0; j < A_BYTES / 16 / 128; ++j) {
+            const int i = hid + j * 128;
+            const float4 x = a0[i];
+            float4 h, l;
+            h.x = tf32_rna(x.x); l.x = tf32_rna(x.x - h.x);
+            h.y = tf32_rna(x.y); l.y = tf32_rna(x.y - h.y);
+            h.z = tf32_rna(x.z); l.z = tf32_rna(x.z - h.z);
+            h.w = tf32_rna(x.w); l.w = tf32_rna(x.w - h.w);
+            a0[i] = h;
+            a1[i] = l;
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(su32(&split[s]));
+        }
+        if (!ok) {
+          fail();
+          break;
+        }
+      }
+      const int buf = uc & 1;
+      if (!wait_parity(su32(&accf[buf]), (uint32_t)((uc >> 1) & 1))) {
+        fail();
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int row = q * 32 + lane;
+      const qc_op o = ops[t.op];
+      const float alpha = (float)o.alpha;
+      float *dst = nullptr;
+      if (row < t.m_valid) dst = C + o.c_base + crow[t.c_off + row] + t.b_c1;
+      const int ncol = t.n_valid < BN ? t.n_valid : BN;
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * BN);
+      for (int c0 = 0; c0 < ncol; c0 += 16) {
+        uint32_t r[16];
+        tmem_ld16(taddr + (uint32_t)c0, r);
+        if (dst) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (c0 + j < ncol) dst[c0 + j] = alpha * __uint_as_float(r[j]);
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(su32(&acce[buf]));
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
+  }
+}
+
+// hi = tf32(x), lo = tf32(x - hi), in place into hi (n values)
+__global__ void k_tf32_split(float *__restrict__ hi, float *__restrict__ lo, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float x = hi[i];
+    const float h = tf32_rna(x);
+    hi[i] = h;
+    lo[i] = tf32_rna(x - h);
+  }
+}
+
+int *g_tp_err = nullptr;
+int g_nsm = 0;
+std::mutex g_tp_mu;
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+constexpr int TP_BN = 128;
+constexpr int TP_S = 3;
+constexpr size_t tp_dsmem() { return (size_t)TP_S * stage_bytes<TP_BN>() + 1024; }
+
+}  // namespace
+
+static thread_local std::string g_tperr;
+
+extern "C" int qc_tmap_encode(int n, const void *descs, void *out_maps) {
+  if (n < 0 || (n > 0 && (!descs || !out_maps))) return QC_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lock(g_tp_mu);
+    if (!g_encode) {
+      cudaDriverEntryPointQueryResult q;
+      void *fn = nullptr;
+      if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+          q != cudaDriverEntryPointSuccess || !fn) {
+        fprintf(stderr, "[qcgpu] qc_tmap_encode: cuTensorMapEncodeTiled not available\n");
+        return QC_ERR_CUDA;
+      }
+      g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+  }
+  const qc_tmdesc *d = (const qc_tmdesc *)descs;
+  CUtensorMap *m = (CUtensorMap *)out_maps;
+  for (int i = 0; i < n; ++i) {
+    const qc_tmdesc &x = d[i];
+    if (x.rank < 2 || x.rank > 5 || (x.addr & 15)) return QC_ERR_ARG;
+    cuuint64_t dims[5], strides[4];
+    cuuint32_t box[5], es[5];
+    for (int r = 0; r < x.rank; ++r) {
+      if (x.dims[r] < 1 || x.box[r] < 1 || x.box[r] > 256) return QC_ERR_ARG;
+      dims[r] = (cuuint64_t)x.dims[r];
+      box[r] = (cuuint32_t)x.box[r];
+      es[r] = 1;
+      if (r > 0) {
+        if (x.strides[r - 1] <= 0 || (x.strides[r - 1] & 15)) return QC_ERR_ARG;
+        strides[r - 1] = (cuuint64_t)x.strides[r - 1];
+      }
+    }
+    if (x.swizzle == 3 && box[0] * 4 > 128) return QC_ERR_ARG;
+    CUresult rc = g_encode(&m[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)x.rank, (void *)x.addr, dims, strides,
+                           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, (CUtensorMapSwizzle)x.swizzle,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (rc != CUDA_SUCCESS) {
+      fprintf(stderr, "[qcgpu] qc_tmap_encode: map %d rejected (CUresult %d)\n", i, (int)rc);
+      return QC_ERR_ARG;
+    }
+  }
+  return QC_OK;
+}
+
+// C rows (through the row table) = A . B^T on the tensor cores, A split into TF32 hi/lo
+// in the kernel, B given as pre-split hi/lo planes (maps of rank 4, plane dimension last).
+extern "C" int qc_tcpanel_f32(const void *units, long long nunits, const void *maps, const void *ops,
+                              const long long *crow, float *C, void *stream) {
+  if (nunits <= 0) return QC_OK;
+  if (nunits > 0x7fffffffLL || !units || !maps || !ops || !crow || !C) return QC_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  {
+    std::lock_guard<std::mutex> lock(g_tp_mu);
+    if (!g_tp_err) {
+      if (cudaMalloc(&g_tp_err, sizeof(int)) != cudaSuccess) return QC_ERR_CUDA;
+      if (cudaMemset(g_tp_err, 0, sizeof(int)) != cudaSuccess) return QC_ERR_CUDA;
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&g_nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (cudaFuncSetAttribute(k_tcpanel<true, TP_BN, TP_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)tp_dsmem()) != cudaSuccess)
+        return QC_ERR_CUDA;
+    }
+  }
+  const int grid = (int)(nunits < (long long)g_nsm ? nunits : (long long)g_nsm);
+  k_tcpanel<true, TP_BN, TP_S><<<grid, TP_THREADS, tp_dsmem(), s>>>(
+      (const qc_tcunit *)units, (int)nunits, (const CUtensorMap *)maps, (const qc_op *)ops, crow, C, g_tp_err);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_tperr = cudaGetErrorString(e);
+    fprintf(stderr, "[qcgpu] qc_tcpanel_f32: %s\n", g_tperr.c_str());
+    return QC_ERR_CUDA;
+  }
+  return QC_OK;
+}
+
+extern "C" int qc_tf32_split(float *hi, float *lo, long long n, void *stream) {
+  if (n <= 0) return QC_OK;
+  if (!hi || !lo) return QC_ERR_ARG;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 65535) blocks = 65535;
+  k_tf32_split<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(hi, lo, n);
+  return cudaGetLastError() == cudaSuccess ? QC_OK : QC_ERR_CUDA;
+}
+
+// Error flag of the tensor-core panel kernel (1 after a wait gave up); reset with clear != 0.
+extern "C" int qc_tcpanel_status(int clear) {
+  if (!g_tp_err) return 0;
+  int h = 0;
+  if (cudaMemcpy(&h, g_tp_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return QC_ERR_CUDA;
+  if (clear && cudaMemset(g_tp_err, 0, sizeof(int)) != cudaSuccess) return QC_ERR_CUDA;
+  return h;
+}

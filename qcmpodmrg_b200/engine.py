@@ -206,7 +206,9 @@ def panel_sigma4(t3lay, Rl, psi, t4):
     rowoff = crs - crs[numpy.minimum(sstart[rb_s], len(crs) - 1)]
     Mrb = numpy.bincount(rb_s, weights=Dl, minlength=nrb).astype(numpy.int64)
     used = numpy.flatnonzero(Mrb > 0)
-    tsz = Mrb * Krb
+    # T3 panel rows padded to a multiple of 4 elements: 16-byte row stride (tensor-map rule)
+    Kp = (Krb + 3) // 4 * 4
+    tsz = Mrb * Kp
     t3pan = numpy.cumsum(tsz) - tsz
     # T3 block -> (panel of its r', row block of its sigma block, column slab of its c)
     spos_by_blk = dict(zip(us.tolist(), range(len(us))))
@@ -214,8 +216,8 @@ def panel_sigma4(t3lay, Rl, psi, t4):
     t3off = numpy.zeros(int(t3lay.nblks), dtype=numpy.int64)
     t3fhs = numpy.zeros(int(t3lay.nblks), dtype=numpy.int64)
     t3flo = numpy.ones(int(t3lay.nblks), dtype=numpy.int64)
-    t3off[i3] = t3pan[rbR] + rowoff[sidx] * Krb[rbR] + koffU[posU[iR]]
-    t3fhs[i3] = Krb[rbR]
+    t3off[i3] = t3pan[rbR] + rowoff[sidx] * Kp[rbR] + koffU[posU[iR]]
+    t3fhs[i3] = Kp[rbR]
     t3flo[i3] = dR[:, 2]                     # fibers (l, r): r is the fast fiber index
     # row table: panel row -> element offset of that row in its sigma block
     crow = numpy.concatenate([psi.ioff[us] [k] + numpy.arange(Dl[k]) * Drb_sec[rb_s[k]] for k in range(len(us))]) \
@@ -224,14 +226,22 @@ def panel_sigma4(t3lay, Rl, psi, t4):
     crow_base[used] = (numpy.cumsum(Mrb) - Mrb)[used]
     rperm = (Rl.ioff[uR], poff[rbU] + koffU * dU[:, 1], dU)
     gemm = (t3pan[used], poff[used], numpy.zeros(len(used), dtype=numpy.int64), Mrb[used], Drb_sec[used],
-            Krb[used], crow_base[used])
+            Krb[used], crow_base[used], Kp[used])
+    # the R panels transposed ([D_r' x K_r'], k contiguous, row stride Kp) for the tensor-core
+    # kernel: R block (c, r', r) element -> rtoff[r'] + r' * Kp + koff + r * D_c + c
+    rtsz = Drb_sec * Kp
+    rtoff = numpy.cumsum(rtsz) - rtsz
+    rperm_t = (Rl.ioff[uR], rtoff[rbU] + koffU, dU, Kp[rbU])
     return {"t3off": t3off, "t3fhs": t3fhs, "t3flo": t3flo, "t3size": int(tsz.sum()), "needed": i3,
-            "rperm": rperm, "gemm": gemm, "crow": crow.astype(numpy.int64)}
+            "rperm": rperm, "gemm": gemm, "crow": crow.astype(numpy.int64),
+            "sectors": {"used": used, "M": Mrb[used], "N": Drb_sec[used], "K": Krb[used], "Kp": Kp[used],
+                        "t3pan": t3pan[used], "rtoff": rtoff[used], "crow_base": crow_base[used]},
+            "rperm_t": rperm_t, "rtsize": int(rtsz.sum())}
 
 
 PTASK_DT = numpy.dtype([("a_off", "<i8"), ("b_off", "<i8"), ("c_off", "<i8"), ("M", "<i4"), ("N", "<i4"),
                         ("K", "<i4"), ("m0", "<i4"), ("n0", "<i4"), ("op_b", "<i4"), ("op_e", "<i4"),
-                        ("crow", "<i4"), ("pad", "<i4", (2,))])
+                        ("crow", "<i4"), ("lda", "<i4"), ("pad", "<i4")])
 assert PTASK_DT.itemsize == 64
 PANEL_TILES = {0: (128, 64), 1: (128, 32), 2: (128, 16)}
 
@@ -248,6 +258,7 @@ def compile_panels(gemm, op_range, tensor_cores=False):
     returned separately as grouped-GEMM work items {TC_CFG: (tasks, contribs, flops)}."""
     a_off, b_off, c_off, M, N, K = (numpy.asarray(x, dtype=numpy.int64) for x in gemm[:6])
     crow = numpy.asarray(gemm[6], dtype=numpy.int64) if len(gemm) > 6 else numpy.full(len(M), -1, dtype=numpy.int64)
+    lda = numpy.asarray(gemm[7], dtype=numpy.int64) if len(gemm) > 7 else K.copy()
     # rows scattered through a row table run on the CUDA-core panel kernel
     tcsel = (M >= 64) & (N > 24) & (K >= 8) & (crow < 0) if tensor_cores else numpy.zeros(len(M), dtype=bool)
     tc = {}
@@ -282,7 +293,7 @@ def compile_panels(gemm, op_range, tensor_cores=False):
         nop = op_range[1] - op_range[0]
         tc[TC_CFG] = (tasks, contribs, 2.0 * float((M[sel] * N[sel] * K[sel]).sum()) * nop)
         keep = numpy.flatnonzero(~tcsel)
-        a_off, b_off, c_off, M, N, K, crow = (x[keep] for x in (a_off, b_off, c_off, M, N, K, crow))
+        a_off, b_off, c_off, M, N, K, crow, lda = (x[keep] for x in (a_off, b_off, c_off, M, N, K, crow, lda))
     cls = panel_class(N)
     out = {}
     for k in numpy.unique(cls):
@@ -301,6 +312,7 @@ def compile_panels(gemm, op_range, tensor_cores=False):
         tasks["n0"] = (loc % nn[pid]) * tn
         tasks["op_b"], tasks["op_e"] = op_range
         tasks["crow"] = crow[g]
+        tasks["lda"] = lda[g]
         nop = op_range[1] - op_range[0]
         out[int(k)] = (tasks, 2.0 * float((M[sel] * N[sel] * K[sel]).sum()) * nop)
     if tensor_cores:
@@ -794,3 +806,101 @@ def fiber_stages(parts, device, name, ops):
     for p in parts:
         by.setdefault(p[6], []).append(p)
     return [FiberStage(v, device, name, ops) for k, v in sorted(by.items())]
+
+
+# ---------------------------------------------------------------- tensor-core panel GEMM (qc_tcpanel_f32)
+TCUNIT_DT = numpy.dtype([("a_map", "<i4"), ("b_map", "<i4"), ("a_c1", "<i4"), ("b_c1", "<i4"), ("a_c2", "<i4"),
+                         ("b_c2", "<i4"), ("nk", "<i4"), ("m_valid", "<i4"), ("n_valid", "<i4"), ("op", "<i4"),
+                         ("pad0", "<i4"), ("pad1", "<i4"), ("c_off", "<i8"), ("pad2", "<i8")])
+TMDESC_DT = numpy.dtype([("addr", "<i8"), ("rank", "<i4"), ("swizzle", "<i4"), ("dims", "<i8", (5,)),
+                         ("strides", "<i8", (4,)), ("box", "<i4", (5,)), ("pad", "<i4")])
+assert TCUNIT_DT.itemsize == 64 and TMDESC_DT.itemsize == 112
+TC_BM, TC_BN, TC_BK = 128, 128, 32
+SWIZZLE_128B = 3
+
+
+class TCPanelStage(object):
+    """Panel GEMMs C[rows] = A . B^T on the tensor cores (split TF32), A and B read by TMA.
+
+    maps: list of (operand, element offset, dims, element strides of dims 1.., box) with
+    operand "A" (the raw FP32 buffer passed to run) or "B" (the pre-split hi/lo buffer);
+    units: TCUNIT_DT records indexing those maps, the stage's operator table and row table.
+    The tensor maps embed buffer addresses: they are encoded on the host whenever run sees
+    buffers other than the last ones."""
+
+    def __init__(self, name, units, maps, ops, crow, flops, device):
+        self.name = name
+        self.h_units = units
+        self.d_units = upload(units, device)
+        self.map_specs = maps
+        self.d_ops = upload(ops, device)
+        self.host_ops = ops
+        self.d_crow = torch.from_numpy(numpy.ascontiguousarray(crow, dtype=numpy.int64)).to(device)
+        self.flops = flops
+        self.bytes = 0.0
+        self.ntasks = len(units)
+        self.device = device
+        self._key = None
+        self._maps = None
+
+    def maps(self, A, B):
+        key = (A.data_ptr(), B.data_ptr())
+        if key != self._key:
+            d = numpy.zeros(len(self.map_specs), TMDESC_DT)
+            for i, (which, off, dims, strides, box) in enumerate(self.map_specs):
+                base = A if which == "A" else B
+                d[i]["addr"] = base.data_ptr() + 4 * int(off)
+                d[i]["rank"] = len(dims)
+                d[i]["swizzle"] = SWIZZLE_128B
+                d[i]["dims"][:len(dims)] = dims
+                d[i]["strides"][:len(strides)] = [4 * int(x) for x in strides]
+                d[i]["box"][:len(box)] = box
+            out = numpy.zeros(max(len(d), 1) * 128, dtype=numpy.uint8)
+            check(native.lib().qc_tmap_encode(len(d), d.ctypes.data, out.ctypes.data), "qc_tmap_encode")
+            self._maps = torch.from_numpy(out).to(self.device)
+            self._key = key
+        return self._maps
+
+    def run(self, A, B, C, kind="tf32x3", stream=None):
+        if self.ntasks == 0:
+            return
+        lib = native.lib()
+        s = stream if stream is not None else torch.cuda.current_stream(C.device).cuda_stream
+        maps = self.maps(A, B)
+        if LOG.enabled:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+        check(lib.qc_tcpanel_f32(self.d_units.data_ptr(), self.ntasks, maps.data_ptr(), self.d_ops.data_ptr(),
+                                 self.d_crow.data_ptr(), C.data_ptr(), s), "qc_tcpanel_f32")
+        LOG.launches += 1
+        if LOG.enabled:
+            e1.record()
+            LOG.records.append((self.name, e0, e1, self.flops, self.bytes * 0.5))
+
+
+def tc_sigma4_units(classes, order_pos, t3_base_of_class, rt_base_of_class, rt_opstride, rt_total):
+    """Work units and tensor maps of the .R contraction on the tensor cores.
+
+    classes: list of (op positions in the stage's operator table, pan4 sectors dict, T3 op stride).
+    Unit order: per operator and sector all row tiles back to back (they share the R panel)."""
+    units, maps = [], []
+    for ci, (poss, sec, t3stride) in enumerate(classes):
+        nops = len(poss)
+        amap0 = len(maps)
+        for j in range(len(sec["used"])):
+            K, M, N, Kp = int(sec["K"][j]), int(sec["M"][j]), int(sec["N"][j]), int(sec["Kp"][j])
+            maps.append(("A", t3_base_of_class[ci] + int(sec["t3pan"][j]), (K, M, nops), (Kp, t3stride),
+                         (TC_BK, TC_BM, 1)))
+            maps.append(("B", rt_base_of_class[ci] + int(sec["rtoff"][j]), (K, N, nops, 2),
+                         (Kp, rt_opstride[ci], rt_total), (TC_BK, TC_BN, 1, 2)))
+        for q, pos in enumerate(poss):
+            for j in range(len(sec["used"])):
+                K, M, N = int(sec["K"][j]), int(sec["M"][j]), int(sec["N"][j])
+                for n0 in range(0, N, TC_BN):
+                    for m0 in range(0, M, TC_BM):
+                        units.append((amap0 + 2 * j, amap0 + 2 * j + 1, m0, n0, q, q, (K + TC_BK - 1) // TC_BK,
+                                      min(TC_BM, M - m0), min(TC_BN, N - n0), pos, 0, 0,
+                                      int(sec["crow_base"][j]) + m0, 0))
+    u = numpy.array(units, dtype=TCUNIT_DT) if units else numpy.zeros(0, TCUNIT_DT)
+    return u, maps

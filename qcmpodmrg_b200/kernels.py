@@ -112,6 +112,14 @@ def convert(src, out):
     return out
 
 
+def tf32_split(hi, lo):
+    """hi = tf32(x), lo = tf32(x - hi) for the FP32 values x held in hi (qc_tf32_split)."""
+    check(native.lib().qc_tf32_split(hi.data_ptr(), lo.data_ptr(), hi.numel(), _stream(hi.device)),
+          "qc_tf32_split")
+    LOG.launches += 1
+    return hi, lo
+
+
 def reduce_ops(part, nops, n, out):
     """out = sum over operators of the per-operator partial vectors (qc_reduce_ops_*)."""
     lib = native.lib()
@@ -159,6 +167,11 @@ class SigmaOperator(object):
         self.ws, self.psi, self.precision = ws, psi_layout, precision
         # tcgen05 tiles for the two large contractions (L.psi and .R) in TF32 modes
         tc = (precision in ("tf32", "tf32x3")) if tensor_cores is None else tensor_cores
+        # tf32x3: the .R panel GEMMs on the TMA-fed tcgen05 kernel (qc_tcpanel_f32); the older
+        # gathered tensor-core tiles (qc_bgemm_tf32*) stay for plain tf32 and explicit requests
+        want_tc4 = precision == "tf32x3" and tensor_cores is None and use_fiber and panel4
+        if want_tc4:
+            tc = False
         self.L, self.R, self.Wi, self.Wj = L, R, Wi, Wj
         self._lays = (list(L.layouts), list(R.layouts))      # held: identity is the plan's key
         dev = ws.device
@@ -221,6 +234,7 @@ class SigmaOperator(object):
                 size = pan["t1size"] if (s == 0 and pan is not None) else c.out.size
                 if s == 2 and pan4 is not None:
                     size = pan4["t3size"]
+                size = (int(size) + 31) // 32 * 32      # 128-byte aligned operator slices (TMA)
                 for i in ops:
                     bases[s][i] = tot[s]
                     tot[s] += size
@@ -253,6 +267,7 @@ class SigmaOperator(object):
         rperm = []
         p4st, p4st_tc = {}, {}          # panel GEMM parts of the .R contraction
         crow_all, crow_n = [], 0        # their row table (panel row -> sigma element offset)
+        tc4_classes = []                # (operator range, pan4, row-table base) for the tensor-core .R
         any4 = any(v[8] is not None for v in plans.values())
         for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
             rng = (pos, pos + len(ops))
@@ -289,7 +304,9 @@ class SigmaOperator(object):
                 rperm.append(d)
             if pan4 is not None:
                 g4 = pan4["gemm"]
-                g4 = g4[:6] + (g4[6] + crow_n,)          # row-table indices into the stage's table
+                g4 = g4[:6] + (g4[6] + crow_n,) + tuple(g4[7:])     # row-table indices into the stage's table
+                if want_tc4:
+                    tc4_classes.append((rng, pan4, crow_n))
                 crow_all.append(pan4["crow"])
                 crow_n += len(pan4["crow"])
                 parts = compile_panels(g4, rng, tensor_cores=bool(tc))
@@ -361,6 +378,12 @@ class SigmaOperator(object):
             self._rperm_ops_d = upload(rops, dev)
             self._rperm_span = int(max(len(v[0]) for v in plans.values()))
             self._build_rpan()
+        # the .R contraction on the tensor cores: R panels transposed and split into TF32
+        # hi / lo planes once per dot, T3 read raw by TMA and split in the kernel
+        self.tc4 = None
+        if tc4_classes:
+            self._setup_tc4(tc4_classes, order, bases[2], R, st4_ops=tabs[3],
+                            crow=numpy.concatenate(crow_all) if crow_all else numpy.zeros(1, numpy.int64))
         # fused W stage (T1 -> T3) and the per-dot two-site MPO blocks it reads
         self.fused = None
         self.wtot = wtot
@@ -397,6 +420,8 @@ class SigmaOperator(object):
                 fb += stage_bytes(fused[1], fused[2], len(ops), False)
         if self.fused is not None:
             self.fused.bytes = float(fb)
+        if self.tc4 is not None:
+            self.tc4.bytes = self.stages[3].bytes
         # FLOPs of the reference's four-contraction chain (tensordotCAL pair GEMMs),
         # whatever the fusion used here
         self.flops = 0.0
@@ -416,6 +441,55 @@ class SigmaOperator(object):
             self._build_lpan()
         if self.rperm is not None:
             self._build_rpan()
+        if self.tc4 is not None:
+            self._build_rpan_tc()
+
+    def _setup_tc4(self, tc4_classes, order, t3bases, R, st4_ops, crow):
+        from .engine import TCPanelStage, tc_sigma4_units
+        dev = self.ws.device
+        classes, t3b, rtb, rts, descs = [], [], [], [], []
+        rt_tot = 0
+        flops = 0.0
+        for (rng, pan4, crow_n) in tc4_classes:
+            sec = dict(pan4["sectors"])
+            sec["crow_base"] = sec["crow_base"] + crow_n
+            ops_c = order[rng[0]:rng[1]]
+            t3stride = int(t3bases[ops_c[1]] - t3bases[ops_c[0]]) if len(ops_c) > 1 else \
+                (int(pan4["t3size"]) + 31) // 32 * 32
+            opstride = (int(pan4["rtsize"]) + 31) // 32 * 32
+            classes.append((list(range(rng[0], rng[1])), sec, t3stride))
+            t3b.append(int(t3bases[ops_c[0]]))
+            rtb.append(rt_tot)
+            rts.append(opstride)
+            src, dst, dU, kp = pan4["rperm_t"]
+            d = numpy.zeros(len(src), BPERM_DT)
+            d["src_off"], d["dst_off"] = src, dst
+            d["d0"], d["d1"], d["d2"] = dU[:, 0], dU[:, 1], dU[:, 2]
+            d["s0"], d["s1"], d["s2"] = 1, kp, dU[:, 0]
+            d["op_b"], d["op_e"] = rng
+            descs.append(d)
+            rt_tot += opstride * len(ops_c)
+            flops += 2.0 * float((sec["M"] * sec["N"] * sec["K"]).sum()) * len(ops_c)
+        rt_tot = (rt_tot + 31) // 32 * 32
+        units, maps = tc_sigma4_units(classes, None, t3b, rtb, rts, rt_tot)
+        self.tc4 = TCPanelStage("sigma4", units, maps, st4_ops, crow, flops, dev)
+        self._rt_total = rt_tot
+        self._rt_descs = numpy.concatenate(descs)
+        self._rt_descs_d = upload(self._rt_descs, dev)
+        base = numpy.zeros(len(order), dtype=numpy.int64)
+        for (poss, sec, _), b0, st in zip(classes, rtb, rts):
+            base[poss] = b0 + st * numpy.arange(len(poss))
+        self._rt_ops_d = upload(op_table(R.offsets[order], 0, base, 1.0), dev)
+        self._rt_span = int(max(len(c[0]) for c in classes))
+        self._build_rpan_tc()
+
+    def _build_rpan_tc(self):
+        """R panels of the tensor-core .R kernel: [D_r' x K_r'] per sector, FP32 hi plane then lo plane."""
+        n = self._rt_total
+        self.rpan_tc = torch.zeros(2 * max(n, 1), dtype=torch.float32, device=self.ws.device)
+        block_permute(self._rt_descs_d, len(self._rt_descs), self._rt_span, self._rt_ops_d, self.R.values,
+                      self.rpan_tc)
+        tf32_split(self.rpan_tc[:n], self.rpan_tc[n:2 * n])
 
     def _build_rpan(self):
         self.Rpan = torch.empty(max(self.R.total, 1), dtype=torch.float64, device=self.ws.device)
@@ -459,6 +533,7 @@ class SigmaOperator(object):
         self.L = self.R = None
         self.Lpan = self._Lpan32 = None
         self.Rpan = self._Rpan32 = None
+        self.rpan_tc = None
 
     def wij32(self):
         if self._Wij32 is None:
@@ -497,6 +572,8 @@ class SigmaOperator(object):
             walk(st, si)
             if si == 1:
                 walk(self.fused, 1, native.GROUP_FIBER)
+            if si == 3 and self.tc4 is not None:
+                out.append((3, native.GROUP_PANEL, self.tc4.d_units.data_ptr(), self.tc4.ntasks, 1, 0, 0))
         return out
 
     def __call__(self, x, y=None, precision=None):
@@ -537,7 +614,10 @@ class SigmaOperator(object):
         if self.fused is not None:
             self.fused.run(T1, self.wij32(), T3, "f32")
         P[:self.nops * self.ndim0].zero_()
-        s[3].run(T3, self.b4("f32"), P, kind)
+        if self.tc4 is not None and kind == "tf32x3":
+            self.tc4.run(T3, self.rpan_tc, P)
+        else:
+            s[3].run(T3, self.b4("f32"), P, kind)
         reduce_ops(P, self.nops, self.ndim0, y32)
         convert(y32, y)
         return y

@@ -69,6 +69,10 @@ _SIGS = {
     "qc_scatter_f64": (c_int, [c_vp, c_vp, c_vp, c_ll, c_ll, c_vp]),
     "qc_convert_f64_to_f32": (c_int, [c_vp, c_vp, c_ll, c_vp]),
     "qc_convert_f32_to_f64": (c_int, [c_vp, c_vp, c_ll, c_vp]),
+    "qc_tmap_encode": (c_int, [c_int, c_vp, c_vp]),
+    "qc_tcpanel_f32": (c_int, [c_vp, c_ll, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "qc_tf32_split": (c_int, [c_vp, c_vp, c_ll, c_vp]),
+    "qc_tcpanel_status": (c_int, [c_int]),
 }
 
 

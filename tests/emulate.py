@@ -56,7 +56,8 @@ def patch_stage_run(monkeypatch):
                 for op in range(t["op_b"], t["op_e"]):
                     o = self.host_ops[op]
                     M, N, K = int(t["M"]), int(t["N"]), int(t["K"])
-                    Am = a[o["a_base"] + t["a_off"]:][:M * K].reshape(M, K)
+                    lda = int(t["lda"]) or K
+                    Am = a[o["a_base"] + t["a_off"] + numpy.arange(M)[:, None] * lda + numpy.arange(K)[None, :]]
                     Bm = b[o["b_base"] + t["b_off"]:][:K * N].reshape(K, N)
                     m1, n1 = min(M, t["m0"] + tm), min(N, t["n0"] + tn)
                     blk = o["alpha"] * (Am[t["m0"]:m1] @ Bm[:, t["n0"]:n1])
@@ -113,6 +114,21 @@ def patch_stage_run(monkeypatch):
     monkeypatch.setattr(kernels, "reduce_ops", reduce_ops)
     monkeypatch.setattr(kernels, "convert", convert)
 
+    def tf32_split(hi, lo):          # exact in the interpreter: hi keeps x, lo = 0
+        lo.zero_()
+        return hi, lo
+
+    monkeypatch.setattr(kernels, "tf32_split", tf32_split)
+
+    def tcrun(self, A, B, C, kind="tf32x3", stream=None):
+        a = _f64(A)
+        b = _f64(B)
+        c = _f64(C)
+        _run_tcpanel(self, a, b, c)
+        C.copy_(torch.from_numpy(c).to(C.dtype))
+
+    monkeypatch.setattr(engine.TCPanelStage, "run", tcrun)
+
 
 def _run_fiber(st, A, W, C):
     """Reference semantics of k_fiber: out[f, c] = alpha * sum_pairs sum_r in[r, f] * W[r, c]."""
@@ -162,3 +178,25 @@ def _run_tiled(tasks, contribs, ops, summed, A, B, C, tm, tn):
             co = cbase + t["c_off"] + _idx(ms, t["mlo"], t["c_mh"], t["c_ml"])[:, None] + \
                 _idx(ns, t["nlo"], t["c_nh"], t["c_nl"])[None, :]
             C[co] = acc
+
+
+def _run_tcpanel(st, A, B, C):
+    """Reference semantics of qc_tcpanel_f32: per unit, C[row table rows, n0 + n] = alpha * A . B^T,
+    A and B addressed through the unit's tensor-map specifications (B as hi + lo planes)."""
+    for u in st.h_units:
+        wa, offa, dima, stra, _ = st.map_specs[int(u["a_map"])]
+        wb, offb, dimb, strb, _ = st.map_specs[int(u["b_map"])]
+        assert wa == "A" and wb == "B"
+        K = int(dima[0])
+        assert int(dimb[0]) == K
+        m = int(u["a_c1"]) + numpy.arange(int(u["m_valid"]))
+        n = int(u["b_c1"]) + numpy.arange(int(u["n_valid"]))
+        assert m.max() < dima[1] and n.max() < dimb[1] and u["a_c2"] < dima[2] and u["b_c2"] < dimb[2]
+        k = numpy.arange(K)
+        ia = offa + int(u["a_c2"]) * stra[1] + m[:, None] * stra[0] + k[None, :]
+        ib = offb + int(u["b_c2"]) * strb[1] + n[:, None] * strb[0] + k[None, :]
+        bm = B[ib] + B[ib + strb[2]]
+        o = st.host_ops[int(u["op"])]
+        rows = st.d_crow.cpu().numpy()[int(u["c_off"]) + numpy.arange(int(u["m_valid"]))] + int(u["b_c1"])
+        idx = o["c_base"] + rows[:, None] + numpy.arange(int(u["n_valid"]))[None, :]
+        C[idx] = o["alpha"] * (A[ia] @ bm.T)

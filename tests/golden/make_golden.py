@@ -5,6 +5,7 @@ and the reference's sources (environment QCMPODMRG_REFERENCE); run where they ar
 
     python tests/golden/make_golden.py            # small fixtures (seconds)
     python tests/golden/make_golden.py --config1  # K=12, N=12, D=100, 6 sweeps (~30 min CPU)
+    python tests/golden/make_golden.py --config1-converged   # the same to convergence (hours of CPU)
     python tests/golden/make_golden.py --spin     # spin-projected K=4 / K=5 runs (minutes)
     python tests/golden/make_golden.py --noise    # K=5 / K=6 runs with the pRDM noise term
     python tests/golden/make_golden.py --sliced   # K=5 run with the MPO bond in 3 slices (maxslc=3)
@@ -53,13 +54,15 @@ def qsym_cases(seed=7):
 
 
 def run_case(tag, K, N, D, nsweeps, seed, decay, targets, record_envs=True, npts=None, noise=0.0,
-             quad="GaussLegendre", maxslc=1):
+             quad="GaussLegendre", maxslc=1, tol=1.e-7):
     res, rec = rr.run_reference(K=K, N=N, D=D, nsweeps=nsweeps, seed=seed, decay=decay, targets=targets,
-                                record_envs=record_envs, npts=npts, noise=noise, quad=quad, maxslc=maxslc)
+                                record_envs=record_envs, npts=npts, noise=noise, quad=quad, maxslc=maxslc,
+                                tol=tol)
     sweep = {"K": K, "N": N, "D": D, "seed": seed, "decay": -1.0 if decay is None else float(decay),
              "nsweeps": nsweeps, "eav": res["eav"], "dwt": res["dwt"], "esweeps": res["esweeps"],
              "nmvp": res["nmvp"], "init_mps": {k: v for k, v in res["init_mps"].items() if k != "nsite"},
-             "npts": 0 if npts is None else int(npts), "noise": float(noise), "quad": quad, "maxslc": maxslc}
+             "npts": 0 if npts is None else int(npts), "noise": float(noise), "quad": quad, "maxslc": maxslc,
+             "tol": float(tol)}
     fixtures.save(os.path.join(HERE, "sweep_%s.npz" % tag), sweep)
     if targets:
         recs = []
@@ -78,6 +81,8 @@ def run_case(tag, K, N, D, nsweeps, seed, decay, targets, record_envs=True, npts
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--config1", action="store_true")
+    ap.add_argument("--config1-converged", action="store_true",
+                    help="K=12, N=12, D=100 to convergence (Davidson and sweep tolerance 1e-9, up to 16 sweeps)")
     ap.add_argument("--spin", action="store_true", help="only the spin-projected (SP-MPS) fixtures")
     ap.add_argument("--noise", action="store_true", help="only the fixtures with the pRDM noise term")
     ap.add_argument("--sliced", action="store_true", help="only the run with the MPO bond cut into slices")
@@ -102,6 +107,9 @@ if __name__ == "__main__":
         sys.exit(0)
     if a.config1:
         run_case("C1", 12, 12, 100, 6, 1, None, [], record_envs=False)
+        sys.exit(0)
+    if a.config1_converged:
+        run_case("C1C", 12, 12, 100, 16, 1, None, [], record_envs=False, tol=1.e-9)
         sys.exit(0)
     qsym_cases()
     run_case("K4", 4, 4, 16, 2, 1, None, [(0, "R", 1), (0, "L", 1), (0, "R", 0), (0, "L", 2), (1, "R", 2)])
