@@ -118,8 +118,10 @@ static_assert(sizeof(qc_ptask) == 64, "qc_ptask is 64 bytes");
 //   C[row(m), n0 + n] = alpha * sum_k A[m, k] * B[n0 + n, k]    (m < m_valid, n < n_valid)
 // A and B are read by TMA through tensor maps (maps[a_map], maps[b_map]) of this GPU's
 // own buffers: A rows a_c1 .. a_c1+127 of operator slice a_c2, B rows b_c1 .. of slice
-// b_c2, both K-major (k contiguous), nk stages of 32 k.  Epilogue: row m goes to
-// C + ops[op].c_base + crow[c_off + m] + b_c1 (rows scattered through a row table).
+// b_c2, both K-major (k contiguous), nk stages of 32 k.  Epilogue, row-table form: row m
+// goes to C + ops[op].c_base + crow[c_off + m] + b_c1 (rows scattered through a row table);
+// segment form: the tile's columns are nseg segments (qc_tcseg records from c_off), column
+// c of segment s and tile row m going to C + c_base + seg.off + (a_c1 + m) * seg.ldc + c - seg.col0.
 struct alignas(16) qc_tcunit {
   int a_map, b_map;
   int a_c1, b_c1;
@@ -128,10 +130,19 @@ struct alignas(16) qc_tcunit {
   int m_valid;
   int n_valid;
   int op;
-  int pad0, pad1;
+  int nseg, pad1;
   long long c_off;
   long long pad2;
 };
+
+struct alignas(16) qc_tcseg {
+  long long off;       // element offset (relative to the operator's C base) of the segment's row 0
+  int col0;            // first tile column of the segment
+  int ncol;            // columns of the segment
+  int ldc;             // row stride of the segment's destination
+  int pad0, pad1, pad2;
+};
+static_assert(sizeof(qc_tcseg) == 32, "qc_tcseg is 32 bytes");
 static_assert(sizeof(qc_tcunit) == 64, "qc_tcunit is 64 bytes");
 
 // One tensor map to encode on the host (cuTensorMapEncodeTiled, FP32 elements).

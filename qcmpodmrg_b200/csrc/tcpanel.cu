@@ -137,11 +137,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
 template <int BN>
 __host__ __device__ constexpr int stage_bytes() { return 2 * TP_BM * TP_BK * 4 + 2 * BN * TP_BK * 4; }
 
-template <bool A_SPLIT, int BN, int S>
+constexpr int EPI_ROWS = 0;       // rows through a row table, stored from registers
+constexpr int EPI_SEGMENTS = 1;   // column segments, staged in shared memory, coalesced stores
+constexpr int EPI_HALF = 64;      // columns staged at a time (segment form)
+
+template <bool A_SPLIT, int BN, int S, int EPI>
 __global__ void __launch_bounds__(TP_THREADS, 1)
 k_tcpanel(const qc_tcunit *__restrict__ units, int nunits, const CUtensorMap *__restrict__ maps,
-          const qc_op *__restrict__ ops, const long long *__restrict__ crow, float *__restrict__ C,
-          int *__restrict__ err) {
+          const qc_op *__restrict__ ops, const long long *__restrict__ crow, const qc_tcseg *__restrict__ segs,
+          float *__restrict__ C, int *__restrict__ err) {
   static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N");
   extern __shared__ unsigned char tp_smem_raw[];
   // stage s: [A0 (raw / hi) | A1 (lo) | B0 (hi) | B1 (lo)], each 1024-byte aligned
@@ -315,17 +319,49 @@ k_tcpanel(const qc_tcunit *__restrict__ units, int nunits, const CUtensorMap *__
       const int row = q * 32 + lane;
       const qc_op o = ops[t.op];
       const float alpha = (float)o.alpha;
-      float *dst = nullptr;
-      if (row < t.m_valid) dst = C + o.c_base + crow[t.c_off + row] + t.b_c1;
       const int ncol = t.n_valid < BN ? t.n_valid : BN;
       const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * BN);
-      for (int c0 = 0; c0 < ncol; c0 += 16) {
-        uint32_t r[16];
-        tmem_ld16(taddr + (uint32_t)c0, r);
-        if (dst) {
+      if (EPI == EPI_ROWS) {
+        float *dst = nullptr;
+        if (row < t.m_valid) dst = C + o.c_base + crow[t.c_off + row] + t.b_c1;
+        for (int c0 = 0; c0 < ncol; c0 += 16) {
+          uint32_t r[16];
+          tmem_ld16(taddr + (uint32_t)c0, r);
+          if (dst) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j)
-            if (c0 + j < ncol) dst[c0 + j] = alpha * __uint_as_float(r[j]);
+            for (int j = 0; j < 16; ++j)
+              if (c0 + j < ncol) dst[c0 + j] = alpha * __uint_as_float(r[j]);
+          }
+        }
+      } else {
+        // stage EPI_HALF columns of the tile in shared memory (row stride EPI_HALF + 1: no bank
+        // conflicts), then copy every segment's rows with consecutive threads on consecutive
+        // columns: a segment's rows are contiguous in memory when it spans its row stride
+        float *stg = reinterpret_cast<float *>(smem + S * ST_BYTES);
+        float *Cb = C + o.c_base;
+        for (int h0 = 0; h0 < ncol; h0 += EPI_HALF) {
+          for (int c0 = 0; c0 < EPI_HALF && h0 + c0 < ncol; c0 += 16) {
+            uint32_t r[16];
+            tmem_ld16(taddr + (uint32_t)(h0 + c0), r);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) stg[row * (EPI_HALF + 1) + c0 + j] = alpha * __uint_as_float(r[j]);
+          }
+          asm volatile("bar.sync 1, 128;" ::: "memory");
+          const int hw = (ncol - h0) < EPI_HALF ? (ncol - h0) : EPI_HALF;
+          for (int si = 0; si < t.nseg; ++si) {
+            const qc_tcseg sg = segs[t.c_off + si];
+            const int c_lo = sg.col0 > h0 ? sg.col0 : h0;
+            const int c_hi = (sg.col0 + sg.ncol) < (h0 + hw) ? (sg.col0 + sg.ncol) : (h0 + hw);
+            const int w = c_hi - c_lo;
+            if (w <= 0) continue;
+            const int total = t.m_valid * w;
+            float *db = Cb + sg.off + (long long)t.a_c1 * sg.ldc + (c_lo - sg.col0);
+            for (int i = hid; i < total; i += 128) {
+              const int m = i / w, c = i - m * w;
+              db[(long long)m * sg.ldc + c] = stg[m * (EPI_HALF + 1) + (c_lo - h0) + c];
+            }
+          }
+          asm volatile("bar.sync 1, 128;" ::: "memory");
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -351,6 +387,18 @@ __global__ void k_tf32_split(float *__restrict__ hi, float *__restrict__ lo, lon
   }
 }
 
+// hi[i] = tf32(x[idx[i]]), lo[i] = tf32(x[idx[i]] - hi[i]) (FP64 source; idx < 0: zero)
+__global__ void k_gather_split(const double *__restrict__ x, const long long *__restrict__ idx, long long n,
+                               float *__restrict__ hi, float *__restrict__ lo) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long j = idx[i];
+    const float v = j >= 0 ? (float)x[j] : 0.f;
+    const float h = tf32_rna(v);
+    hi[i] = h;
+    lo[i] = tf32_rna(v - h);
+  }
+}
+
 int *g_tp_err = nullptr;
 int g_nsm = 0;
 std::mutex g_tp_mu;
@@ -358,7 +406,44 @@ PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
 constexpr int TP_BN = 128;
 constexpr int TP_S = 3;
-constexpr size_t tp_dsmem() { return (size_t)TP_S * stage_bytes<TP_BN>() + 1024; }
+constexpr size_t tp_dsmem(int epi) {
+  return (size_t)TP_S * stage_bytes<TP_BN>() + 1024 + (epi == EPI_SEGMENTS ? TP_BM * (EPI_HALF + 1) * 4 : 0);
+}
+bool g_attr[2] = {false, false};
+
+template <bool A_SPLIT, int EPI>
+int launch_tcpanel(const void *units, long long nunits, const void *maps, const void *ops, const long long *crow,
+                   const void *segs, float *C, cudaStream_t s) {
+  if (nunits <= 0) return QC_OK;
+  if (nunits > 0x7fffffffLL || !units || !maps || !ops || !C) return QC_ERR_ARG;
+  if ((EPI == EPI_ROWS && !crow) || (EPI == EPI_SEGMENTS && !segs)) return QC_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lock(g_tp_mu);
+    if (!g_tp_err) {
+      if (cudaMalloc(&g_tp_err, sizeof(int)) != cudaSuccess) return QC_ERR_CUDA;
+      if (cudaMemset(g_tp_err, 0, sizeof(int)) != cudaSuccess) return QC_ERR_CUDA;
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&g_nsm, cudaDevAttrMultiProcessorCount, dev);
+    }
+    if (!g_attr[EPI]) {
+      if (cudaFuncSetAttribute(k_tcpanel<A_SPLIT, TP_BN, TP_S, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)tp_dsmem(EPI)) != cudaSuccess)
+        return QC_ERR_CUDA;
+      g_attr[EPI] = true;
+    }
+  }
+  const int grid = (int)(nunits < (long long)g_nsm ? nunits : (long long)g_nsm);
+  k_tcpanel<A_SPLIT, TP_BN, TP_S, EPI><<<grid, TP_THREADS, tp_dsmem(EPI), s>>>(
+      (const qc_tcunit *)units, (int)nunits, (const CUtensorMap *)maps, (const qc_op *)ops, crow,
+      (const qc_tcseg *)segs, C, g_tp_err);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "[qcgpu] qc_tcpanel: %s\n", cudaGetErrorString(e));
+    return QC_ERR_CUDA;
+  }
+  return QC_OK;
+}
 
 }  // namespace
 
@@ -412,32 +497,13 @@ extern "C" int qc_tmap_encode(int n, const void *descs, void *out_maps) {
 // in the kernel, B given as pre-split hi/lo planes (maps of rank 4, plane dimension last).
 extern "C" int qc_tcpanel_f32(const void *units, long long nunits, const void *maps, const void *ops,
                               const long long *crow, float *C, void *stream) {
-  if (nunits <= 0) return QC_OK;
-  if (nunits > 0x7fffffffLL || !units || !maps || !ops || !crow || !C) return QC_ERR_ARG;
-  cudaStream_t s = (cudaStream_t)stream;
-  {
-    std::lock_guard<std::mutex> lock(g_tp_mu);
-    if (!g_tp_err) {
-      if (cudaMalloc(&g_tp_err, sizeof(int)) != cudaSuccess) return QC_ERR_CUDA;
-      if (cudaMemset(g_tp_err, 0, sizeof(int)) != cudaSuccess) return QC_ERR_CUDA;
-      int dev = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&g_nsm, cudaDevAttrMultiProcessorCount, dev);
-      if (cudaFuncSetAttribute(k_tcpanel<true, TP_BN, TP_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)tp_dsmem()) != cudaSuccess)
-        return QC_ERR_CUDA;
-    }
-  }
-  const int grid = (int)(nunits < (long long)g_nsm ? nunits : (long long)g_nsm);
-  k_tcpanel<true, TP_BN, TP_S><<<grid, TP_THREADS, tp_dsmem(), s>>>(
-      (const qc_tcunit *)units, (int)nunits, (const CUtensorMap *)maps, (const qc_op *)ops, crow, C, g_tp_err);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) {
-    g_tperr = cudaGetErrorString(e);
-    fprintf(stderr, "[qcgpu] qc_tcpanel_f32: %s\n", g_tperr.c_str());
-    return QC_ERR_CUDA;
-  }
-  return QC_OK;
+  return launch_tcpanel<true, EPI_ROWS>(units, nunits, maps, ops, crow, nullptr, C, (cudaStream_t)stream);
+}
+
+// Column segments of C = A . B^T on the tensor cores, both operands pre-split hi/lo planes.
+extern "C" int qc_tcpanel_seg_f32(const void *units, long long nunits, const void *maps, const void *ops,
+                                  const void *segs, float *C, void *stream) {
+  return launch_tcpanel<false, EPI_SEGMENTS>(units, nunits, maps, ops, nullptr, segs, C, (cudaStream_t)stream);
 }
 
 extern "C" int qc_tf32_split(float *hi, float *lo, long long n, void *stream) {
@@ -446,6 +512,16 @@ extern "C" int qc_tf32_split(float *hi, float *lo, long long n, void *stream) {
   long long blocks = (n + 255) / 256;
   if (blocks > 65535) blocks = 65535;
   k_tf32_split<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(hi, lo, n);
+  return cudaGetLastError() == cudaSuccess ? QC_OK : QC_ERR_CUDA;
+}
+
+extern "C" int qc_gather_split_f32(const double *x, const long long *idx, long long n, float *hi, float *lo,
+                                   void *stream) {
+  if (n <= 0) return QC_OK;
+  if (!x || !idx || !hi || !lo) return QC_ERR_ARG;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 65535) blocks = 65535;
+  k_gather_split<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(x, idx, n, hi, lo);
   return cudaGetLastError() == cudaSuccess ? QC_OK : QC_ERR_CUDA;
 }
 

@@ -137,8 +137,16 @@ def panel_sigma1(Ll, psi, t1, nblks_out):
     posP[up] = numpy.arange(len(up))
     t1off = numpy.zeros(int(nblks_out), dtype=numpy.int64)
     t1off[ob] = t1pan[posP[ip]] + rowoff[posL[iL]] * Nj[posP[ip]]
+    # tensor-core form: the L panels with rows padded to Kp (16-byte stride), [M x Kp] per sector
+    Kp_sec = (Dk_sec + 3) // 4 * 4
+    tsz = M_lk * Kp_sec
+    tpoff = numpy.cumsum(tsz) - tsz
+    secs = numpy.unique(lkp)
+    tc = {"sectors": secs, "M": M_lk[secs], "K": Dk_sec[secs], "Kp": Kp_sec[secs], "lpoff": tpoff[secs],
+          "lpsize": int(tsz.sum()), "lperm_t": (lperm_src, tpoff[lkL] + rowoff * Kp_sec[lkL], dL, Kp_sec[lkL]),
+          "blocks": up, "t1pan": t1pan, "Nj": Nj}
     return {"lperm": (lperm_src, lperm_dst, lperm_n), "t1off": t1off, "t1size": int(psz.sum()),
-            "gemm": (pan_off[lkp], psi.ioff[up], t1pan, Mj, Nj, Kj)}
+            "gemm": (pan_off[lkp], psi.ioff[up], t1pan, Mj, Nj, Kj), "tc": tc}
 
 
 def panel_sigma4(t3lay, Rl, psi, t4):
@@ -811,10 +819,11 @@ def fiber_stages(parts, device, name, ops):
 # ---------------------------------------------------------------- tensor-core panel GEMM (qc_tcpanel_f32)
 TCUNIT_DT = numpy.dtype([("a_map", "<i4"), ("b_map", "<i4"), ("a_c1", "<i4"), ("b_c1", "<i4"), ("a_c2", "<i4"),
                          ("b_c2", "<i4"), ("nk", "<i4"), ("m_valid", "<i4"), ("n_valid", "<i4"), ("op", "<i4"),
-                         ("pad0", "<i4"), ("pad1", "<i4"), ("c_off", "<i8"), ("pad2", "<i8")])
+                         ("nseg", "<i4"), ("pad1", "<i4"), ("c_off", "<i8"), ("pad2", "<i8")])
 TMDESC_DT = numpy.dtype([("addr", "<i8"), ("rank", "<i4"), ("swizzle", "<i4"), ("dims", "<i8", (5,)),
                          ("strides", "<i8", (4,)), ("box", "<i4", (5,)), ("pad", "<i4")])
-assert TCUNIT_DT.itemsize == 64 and TMDESC_DT.itemsize == 112
+TCSEG_DT = numpy.dtype([("off", "<i8"), ("col0", "<i4"), ("ncol", "<i4"), ("ldc", "<i4"), ("pad", "<i4", (3,))])
+assert TCUNIT_DT.itemsize == 64 and TMDESC_DT.itemsize == 112 and TCSEG_DT.itemsize == 32
 TC_BM, TC_BN, TC_BK = 128, 128, 32
 SWIZZLE_128B = 3
 
@@ -828,13 +837,18 @@ class TCPanelStage(object):
     The tensor maps embed buffer addresses: they are encoded on the host whenever run sees
     buffers other than the last ones."""
 
-    def __init__(self, name, units, maps, ops, crow, flops, device):
+    def __init__(self, name, units, maps, ops, crow, flops, device, segs=None):
+        """crow: row table (row form); segs: TCSEG_DT column segments (segment form, crow unused)."""
         self.name = name
         self.h_units = units
         self.d_units = upload(units, device)
         self.map_specs = maps
         self.d_ops = upload(ops, device)
         self.host_ops = ops
+        self.h_segs = segs
+        self.d_segs = upload(segs, device) if segs is not None else None
+        if crow is None:
+            crow = numpy.zeros(1, dtype=numpy.int64)
         self.d_crow = torch.from_numpy(numpy.ascontiguousarray(crow, dtype=numpy.int64)).to(device)
         self.flops = flops
         self.bytes = 0.0
@@ -871,8 +885,12 @@ class TCPanelStage(object):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-        check(lib.qc_tcpanel_f32(self.d_units.data_ptr(), self.ntasks, maps.data_ptr(), self.d_ops.data_ptr(),
-                                 self.d_crow.data_ptr(), C.data_ptr(), s), "qc_tcpanel_f32")
+        if self.d_segs is not None:
+            check(lib.qc_tcpanel_seg_f32(self.d_units.data_ptr(), self.ntasks, maps.data_ptr(), self.d_ops.data_ptr(),
+                                         self.d_segs.data_ptr(), C.data_ptr(), s), "qc_tcpanel_seg_f32")
+        else:
+            check(lib.qc_tcpanel_f32(self.d_units.data_ptr(), self.ntasks, maps.data_ptr(), self.d_ops.data_ptr(),
+                                     self.d_crow.data_ptr(), C.data_ptr(), s), "qc_tcpanel_f32")
         LOG.launches += 1
         if LOG.enabled:
             e1.record()
@@ -904,3 +922,83 @@ def tc_sigma4_units(classes, order_pos, t3_base_of_class, rt_base_of_class, rt_o
                                       int(sec["crow_base"][j]) + m0, 0))
     u = numpy.array(units, dtype=TCUNIT_DT) if units else numpy.zeros(0, TCUNIT_DT)
     return u, maps
+
+
+def psi_panels(psi):
+    """The wavefunction as the B operand of the tensor-core L.psi GEMMs: per first-index
+    sector l' the psi blocks (l', n1, n2, r) of that sector side by side as columns,
+    transposed to [sum_j N_j x Kp] (k = l' index contiguous, rows padded to Kp = D_l'
+    rounded up to 4).  Returns (gather index into the packed vector, -1 for padding),
+    {sector: (offset, N total, K, Kp)} and {block: (sector, first column)}."""
+    blocks = numpy.asarray(psi.idx_allowed, dtype=numpy.int64)
+    sec = psi.block_sectors(blocks)[0]
+    d = psi.block_dims(blocks)
+    K = d[:, 0]
+    N = numpy.prod(d[:, 1:], axis=1)
+    info, cols = {}, {}
+    idx = []
+    off = 0
+    for s_ in numpy.unique(sec):
+        sel = numpy.flatnonzero(sec == s_)
+        k = int(K[sel[0]])
+        kp = (k + 3) // 4 * 4
+        ntot = int(N[sel].sum())
+        info[int(s_)] = (off, ntot, k, kp)
+        g = numpy.full((ntot, kp), -1, dtype=numpy.int64)
+        c = 0
+        for j in sel:
+            n = int(N[j])
+            g[c:c + n, :k] = psi.ioff[blocks[j]] + numpy.arange(k)[None, :] * n + numpy.arange(n)[:, None]
+            cols[int(blocks[j])] = (int(s_), c)
+            c += n
+        idx.append(g.ravel())
+        off += ntot * kp
+    gidx = numpy.concatenate(idx) if idx else numpy.zeros(0, dtype=numpy.int64)
+    return gidx, info, cols
+
+
+def tc_sigma1_units(classes, psi_info, psi_cols, lp_base, lp_opstride, lp_total, psi_total):
+    """Work units, column segments and tensor maps of L.psi on the tensor cores.
+
+    classes: list of (op positions, pan["tc"] dict).  A: the class's TC L panels (pre-split
+    planes, lp_total apart); B: the psi panels of the sector (psi_info, planes psi_total apart).
+    The T1 destination of psi block j is its panel [M x N_j] at t1pan_j (rows = L panel rows)."""
+    units, maps, segs = [], [], []
+    bmap = {}
+    for s_, (off, ntot, k, kp) in sorted(psi_info.items()):
+        bmap[s_] = len(maps)
+        maps.append(("B", off, (k, ntot, 1, 2), (kp, ntot * kp, psi_total), (TC_BK, TC_BN, 1, 2)))
+    for ci, (poss, tc) in enumerate(classes):
+        nops = len(poss)
+        col_of = {}
+        for b, t1p, nj in zip(tc["blocks"].tolist(), tc["t1pan"].tolist(), tc["Nj"].tolist()):
+            s_, c = psi_cols[b]
+            col_of.setdefault(s_, []).append((c, nj, t1p))
+        per_sec = []
+        for j, s_ in enumerate(tc["sectors"].tolist()):
+            amap = len(maps)
+            K, M, Kp = int(tc["K"][j]), int(tc["M"][j]), int(tc["Kp"][j])
+            maps.append(("A", lp_base[ci] + int(tc["lpoff"][j]), (K, M, nops, 2), (Kp, lp_opstride[ci], lp_total),
+                         (TC_BK, TC_BM, 1, 2)))
+            ntot = psi_info[s_][1]
+            blocks = sorted(col_of.get(s_, []))
+            tiles = []
+            for n0 in range(0, ntot, TC_BN):
+                w = min(TC_BN, ntot - n0)
+                sb = len(segs)
+                for (c, nj, t1p) in blocks:
+                    lo, hi = max(c, n0), min(c + nj, n0 + w)
+                    if hi > lo:
+                        segs.append((t1p + (lo - c), lo - n0, hi - lo, nj, (0, 0, 0)))
+                if len(segs) > sb:
+                    tiles.append((n0, w, sb, len(segs) - sb))
+            per_sec.append((amap, bmap[s_], K, M, tiles))
+        for q, pos in enumerate(poss):
+            for (amap, bm, K, M, tiles) in per_sec:
+                for (n0, w, sb, ns) in tiles:
+                    for m0 in range(0, M, TC_BM):
+                        units.append((amap, bm, m0, n0, q, 0, (K + TC_BK - 1) // TC_BK, min(TC_BM, M - m0), w, pos,
+                                      ns, 0, sb, 0))
+    u = numpy.array(units, dtype=TCUNIT_DT) if units else numpy.zeros(0, TCUNIT_DT)
+    sg = numpy.array(segs, dtype=TCSEG_DT) if segs else numpy.zeros(1, TCSEG_DT)
+    return u, maps, sg

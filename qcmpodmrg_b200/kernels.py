@@ -112,6 +112,14 @@ def convert(src, out):
     return out
 
 
+def gather_split(x, idx, hi, lo):
+    """hi[i] = tf32(x[idx[i]]), lo[i] = tf32(x[idx[i]] - hi[i]); idx < 0 gives 0 (qc_gather_split_f32)."""
+    check(native.lib().qc_gather_split_f32(x.data_ptr(), idx.data_ptr(), idx.numel(), hi.data_ptr(), lo.data_ptr(),
+                                           _stream(hi.device)), "qc_gather_split_f32")
+    LOG.launches += 1
+    return hi, lo
+
+
 def tf32_split(hi, lo):
     """hi = tf32(x), lo = tf32(x - hi) for the FP32 values x held in hi (qc_tf32_split)."""
     check(native.lib().qc_tf32_split(hi.data_ptr(), lo.data_ptr(), hi.numel(), _stream(hi.device)),
@@ -170,7 +178,8 @@ class SigmaOperator(object):
         # tf32x3: the .R panel GEMMs on the TMA-fed tcgen05 kernel (qc_tcpanel_f32); the older
         # gathered tensor-core tiles (qc_bgemm_tf32*) stay for plain tf32 and explicit requests
         want_tc4 = precision == "tf32x3" and tensor_cores is None and use_fiber and panel4
-        if want_tc4:
+        want_tc1 = precision == "tf32x3" and tensor_cores is None and panel1
+        if want_tc4 or want_tc1:
             tc = False
         self.L, self.R, self.Wi, self.Wj = L, R, Wi, Wj
         self._lays = (list(L.layouts), list(R.layouts))      # held: identity is the plan's key
@@ -268,6 +277,7 @@ class SigmaOperator(object):
         p4st, p4st_tc = {}, {}          # panel GEMM parts of the .R contraction
         crow_all, crow_n = [], 0        # their row table (panel row -> sigma element offset)
         tc4_classes = []                # (operator range, pan4, row-table base) for the tensor-core .R
+        tc1_classes = []                # (operator range, pan["tc"]) for the tensor-core L.psi
         any4 = any(v[8] is not None for v in plans.values())
         for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
             rng = (pos, pos + len(ops))
@@ -329,6 +339,8 @@ class SigmaOperator(object):
                 if (si == 2 and fib3 is not None) or (si == 3 and pan4 is not None):
                     continue
                 if si == 0 and pan is not None:
+                    if want_tc1:
+                        tc1_classes.append((rng, pan["tc"]))
                     parts = compile_panels(pan["gemm"], rng, tensor_cores=bool(tc))
                     if tc:
                         parts, tcp = parts
@@ -351,6 +363,8 @@ class SigmaOperator(object):
         for si in range(4):
             g = Stage(st[si], dev, "sigma%d" % (si + 1), tabs[si]) if st[si] else None
             f = fiber_stages(fib[si], dev, "sigma%d" % (si + 1), tabs[si]) if fib[si] else []
+            if si == 0:
+                self._s0_generic = g
             if si == 0 and (pst or pst_tc):
                 f = [PanelStage(pst, dev, "sigma1", tabs[0], pst_tc)]
             if si == 3 and (p4st or p4st_tc):
@@ -380,6 +394,9 @@ class SigmaOperator(object):
             self._build_rpan()
         # the .R contraction on the tensor cores: R panels transposed and split into TF32
         # hi / lo planes once per dot, T3 read raw by TMA and split in the kernel
+        self.tc1 = None
+        if tc1_classes:
+            self._setup_tc1(tc1_classes, order, L, tabs[0])
         self.tc4 = None
         if tc4_classes:
             self._setup_tc4(tc4_classes, order, bases[2], R, st4_ops=tabs[3],
@@ -422,6 +439,8 @@ class SigmaOperator(object):
             self.fused.bytes = float(fb)
         if self.tc4 is not None:
             self.tc4.bytes = self.stages[3].bytes
+        if self.tc1 is not None:
+            self.tc1.bytes = self.stages[0].bytes
         # FLOPs of the reference's four-contraction chain (tensordotCAL pair GEMMs),
         # whatever the fusion used here
         self.flops = 0.0
@@ -443,6 +462,8 @@ class SigmaOperator(object):
             self._build_rpan()
         if self.tc4 is not None:
             self._build_rpan_tc()
+        if self.tc1 is not None:
+            self._build_lpan_tc()
 
     def _setup_tc4(self, tc4_classes, order, t3bases, R, st4_ops, crow):
         from .engine import TCPanelStage, tc_sigma4_units
@@ -482,6 +503,48 @@ class SigmaOperator(object):
         self._rt_ops_d = upload(op_table(R.offsets[order], 0, base, 1.0), dev)
         self._rt_span = int(max(len(c[0]) for c in classes))
         self._build_rpan_tc()
+
+    def _setup_tc1(self, tc1_classes, order, L, st1_ops):
+        from .engine import TCPanelStage, tc_sigma1_units, psi_panels
+        dev = self.ws.device
+        gidx, info, cols = psi_panels(self.psi)
+        self._psi_total = (len(gidx) + 31) // 32 * 32
+        self._psi_gidx = torch.from_numpy(numpy.concatenate(
+            [gidx, numpy.full(self._psi_total - len(gidx), -1, dtype=numpy.int64)])).to(dev)
+        classes, lpb, lps, descs = [], [], [], []
+        tot = 0
+        base = numpy.zeros(len(order), dtype=numpy.int64)
+        for (rng, tcd) in tc1_classes:
+            poss = list(range(rng[0], rng[1]))
+            stride = (int(tcd["lpsize"]) + 31) // 32 * 32
+            classes.append((poss, tcd))
+            lpb.append(tot)
+            lps.append(stride)
+            base[poss] = tot + stride * numpy.arange(len(poss))
+            src, dst, dL, kp = tcd["lperm_t"]
+            d = numpy.zeros(len(src), BPERM_DT)
+            d["src_off"], d["dst_off"] = src, dst
+            d["d0"], d["d1"], d["d2"] = dL[:, 0], dL[:, 1], dL[:, 2]
+            d["s0"], d["s1"], d["s2"] = dL[:, 1] * kp, kp, 1
+            d["op_b"], d["op_e"] = rng
+            descs.append(d)
+            tot += stride * len(poss)
+        self._lp_total = (tot + 31) // 32 * 32
+        units, maps, segs = tc_sigma1_units(classes, info, cols, lpb, lps, self._lp_total, self._psi_total)
+        self.tc1 = TCPanelStage("sigma1", units, maps, st1_ops, None, self.stages[0].flops, dev, segs=segs)
+        self._lp_descs = numpy.concatenate(descs)
+        self._lp_descs_d = upload(self._lp_descs, dev)
+        self._lp_ops_d = upload(op_table(L.offsets[order], 0, base, 1.0), dev)
+        self._lp_span = int(max(len(c[0]) for c in classes))
+        self._build_lpan_tc()
+
+    def _build_lpan_tc(self):
+        """L panels of the tensor-core L.psi kernel: [M x Kp] per sector, FP32 hi plane then lo plane."""
+        n = self._lp_total
+        self.lpan_tc = torch.zeros(2 * max(n, 1), dtype=torch.float32, device=self.ws.device)
+        block_permute(self._lp_descs_d, len(self._lp_descs), self._lp_span, self._lp_ops_d, self.L.values,
+                      self.lpan_tc)
+        tf32_split(self.lpan_tc[:n], self.lpan_tc[n:2 * n])
 
     def _build_rpan_tc(self):
         """R panels of the tensor-core .R kernel: [D_r' x K_r'] per sector, FP32 hi plane then lo plane."""
@@ -534,6 +597,7 @@ class SigmaOperator(object):
         self.Lpan = self._Lpan32 = None
         self.Rpan = self._Rpan32 = None
         self.rpan_tc = None
+        self.lpan_tc = None
 
     def wij32(self):
         if self._Wij32 is None:
@@ -574,6 +638,8 @@ class SigmaOperator(object):
                 walk(self.fused, 1, native.GROUP_FIBER)
             if si == 3 and self.tc4 is not None:
                 out.append((3, native.GROUP_PANEL, self.tc4.d_units.data_ptr(), self.tc4.ntasks, 1, 0, 0))
+            if si == 0 and self.tc1 is not None:
+                out.append((0, native.GROUP_PANEL, self.tc1.d_units.data_ptr(), self.tc1.ntasks, 1, 0, 0))
         return out
 
     def __call__(self, x, y=None, precision=None):
@@ -608,7 +674,14 @@ class SigmaOperator(object):
         convert(x, x32)
         P = ws.get("part32", self.nops * self.ndim0, torch.float32)
         s = self.stages
-        s[0].run(self.a1("f32"), x32, T1, kind)
+        if self.tc1 is not None and kind == "tf32x3":
+            pt = ws.get("psiT", 2 * self._psi_total, torch.float32)
+            gather_split(x, self._psi_gidx, pt[:self._psi_total], pt[self._psi_total:2 * self._psi_total])
+            self.tc1.run(self.lpan_tc, pt, T1)
+            if self._s0_generic is not None:
+                self._s0_generic.run(self.a1("f32"), x32, T1, "f32")
+        else:
+            s[0].run(self.a1("f32"), x32, T1, kind)
         s[1].run(T1, self.Wi.f32(), T2, "f32")
         s[2].run(T2, self.Wj.f32(), T3, "f32")
         if self.fused is not None:

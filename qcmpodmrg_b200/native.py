@@ -73,6 +73,8 @@ _SIGS = {
     "qc_tcpanel_f32": (c_int, [c_vp, c_ll, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "qc_tf32_split": (c_int, [c_vp, c_vp, c_ll, c_vp]),
     "qc_tcpanel_status": (c_int, [c_int]),
+    "qc_tcpanel_seg_f32": (c_int, [c_vp, c_ll, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "qc_gather_split_f32": (c_int, [c_vp, c_vp, c_ll, c_vp, c_vp, c_vp]),
 }
 
 

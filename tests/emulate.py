@@ -120,6 +120,15 @@ def patch_stage_run(monkeypatch):
 
     monkeypatch.setattr(kernels, "tf32_split", tf32_split)
 
+    def gather_split(x, idx, hi, lo):
+        i = idx.cpu().numpy()
+        v = numpy.where(i >= 0, _f64(x)[numpy.maximum(i, 0)], 0.0)
+        hi.copy_(torch.from_numpy(v).to(hi.dtype))
+        lo.zero_()
+        return hi, lo
+
+    monkeypatch.setattr(kernels, "gather_split", gather_split)
+
     def tcrun(self, A, B, C, kind="tf32x3", stream=None):
         a = _f64(A)
         b = _f64(B)
@@ -195,8 +204,17 @@ def _run_tcpanel(st, A, B, C):
         k = numpy.arange(K)
         ia = offa + int(u["a_c2"]) * stra[1] + m[:, None] * stra[0] + k[None, :]
         ib = offb + int(u["b_c2"]) * strb[1] + n[:, None] * strb[0] + k[None, :]
+        am = A[ia] + (A[ia + stra[2]] if len(dima) == 4 else 0.0)       # pre-split A: hi + lo planes
         bm = B[ib] + B[ib + strb[2]]
         o = st.host_ops[int(u["op"])]
-        rows = st.d_crow.cpu().numpy()[int(u["c_off"]) + numpy.arange(int(u["m_valid"]))] + int(u["b_c1"])
-        idx = o["c_base"] + rows[:, None] + numpy.arange(int(u["n_valid"]))[None, :]
-        C[idx] = o["alpha"] * (A[ia] @ bm.T)
+        tile = o["alpha"] * (am @ bm.T)
+        if st.h_segs is None:
+            rows = st.d_crow.cpu().numpy()[int(u["c_off"]) + numpy.arange(int(u["m_valid"]))] + int(u["b_c1"])
+            idx = o["c_base"] + rows[:, None] + numpy.arange(int(u["n_valid"]))[None, :]
+            C[idx] = tile
+        else:
+            for sg in st.h_segs[int(u["c_off"]):int(u["c_off"]) + int(u["nseg"])]:
+                c = numpy.arange(int(sg["ncol"]))
+                mm = numpy.arange(int(u["m_valid"]))
+                idx = o["c_base"] + sg["off"] + (int(u["a_c1"]) + mm[:, None]) * int(sg["ldc"]) + c[None, :]
+                C[idx] = tile[:, int(sg["col0"]) + c]

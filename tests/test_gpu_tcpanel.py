@@ -60,10 +60,12 @@ def test_tcpanel_dense_known_answer(cuda, shape):
 
 
 @pytest.mark.parametrize("tag", ["K5", "K6", "K5N8"])
-def test_sigma_with_tensor_core_R(tag, cuda):
+def test_sigma_with_tensor_core_panels(tag, cuda):
+    """L.psi and .R both on the TMA-fed tensor-core kernel (column segments into the T1
+    panels, row table into sigma)."""
     for r in load("kernels_%s.npz" % tag)["records"]:
         sig, _, _ = record_operators(r, cuda, precision="tf32x3", use_fiber=True, fuse_w=False)
-        assert sig.tc4 is not None
+        assert sig.tc4 is not None and sig.tc1 is not None
         x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64)).to(cuda)
         native.lib().qc_tcpanel_status(1)
         y = sig(x).cpu().numpy()

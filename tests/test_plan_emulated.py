@@ -66,13 +66,15 @@ def test_sigma_tensor_core_panels_emulated(tag, monkeypatch):
 
 
 @pytest.mark.parametrize("tag", ["K5", "K6", "K5N8"])
-def test_sigma_tma_tensor_core_R_units_emulated(tag, monkeypatch):
-    """The .R contraction as tensor-core work units (tensor-map boxes, row table, padded T3
-    rows, transposed R panels) has the semantics of HVecQt's top4 (interpreter, FP32 buffers)."""
+def test_sigma_tma_tensor_core_units_emulated(tag, monkeypatch):
+    """L.psi and .R as tensor-core work units (tensor-map boxes, column segments of the T1
+    panels, row table, padded rows, transposed R panels, psi panels) have the semantics of
+    HVecQt's top1 / top4 (interpreter, FP32 buffers)."""
     patch_stage_run(monkeypatch)
     for r in load("kernels_%s.npz" % tag)["records"]:
         sig, dg, ws = record_operators(r, "cpu", precision="tf32x3", use_fiber=True, fuse_w=False)
         assert sig.tc4 is not None and sig.tc4.ntasks > 0
+        assert sig.tc1 is not None and sig.tc1.ntasks > 0
         x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))
         ref = numpy.asarray(r["hvec_y"])
         y = sig(x).numpy()
