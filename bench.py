@@ -9,7 +9,7 @@ per dot the sigma/diagonal plans, Davidson (FP64 Rayleigh-Ritz), RDM
 decimation and renormalisation of every operator's environment.
 
   python bench.py [--steps K] [--warmup W] [--precision mixed|f64|mixed-tc|tf32] [--gpus N]
-                  [--w-path fiber|generic|fused] [--plan-cache] [--sites K] [--dmax D]
+                  [--w-path fiber|generic|fused] [--no-plan-cache] [--sites K] [--dmax D]
   python bench.py --impl reference      # the reference algorithm (oracle port) on the host CPU
   python bench.py --workload batched    # lockstep independent instances vs one after another
   python bench.py --workload sp --sites 12 --dmax 100 --npts 4   # spin-projected (S=0) sweeps, FP64
@@ -482,7 +482,9 @@ def main():
     ap.add_argument("--no-cpu", dest="cpu_baseline", action="store_false")
     ap.add_argument("--w-path", default="fiber", choices=["generic", "fiber", "fused"],
                     help="kernels of the two MPO-site contractions of sigma")
-    ap.add_argument("--plan-cache", action="store_true", help="reuse compiled plans of unchanged dots")
+    ap.add_argument("--no-plan-cache", dest="plan_cache", action="store_false",
+                    help="compile every dot's plans afresh (default: reuse the plans of dots whose sectors did not "
+                         "change)")
     ap.add_argument("--f64-steps", type=int, default=3,
                     help="sweeps timed on the plain FP64 GPU arm after the same warm-up (0: no FP64 arm)")
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "learned"],

@@ -102,23 +102,71 @@ def SDiag(info, ndim0, prjmap):
     return sd().cpu().numpy()
 
 
-def renorm(dmrg, isite, ncsite, flst, flstN, site, status):
-    """New environments of every operator; stored in flstN[0][0] and in dmrg's env table
-    (with spin projection also the projector's, renormQt_S00, in flstN[0][1]).
+class QtSite(object):
+    """A site tensor handed over by the reference (its ``qtensor``: status, qsyms, ndims and
+    the packed ``value`` array, source/qtensor/qtensor.py:108-149) as the device operators
+    take it: the packed layout and the values on the device."""
 
-    ``site`` is a qcmpodmrg_b200.dmrg.SiteTensor (packed values on the device).
+    def __init__(self, qt, device):
+        from .qtensor import Layout
+        self.layout = Layout(numpy.asarray(qt.status, dtype=bool),
+                             [numpy.asarray(q, dtype=numpy.float64) for q in qt.qsyms],
+                             [numpy.asarray(n, dtype=numpy.int64) for n in qt.ndims])
+        self.values = torch.from_numpy(numpy.ascontiguousarray(qt.value, dtype=numpy.float64)).to(device)
+
+    def bond_qnums(self, index):
+        """Per-state quantum numbers of one index, sector by sector (its classification
+        returns the same sectors in the same order)."""
+        q = self.layout.qsyms[index]
+        n = self.layout.ndims[index]
+        return numpy.repeat(numpy.asarray(q, dtype=numpy.float64).reshape(len(n), -1), n, axis=0)
+
+
+def renorm(dmrg, isite, ncsite, flst, flstN, site, status):
+    """New environments of every operator; stored in flstN[0][0] (when given) and in dmrg's
+    env table (with spin projection also the projector's, renormQt_S00, in flstN[0][1]).
+
+    ``site`` is a qcmpodmrg_b200.dmrg.SiteTensor (packed values on the device) or the
+    reference's own qtensor site (mpo_dmrg_opt.sweep passes it, source/mpo_dmrg_opt.py:66):
+    then its values are copied to the device and the new bond's quantum numbers (its right
+    index for 'L', left index for 'R') become those of the next dots.
     """
     if ncsite != 2:
         raise NotImplementedError("only the two-site dot is implemented")
     j = isite if status == "L" else isite + ncsite - 1
+    if not hasattr(site, "layout"):
+        site = QtSite(site, dmrg.device)
+        if status == "L":
+            dmrg.qnuml[j + 1] = site.bond_qnums(2)
+        else:
+            dmrg.qnumr[j] = site.bond_qnums(0)
     dmrg.renormalize(j, status, site)
     sp = getattr(dmrg, "ifs2proj", False)
     new = dmrg.lenv[j] if status == "L" else dmrg.renv[j]
     if flstN is not None:
-        flstN[0][0] = new
-        if sp:
-            flstN[0][1] = dmrg.plenv[j] if status == "L" else dmrg.prenv[j]
+        if hasattr(flstN[0][0], "create_group"):
+            # the reference's own environment file: the values stay on the device; the
+            # block headers its dot set-up reads (genDimensions, source/mpo_dmrg_dotutil.py:60-80)
+            # are written as renormQt_H00's dumpSLC would (qtensor.dump, qtensor.py:195-206)
+            _write_env_headers(flstN[0][0], new)
+        else:
+            flstN[0][0] = new
+            if sp:
+                flstN[0][1] = dmrg.plenv[j] if status == "L" else dmrg.prenv[j]
     return 0
+
+
+def _write_env_headers(f, tset):
+    for i, lay in enumerate(tset.layouts):
+        g = f.create_group("opers%d_slc0" % i)
+        g.attrs["rank"] = int(lay.rank)
+        g.attrs["nqnum"] = 2
+        g.attrs["nsyms"] = numpy.asarray(lay.nsyms, dtype=numpy.int64)
+        g.attrs["shape"] = numpy.asarray(lay.shape, dtype=numpy.int64)
+        g.attrs["size"] = int(numpy.prod(lay.shape))
+        g.attrs["nblks_allowed"] = int(len(lay.idx_allowed))
+        g.attrs["size_allowed"] = int(lay.size)
+        g.attrs["status"] = numpy.asarray(lay.status, dtype=bool)
 
 
 def pRDM(cimat, info):

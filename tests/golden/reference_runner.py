@@ -81,12 +81,16 @@ class Recorder(object):
 
 def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.0,
                   tol=1.e-7, maxslc=1, record_envs=True, workdir=None, npts=None, sval=0.0, sz=0.0,
-                  quad="GaussLegendre"):
+                  quad="GaussLegendre", gpu=None):
     """Run the reference flow; return (result dict, recorder).
 
     npts: spin projection (SP-MPS) with ``npts`` quadrature points for <S^2> = sval(sval+1),
     Sz = sz, set as examples/examples_spmpsQt/main_spmps.py does (ifs2proj, s2quad); quad
     selects the reference's quadrature rule (GaussLegendre or Simpson).
+    gpu: a factory init_mps -> qcmpodmrg_b200.dmrg.DMRG.  The reference's own sweep then runs
+    with its kernel dispatcher patched as INTEGRATION.md shows (HVec / HDiag / renorm of the
+    Qt two-site dot to qcmpodmrg_b200.mpo_dmrg_kernel, dmrg.gpu the device object); its
+    Davidson, decimation, site updates and schedule stay the reference's.
     """
     mpo_dmrg_class, mpo_dmrg_schedule, mpo_dmrg_kernel, qtensor_api, qtensor, class_molinfo = _ref()
     from qcmpodmrg.source import mpo_dmrg_io
@@ -157,8 +161,33 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
         dmrg2.loadInts(mol)
         dmrg2.dumpMPO()
 
+        base = orig
+        if gpu is not None:
+            from qcmpodmrg_b200 import mpo_dmrg_kernel as _gpu
+            dmrg2.gpu = gpu(init_mps)
+
+            def _on_gpu(d, ncsite):
+                return getattr(d, "gpu", None) is not None and d.ifQt and ncsite == 2
+
+            def d_hvec(vec0, info, ndim0, prjmap):
+                if _on_gpu(info[0], info[2]):
+                    return _gpu.HVec(vec0, [info[0].gpu] + list(info[1:]), ndim0, prjmap)
+                return orig[0](vec0, info, ndim0, prjmap)
+
+            def d_hdiag(info, ndim0, prjmap):
+                if _on_gpu(info[0], info[2]):
+                    return _gpu.HDiag([info[0].gpu] + list(info[1:]), ndim0, prjmap)
+                return orig[1](info, ndim0, prjmap)
+
+            def d_renorm(d, isite, ncsite, flst, flstN, site, status):
+                if _on_gpu(d, ncsite):
+                    return _gpu.renorm(d.gpu, isite, ncsite, flst, flstN, site, status)
+                return orig[2](d, isite, ncsite, flst, flstN, site, status)
+
+            base = (d_hvec, d_hdiag, d_renorm) + tuple(orig[3:])
+
         def hvec_hook(vec0, info, ndim0, prjmap):
-            out = orig[0](vec0, info, ndim0, prjmap)
+            out = base[0](vec0, info, ndim0, prjmap)
             d, isite, ncsite, flst, status, ifsym = info
             k = (d.isweep, status, isite)
             r = rec.records.setdefault(k, {})
@@ -211,7 +240,7 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
             return out
 
         def hdiag_hook(info, ndim0, prjmap):
-            out = orig[1](info, ndim0, prjmap)
+            out = base[1](info, ndim0, prjmap)
             d, isite, ncsite, flst, status, ifsym = info
             k = (d.isweep, status, isite)
             r = rec.records.setdefault(k, {})
@@ -220,7 +249,9 @@ def run_reference(K, N, D, nsweeps, seed, decay=None, D0=5, targets=(), noise=0.
             return out
 
         def renorm_hook(d, isite, ncsite, flst, flstN, site, status):
-            out = orig[2](d, isite, ncsite, flst, flstN, site, status)
+            out = base[2](d, isite, ncsite, flst, flstN, site, status)
+            if gpu is not None:
+                return out
             k = (d.isweep, status, isite)
             r = rec.records.setdefault(k, {})
             if k in rec.targets and "renorm_site" not in r:
