@@ -140,6 +140,179 @@ k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, cons
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// Persistent fiber-group kernel.  Same work items as k_fiber, processed as a flat list of
+// (task, operator) items by a grid of resident CTAs.  While a CTA multiplies one item out
+// of shared memory, the next item's input rows and every W block it needs are already in
+// flight into the other shared-memory buffer (cp.async, zero fill beyond the tile), so the
+// HBM reads of T overlap the FMAs.  W blocks are staged with their rows padded to a
+// multiple of 4 elements (16-byte aligned), read as float4 / double2 broadcasts.
+__device__ __forceinline__ void cp_async4(void *dst, const void *src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src, bool valid) {
+  if (sizeof(T) == 8) cp_async8(dst, valid ? src : nullptr, valid);
+  else cp_async4(dst, valid ? src : nullptr, valid);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// eight consecutive W values (16-byte aligned) from shared memory
+__device__ __forceinline__ void ld8(const float *p, float (&w)[CB]) {
+  const float4 a = *reinterpret_cast<const float4 *>(p), b = *reinterpret_cast<const float4 *>(p + 4);
+  w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w; w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
+}
+__device__ __forceinline__ void ld8(const double *p, double (&w)[CB]) {
+#pragma unroll
+  for (int i = 0; i < CB; i += 2) {
+    const double2 a = *reinterpret_cast<const double2 *>(p + i);
+    w[i] = a.x;
+    w[i + 1] = a.y;
+  }
+}
+
+template <typename T, int FPL>
+__global__ void __launch_bounds__(FT_THREADS)
+k_fiber2(const int2 *__restrict__ work, int nwork, const qc_ftask *__restrict__ tasks,
+         const qc_fin *__restrict__ fin, const qc_fout *__restrict__ fout, const qc_fpair *__restrict__ fpair,
+         const int *__restrict__ pair_wsm, const qc_op *__restrict__ ops, int max_rows, int max_w,
+         const T *__restrict__ A, const T *__restrict__ W, T *__restrict__ C) {
+  constexpr int FT = 32 * FPL;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *const As0 = reinterpret_cast<T *>(smem_raw);
+  T *const Ws0 = As0 + 2 * max_rows * FT;
+  const int a_stride = max_rows * FT, w_stride = max_w + 8;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = FT_THREADS / 32;
+
+  auto issue = [&](int wi, int b) {
+    const int2 wk = work[wi];
+    const qc_ftask t = tasks[wk.x];
+    const qc_op o = ops[wk.y];
+    const int nf = min(FT, t.F - t.f0);
+    const T *Ab = A + o.a_base;
+    for (int i = t.in_b; i < t.in_e; ++i) {
+      const qc_fin bk = fin[i];
+      const T *src = Ab + bk.a_off;
+      const int n = bk.rows * FT;
+      T *dst = As0 + b * a_stride + bk.srow * FT;
+      if (!bk.fiber_major) {
+        for (int idx = tid; idx < n; idx += FT_THREADS) {
+          const int r = idx / FT, f = idx - r * FT;
+          cp_async_elem(dst + idx, src + (long long)r * t.F + t.f0 + f, f < nf);
+        }
+      } else {
+        for (int idx = tid; idx < n; idx += FT_THREADS) {
+          const int f = idx / bk.rows, r = idx - f * bk.rows;
+          cp_async_elem(dst + r * FT + f, src + (long long)(t.f0 + f) * bk.rows + r, f < nf);
+        }
+      }
+    }
+    const T *Wb = W + o.b_base;
+    for (int j = t.out_b; j < t.out_e; ++j) {
+      const qc_fout ob = fout[j];
+      const int nc = ob.ncols, ncp = (nc + 3) & ~3;
+      for (int p = ob.pair_b; p < ob.pair_e; ++p) {
+        const qc_fpair pr = fpair[p];
+        const T *src = Wb + pr.w_off;
+        T *dst = Ws0 + b * w_stride + pair_wsm[p];
+        const int n = pr.rows * nc;
+        for (int e = tid; e < n; e += FT_THREADS) {
+          const int r = e / nc, c = e - r * nc;
+          cp_async_elem(dst + r * ncp + c, src + e, true);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+
+  int buf = 0;
+  int wi = blockIdx.x;
+  if (wi < nwork) issue(wi, 0);
+  for (; wi < nwork; wi += gridDim.x) {
+    const int nxt = wi + gridDim.x;
+    if (nxt < nwork) {
+      issue(nxt, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int2 wk = work[wi];
+    const qc_ftask t = tasks[wk.x];
+    const qc_op o = ops[wk.y];
+    const int nf = min(FT, t.F - t.f0);
+    const T alpha = T(o.alpha);
+    T *Cb = C + o.c_base;
+    const T *as = As0 + buf * a_stride;
+    const T *ws = Ws0 + buf * w_stride;
+    int j = t.out_b, cb = 0, skip = warp;
+    while (j < t.out_e) {
+      const int ncb = (fout[j].ncols + CB - 1) / CB;
+      if (skip < ncb - cb) { cb += skip; break; }
+      skip -= ncb - cb;
+      cb = 0;
+      ++j;
+    }
+    while (j < t.out_e) {
+      const qc_fout ob = fout[j];
+      const int nc = ob.ncols, ncp = (nc + 3) & ~3;
+      const int c0 = cb * CB;
+      const int nb = min(CB, nc - c0);
+      T acc[FPL][CB];
+#pragma unroll
+      for (int q = 0; q < FPL; ++q)
+#pragma unroll
+        for (int i = 0; i < CB; ++i) acc[q][i] = T(0);
+      for (int p = ob.pair_b; p < ob.pair_e; ++p) {
+        const qc_fpair pr = fpair[p];
+        const T *w = ws + pair_wsm[p] + c0;
+        const T *a = as + pr.srow * FT + lane;
+#pragma unroll 2
+        for (int r = 0; r < pr.rows; ++r) {
+          T av[FPL];
+#pragma unroll
+          for (int q = 0; q < FPL; ++q) av[q] = a[r * FT + 32 * q];
+          T wv[CB];
+          ld8(w + r * ncp, wv);
+#pragma unroll
+          for (int i = 0; i < CB; ++i)
+#pragma unroll
+            for (int q = 0; q < FPL; ++q) acc[q][i] = fma(av[q], wv[i], acc[q][i]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < FPL; ++q) {
+        const int fl = lane + 32 * q;
+        if (fl < nf) {
+          const int fg = t.f0 + fl;
+          T *dst = Cb + ob.c_off + (long long)(fg / ob.flo) * ob.fhs + (long long)(fg % ob.flo) * nc + c0;
+#pragma unroll
+          for (int i = 0; i < CB; ++i)
+            if (i < nb) dst[i] = alpha * acc[q][i];
+        }
+      }
+      int adv = NW;
+      while (j < t.out_e && adv > 0) {
+        const int ncb = (fout[j].ncols + CB - 1) / CB;
+        if (cb + adv < ncb) { cb += adv; adv = 0; break; }
+        adv -= ncb - cb;
+        cb = 0;
+        ++j;
+      }
+    }
+    __syncthreads();
+    buf ^= 1;
+  }
+}
+
 // dst[dst_off + i0*s0 + i1*s1 + i2*s2] = src[src_off + (i0*d1 + i1)*d2 + i2] for every
 // block (blockIdx.x, grid-stride over its elements) and operator (blockIdx.y).
 template <typename TD>
@@ -202,7 +375,72 @@ int launch_fiber(const void *tasks, long long ntasks, int opspan, const void *fi
   return QC_OK;
 }
 
+template <typename T>
+int launch_fiber2(const void *work, long long nwork, const void *tasks, const void *fin, const void *fout,
+                  const void *fpair, const int *pair_wsm, const void *ops, int max_rows, int max_w, int fiber_tile,
+                  const T *A, const T *W, T *C, cudaStream_t s) {
+  if (nwork <= 0) return QC_OK;
+  if (nwork > 0x7fffffffLL || max_rows < 1 || max_w < 0 || !pair_wsm) return QC_ERR_ARG;
+  if (fiber_tile != 32 && fiber_tile != 64) return QC_ERR_ARG;
+  const size_t smem = (size_t)(2 * max_rows * fiber_tile + 2 * (max_w + 8)) * sizeof(T);
+  if (smem > 200 * 1024) return QC_ERR_ARG;
+  static bool attr_set[2] = {false, false};
+  static int nsm = 0;
+  const int v = (fiber_tile == 32) ? 0 : 1;
+  if (!attr_set[v]) {
+    cudaError_t ea = (v == 0) ? cudaFuncSetAttribute(k_fiber2<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     200 * 1024)
+                              : cudaFuncSetAttribute(k_fiber2<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     200 * 1024);
+    if (ea != cudaSuccess) {
+      fprintf(stderr, "[qcgpu] qc_fiber2: %s\n", cudaGetErrorString(ea));
+      return QC_ERR_CUDA;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    attr_set[v] = true;
+  }
+  int per_sm = 1;
+  if (v == 0)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fiber2<T, 1>, FT_THREADS, smem);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fiber2<T, 2>, FT_THREADS, smem);
+  if (per_sm < 1) per_sm = 1;
+  long long g = (long long)nsm * per_sm;
+  if (g > nwork) g = nwork;
+  const int grid = (int)g;
+  if (v == 0)
+    k_fiber2<T, 1><<<grid, FT_THREADS, smem, s>>>((const int2 *)work, (int)nwork, (const qc_ftask *)tasks,
+                                                  (const qc_fin *)fin, (const qc_fout *)fout, (const qc_fpair *)fpair,
+                                                  pair_wsm, (const qc_op *)ops, max_rows, max_w, A, W, C);
+  else
+    k_fiber2<T, 2><<<grid, FT_THREADS, smem, s>>>((const int2 *)work, (int)nwork, (const qc_ftask *)tasks,
+                                                  (const qc_fin *)fin, (const qc_fout *)fout, (const qc_fpair *)fpair,
+                                                  pair_wsm, (const qc_op *)ops, max_rows, max_w, A, W, C);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "[qcgpu] qc_fiber2: %s\n", cudaGetErrorString(e));
+    return QC_ERR_CUDA;
+  }
+  return QC_OK;
+}
+
 }  // namespace
+
+extern "C" int qc_fiber2_f64(const void *work, long long nwork, const void *tasks, const void *fin, const void *fout,
+                             const void *fpair, const int *pair_wsm, const void *ops, int max_rows, int max_w,
+                             int fiber_tile, const double *A, const double *W, double *C, void *stream) {
+  return launch_fiber2<double>(work, nwork, tasks, fin, fout, fpair, pair_wsm, ops, max_rows, max_w, fiber_tile, A,
+                               W, C, (cudaStream_t)stream);
+}
+
+extern "C" int qc_fiber2_f32(const void *work, long long nwork, const void *tasks, const void *fin, const void *fout,
+                             const void *fpair, const int *pair_wsm, const void *ops, int max_rows, int max_w,
+                             int fiber_tile, const float *A, const float *W, float *C, void *stream) {
+  return launch_fiber2<float>(work, nwork, tasks, fin, fout, fpair, pair_wsm, ops, max_rows, max_w, fiber_tile, A,
+                              W, C, (cudaStream_t)stream);
+}
 
 extern "C" int qc_block_permute(const void *descs, long long ndescs, int opspan, const void *ops, const double *src,
                                 void *dst, int dst_f32, void *stream) {

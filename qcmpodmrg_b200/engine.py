@@ -571,6 +571,7 @@ assert BPERM_DT.itemsize == 64
 FPAIR_DT = numpy.dtype([("w_off", "<i8"), ("srow", "<i4"), ("rows", "<i4")])
 assert FTASK_DT.itemsize == 32 and FIN_DT.itemsize == 32 and FOUT_DT.itemsize == 32 and FPAIR_DT.itemsize == 16
 FIBER_TILE = 32
+FIBER_PERSISTENT = True   # the persistent, double-buffered fiber kernel (qc_fiber2_*); False: qc_fiber_*
 FIBER_ROWS_WIDE = 128     # staged rows up to which a tile holds 64 fibers (two per lane)
 FIBER_MAX_ROWS = 256
 
@@ -721,20 +722,57 @@ class FiberStage(object):
         self.span = int(max(1, (self.h_tasks["op_e"] - self.h_tasks["op_b"]).max())) if self.ntasks else 1
         self.name = name
         self.bytes = 0.0
+        # persistent kernel: (task, operator) work items and the shared-memory place of every
+        # pair's W block inside its fiber group's W area (rows padded to 4 elements)
+        self.persistent = FIBER_PERSISTENT
+        if self.ntasks:
+            n_op = (self.h_tasks["op_e"] - self.h_tasks["op_b"]).astype(numpy.int64)
+            tix = numpy.repeat(numpy.arange(self.ntasks), n_op)
+            opx = numpy.repeat(self.h_tasks["op_b"].astype(numpy.int64), n_op) + \
+                (numpy.arange(int(n_op.sum())) - numpy.repeat(numpy.cumsum(n_op) - n_op, n_op))
+            self.h_work = numpy.stack([tix, opx], axis=1).astype(numpy.int32)
+            fo = self.h_fout
+            npair_o = (fo["pair_e"] - fo["pair_b"]).astype(numpy.int64)
+            ncp = (fo["ncols"].astype(numpy.int64) + 3) // 4 * 4
+            wsz = numpy.zeros(len(self.h_fpair), dtype=numpy.int64)
+            own = numpy.repeat(numpy.arange(len(fo)), npair_o)
+            pidx = numpy.repeat(fo["pair_b"].astype(numpy.int64), npair_o) + \
+                (numpy.arange(int(npair_o.sum())) - numpy.repeat(numpy.cumsum(npair_o) - npair_o, npair_o))
+            wsz[pidx] = self.h_fpair["rows"][pidx].astype(numpy.int64) * ncp[own]
+            wsm = numpy.zeros(len(self.h_fpair), dtype=numpy.int64)
+            mw = 0
+            for ob, oe in numpy.unique(numpy.stack([self.h_tasks["out_b"], self.h_tasks["out_e"]], axis=1), axis=0):
+                if oe <= ob:
+                    continue
+                pb, pe = int(fo["pair_b"][ob]), int(fo["pair_e"][oe - 1])
+                c = numpy.cumsum(wsz[pb:pe])
+                wsm[pb:pe] = c - wsz[pb:pe]
+                mw = max(mw, int(c[-1]) if len(c) else 0)
+            self.h_wsm = wsm.astype(numpy.int32)
+            self.max_w = (mw + 3) // 4 * 4
+            self.d_work = upload(self.h_work, device)
+            self.d_wsm = upload(self.h_wsm, device)
 
     def run(self, A, B, C, kind="f64", stream=None):
         if self.ntasks == 0:
             return
         lib = native.lib()
         s = stream if stream is not None else torch.cuda.current_stream(C.device).cuda_stream
-        fn = lib.qc_fiber_f64 if kind == "f64" else lib.qc_fiber_f32
         if LOG.enabled:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-        check(fn(self.d[0].data_ptr(), self.ntasks, self.span, self.d[1].data_ptr(), self.d[2].data_ptr(),
-                 self.d[3].data_ptr(), self.d[4].data_ptr(), self.max_rows, self.tile, A.data_ptr(), B.data_ptr(),
-                 C.data_ptr(), s), "qc_fiber_" + kind)
+        if self.persistent:
+            fn = lib.qc_fiber2_f64 if kind == "f64" else lib.qc_fiber2_f32
+            check(fn(self.d_work.data_ptr(), len(self.h_work), self.d[0].data_ptr(), self.d[1].data_ptr(),
+                     self.d[2].data_ptr(), self.d[3].data_ptr(), self.d_wsm.data_ptr(), self.d[4].data_ptr(),
+                     self.max_rows, self.max_w, self.tile, A.data_ptr(), B.data_ptr(), C.data_ptr(), s),
+                  "qc_fiber2_" + kind)
+        else:
+            fn = lib.qc_fiber_f64 if kind == "f64" else lib.qc_fiber_f32
+            check(fn(self.d[0].data_ptr(), self.ntasks, self.span, self.d[1].data_ptr(), self.d[2].data_ptr(),
+                     self.d[3].data_ptr(), self.d[4].data_ptr(), self.max_rows, self.tile, A.data_ptr(), B.data_ptr(),
+                     C.data_ptr(), s), "qc_fiber_" + kind)
         LOG.launches += 1
         if LOG.enabled:
             e1.record()

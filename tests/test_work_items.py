@@ -121,3 +121,36 @@ def test_panel_layouts_cover_the_intermediates_once(tag, monkeypatch):
             for o, n in zip(pan["t1off"][ob], size):
                 cover[o:o + n] += 1
             assert (cover == 1).all()
+
+
+@pytest.mark.parametrize("tag", ["K5", "K6"])
+def test_persistent_fiber_staging_in_bounds(tag, monkeypatch):
+    """Persistent fiber kernel: every (task, operator) pair is one work item; inside a fiber
+    group the W blocks of its pairs get disjoint shared-memory areas (rows padded to 4) within
+    max_w, and the 8-wide W reads of the last column block stay inside max_w + 8."""
+    patch_stage_run(monkeypatch)
+    for r in load("kernels_%s.npz" % tag)["records"]:
+        sig, _, _ = record_operators(r, "cpu", use_fiber=True, fuse_w=False)
+        for st in sig.stages:
+            for sub in _subs(st):
+                if not (isinstance(sub, FiberStage) and sub.ntasks):
+                    continue
+                t = sub.h_tasks
+                assert len(sub.h_work) == int((t["op_e"] - t["op_b"]).sum())
+                assert (sub.h_work[:, 1] >= t["op_b"][sub.h_work[:, 0]]).all()
+                assert (sub.h_work[:, 1] < t["op_e"][sub.h_work[:, 0]]).all()
+                fo = sub.h_fout
+                for ob, oe in set(zip(t["out_b"].tolist(), t["out_e"].tolist())):
+                    spans = []
+                    for j in range(ob, oe):
+                        ncp = (int(fo["ncols"][j]) + 3) // 4 * 4
+                        for p in range(int(fo["pair_b"][j]), int(fo["pair_e"][j])):
+                            lo = int(sub.h_wsm[p])
+                            hi = lo + int(sub.h_fpair["rows"][p]) * ncp
+                            assert lo % 4 == 0 and hi <= sub.max_w
+                            last = lo + (int(sub.h_fpair["rows"][p]) - 1) * ncp + \
+                                ((int(fo["ncols"][j]) - 1) // 8) * 8 + 7
+                            assert last < sub.max_w + 8
+                            spans.append((lo, hi))
+                    spans.sort()
+                    assert all(a[1] <= b[0] for a, b in zip(spans, spans[1:]))
