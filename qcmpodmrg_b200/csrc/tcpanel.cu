@@ -37,6 +37,7 @@ constexpr int TP_BM = 128;
 constexpr int TP_BK = 32;                  // 32 FP32 = 128 bytes: one swizzle row
 constexpr int TP_THREADS = 192;
 constexpr long long TP_SPIN = 1LL << 26;   // polls before a wait gives up (~seconds)
+constexpr int TP_CHUNK = 2;                 // K stages accumulated in TMEM before promotion to FP32 registers
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
@@ -223,47 +224,54 @@ k_tcpanel(const qc_tcunit *__restrict__ units, int nunits, const CUtensorMap *__
     }
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
+    // A unit's K stages go in chunks of TP_CHUNK stages; chunk g (counted over all units of
+    // this CTA) accumulates in TMEM buffer g & 1 from zero, and the helpers add it to FP32
+    // registers: the tensor core's accumulation only ever spans TP_CHUNK * 32 products.
     if (lane == 0) {
-      int it = 0, uc = 0;
+      int it = 0, g = 0;
       bool any = false;
-      for (int u = blockIdx.x; u < nunits && !abort_flag; u += gridDim.x, ++uc) {
+      for (int u = blockIdx.x; u < nunits && !abort_flag; u += gridDim.x) {
         const qc_tcunit t = units[u];
-        const int buf = uc & 1;
-        if (!wait_parity(su32(&acce[buf]), (uint32_t)(((uc >> 1) & 1) ^ 1))) {
-          fail();
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t d = tmem + (uint32_t)(buf * BN);
         const int nmma = ((t.n_valid + 15) / 16) * 16;
         const uint32_t idesc = idesc_tf32(nmma > BN ? BN : nmma);
         bool ok = true;
-        for (int k = 0; k < t.nk; ++k, ++it) {
-          const int s = it % S;
-          const uint32_t ph = (uint32_t)((it / S) & 1);
-          if (!wait_parity(su32(A_SPLIT ? &split[s] : &full[s]), ph)) {
+        for (int k0 = 0; k0 < t.nk && ok; k0 += TP_CHUNK, ++g) {
+          const int buf = g & 1;
+          if (!wait_parity(su32(&acce[buf]), (uint32_t)(((g >> 1) & 1) ^ 1))) {
             ok = false;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t st = su32(smem + s * ST_BYTES);
-          const uint32_t a_hi = st, a_lo = st + A_BYTES, b_hi = st + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
+          const uint32_t d = tmem + (uint32_t)(buf * BN);
+          const int k1 = (k0 + TP_CHUNK < t.nk) ? k0 + TP_CHUNK : t.nk;
+          for (int k = k0; k < k1; ++k, ++it) {
+            const int s = it % S;
+            const uint32_t ph = (uint32_t)((it / S) & 1);
+            if (!wait_parity(su32(A_SPLIT ? &split[s] : &full[s]), ph)) {
+              ok = false;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = su32(smem + s * ST_BYTES);
+            const uint32_t a_hi = st, a_lo = st + A_BYTES, b_hi = st + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
 #pragma unroll
-          for (int kk = 0; kk < TP_BK / 8; ++kk) {
-            const uint32_t off = kk * 32;              // 8 TF32 = 32 bytes along the swizzled row
-            const uint32_t first = (k == 0 && kk == 0) ? 0u : 1u;
-            mma_tf32(d, desc_sw128(a_lo + off), desc_sw128(b_hi + off), idesc, first);
-            mma_tf32(d, desc_sw128(a_hi + off), desc_sw128(b_lo + off), idesc, 1u);
-            mma_tf32(d, desc_sw128(a_hi + off), desc_sw128(b_hi + off), idesc, 1u);
+            for (int kk = 0; kk < TP_BK / 8; ++kk) {
+              const uint32_t off = kk * 32;            // 8 TF32 = 32 bytes along the swizzled row
+              const uint32_t first = (k == k0 && kk == 0) ? 0u : 1u;
+              mma_tf32(d, desc_sw128(a_lo + off), desc_sw128(b_hi + off), idesc, first);
+              mma_tf32(d, desc_sw128(a_hi + off), desc_sw128(b_lo + off), idesc, 1u);
+              mma_tf32(d, desc_sw128(a_hi + off), desc_sw128(b_hi + off), idesc, 1u);
+            }
+            mma_commit(su32(&empty[s]));
+            any = true;
           }
-          mma_commit(su32(&empty[s]));
-          any = true;
+          if (!ok) break;
+          mma_commit(su32(&accf[buf]));
         }
         if (!ok) {
           fail();
           break;
         }
-        mma_commit(su32(&accf[buf]));
       }
       // every product issued has finished before the tensor memory is released (bounded)
       if (any) {
@@ -272,21 +280,25 @@ k_tcpanel(const qc_tcunit *__restrict__ units, int nunits, const CUtensorMap *__
       }
     }
   } else {
-    // ------------------------------------------------------------ split + epilogue (warps 2-5)
+    // ------------------------------------------------------------ split + promotion + epilogue (warps 2-5)
     const int hid = threadIdx.x - 64;          // 0 .. 127
     const int q = warp & 3;                    // TMEM lane quarter of this warp
-    int it = 0, uc = 0;
-    for (int u = blockIdx.x; u < nunits && !abort_flag; u += gridDim.x, ++uc) {
-      const qc_tcunit t = units[u];
+    const int row = q * 32 + lane;
+    float acc[BN];
+    int it = 0;                                // stages split so far
+    // the chunk stream (unit, first stage) in the order the MMA issuer takes it; the next
+    // chunk's stages are split before the current chunk is drained, so the tensor core
+    // never waits for a drain
+    int su = blockIdx.x, sk = 0;               // next chunk to split
+    auto split_chunk = [&]() -> bool {
+      if (su >= nunits) return true;
+      const int nk = units[su].nk;
+      const int k1 = (sk + TP_CHUNK < nk) ? sk + TP_CHUNK : nk;
       if (A_SPLIT) {
-        bool ok = true;
-        for (int k = 0; k < t.nk; ++k, ++it) {
+        for (int k = sk; k < k1; ++k, ++it) {
           const int s = it % S;
           const uint32_t ph = (uint32_t)((it / S) & 1);
-          if (!wait_parity(su32(&full[s]), ph)) {
-            ok = false;
-            break;
-          }
+          if (!wait_parity(su32(&full[s]), ph)) return false;
           float4 *a0 = reinterpret_cast<float4 *>(smem + s * ST_BYTES);
           float4 *a1 = reinterpret_cast<float4 *>(smem + s * ST_BYTES + A_BYTES);
 #pragma unroll
@@ -305,69 +317,83 @@ k_tcpanel(const qc_tcunit *__restrict__ units, int nunits, const CUtensorMap *__
           __syncwarp();
           if (lane == 0) mbar_arrive(su32(&split[s]));
         }
-        if (!ok) {
-          fail();
+      }
+      sk = k1;
+      if (sk >= nk) {
+        su += gridDim.x;
+        sk = 0;
+      }
+      return true;
+    };
+    bool ok = split_chunk();
+    int g = 0;
+    for (int u = blockIdx.x; u < nunits && ok && !abort_flag; u += gridDim.x) {
+      const qc_tcunit t = units[u];
+      const int ncol = t.n_valid < BN ? t.n_valid : BN;
+      for (int k0 = 0; k0 < t.nk; k0 += TP_CHUNK, ++g) {
+        ok = split_chunk();
+        if (!ok) break;
+        const int buf = g & 1;
+        if (!wait_parity(su32(&accf[buf]), (uint32_t)((g >> 1) & 1))) {
+          ok = false;
           break;
         }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * BN);
+#pragma unroll
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+          if (c0 < ncol) {
+            uint32_t r[16];
+            tmem_ld16(taddr + (uint32_t)c0, r);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[c0 + j] = (k0 == 0) ? __uint_as_float(r[j]) : acc[c0 + j] + __uint_as_float(r[j]);
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(su32(&acce[buf]));
       }
-      const int buf = uc & 1;
-      if (!wait_parity(su32(&accf[buf]), (uint32_t)((uc >> 1) & 1))) {
-        fail();
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int row = q * 32 + lane;
+      if (!ok) break;
+      // ---- epilogue of unit u from the FP32 registers
       const qc_op o = ops[t.op];
       const float alpha = (float)o.alpha;
-      const int ncol = t.n_valid < BN ? t.n_valid : BN;
-      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * BN);
       if (EPI == EPI_ROWS) {
-        float *dst = nullptr;
-        if (row < t.m_valid) dst = C + o.c_base + crow[t.c_off + row] + t.b_c1;
-        for (int c0 = 0; c0 < ncol; c0 += 16) {
-          uint32_t r[16];
-          tmem_ld16(taddr + (uint32_t)c0, r);
-          if (dst) {
+        if (row < t.m_valid) {
+          float *dst = C + o.c_base + crow[t.c_off + row] + t.b_c1;
 #pragma unroll
-            for (int j = 0; j < 16; ++j)
-              if (c0 + j < ncol) dst[c0 + j] = alpha * __uint_as_float(r[j]);
-          }
+          for (int c = 0; c < BN; ++c)
+            if (c < ncol) dst[c] = alpha * acc[c];
         }
       } else {
-        // stage EPI_HALF columns of the tile in shared memory (row stride EPI_HALF + 1: no bank
-        // conflicts), then copy every segment's rows with consecutive threads on consecutive
-        // columns: a segment's rows are contiguous in memory when it spans its row stride
+        // stage EPI_HALF columns at a time in shared memory (row stride EPI_HALF + 1: no bank
+        // conflicts), then each warp copies whole rows of every segment, lanes on consecutive
+        // columns (coalesced: a segment row is contiguous in memory)
         float *stg = reinterpret_cast<float *>(smem + S * ST_BYTES);
         float *Cb = C + o.c_base;
-        for (int h0 = 0; h0 < ncol; h0 += EPI_HALF) {
-          for (int c0 = 0; c0 < EPI_HALF && h0 + c0 < ncol; c0 += 16) {
-            uint32_t r[16];
-            tmem_ld16(taddr + (uint32_t)(h0 + c0), r);
 #pragma unroll
-            for (int j = 0; j < 16; ++j) stg[row * (EPI_HALF + 1) + c0 + j] = alpha * __uint_as_float(r[j]);
-          }
-          asm volatile("bar.sync 1, 128;" ::: "memory");
-          const int hw = (ncol - h0) < EPI_HALF ? (ncol - h0) : EPI_HALF;
-          for (int si = 0; si < t.nseg; ++si) {
-            const qc_tcseg sg = segs[t.c_off + si];
-            const int c_lo = sg.col0 > h0 ? sg.col0 : h0;
-            const int c_hi = (sg.col0 + sg.ncol) < (h0 + hw) ? (sg.col0 + sg.ncol) : (h0 + hw);
-            const int w = c_hi - c_lo;
-            if (w <= 0) continue;
-            const int total = t.m_valid * w;
-            float *db = Cb + sg.off + (long long)t.a_c1 * sg.ldc + (c_lo - sg.col0);
-            for (int i = hid; i < total; i += 128) {
-              const int m = i / w, c = i - m * w;
-              db[(long long)m * sg.ldc + c] = stg[m * (EPI_HALF + 1) + (c_lo - h0) + c];
+        for (int h0 = 0; h0 < BN; h0 += EPI_HALF) {
+          if (h0 < ncol) {
+#pragma unroll
+            for (int c = 0; c < EPI_HALF; ++c) stg[row * (EPI_HALF + 1) + c] = alpha * acc[h0 + c];
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            const int hw = (ncol - h0) < EPI_HALF ? (ncol - h0) : EPI_HALF;
+            for (int si = 0; si < t.nseg; ++si) {
+              const qc_tcseg sg = segs[t.c_off + si];
+              const int c_lo = sg.col0 > h0 ? sg.col0 : h0;
+              const int c_hi = (sg.col0 + sg.ncol) < (h0 + hw) ? (sg.col0 + sg.ncol) : (h0 + hw);
+              const int w = c_hi - c_lo;
+              if (w <= 0) continue;
+              float *db = Cb + sg.off + (long long)t.a_c1 * sg.ldc + (c_lo - sg.col0);
+              const float *sb = stg + (c_lo - h0);
+              for (int m = q; m < t.m_valid; m += 4)
+                for (int c = lane; c < w; c += 32) db[(long long)m * sg.ldc + c] = sb[m * (EPI_HALF + 1) + c];
             }
+            asm volatile("bar.sync 1, 128;" ::: "memory");
           }
-          asm volatile("bar.sync 1, 128;" ::: "memory");
         }
       }
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(su32(&acce[buf]));
     }
+    if (!ok) fail();
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
