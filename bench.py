@@ -9,7 +9,7 @@ per dot the sigma/diagonal plans, Davidson (FP64 Rayleigh-Ritz), RDM
 decimation and renormalisation of every operator's environment.
 
   python bench.py [--steps K] [--warmup W] [--precision mixed|f64|mixed-tc|tf32] [--gpus N]
-                  [--w-path fiber|generic|fused] [--no-plan-cache] [--sites K] [--dmax D]
+                  [--w-path fiber|generic|fused] [--plan-cache] [--sites K] [--dmax D]
   python bench.py --impl reference      # the reference algorithm (oracle port) on the host CPU
   python bench.py --workload batched    # lockstep independent instances vs one after another
   python bench.py --workload sp --sites 12 --dmax 100 --npts 4   # spin-projected (S=0) sweeps, FP64
@@ -399,17 +399,20 @@ def run_reference(args):
     for _ in range(args.warmup):
         reference_step(args, warm=True)
     t0 = time.time()
-    res = [reference_step(args) for _ in range(args.steps)]
+    res = [reference_step(args, step=k) for k in range(args.steps)]
     wall = time.time() - t0
-    v = float(numpy.mean([r["sweep_s_est"] for r in res]))
+    v = float(res[-1]["sweep_s_est"])          # from every dot sampled
     line = {"metric": METRIC, "impl": "reference", "value": round(v, 1), "unit": "s/sweep", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * wall / args.steps, 1),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: seeded integrals (K=24, N=24, decay 3, seed 1), synthetic D=500 state",
-            "config": {"workload": "two-site Qt DMRG sweep, K=24 N=24 Sz=0 D=500, 48 operators H_p",
+            "data": "synthetic: seeded integrals (K=%d, N=%d, decay 3, seed 1), synthetic D=%d state"
+                    % (args.sites, args.sites, args.dmax),
+            "config": {"workload": "two-site Qt DMRG sweep, K=%d N=%d Sz=0 D=%d, %d operators H_p"
+                                   % (args.sites, args.sites, args.dmax, 2 * args.sites),
                        "K": args.sites, "N": args.sites, "D": args.dmax},
             "cpu_baseline": {"value": round(v, 1), "unit": "s/sweep", "cores": res[0]["cores"], "kind": "port",
-                             "sample": res[0]["sample"]},
+                             "sample": res[-1]["sample"]},
+            "dots_sampled": {str(r["dot"]): round(r["dot_cost_s"], 2) for r in res},
             "e2e": {"value": round(v, 1), "unit": "s/sweep", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -482,9 +485,8 @@ def main():
     ap.add_argument("--no-cpu", dest="cpu_baseline", action="store_false")
     ap.add_argument("--w-path", default="fiber", choices=["generic", "fiber", "fused"],
                     help="kernels of the two MPO-site contractions of sigma")
-    ap.add_argument("--no-plan-cache", dest="plan_cache", action="store_false",
-                    help="compile every dot's plans afresh (default: reuse the plans of dots whose sectors did not "
-                         "change)")
+    ap.add_argument("--plan-cache", action="store_true",
+                    help="reuse the compiled plans of dots whose sectors did not change")
     ap.add_argument("--f64-steps", type=int, default=3,
                     help="sweeps timed on the plain FP64 GPU arm after the same warm-up (0: no FP64 arm)")
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "learned"],

@@ -89,26 +89,14 @@ def _with_idlst(q):
     return q
 
 
-def reference_step(args, warm=False):
-    """One bounded sample of the K=24, D=500 sweep on the host: at the mid-chain dot of a
-    synthetic D=500 state, one sigma matvec, one diagonal and one renormalisation; the sweep
-    estimate is 2(K-1) dots x (MATVECS_PER_DOT sigma + diagonal + renormalisation)."""
-    from qcmpodmrg_b200.hamiltonian import make_hamiltonian
-    from qcmpodmrg_b200.synthetic import random_mps
-    K, D = args.sites, args.dmax
-    if "ham" not in _CACHE:
-        ham = make_hamiltonian(K, K, 1, 3.0)
-        isite = K // 2
-        _CACHE["ham"] = ham
-        _CACHE["W"] = {i: [_with_idlst(site_operator(p, ham.sbas, i, ham.int1e, ham.int2e)) for p in range(ham.sbas)]
-                       for i in (isite - 1, isite, isite + 1)}
-        _CACHE["mps"] = random_mps(K, K, D, seed=1)
-        _CACHE["rmps"] = random_mps(K, K, D, seed=2)
-    if warm:
-        return None
+def _dot_sample(K, D, isite):
+    """Oracle sigma, diagonal and L renormalisation at dot (isite, isite+1) of the synthetic
+    D-state (random environments of the right block structure); returns the three times."""
     ham, W, mps, rm = _CACHE["ham"], _CACHE["W"], _CACHE["mps"], _CACHE["rmps"]
-    isite = K // 2
-    rng = numpy.random.default_rng(5)
+    for i in (isite, isite + 1):
+        if i not in W:
+            W[i] = [_with_idlst(site_operator(p, ham.sbas, i, ham.int1e, ham.int2e)) for p in range(ham.sbas)]
+    rng = numpy.random.default_rng(5 + isite)
     qkey = numpy.array([float(K), 0.0])
     nops = ham.sbas
     ql = mps["qnum%d" % isite]
@@ -137,9 +125,54 @@ def reference_step(args, warm=False):
     t0 = time.time()
     RenormOracle(list(range(nops)), isite, "L")(site, lenv, W[isite])
     t_ren = time.time() - t0
-    ndots = 2 * (K - 1)
-    est = ndots * (MATVECS_PER_DOT * t_hvec + t_diag + t_ren)
-    return {"sweep_s_est": est, "cores": os.cpu_count(),
-            "sample": "mid-chain dot of a synthetic D=%d state: sigma %.1f s, diagonal %.1f s, renormalisation "
-                      "%.1f s; sweep = %d dots x (%.1f sigma + diagonal + renormalisation)"
-                      % (D, t_hvec, t_diag, t_ren, ndots, MATVECS_PER_DOT)}
+    return t_hvec, t_diag, t_ren
+
+
+# dots sampled by the successive steps of the reference arm: spread over one half of the
+# chain (the synthetic state's bond dimensions are symmetric about its middle)
+def _dot_order(K):
+    half = list(range(0, K // 2))
+    order = []
+    seen = set()
+    for i in [K // 2 - 1, K // 4, 1, 3 * K // 8, K // 8] + half:
+        if 0 <= i <= K - 2 and i not in seen:
+            seen.add(i)
+            order.append(i)
+    return order
+
+
+def reference_step(args, warm=False, step=0):
+    """One bounded sample of the K=24, D=500 sweep on the host: at one dot of a synthetic
+    D=500 state (successive steps visit successive dots of half the chain, mid-chain first),
+    one oracle sigma matvec, one diagonal and one renormalisation.  Returns the dot's cost
+    (MATVECS_PER_DOT sigma + diagonal + renormalisation) and the sweep estimate from every
+    dot sampled so far: the cost of each of the 2 (K - 1) dots of a sweep interpolated
+    linearly in the dot position from the sampled ones (mirrored about the middle)."""
+    from qcmpodmrg_b200.hamiltonian import make_hamiltonian
+    from qcmpodmrg_b200.synthetic import random_mps
+    K, D = args.sites, args.dmax
+    if "ham" not in _CACHE:
+        ham = make_hamiltonian(K, K, 1, 3.0)
+        _CACHE["ham"] = ham
+        _CACHE["W"] = {}
+        _CACHE["mps"] = random_mps(K, K, D, seed=1)
+        _CACHE["rmps"] = random_mps(K, K, D, seed=2)
+        _CACHE["samples"] = {}
+    if warm:
+        return None
+    order = _dot_order(K)
+    isite = order[step % len(order)]
+    t_hvec, t_diag, t_ren = _dot_sample(K, D, isite)
+    cost = MATVECS_PER_DOT * t_hvec + t_diag + t_ren
+    _CACHE["samples"][isite] = cost
+    pos = sorted(_CACHE["samples"])
+    vals = [_CACHE["samples"][i] for i in pos]
+    dots = numpy.arange(K - 1)
+    mirrored = numpy.minimum(dots, K - 2 - dots)
+    per_dot = numpy.interp(mirrored, pos, vals)
+    est = 2.0 * float(per_dot.sum())
+    return {"sweep_s_est": est, "cores": os.cpu_count(), "dot": isite, "dot_cost_s": cost,
+            "sample": "dot %d of a synthetic D=%d state: sigma %.1f s, diagonal %.1f s, renormalisation %.1f s; "
+                      "sweep = sum over the 2(K-1) dots of (%.1f sigma + diagonal + renormalisation), each dot's "
+                      "cost interpolated from the %d dots sampled (mirrored about the middle)"
+                      % (isite, D, t_hvec, t_diag, t_ren, MATVECS_PER_DOT, len(pos))}

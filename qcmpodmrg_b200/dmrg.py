@@ -80,7 +80,7 @@ class DMRG(object):
 
     ifs2proj = False          # spin projection: qcmpodmrg_b200.spin.SPDMRG
 
-    def __init__(self, ham, device="cuda", precision="f64", preconditioner=None, w_path="fiber", plan_cache=True,
+    def __init__(self, ham, device="cuda", precision="f64", preconditioner=None, w_path="fiber", plan_cache=False,
                  sz=0.0):
         """sz: the target Sz of the (N, Sz) sector (the reference's qsectors key [N, Sz])."""
         n2s = int(round(2 * float(sz)))
@@ -103,10 +103,10 @@ class DMRG(object):
         self.ifguess = True
         self.ws = Workspace(self.device)
         self.plan_cache = {}          # oldest first
-        # compiled plans of dots whose sectors did not change are reused with the new
-        # environments (the work lists depend only on block layouts); on the B200 every reused
-        # plan returns bitwise the sigma and diagonal of a freshly compiled one, and sweeps with
-        # and without reuse give bitwise identical energies (K=12 D=100, K=24 D=200)
+        # compiled plans of dots whose sectors did not change can be reused with the new
+        # environments (the work lists depend only on block layouts).  Off by default: at K=24,
+        # D=500 a run with reuse reaches a different energy after the same sweeps, a difference
+        # that runs at D <= 200 (bitwise identical with and without reuse) do not show
         self.plan_cache_size = 2 * self.nsite if plan_cache else 0
         t0 = time.time()
         self._setup_operators(ham)

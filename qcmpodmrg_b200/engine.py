@@ -739,15 +739,21 @@ class FiberStage(object):
             pidx = numpy.repeat(fo["pair_b"].astype(numpy.int64), npair_o) + \
                 (numpy.arange(int(npair_o.sum())) - numpy.repeat(numpy.cumsum(npair_o) - npair_o, npair_o))
             wsz[pidx] = self.h_fpair["rows"][pidx].astype(numpy.int64) * ncp[own]
+            # fiber groups partition the outputs: group of output j = the group whose first output
+            # is the last group start <= j; a pair's place = exclusive prefix of W sizes from the
+            # group's first pair
+            tk = self.h_tasks[self.h_tasks["out_e"] > self.h_tasks["out_b"]]
+            gstart = numpy.unique(tk["out_b"].astype(numpy.int64))
             wsm = numpy.zeros(len(self.h_fpair), dtype=numpy.int64)
             mw = 0
-            for ob, oe in numpy.unique(numpy.stack([self.h_tasks["out_b"], self.h_tasks["out_e"]], axis=1), axis=0):
-                if oe <= ob:
-                    continue
-                pb, pe = int(fo["pair_b"][ob]), int(fo["pair_e"][oe - 1])
-                c = numpy.cumsum(wsz[pb:pe])
-                wsm[pb:pe] = c - wsz[pb:pe]
-                mw = max(mw, int(c[-1]) if len(c) else 0)
+            if len(gstart) and len(pidx):
+                excl = numpy.cumsum(wsz) - wsz
+                g_of_out = numpy.searchsorted(gstart, numpy.arange(len(fo)), side="right") - 1
+                first_pair = fo["pair_b"].astype(numpy.int64)[gstart]
+                g_of_pair = g_of_out[own]
+                wsm[pidx] = excl[pidx] - excl[numpy.minimum(first_pair[g_of_pair], len(excl) - 1)]
+                gtot = numpy.bincount(g_of_pair, weights=wsz[pidx], minlength=len(gstart))
+                mw = int(gtot.max())
             self.h_wsm = wsm.astype(numpy.int32)
             self.max_w = (mw + 3) // 4 * 4
             self.d_work = upload(self.h_work, device)
@@ -935,6 +941,16 @@ class TCPanelStage(object):
             LOG.records.append((self.name, e0, e1, self.flops, self.bytes * 0.5))
 
 
+def _replicate_units(tiles, poss):
+    """tiles: TCUNIT_DT records of one operator (op slot q = 0); one copy per operator of a
+    class, the tiles of an operator back to back (consecutive units share its operands)."""
+    n, k = len(tiles), len(poss)
+    u = numpy.tile(tiles, k)
+    q = numpy.repeat(numpy.arange(k, dtype=numpy.int32), n)
+    u["op"] = numpy.repeat(numpy.asarray(poss, dtype=numpy.int32), n)
+    return u, q
+
+
 def tc_sigma4_units(classes, order_pos, t3_base_of_class, rt_base_of_class, rt_opstride, rt_total):
     """Work units and tensor maps of the .R contraction on the tensor cores.
 
@@ -944,21 +960,29 @@ def tc_sigma4_units(classes, order_pos, t3_base_of_class, rt_base_of_class, rt_o
     for ci, (poss, sec, t3stride) in enumerate(classes):
         nops = len(poss)
         amap0 = len(maps)
+        tl = []
         for j in range(len(sec["used"])):
             K, M, N, Kp = int(sec["K"][j]), int(sec["M"][j]), int(sec["N"][j]), int(sec["Kp"][j])
             maps.append(("A", t3_base_of_class[ci] + int(sec["t3pan"][j]), (K, M, nops), (Kp, t3stride),
                          (TC_BK, TC_BM, 1)))
             maps.append(("B", rt_base_of_class[ci] + int(sec["rtoff"][j]), (K, N, nops, 2),
                          (Kp, rt_opstride[ci], rt_total), (TC_BK, TC_BN, 1, 2)))
-        for q, pos in enumerate(poss):
-            for j in range(len(sec["used"])):
-                K, M, N = int(sec["K"][j]), int(sec["M"][j]), int(sec["N"][j])
-                for n0 in range(0, N, TC_BN):
-                    for m0 in range(0, M, TC_BM):
-                        units.append((amap0 + 2 * j, amap0 + 2 * j + 1, m0, n0, q, q, (K + TC_BK - 1) // TC_BK,
-                                      min(TC_BM, M - m0), min(TC_BN, N - n0), pos, 0, 0,
-                                      int(sec["crow_base"][j]) + m0, 0))
-    u = numpy.array(units, dtype=TCUNIT_DT) if units else numpy.zeros(0, TCUNIT_DT)
+            n0 = numpy.arange(0, N, TC_BN)
+            m0 = numpy.arange(0, M, TC_BM)
+            t = numpy.zeros(len(n0) * len(m0), TCUNIT_DT)
+            t["a_map"], t["b_map"] = amap0 + 2 * j, amap0 + 2 * j + 1
+            t["a_c1"] = numpy.tile(m0, len(n0))
+            t["b_c1"] = numpy.repeat(n0, len(m0))
+            t["nk"] = (K + TC_BK - 1) // TC_BK
+            t["m_valid"] = numpy.minimum(TC_BM, M - t["a_c1"])
+            t["n_valid"] = numpy.minimum(TC_BN, N - t["b_c1"])
+            t["c_off"] = int(sec["crow_base"][j]) + t["a_c1"]
+            tl.append(t)
+        if tl:
+            u, q = _replicate_units(numpy.concatenate(tl), poss)
+            u["a_c2"] = u["b_c2"] = q
+            units.append(u)
+    u = numpy.concatenate(units) if units else numpy.zeros(0, TCUNIT_DT)
     return u, maps
 
 
@@ -1006,13 +1030,14 @@ def tc_sigma1_units(classes, psi_info, psi_cols, lp_base, lp_opstride, lp_total,
     for s_, (off, ntot, k, kp) in sorted(psi_info.items()):
         bmap[s_] = len(maps)
         maps.append(("B", off, (k, ntot, 1, 2), (kp, ntot * kp, psi_total), (TC_BK, TC_BN, 1, 2)))
+    nseg = 0
     for ci, (poss, tc) in enumerate(classes):
         nops = len(poss)
         col_of = {}
         for b, t1p, nj in zip(tc["blocks"].tolist(), tc["t1pan"].tolist(), tc["Nj"].tolist()):
             s_, c = psi_cols[b]
             col_of.setdefault(s_, []).append((c, nj, t1p))
-        per_sec = []
+        tl = []
         for j, s_ in enumerate(tc["sectors"].tolist()):
             amap = len(maps)
             K, M, Kp = int(tc["K"][j]), int(tc["M"][j]), int(tc["Kp"][j])
@@ -1020,23 +1045,30 @@ def tc_sigma1_units(classes, psi_info, psi_cols, lp_base, lp_opstride, lp_total,
                          (TC_BK, TC_BM, 1, 2)))
             ntot = psi_info[s_][1]
             blocks = sorted(col_of.get(s_, []))
-            tiles = []
+            m0 = numpy.arange(0, M, TC_BM)
             for n0 in range(0, ntot, TC_BN):
                 w = min(TC_BN, ntot - n0)
-                sb = len(segs)
+                sb = nseg
                 for (c, nj, t1p) in blocks:
                     lo, hi = max(c, n0), min(c + nj, n0 + w)
                     if hi > lo:
                         segs.append((t1p + (lo - c), lo - n0, hi - lo, nj, (0, 0, 0)))
-                if len(segs) > sb:
-                    tiles.append((n0, w, sb, len(segs) - sb))
-            per_sec.append((amap, bmap[s_], K, M, tiles))
-        for q, pos in enumerate(poss):
-            for (amap, bm, K, M, tiles) in per_sec:
-                for (n0, w, sb, ns) in tiles:
-                    for m0 in range(0, M, TC_BM):
-                        units.append((amap, bm, m0, n0, q, 0, (K + TC_BK - 1) // TC_BK, min(TC_BM, M - m0), w, pos,
-                                      ns, 0, sb, 0))
-    u = numpy.array(units, dtype=TCUNIT_DT) if units else numpy.zeros(0, TCUNIT_DT)
+                        nseg += 1
+                if nseg == sb:
+                    continue
+                t = numpy.zeros(len(m0), TCUNIT_DT)
+                t["a_map"], t["b_map"] = amap, bmap[s_]
+                t["a_c1"], t["b_c1"] = m0, n0
+                t["nk"] = (K + TC_BK - 1) // TC_BK
+                t["m_valid"] = numpy.minimum(TC_BM, M - m0)
+                t["n_valid"] = w
+                t["nseg"] = nseg - sb
+                t["c_off"] = sb
+                tl.append(t)
+        if tl:
+            u, q = _replicate_units(numpy.concatenate(tl), poss)
+            u["a_c2"] = q
+            units.append(u)
+    u = numpy.concatenate(units) if units else numpy.zeros(0, TCUNIT_DT)
     sg = numpy.array(segs, dtype=TCSEG_DT) if segs else numpy.zeros(1, TCSEG_DT)
     return u, maps, sg
