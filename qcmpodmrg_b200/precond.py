@@ -194,11 +194,19 @@ class LearnedPreconditioner(object):
 
     def __call__(self, r, diag, e, x):
         self.it += 1
+        jac = r / ((diag - e).abs() + 1e-4)
         if not self.enabled:
-            return r / ((diag - e).abs() + 1e-4)
+            return jac
         X = features(r, diag, float(e), self.blk, self.nblk, self.it)
         Y, _, _ = self.net.forward(X)
-        return correction(r.contiguous(), diag.contiguous(), float(e), self.blk, Y)
+        c = correction(r.contiguous(), diag.contiguous(), float(e), self.blk, Y)
+        # Davidson uses only the direction: the correction gets the Jacobi step's norm, so a
+        # network scale that collapsed (or blew up) cannot drop the new direction below the
+        # orthogonalisation threshold; a non-finite correction falls back to Jacobi
+        nc = torch.linalg.norm(c)
+        if not bool(torch.isfinite(nc)) or float(nc) == 0.0:
+            return jac
+        return c * (torch.linalg.norm(jac) / nc)
 
     # -- training-pair collection (Davidson record hook)
     def record(self, r, diag, e, x):
