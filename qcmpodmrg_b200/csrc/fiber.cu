@@ -178,139 +178,156 @@ __device__ __forceinline__ void ld8(const double *p, double (&w)[CB]) {
   }
 }
 
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+// Persistent, software-pipelined fiber kernel.  Item i's metadata blob is fetched two
+// items ahead, its input rows and W blocks one item ahead (cp.async, double buffer),
+// so neither the multiply loop nor the staging loop waits on a dependent global load.
+// Work inside an item: (output block, 8-column block, 32-fiber half) units spread over
+// the warps; lane = fiber.
 template <typename T, int FPL>
-__global__ void __launch_bounds__(FT_THREADS)
-k_fiber2(const int2 *__restrict__ work, int nwork, const qc_ftask *__restrict__ tasks,
-         const qc_fin *__restrict__ fin, const qc_fout *__restrict__ fout, const qc_fpair *__restrict__ fpair,
-         const int *__restrict__ pair_wsm, const qc_op *__restrict__ ops, int max_rows, int max_w,
-         const T *__restrict__ A, const T *__restrict__ W, T *__restrict__ C) {
+__global__ void __launch_bounds__(FT_THREADS, 2)
+k_fiber2(const qc_fwork *__restrict__ work, int nwork, const int4 *__restrict__ blobs, const qc_op *__restrict__ ops,
+         int max_rows, int max_w, int max_blob, const T *__restrict__ A, const T *__restrict__ W, T *__restrict__ C) {
   constexpr int FT = 32 * FPL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *const As0 = reinterpret_cast<T *>(smem_raw);
-  T *const Ws0 = As0 + 2 * max_rows * FT;
+  int4 *const meta0 = reinterpret_cast<int4 *>(smem_raw);                    // [3][max_blob]
+  T *const As0 = reinterpret_cast<T *>(meta0 + 3 * max_blob);                // [2][max_rows * FT]
+  T *const Ws0 = As0 + 2 * max_rows * FT;                                    // [2][max_w + 8]
   const int a_stride = max_rows * FT, w_stride = max_w + 8;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NW = FT_THREADS / 32;
 
-  auto issue = [&](int wi, int b) {
-    const int2 wk = work[wi];
-    const qc_ftask t = tasks[wk.x];
-    const qc_op o = ops[wk.y];
-    const int nf = min(FT, t.F - t.f0);
-    const T *Ab = A + o.a_base;
-    for (int i = t.in_b; i < t.in_e; ++i) {
-      const qc_fin bk = fin[i];
-      const T *src = Ab + bk.a_off;
-      const int n = bk.rows * FT;
-      T *dst = As0 + b * a_stride + bk.srow * FT;
-      if (!bk.fiber_major) {
-        for (int idx = tid; idx < n; idx += FT_THREADS) {
-          const int r = idx / FT, f = idx - r * FT;
-          cp_async_elem(dst + idx, src + (long long)r * t.F + t.f0 + f, f < nf);
-        }
-      } else {
-        for (int idx = tid; idx < n; idx += FT_THREADS) {
-          const int f = idx / bk.rows, r = idx - f * bk.rows;
-          cp_async_elem(dst + r * FT + f, src + (long long)(t.f0 + f) * bk.rows + r, f < nf);
+  auto issue_meta = [&](int wi, int slot) {
+    if (wi < nwork) {
+      const qc_fwork wk = work[wi];
+      int4 *dst = meta0 + slot * max_blob;
+      for (int i = tid; i < wk.blob_len; i += FT_THREADS) cp_async16(dst + i, blobs + wk.blob + i);
+    }
+    cp_async_commit();
+  };
+  auto issue_data = [&](int wi, int slot, int b) {
+    if (wi < nwork) {
+      const qc_fwork wk = work[wi];
+      const int4 *m = meta0 + slot * max_blob;
+      const qc_fblob_head h = *reinterpret_cast<const qc_fblob_head *>(m);
+      const qc_fin *fin = reinterpret_cast<const qc_fin *>(m + 1);
+      const qc_fout *fout = reinterpret_cast<const qc_fout *>(m + 1 + 2 * h.n_in);
+      const qc_fpair2 *fpair = reinterpret_cast<const qc_fpair2 *>(m + 1 + 2 * h.n_in + 2 * h.n_out);
+      const qc_op o = ops[wk.op];
+      const int nf = min(FT, wk.F - wk.f0);
+      const T *Ab = A + o.a_base;
+      T *as = As0 + b * a_stride;
+      for (int i = 0; i < h.n_in; ++i) {
+        const qc_fin bk = fin[i];
+        const T *src = Ab + bk.a_off;
+        const int n = bk.rows * FT;
+        T *dst = as + bk.srow * FT;
+        if (!bk.fiber_major) {
+          for (int idx = tid; idx < n; idx += FT_THREADS) {
+            const int r = idx / FT, f = idx - r * FT;
+            cp_async_elem(dst + idx, src + (long long)r * wk.F + wk.f0 + f, f < nf);
+          }
+        } else {
+          for (int idx = tid; idx < n; idx += FT_THREADS) {
+            const int f = idx / bk.rows, r = idx - f * bk.rows;
+            cp_async_elem(dst + r * FT + f, src + (long long)(wk.f0 + f) * bk.rows + r, f < nf);
+          }
         }
       }
-    }
-    const T *Wb = W + o.b_base;
-    for (int j = t.out_b; j < t.out_e; ++j) {
-      const qc_fout ob = fout[j];
-      const int nc = ob.ncols, ncp = (nc + 3) & ~3;
-      for (int p = ob.pair_b; p < ob.pair_e; ++p) {
-        const qc_fpair pr = fpair[p];
-        const T *src = Wb + pr.w_off;
-        T *dst = Ws0 + b * w_stride + pair_wsm[p];
-        const int n = pr.rows * nc;
-        for (int e = tid; e < n; e += FT_THREADS) {
-          const int r = e / nc, c = e - r * nc;
-          cp_async_elem(dst + r * ncp + c, src + e, true);
+      const T *Wb = W + o.b_base;
+      T *ws = Ws0 + b * w_stride;
+      for (int j = 0; j < h.n_out; ++j) {
+        const qc_fout ob = fout[j];
+        const int nc = ob.ncols, ncp = (nc + 3) & ~3;
+        for (int p = ob.pair_b; p < ob.pair_e; ++p) {
+          const qc_fpair2 pr = fpair[p];
+          const T *src = Wb + pr.w_off;
+          T *dst = ws + pr.wsm;
+          const int n = pr.rows * nc;
+          for (int e = tid; e < n; e += FT_THREADS) {
+            const int r = e / nc, c = e - r * nc;
+            cp_async_elem(dst + r * ncp + c, src + e, true);
+          }
         }
       }
     }
     cp_async_commit();
   };
 
-  int buf = 0;
-  int wi = blockIdx.x;
-  if (wi < nwork) issue(wi, 0);
-  for (; wi < nwork; wi += gridDim.x) {
-    const int nxt = wi + gridDim.x;
-    if (nxt < nwork) {
-      issue(nxt, buf ^ 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
+  const int w0 = blockIdx.x;
+  if (w0 >= nwork) return;
+  issue_meta(w0, 0);
+  issue_meta(w0 + gridDim.x, 1);
+  cp_async_wait<1>();
+  __syncthreads();
+  issue_data(w0, 0, 0);
+  int k = 0;
+  for (int wi = w0; wi < nwork; wi += gridDim.x, ++k) {
+    const int slot = k % 3, buf = k & 1;
+    issue_meta(wi + 2 * gridDim.x, (k + 2) % 3);
+    cp_async_wait<1>();
     __syncthreads();
-    const int2 wk = work[wi];
-    const qc_ftask t = tasks[wk.x];
-    const qc_op o = ops[wk.y];
-    const int nf = min(FT, t.F - t.f0);
+    issue_data(wi + gridDim.x, (k + 1) % 3, buf ^ 1);
+    // ---- multiply item wi out of shared memory
+    const qc_fwork wk = work[wi];
+    const int4 *m = meta0 + slot * max_blob;
+    const qc_fblob_head h = *reinterpret_cast<const qc_fblob_head *>(m);
+    const qc_fout *fout = reinterpret_cast<const qc_fout *>(m + 1 + 2 * h.n_in);
+    const qc_fpair2 *fpair = reinterpret_cast<const qc_fpair2 *>(m + 1 + 2 * h.n_in + 2 * h.n_out);
+    const qc_op o = ops[wk.op];
+    const int nf = min(FT, wk.F - wk.f0);
     const T alpha = T(o.alpha);
     T *Cb = C + o.c_base;
     const T *as = As0 + buf * a_stride;
     const T *ws = Ws0 + buf * w_stride;
-    int j = t.out_b, cb = 0, skip = warp;
-    while (j < t.out_e) {
-      const int ncb = (fout[j].ncols + CB - 1) / CB;
-      if (skip < ncb - cb) { cb += skip; break; }
-      skip -= ncb - cb;
-      cb = 0;
-      ++j;
-    }
-    while (j < t.out_e) {
+    // units (output j, column block cb, fiber half q), output by output; warp w takes units w, w+NW, ...
+    int j = 0, u0 = 0;
+    for (int target = warp;; target += NW) {
+      while (j < h.n_out) {
+        const int nu = ((fout[j].ncols + CB - 1) / CB) * FPL;
+        if (target < u0 + nu) break;
+        u0 += nu;
+        ++j;
+      }
+      if (j >= h.n_out) break;
       const qc_fout ob = fout[j];
       const int nc = ob.ncols, ncp = (nc + 3) & ~3;
+      const int uu = target - u0;
+      const int cb = uu / FPL, q = uu - cb * FPL;
       const int c0 = cb * CB;
       const int nb = min(CB, nc - c0);
-      T acc[FPL][CB];
+      const int fl = lane + 32 * q;
+      T acc[CB];
 #pragma unroll
-      for (int q = 0; q < FPL; ++q)
-#pragma unroll
-        for (int i = 0; i < CB; ++i) acc[q][i] = T(0);
+      for (int i = 0; i < CB; ++i) acc[i] = T(0);
       for (int p = ob.pair_b; p < ob.pair_e; ++p) {
-        const qc_fpair pr = fpair[p];
-        const T *w = ws + pair_wsm[p] + c0;
-        const T *a = as + pr.srow * FT + lane;
-#pragma unroll 2
+        const qc_fpair2 pr = fpair[p];
+        const T *w = ws + pr.wsm + c0;
+        const T *a = as + pr.srow * FT + fl;
+#pragma unroll 4
         for (int r = 0; r < pr.rows; ++r) {
-          T av[FPL];
-#pragma unroll
-          for (int q = 0; q < FPL; ++q) av[q] = a[r * FT + 32 * q];
+          const T av = a[r * FT];
           T wv[CB];
           ld8(w + r * ncp, wv);
 #pragma unroll
-          for (int i = 0; i < CB; ++i)
-#pragma unroll
-            for (int q = 0; q < FPL; ++q) acc[q][i] = fma(av[q], wv[i], acc[q][i]);
+          for (int i = 0; i < CB; ++i) acc[i] = fma(av, wv[i], acc[i]);
         }
       }
+      if (fl < nf) {
+        const int fg = wk.f0 + fl;
+        T *dst = Cb + ob.c_off + (long long)(fg / ob.flo) * ob.fhs + (long long)(fg % ob.flo) * nc + c0;
 #pragma unroll
-      for (int q = 0; q < FPL; ++q) {
-        const int fl = lane + 32 * q;
-        if (fl < nf) {
-          const int fg = t.f0 + fl;
-          T *dst = Cb + ob.c_off + (long long)(fg / ob.flo) * ob.fhs + (long long)(fg % ob.flo) * nc + c0;
-#pragma unroll
-          for (int i = 0; i < CB; ++i)
-            if (i < nb) dst[i] = alpha * acc[q][i];
-        }
-      }
-      int adv = NW;
-      while (j < t.out_e && adv > 0) {
-        const int ncb = (fout[j].ncols + CB - 1) / CB;
-        if (cb + adv < ncb) { cb += adv; adv = 0; break; }
-        adv -= ncb - cb;
-        cb = 0;
-        ++j;
+        for (int i = 0; i < CB; ++i)
+          if (i < nb) dst[i] = alpha * acc[i];
       }
     }
     __syncthreads();
-    buf ^= 1;
   }
+  cp_async_wait<0>();
 }
 
 // dst[dst_off + i0*s0 + i1*s1 + i2*s2] = src[src_off + (i0*d1 + i1)*d2 + i2] for every
@@ -376,13 +393,12 @@ int launch_fiber(const void *tasks, long long ntasks, int opspan, const void *fi
 }
 
 template <typename T>
-int launch_fiber2(const void *work, long long nwork, const void *tasks, const void *fin, const void *fout,
-                  const void *fpair, const int *pair_wsm, const void *ops, int max_rows, int max_w, int fiber_tile,
-                  const T *A, const T *W, T *C, cudaStream_t s) {
+int launch_fiber2(const void *work, long long nwork, const void *blobs, const void *ops, int max_rows, int max_w,
+                  int max_blob, int fiber_tile, const T *A, const T *W, T *C, cudaStream_t s) {
   if (nwork <= 0) return QC_OK;
-  if (nwork > 0x7fffffffLL || max_rows < 1 || max_w < 0 || !pair_wsm) return QC_ERR_ARG;
+  if (nwork > 0x7fffffffLL || max_rows < 1 || max_w < 0 || max_blob < 1 || !work || !blobs) return QC_ERR_ARG;
   if (fiber_tile != 32 && fiber_tile != 64) return QC_ERR_ARG;
-  const size_t smem = (size_t)(2 * max_rows * fiber_tile + 2 * (max_w + 8)) * sizeof(T);
+  const size_t smem = (size_t)3 * max_blob * 16 + (size_t)(2 * max_rows * fiber_tile + 2 * (max_w + 8)) * sizeof(T);
   if (smem > 200 * 1024) return QC_ERR_ARG;
   static bool attr_set[2] = {false, false};
   static int nsm = 0;
@@ -411,13 +427,11 @@ int launch_fiber2(const void *work, long long nwork, const void *tasks, const vo
   if (g > nwork) g = nwork;
   const int grid = (int)g;
   if (v == 0)
-    k_fiber2<T, 1><<<grid, FT_THREADS, smem, s>>>((const int2 *)work, (int)nwork, (const qc_ftask *)tasks,
-                                                  (const qc_fin *)fin, (const qc_fout *)fout, (const qc_fpair *)fpair,
-                                                  pair_wsm, (const qc_op *)ops, max_rows, max_w, A, W, C);
+    k_fiber2<T, 1><<<grid, FT_THREADS, smem, s>>>((const qc_fwork *)work, (int)nwork, (const int4 *)blobs,
+                                                  (const qc_op *)ops, max_rows, max_w, max_blob, A, W, C);
   else
-    k_fiber2<T, 2><<<grid, FT_THREADS, smem, s>>>((const int2 *)work, (int)nwork, (const qc_ftask *)tasks,
-                                                  (const qc_fin *)fin, (const qc_fout *)fout, (const qc_fpair *)fpair,
-                                                  pair_wsm, (const qc_op *)ops, max_rows, max_w, A, W, C);
+    k_fiber2<T, 2><<<grid, FT_THREADS, smem, s>>>((const qc_fwork *)work, (int)nwork, (const int4 *)blobs,
+                                                  (const qc_op *)ops, max_rows, max_w, max_blob, A, W, C);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     fprintf(stderr, "[qcgpu] qc_fiber2: %s\n", cudaGetErrorString(e));
@@ -428,18 +442,18 @@ int launch_fiber2(const void *work, long long nwork, const void *tasks, const vo
 
 }  // namespace
 
-extern "C" int qc_fiber2_f64(const void *work, long long nwork, const void *tasks, const void *fin, const void *fout,
-                             const void *fpair, const int *pair_wsm, const void *ops, int max_rows, int max_w,
-                             int fiber_tile, const double *A, const double *W, double *C, void *stream) {
-  return launch_fiber2<double>(work, nwork, tasks, fin, fout, fpair, pair_wsm, ops, max_rows, max_w, fiber_tile, A,
-                               W, C, (cudaStream_t)stream);
+extern "C" int qc_fiber2_f64(const void *work, long long nwork, const void *blobs, const void *ops, int max_rows,
+                             int max_w, int max_blob, int fiber_tile, const double *A, const double *W, double *C,
+                             void *stream) {
+  return launch_fiber2<double>(work, nwork, blobs, ops, max_rows, max_w, max_blob, fiber_tile, A, W, C,
+                               (cudaStream_t)stream);
 }
 
-extern "C" int qc_fiber2_f32(const void *work, long long nwork, const void *tasks, const void *fin, const void *fout,
-                             const void *fpair, const int *pair_wsm, const void *ops, int max_rows, int max_w,
-                             int fiber_tile, const float *A, const float *W, float *C, void *stream) {
-  return launch_fiber2<float>(work, nwork, tasks, fin, fout, fpair, pair_wsm, ops, max_rows, max_w, fiber_tile, A,
-                              W, C, (cudaStream_t)stream);
+extern "C" int qc_fiber2_f32(const void *work, long long nwork, const void *blobs, const void *ops, int max_rows,
+                             int max_w, int max_blob, int fiber_tile, const float *A, const float *W, float *C,
+                             void *stream) {
+  return launch_fiber2<float>(work, nwork, blobs, ops, max_rows, max_w, max_blob, fiber_tile, A, W, C,
+                              (cudaStream_t)stream);
 }
 
 extern "C" int qc_block_permute(const void *descs, long long ndescs, int opspan, const void *ops, const double *src,

@@ -156,3 +156,30 @@ struct alignas(16) qc_tmdesc {
   int pad;
 };
 static_assert(sizeof(qc_tmdesc) == 112, "qc_tmdesc is 112 bytes");
+
+// ---- persistent fiber kernel: per-item work records and per-group metadata blobs ----
+// A fiber group's records (inputs, outputs, pairs with their W places) are packed on the
+// host into one contiguous blob of 16-byte units: [header][fin x n_in][fout x n_out][fpair2 x n_pair]
+// (fout.pair_b / pair_e index the blob's pairs).  A work item is one tile of fibers of one
+// group for one operator.
+struct alignas(16) qc_fwork {
+  int blob;            // first 16-byte unit of the group's blob
+  int blob_len;        // blob length in 16-byte units
+  int f0, F;           // first fiber of the tile, fibers of the group
+  int op;              // operator (index into the operator table)
+  int pad0, pad1, pad2;
+};
+static_assert(sizeof(qc_fwork) == 32, "qc_fwork is 32 bytes");
+
+struct alignas(16) qc_fblob_head {
+  int n_in, n_out, n_pair, pad;
+};
+static_assert(sizeof(qc_fblob_head) == 16, "qc_fblob_head is 16 bytes");
+
+struct alignas(16) qc_fpair2 {
+  long long w_off;     // W block offset (relative to the operator's B base)
+  int srow, rows;      // shared-memory rows of the input block, contracted extent
+  int wsm;             // place of this pair's W block in the item's W area (rows padded to 4)
+  int pad0, pad1, pad2;
+};
+static_assert(sizeof(qc_fpair2) == 32, "qc_fpair2 is 32 bytes");

@@ -572,6 +572,10 @@ FPAIR_DT = numpy.dtype([("w_off", "<i8"), ("srow", "<i4"), ("rows", "<i4")])
 assert FTASK_DT.itemsize == 32 and FIN_DT.itemsize == 32 and FOUT_DT.itemsize == 32 and FPAIR_DT.itemsize == 16
 FIBER_TILE = 32
 FIBER_PERSISTENT = True   # the persistent, double-buffered fiber kernel (qc_fiber2_*); False: qc_fiber_*
+FWORK_DT = numpy.dtype([("blob", "<i4"), ("blob_len", "<i4"), ("f0", "<i4"), ("F", "<i4"), ("op", "<i4"),
+                        ("pad", "<i4", (3,))])
+FPAIR2_DT = numpy.dtype([("w_off", "<i8"), ("srow", "<i4"), ("rows", "<i4"), ("wsm", "<i4"), ("pad", "<i4", (3,))])
+assert FWORK_DT.itemsize == 32 and FPAIR2_DT.itemsize == 32
 FIBER_ROWS_WIDE = 128     # staged rows up to which a tile holds 64 fibers (two per lane)
 FIBER_MAX_ROWS = 256
 
@@ -722,42 +726,95 @@ class FiberStage(object):
         self.span = int(max(1, (self.h_tasks["op_e"] - self.h_tasks["op_b"]).max())) if self.ntasks else 1
         self.name = name
         self.bytes = 0.0
-        # persistent kernel: (task, operator) work items and the shared-memory place of every
-        # pair's W block inside its fiber group's W area (rows padded to 4 elements)
+        # persistent kernel: per fiber group one metadata blob (inputs, outputs, pairs with the
+        # place of their W block in the item's W area, rows padded to 4), per (task, operator)
+        # one work record
         self.persistent = FIBER_PERSISTENT
         if self.ntasks:
-            n_op = (self.h_tasks["op_e"] - self.h_tasks["op_b"]).astype(numpy.int64)
-            tix = numpy.repeat(numpy.arange(self.ntasks), n_op)
-            opx = numpy.repeat(self.h_tasks["op_b"].astype(numpy.int64), n_op) + \
-                (numpy.arange(int(n_op.sum())) - numpy.repeat(numpy.cumsum(n_op) - n_op, n_op))
-            self.h_work = numpy.stack([tix, opx], axis=1).astype(numpy.int32)
-            fo = self.h_fout
-            npair_o = (fo["pair_e"] - fo["pair_b"]).astype(numpy.int64)
-            ncp = (fo["ncols"].astype(numpy.int64) + 3) // 4 * 4
-            wsz = numpy.zeros(len(self.h_fpair), dtype=numpy.int64)
-            own = numpy.repeat(numpy.arange(len(fo)), npair_o)
-            pidx = numpy.repeat(fo["pair_b"].astype(numpy.int64), npair_o) + \
-                (numpy.arange(int(npair_o.sum())) - numpy.repeat(numpy.cumsum(npair_o) - npair_o, npair_o))
-            wsz[pidx] = self.h_fpair["rows"][pidx].astype(numpy.int64) * ncp[own]
-            # fiber groups partition the outputs: group of output j = the group whose first output
-            # is the last group start <= j; a pair's place = exclusive prefix of W sizes from the
-            # group's first pair
-            tk = self.h_tasks[self.h_tasks["out_e"] > self.h_tasks["out_b"]]
-            gstart = numpy.unique(tk["out_b"].astype(numpy.int64))
-            wsm = numpy.zeros(len(self.h_fpair), dtype=numpy.int64)
-            mw = 0
-            if len(gstart) and len(pidx):
-                excl = numpy.cumsum(wsz) - wsz
-                g_of_out = numpy.searchsorted(gstart, numpy.arange(len(fo)), side="right") - 1
-                first_pair = fo["pair_b"].astype(numpy.int64)[gstart]
-                g_of_pair = g_of_out[own]
-                wsm[pidx] = excl[pidx] - excl[numpy.minimum(first_pair[g_of_pair], len(excl) - 1)]
-                gtot = numpy.bincount(g_of_pair, weights=wsz[pidx], minlength=len(gstart))
-                mw = int(gtot.max())
-            self.h_wsm = wsm.astype(numpy.int32)
-            self.max_w = (mw + 3) // 4 * 4
-            self.d_work = upload(self.h_work, device)
-            self.d_wsm = upload(self.h_wsm, device)
+            self._build_persistent(device)
+
+    def _build_persistent(self, device):
+        fo, fi, fp = self.h_fout, self.h_fin, self.h_fpair
+        tk = self.h_tasks[self.h_tasks["out_e"] > self.h_tasks["out_b"]]
+        gs, first = numpy.unique(tk["out_b"].astype(numpy.int64), return_index=True)
+        g_in_b = tk["in_b"][first].astype(numpy.int64)
+        g_in_e = tk["in_e"][first].astype(numpy.int64)
+        g_out_b = gs
+        g_out_e = tk["out_e"][first].astype(numpy.int64)
+        n_in, n_out = g_in_e - g_in_b, g_out_e - g_out_b
+        # outputs written as zeros have an empty pair range at an arbitrary index: a group's
+        # pairs are the union of its outputs' non-empty ranges (contiguous, in output order)
+        pb_all = fo["pair_b"].astype(numpy.int64)
+        pe_all = fo["pair_e"].astype(numpy.int64)
+        nonempty = pe_all > pb_all
+        big = numpy.iinfo(numpy.int64).max
+        g_of_out = numpy.searchsorted(gs, numpy.arange(len(fo)), side="right") - 1
+        in_grp = (g_of_out >= 0) & (numpy.arange(len(fo)) < g_out_e[numpy.maximum(g_of_out, 0)]) & nonempty
+        g_pb = numpy.full(len(gs), big, dtype=numpy.int64)
+        g_pe = numpy.zeros(len(gs), dtype=numpy.int64)
+        numpy.minimum.at(g_pb, g_of_out[in_grp], pb_all[in_grp])
+        numpy.maximum.at(g_pe, g_of_out[in_grp], pe_all[in_grp])
+        g_pb[g_pb == big] = 0
+        g_pe = numpy.maximum(g_pe, g_pb)
+        n_pair = g_pe - g_pb
+        owner = numpy.zeros(len(fp), dtype=numpy.int64)
+        ne = numpy.flatnonzero(nonempty)
+        cnt = pe_all[ne] - pb_all[ne]
+        owner[numpy.repeat(pb_all[ne], cnt) + (numpy.arange(int(cnt.sum())) - numpy.repeat(numpy.cumsum(cnt) - cnt, cnt))] = \
+            numpy.repeat(ne, cnt)
+        blen = 1 + 2 * (n_in + n_out + n_pair)
+        boff = numpy.cumsum(blen) - blen
+        tot = int(blen.sum())
+        blob = numpy.zeros((tot, 4), dtype=numpy.int32)
+        blob[boff, 0], blob[boff, 1], blob[boff, 2] = n_in, n_out, n_pair
+
+        def ranges(b, n):
+            g = numpy.repeat(numpy.arange(len(n)), n)
+            return g, numpy.arange(int(n.sum())) - numpy.repeat(numpy.cumsum(n) - n, n)
+
+        def put(rec_i32, g, loc, base):
+            dst = boff[g] + base[g] + 2 * loc
+            blob[dst] = rec_i32[:, 0:4]
+            blob[dst + 1] = rec_i32[:, 4:8]
+
+        g, loc = ranges(g_in_b, n_in)
+        put(fi[g_in_b[g] + loc].view(numpy.int32).reshape(-1, 8), g, loc, numpy.ones(len(gs), dtype=numpy.int64))
+        g, loc = ranges(g_out_b, n_out)
+        fo_g = fo[g_out_b[g] + loc].copy()
+        empty = fo_g["pair_e"] <= fo_g["pair_b"]
+        fo_g["pair_b"] = numpy.where(empty, 0, fo_g["pair_b"] - g_pb[g]).astype(numpy.int32)
+        fo_g["pair_e"] = numpy.where(empty, 0, fo_g["pair_e"] - g_pb[g]).astype(numpy.int32)
+        put(fo_g.view(numpy.int32).reshape(-1, 8), g, loc, 1 + 2 * n_in)
+        # W places: exclusive prefix of the padded W sizes inside the group
+        g, loc = ranges(g_pb, n_pair)
+        pidx = g_pb[g] + loc
+        own = owner[pidx]
+        ncp = (fo["ncols"].astype(numpy.int64) + 3) // 4 * 4
+        wsz = fp["rows"][pidx].astype(numpy.int64) * ncp[own]
+        excl = numpy.cumsum(wsz) - wsz
+        gstart = numpy.cumsum(n_pair) - n_pair
+        wsm = excl - excl[numpy.minimum(gstart[g], max(len(excl) - 1, 0))] if len(excl) else excl
+        p2 = numpy.zeros(len(pidx), FPAIR2_DT)
+        p2["w_off"], p2["srow"], p2["rows"], p2["wsm"] = fp["w_off"][pidx], fp["srow"][pidx], fp["rows"][pidx], wsm
+        put(p2.view(numpy.int32).reshape(-1, 8), g, loc, 1 + 2 * (n_in + n_out))
+        gw = numpy.bincount(g, weights=wsz, minlength=len(gs)) if len(g) else numpy.zeros(len(gs))
+        self.max_w = (int(gw.max()) + 3) // 4 * 4 if len(gw) else 0
+        self.max_blob = int(blen.max()) if len(blen) else 1
+        # work records: every (task, operator)
+        gid = numpy.searchsorted(gs, tk["out_b"].astype(numpy.int64))
+        n_op = (tk["op_e"] - tk["op_b"]).astype(numpy.int64)
+        t_of = numpy.repeat(numpy.arange(len(tk)), n_op)
+        opx = numpy.repeat(tk["op_b"].astype(numpy.int64), n_op) + \
+            (numpy.arange(int(n_op.sum())) - numpy.repeat(numpy.cumsum(n_op) - n_op, n_op))
+        wk = numpy.zeros(len(t_of), FWORK_DT)
+        wk["blob"] = boff[gid[t_of]]
+        wk["blob_len"] = blen[gid[t_of]]
+        wk["f0"], wk["F"] = tk["f0"][t_of], tk["F"][t_of]
+        wk["op"] = opx
+        self.h_work, self.h_blob = wk, blob
+        self.h_wsm_pairs = (pidx, wsm, own)
+        self.d_work = upload(wk, device)
+        self.d_blob = upload(blob, device)
 
     def run(self, A, B, C, kind="f64", stream=None):
         if self.ntasks == 0:
@@ -770,10 +827,9 @@ class FiberStage(object):
             e0.record()
         if self.persistent:
             fn = lib.qc_fiber2_f64 if kind == "f64" else lib.qc_fiber2_f32
-            check(fn(self.d_work.data_ptr(), len(self.h_work), self.d[0].data_ptr(), self.d[1].data_ptr(),
-                     self.d[2].data_ptr(), self.d[3].data_ptr(), self.d_wsm.data_ptr(), self.d[4].data_ptr(),
-                     self.max_rows, self.max_w, self.tile, A.data_ptr(), B.data_ptr(), C.data_ptr(), s),
-                  "qc_fiber2_" + kind)
+            check(fn(self.d_work.data_ptr(), len(self.h_work), self.d_blob.data_ptr(), self.d[4].data_ptr(),
+                     self.max_rows, self.max_w, self.max_blob, self.tile, A.data_ptr(), B.data_ptr(), C.data_ptr(),
+                     s), "qc_fiber2_" + kind)
         else:
             fn = lib.qc_fiber_f64 if kind == "f64" else lib.qc_fiber_f32
             check(fn(self.d[0].data_ptr(), self.ntasks, self.span, self.d[1].data_ptr(), self.d[2].data_ptr(),

@@ -12,7 +12,8 @@ the GPU through hand-written forward/backward/Adam kernels (csrc/mlp.cu).
 It is trained on pairs the solver produces itself: for every Davidson
 iteration k of a dot, the residual r_k and, once the dot has converged to x*,
 the exact correction direction t_k = x* - (x*.x_k) x_k; the loss is
-1 - cos(c(r_k), t_k).  Untrained or disabled, the fallback is the reference's
+1 - cos^2(c(r_k), t_k) (Davidson adds span{c}: the sign of c is irrelevant).
+Untrained, or not better than Jacobi on held-out pairs, the fallback is the reference's
 Jacobi formula (alpha = 1, sigma = 1e-4).  The preconditioner only changes the
 search directions, never the Rayleigh-Ritz eigenvalue.
 """
@@ -126,7 +127,9 @@ def correction(r, d, e, blk, Y):
 
 
 def loss_and_grad(r, d, e, blk, nblk, Y, t):
-    """1 - cos(c, t) and dL/dY (per block) for c = correction(r, d, e, blk, Y)."""
+    """1 - cos^2(c, t) and dL/dY (per block) for c = correction(r, d, e, blk, Y).  Davidson
+    adds span{c} to its subspace, so only the direction of c up to sign matters: the loss is
+    sign-invariant (1 - cos would push a correct direction of the opposite sign away)."""
     blk64 = blk.long()
     Yd = Y.double()
     inside = ((Yd > -YCLAMP) & (Yd < YCLAMP)).double()          # clamp(Y): zero gradient outside
@@ -138,10 +141,10 @@ def loss_and_grad(r, d, e, blk, nblk, Y, t):
     nc = torch.linalg.norm(c) + 1e-300
     nt = torch.linalg.norm(t) + 1e-300
     cos = torch.dot(c, t) / (nc * nt)
-    dc = -(t / (nc * nt) - cos * c / (nc * nc))
+    dc = -2.0 * cos * (t / (nc * nt) - cos * c / (nc * nc))
     g_la = torch.zeros(nblk, dtype=torch.float64, device=r.device).index_add_(0, blk64, dc * c)
     g_ls = torch.zeros(nblk, dtype=torch.float64, device=r.device).index_add_(0, blk64, -dc * c * sigma / den)
-    return float(1.0 - cos), (torch.stack([g_la, g_ls], dim=1) * inside).float().contiguous()
+    return float(1.0 - cos * cos), (torch.stack([g_la, g_ls], dim=1) * inside).float().contiguous()
 
 
 class LearnedPreconditioner(object):
@@ -169,18 +172,26 @@ class LearnedPreconditioner(object):
             self.collect = True
 
     def end_sweep(self):
-        """Schedule hook: after train_sweeps sweeps of collected pairs, train and enable."""
+        """Schedule hook: after train_sweeps sweeps of collected pairs, train on the GPU and
+        switch the network on only if it beats Jacobi on held-out pairs (every fifth pair,
+        not trained on) by at least 5 %; otherwise the Jacobi fallback stays."""
         self.sweeps += 1
         if self.train_sweeps > 0 and self.sweeps == self.train_sweeps:
             self.collect = False
             import time as _t
             t0 = _t.time()
-            jac = self.jacobi_loss()
+            held = self.pairs[4::5]
+            train = [p for i, p in enumerate(self.pairs) if i % 5 != 4]
+            self.pairs = train
             losses = self.train(epochs=self.epochs)
-            self.enabled = True
-            self.train_info = {"pairs": len(self.pairs), "epochs": self.epochs, "train_s": round(_t.time() - t0, 2),
+            self.pairs = held
+            jac, mod = self.jacobi_loss(), self.model_loss()
+            self.enabled = bool(held) and mod < 0.95 * jac
+            self.train_info = {"pairs": len(train), "held_out": len(held), "epochs": self.epochs,
+                               "train_s": round(_t.time() - t0, 2),
                                "loss_first": losses[0] if losses else None,
-                               "loss_last": losses[-1] if losses else None, "jacobi_loss": jac}
+                               "loss_last": losses[-1] if losses else None,
+                               "held_out_loss_jacobi": jac, "held_out_loss_network": mod}
             self.pairs = []              # the device copies are not needed any more
 
     def summary(self):

@@ -41,7 +41,10 @@ def patch_stage_run(monkeypatch):
         a = _f64(A)
         w = _f64(B)
         c = _f64(C)
-        _run_fiber(self, a, w, c)
+        if self.persistent:
+            _run_fiber2(self, a, w, c)
+        else:
+            _run_fiber(self, a, w, c)
         C.copy_(torch.from_numpy(c).to(C.dtype))
 
     monkeypatch.setattr(engine.FiberStage, "run", frun)
@@ -218,3 +221,40 @@ def _run_tcpanel(st, A, B, C):
                 mm = numpy.arange(int(u["m_valid"]))
                 idx = o["c_base"] + sg["off"] + (int(u["a_c1"]) + mm[:, None]) * int(sg["ldc"]) + c[None, :]
                 C[idx] = tile[:, int(sg["col0"]) + c]
+
+
+def decode_blob(st, wk):
+    """The metadata blob of a persistent-fiber work record: (fins, fouts, pairs2)."""
+    from qcmpodmrg_b200.engine import FIN_DT, FOUT_DT, FPAIR2_DT
+    b = st.h_blob[int(wk["blob"]):int(wk["blob"]) + int(wk["blob_len"])]
+    n_in, n_out, n_pair = (int(x) for x in b[0, :3])
+    raw = b[1:].copy().view(numpy.uint8).ravel()
+    fins = raw[:32 * n_in].view(FIN_DT)
+    fouts = raw[32 * n_in:32 * (n_in + n_out)].view(FOUT_DT)
+    pairs = raw[32 * (n_in + n_out):32 * (n_in + n_out + n_pair)].view(FPAIR2_DT)
+    return fins, fouts, pairs
+
+
+def _run_fiber2(st, A, W, C):
+    """Reference semantics of the persistent fiber kernel, from its work records and blobs only."""
+    FT = st.tile
+    for wk in st.h_work:
+        fins, fouts, pairs = decode_blob(st, wk)
+        o = st.host_ops[int(wk["op"])]
+        nf = min(FT, int(wk["F"]) - int(wk["f0"]))
+        f = int(wk["f0"]) + numpy.arange(nf)
+        rows = {}
+        for fi in fins:
+            base = o["a_base"] + fi["a_off"]
+            r = numpy.arange(fi["rows"])[:, None]
+            idx = base + (f[None, :] * fi["rows"] + r if fi["fiber_major"] else r * int(wk["F"]) + f[None, :])
+            rows[int(fi["srow"])] = A[idx]
+        for fo in fouts:
+            nc = int(fo["ncols"])
+            acc = numpy.zeros((nf, nc))
+            for p in pairs[int(fo["pair_b"]):int(fo["pair_e"])]:
+                wi = o["b_base"] + p["w_off"] + numpy.arange(p["rows"])[:, None] * nc + numpy.arange(nc)[None, :]
+                acc += rows[int(p["srow"])].T @ W[wi]
+            ci = o["c_base"] + fo["c_off"] + ((f // fo["flo"]) * fo["fhs"] + (f % fo["flo"]) * nc)[:, None] \
+                + numpy.arange(nc)[None, :]
+            C[ci] = o["alpha"] * acc

@@ -42,7 +42,7 @@ def test_mlp_forward_and_gradients_match_oracle(cuda):
 
 def test_training_beats_jacobi_on_solver_pairs(cuda):
     """Pairs from the first sweep train the network; held-out pairs from the next
-    sweep show the loss (1 - cos to the exact correction) it gains over Jacobi."""
+    sweep show the loss (1 - cos^2 to the exact correction) it gains over Jacobi."""
     from qcmpodmrg_b200.hamiltonian import make_hamiltonian
     from qcmpodmrg_b200.synthetic import product_mps
     from qcmpodmrg_b200.dmrg import DMRG
@@ -66,5 +66,36 @@ def test_training_beats_jacobi_on_solver_pairs(cuda):
     assert losses[-1] < losses[0]
     pc.pairs = held
     jac, mod = pc.jacobi_loss(), pc.model_loss()
-    print("held-out 1-cos: jacobi %.4f  learned %.4f" % (jac, mod))
+    print("held-out 1-cos^2: jacobi %.4f  learned %.4f" % (jac, mod))
     assert mod < jac
+
+
+def test_learned_preconditioner_in_sweeps(cuda):
+    """The trained, gated preconditioner in a DMRG run (trained on the pairs of the first two
+    sweeps): the same final energy as Jacobi (a preconditioner only changes the search
+    directions) and no more Davidson matrix-vector products on the later sweeps."""
+    from qcmpodmrg_b200.hamiltonian import make_hamiltonian
+    from qcmpodmrg_b200.synthetic import product_mps
+    from qcmpodmrg_b200.dmrg import DMRG
+    from qcmpodmrg_b200.precond import LearnedPreconditioner
+    ham = make_hamiltonian(12, 12, 3, 3.0)
+
+    def run(pc):
+        d = DMRG(ham, device=cuda, preconditioner=pc)
+        d.load_mps(product_mps(ham))
+        nm, e = [], None
+        for D in (16, 32, 64, 64, 64, 64):
+            n0 = d.stats["nmvp"]
+            d.sweep("R", D, 1e-8)
+            _, e, _, _, _ = d.sweep("L", D, 1e-8)
+            if pc is not None:
+                pc.end_sweep()
+            nm.append(d.stats["nmvp"] - n0)
+        return nm, e
+
+    nj, ej = run(None)
+    pc = LearnedPreconditioner(cuda, seed=1, train_sweeps=2, epochs=30)
+    nl, el = run(pc)
+    print("matvecs jacobi %s learned %s; %s" % (nj, nl, pc.summary()))
+    assert abs(el - ej) <= 1e-6
+    assert sum(nl[2:]) <= 1.05 * sum(nj[2:])
