@@ -8,17 +8,19 @@
 // the sigma rows of that sector; the K extent (sum over MPO sectors c of D_c * D_r)
 // is long, the N extent (D_r') short.
 //
-// Persistent, warp-specialised CTA (6 warps):
+// Persistent, warp-specialised CTA (10 warps):
 //   warp 0     one thread issues the TMA loads (cp.async.bulk.tensor, 128-byte swizzle)
 //              of every 32-wide K stage into a ring of S shared-memory stages;
 //   warp 1     owns the tensor memory (2 x BN columns: two accumulators) and one thread
 //              issues tcgen05.mma kind::tf32, 12 per stage: a_lo.b_hi + a_hi.b_lo +
 //              a_hi.b_hi for each 8-wide K step, committed to the stage's "empty"
 //              barrier and, after a unit's last stage, to the accumulator's "full" one;
-//   warps 2-5  split each raw FP32 A stage in place into hi = tf32(x) and a lo plane
-//              tf32(x - hi) (A_SPLIT), then read a finished accumulator with
-//              tcgen05.ld (warp w owns TMEM lanes 32*(w%4) ..) and store its rows through
-//              the row table; the other accumulator meanwhile takes the next unit.
+//   warps 2-9  split each raw FP32 A stage in place into hi = tf32(x) and a lo plane
+//              tf32(x - hi) (A_SPLIT); every 2 K stages add the TMEM accumulator into FP32
+//              registers (tcgen05.ld: warp w owns TMEM lanes 32*(w%4) .. and one half of the
+//              columns), and store the finished tile (rows through the row table, or
+//              column segments staged in shared memory); the other TMEM accumulator
+//              meanwhile takes the next chunk.
 // No cluster, no multicast: every CTA loads its own tiles of this GPU's own memory.
 // Every wait is bounded: on expiry the CTA raises *err, stops issuing work, waits
 // (bounded) for its loads and products in flight and still frees its tensor memory.
@@ -35,7 +37,8 @@ namespace {
 
 constexpr int TP_BM = 128;
 constexpr int TP_BK = 32;                  // 32 FP32 = 128 bytes: one swizzle row
-constexpr int TP_THREADS = 192;
+constexpr int TP_THREADS = 320;             // producer warp, MMA warp, 8 helper warps
+constexpr int TP_HELPERS = 8;
 constexpr long long TP_SPIN = 1LL << 26;   // polls before a wait gives up (~seconds)
 constexpr int TP_CHUNK = 2;                 // K stages accumulated in TMEM before promotion to FP32 registers
 
@@ -140,7 +143,6 @@ __host__ __device__ constexpr int stage_bytes() { return 2 * TP_BM * TP_BK * 4 +
 
 constexpr int EPI_ROWS = 0;       // rows through a row table, stored from registers
 constexpr int EPI_SEGMENTS = 1;   // column segments, staged in shared memory, coalesced stores
-constexpr int EPI_HALF = 64;      // columns staged at a time (segment form)
 
 template <bool A_SPLIT, int BN, int S, int EPI>
 __global__ void __launch_bounds__(TP_THREADS, 1)
@@ -170,11 +172,11 @@ k_tcpanel(const qc_tcunit *__restrict__ units, int nunits, const CUtensorMap *__
     for (int s = 0; s < S; ++s) {
       mbar_init(su32(&full[s]), 1);
       mbar_init(su32(&empty[s]), 1);
-      mbar_init(su32(&split[s]), 4);
+      mbar_init(su32(&split[s]), TP_HELPERS);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(su32(&accf[b]), 1);
-      mbar_init(su32(&acce[b]), 4);
+      mbar_init(su32(&acce[b]), TP_HELPERS);
     }
     mbar_init(su32(&fin), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -280,11 +282,15 @@ k_tcpanel(const qc_tcunit *__restrict__ units, int nunits, const CUtensorMap *__
       }
     }
   } else {
-    // ------------------------------------------------------------ split + promotion + epilogue (warps 2-5)
-    const int hid = threadIdx.x - 64;          // 0 .. 127
+    // ------------------------------------------------------------ split + promotion + epilogue (warps 2-9)
+    // two warpgroups: warp w reads TMEM lanes 32*(w%4) .. (its quarter of the rows) and the
+    // accumulator columns of its group, [BN/2 * gw, BN/2 * (gw + 1))
+    constexpr int HALF = BN / 2;
+    const int hid = threadIdx.x - 64;          // 0 .. 255
     const int q = warp & 3;                    // TMEM lane quarter of this warp
+    const int gw = (warp - 2) >> 2;            // column half of this warp's group
     const int row = q * 32 + lane;
-    float acc[BN];
+    float acc[HALF];
     int it = 0;                                // stages split so far
     // the chunk stream (unit, first stage) in the order the MMA issuer takes it; the next
     // chunk's stages are split before the current chunk is drained, so the tensor core
@@ -302,8 +308,8 @@ k_tcpanel(const qc_tcunit *__restrict__ units, int nunits, const CUtensorMap *__
           float4 *a0 = reinterpret_cast<float4 *>(smem + s * ST_BYTES);
           float4 *a1 = reinterpret_cast<float4 *>(smem + s * ST_BYTES + A_BYTES);
 #pragma unroll
-          for (int j = 0; j < A_BYTES / 16 / 128; ++j) {
-            const int i = hid + j * 128;
+          for (int j = 0; j < A_BYTES / 16 / (32 * TP_HELPERS); ++j) {
+            const int i = hid + j * 32 * TP_HELPERS;
             const float4 x = a0[i];
             float4 h, l;
             h.x = tf32_rna(x.x); l.x = tf32_rna(x.x - h.x);
@@ -339,10 +345,10 @@ k_tcpanel(const qc_tcunit *__restrict__ units, int nunits, const CUtensorMap *__
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * BN);
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * BN + gw * HALF);
 #pragma unroll
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-          if (c0 < ncol) {
+        for (int c0 = 0; c0 < HALF; c0 += 16) {
+          if (gw * HALF + c0 < ncol) {
             uint32_t r[16];
             tmem_ld16(taddr + (uint32_t)c0, r);
 #pragma unroll
@@ -359,38 +365,29 @@ k_tcpanel(const qc_tcunit *__restrict__ units, int nunits, const CUtensorMap *__
       const float alpha = (float)o.alpha;
       if (EPI == EPI_ROWS) {
         if (row < t.m_valid) {
-          float *dst = C + o.c_base + crow[t.c_off + row] + t.b_c1;
+          float *dst = C + o.c_base + crow[t.c_off + row] + t.b_c1 + gw * HALF;
 #pragma unroll
-          for (int c = 0; c < BN; ++c)
-            if (c < ncol) dst[c] = alpha * acc[c];
+          for (int c = 0; c < HALF; ++c)
+            if (gw * HALF + c < ncol) dst[c] = alpha * acc[c];
         }
       } else {
-        // stage EPI_HALF columns at a time in shared memory (row stride EPI_HALF + 1: no bank
-        // conflicts), then each warp copies whole rows of every segment, lanes on consecutive
-        // columns (coalesced: a segment row is contiguous in memory)
+        // the whole tile staged in shared memory (row stride BN + 1: no bank conflicts), then
+        // each warp copies whole rows of every segment, lanes on consecutive columns
+        // (coalesced: a segment row is contiguous in memory)
         float *stg = reinterpret_cast<float *>(smem + S * ST_BYTES);
         float *Cb = C + o.c_base;
 #pragma unroll
-        for (int h0 = 0; h0 < BN; h0 += EPI_HALF) {
-          if (h0 < ncol) {
-#pragma unroll
-            for (int c = 0; c < EPI_HALF; ++c) stg[row * (EPI_HALF + 1) + c] = alpha * acc[h0 + c];
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-            const int hw = (ncol - h0) < EPI_HALF ? (ncol - h0) : EPI_HALF;
-            for (int si = 0; si < t.nseg; ++si) {
-              const qc_tcseg sg = segs[t.c_off + si];
-              const int c_lo = sg.col0 > h0 ? sg.col0 : h0;
-              const int c_hi = (sg.col0 + sg.ncol) < (h0 + hw) ? (sg.col0 + sg.ncol) : (h0 + hw);
-              const int w = c_hi - c_lo;
-              if (w <= 0) continue;
-              float *db = Cb + sg.off + (long long)t.a_c1 * sg.ldc + (c_lo - sg.col0);
-              const float *sb = stg + (c_lo - h0);
-              for (int m = q; m < t.m_valid; m += 4)
-                for (int c = lane; c < w; c += 32) db[(long long)m * sg.ldc + c] = sb[m * (EPI_HALF + 1) + c];
-            }
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-          }
+        for (int c = 0; c < HALF; ++c) stg[row * (BN + 1) + gw * HALF + c] = alpha * acc[c];
+        asm volatile("bar.sync 1, %0;" ::"n"(32 * TP_HELPERS) : "memory");
+        for (int si = 0; si < t.nseg; ++si) {
+          const qc_tcseg sg = segs[t.c_off + si];
+          const int w = sg.ncol;
+          float *db = Cb + sg.off + (long long)t.a_c1 * sg.ldc;
+          const float *sb = stg + sg.col0;
+          for (int m = warp - 2; m < t.m_valid; m += TP_HELPERS)
+            for (int c = lane; c < w; c += 32) db[(long long)m * sg.ldc + c] = sb[m * (BN + 1) + c];
         }
+        asm volatile("bar.sync 1, %0;" ::"n"(32 * TP_HELPERS) : "memory");
       }
     }
     if (!ok) fail();
@@ -432,8 +429,9 @@ PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
 constexpr int TP_BN = 128;
 constexpr int TP_S = 3;
+constexpr int tp_stages(int epi) { return epi == EPI_SEGMENTS ? 2 : TP_S; }
 constexpr size_t tp_dsmem(int epi) {
-  return (size_t)TP_S * stage_bytes<TP_BN>() + 1024 + (epi == EPI_SEGMENTS ? TP_BM * (EPI_HALF + 1) * 4 : 0);
+  return (size_t)tp_stages(epi) * stage_bytes<TP_BN>() + 1024 + (epi == EPI_SEGMENTS ? TP_BM * (TP_BN + 1) * 4 : 0);
 }
 bool g_attr[2] = {false, false};
 
@@ -453,14 +451,14 @@ int launch_tcpanel(const void *units, long long nunits, const void *maps, const 
       cudaDeviceGetAttribute(&g_nsm, cudaDevAttrMultiProcessorCount, dev);
     }
     if (!g_attr[EPI]) {
-      if (cudaFuncSetAttribute(k_tcpanel<A_SPLIT, TP_BN, TP_S, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      if (cudaFuncSetAttribute(k_tcpanel<A_SPLIT, TP_BN, tp_stages(EPI), EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)tp_dsmem(EPI)) != cudaSuccess)
         return QC_ERR_CUDA;
       g_attr[EPI] = true;
     }
   }
   const int grid = (int)(nunits < (long long)g_nsm ? nunits : (long long)g_nsm);
-  k_tcpanel<A_SPLIT, TP_BN, TP_S, EPI><<<grid, TP_THREADS, tp_dsmem(EPI), s>>>(
+  k_tcpanel<A_SPLIT, TP_BN, tp_stages(EPI), EPI><<<grid, TP_THREADS, tp_dsmem(EPI), s>>>(
       (const qc_tcunit *)units, (int)nunits, (const CUtensorMap *)maps, (const qc_op *)ops, crow,
       (const qc_tcseg *)segs, C, g_tp_err);
   cudaError_t e = cudaGetLastError();
