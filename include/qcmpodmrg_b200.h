@@ -207,6 +207,42 @@ int qc_fiber_f32(const void *tasks_dev, long long ntasks, int opspan, const void
                  const void *fout_dev, const void *fpair_dev, const void *ops_dev, int max_rows,
                  int fiber_tile, const float *A, const float *W, float *C, void *stream);
 
+/* Persistent form of the fiber-group contraction (default): every (task, operator) item is
+ * a qc_fwork record (32 B) whose fiber group's records are one metadata blob (qc_fblob_head,
+ * qc_fin x n_in, qc_fout x n_out, qc_fpair2 x n_pair, 16-byte units, blobs_dev); resident
+ * CTAs prefetch an item's blob two items ahead and its input rows and W blocks (rows padded
+ * to 4 in a W area of max_w elements) one item ahead with cp.async.  Same result as
+ * qc_fiber_*.  Replaces the same loops as qc_fiber_* (kernelQt.py:269-306). */
+int qc_fiber2_f64(const void *work_dev, long long nwork, const void *blobs_dev, const void *ops_dev, int max_rows,
+                  int max_w, int max_blob, int fiber_tile, const double *A, const double *W, double *C,
+                  void *stream);
+int qc_fiber2_f32(const void *work_dev, long long nwork, const void *blobs_dev, const void *ops_dev, int max_rows,
+                  int max_w, int max_blob, int fiber_tile, const float *A, const float *W, float *C,
+                  void *stream);
+
+/* ---------------------------------------------- tensor-core panel GEMM (TMA + tcgen05)
+ * Replaces the pair loops of top1 = tensordot(L, psi) and top4 = tensordot(top3, R)
+ * (source/mpo_dmrg_kernelQt.py:269-273, 302-306; tensordotCAL, qtensor.py:642-659) in the
+ * split-TF32 precision: per work unit (qc_tcunit, 64 B) a 128-row tile C = A . B^T with A
+ * and B read by TMA through tensor maps (maps_dev: CUtensorMap records encoded by
+ * qc_tmap_encode) of this GPU's own buffers, K-major, 128-byte swizzle; FP32 output. */
+/* Encodes n tensor maps (qc_tmdesc records, FP32 elements) into out_maps (n x 128 bytes, host). */
+int qc_tmap_encode(int n, const void *descs, void *out_maps);
+/* Row form: A raw FP32 (split into TF32 hi/lo in the kernel), B pre-split planes; row m of a
+ * unit goes to C + ops[op].c_base + crow[c_off + m] + b_c1 (the .R contraction into sigma). */
+int qc_tcpanel_f32(const void *units_dev, long long nunits, const void *maps_dev, const void *ops_dev,
+                   const long long *crow_dev, float *C, void *stream);
+/* Segment form: A and B pre-split planes; a unit's columns are nseg qc_tcseg segments, each
+ * with its own destination and row stride (the L.psi contraction into the T1 panels). */
+int qc_tcpanel_seg_f32(const void *units_dev, long long nunits, const void *maps_dev, const void *ops_dev,
+                       const void *segs_dev, float *C, void *stream);
+/* hi[i] = tf32(x[i]) in place, lo[i] = tf32(x[i] - hi[i]) (n values). */
+int qc_tf32_split(float *hi, float *lo, long long n, void *stream);
+/* hi[i] = tf32(x[idx[i]]), lo[i] = tf32(x[idx[i]] - hi[i]) from an FP64 vector (idx < 0: 0). */
+int qc_gather_split_f32(const double *x, const long long *idx, long long n, float *hi, float *lo, void *stream);
+/* 1 if a tensor-core panel launch reported a timed-out wait since the last clear, else 0. */
+int qc_tcpanel_status(int clear);
+
 /* dst[i] = src[idx[i]] (FP64), i < n.  Used for diag[prjmap] (kernelQt.py:122) and, with
  * spin projection, for projectionNMs of the N-symmetry sigma back to the (N, Sz) layout
  * (qtensor.py:546-560, called at kernelQt.py:310 and :445). */
