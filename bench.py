@@ -294,9 +294,12 @@ def run_ours(args):
 
 def stage_kernel(stage, w_path, prec):
     panel = w_path in ("fiber", "fused")
-    return {"sigma1": "k_pgemm" if panel else "k_bgemm", "sigma2": "k_fiber" if panel else "k_bgemm",
-            "sigma3": "k_fiber" if panel else "k_bgemm", "sigma23": "k_fiber",
-            "sigma4": ("k_tcpanel" if prec == "tf32x3" else "k_pgemm") if panel else "k_bgemm"}.get(stage, "k_bgemm")
+    from qcmpodmrg_b200.engine import FIBER_FGEMM
+    fk = "k_fgemm" if FIBER_FGEMM else "k_fiber"
+    tc = "k_tcpanel" if prec == "tf32x3" else "k_pgemm"
+    return {"sigma1": tc if panel else "k_bgemm", "sigma2": fk if panel else "k_bgemm",
+            "sigma3": fk if panel else "k_bgemm", "sigma23": fk,
+            "sigma4": tc if panel else "k_bgemm"}.get(stage, "k_bgemm")
 
 
 # DRAM bytes per launch measured by ncu for a stage's kernel, scaled to the launch's

@@ -182,8 +182,10 @@ int qc_tc_status(void);
  * operators op_b .. op_e (grid.y, at most opspan).  Input blocks fin[in_b..in_e)
  * (qc_fin, 32 B: offset, rows, storage order [rows][F] or [F][rows], first row in
  * the staged tile) are staged once; each output block fout[out_b..out_e)
- * (qc_fout, 32 B: offset, fiber strides fhs/flo, ncols, pair range) is written as
- *   C[c_base + c_off + (f/flo)*fhs + (f%flo)*ncols + c]
+ * (qc_fout, 32 B: offset, fiber strides fhs/flo, column-major flag, ncols, pair range)
+ * is written as
+ *   C[c_base + c_off + (f/flo)*fhs + (f%flo)*ncols + c]      (colmajor = 0)
+ *   C[c_base + c_off + c*F + f]                              (colmajor = 1)
  *       = alpha * sum_pairs sum_r in[srow+r][f] * W[b_base + w_off + r*ncols + c]
  * (an empty pair range writes zeros)
  * with pairs fpair[pair_b..pair_e) (qc_fpair, 16 B).  fiber_tile (32 or 64) is
@@ -207,18 +209,25 @@ int qc_fiber_f32(const void *tasks_dev, long long ntasks, int opspan, const void
                  const void *fout_dev, const void *fpair_dev, const void *ops_dev, int max_rows,
                  int fiber_tile, const float *A, const float *W, float *C, void *stream);
 
-/* Persistent form of the fiber-group contraction (default): every (task, operator) item is
- * a qc_fwork record (32 B) whose fiber group's records are one metadata blob (qc_fblob_head,
- * qc_fin x n_in, qc_fout x n_out, qc_fpair2 x n_pair, 16-byte units, blobs_dev); resident
- * CTAs prefetch an item's blob two items ahead and its input rows and W blocks (rows padded
- * to 4 in a W area of max_w elements) one item ahead with cp.async.  Same result as
- * qc_fiber_*.  Replaces the same loops as qc_fiber_* (kernelQt.py:269-306). */
-int qc_fiber2_f64(const void *work_dev, long long nwork, const void *blobs_dev, const void *ops_dev, int max_rows,
-                  int max_w, int max_blob, int fiber_tile, const double *A, const double *W, double *C,
-                  void *stream);
-int qc_fiber2_f32(const void *work_dev, long long nwork, const void *blobs_dev, const void *ops_dev, int max_rows,
-                  int max_w, int max_blob, int fiber_tile, const float *A, const float *W, float *C,
-                  void *stream);
+/* Dense fiber-group GEMM (default form of the .W_i / .W_{i+1} contractions,
+ * kernelQt.py:301-306): inside a fiber group every output block reads every input block,
+ * so group g is C_g[F x CT] = alpha * A_g[F x R] . W_g[R x CT].  items_dev: qc_fgitem
+ * records (32 B: one tile of fibers of one group, a range of operators); groups_dev:
+ * qc_fggrp (48 B); rows_dev: qc_fgrow (16 B, A_g row r at a_base + off + f * fs);
+ * cols_dev: qc_fgcol (32 B, C_g column at c_base + off + (f / flo) * fhs + (f % flo) * fs);
+ * Wp: the W panels (qc_wpanel_*).  max_a / max_w (multiples of 4) and max_ct bound the
+ * items' staged A tile (R x FT), W panel (R x CTs) and columns.  Persistent CTAs of 128
+ * threads, two cp.async buffers.  Returns QC_ERR_ARG when the buffers exceed 220 KB of
+ * shared memory. */
+int qc_fgemm_f64(const void *items_dev, long long nitems, const void *groups_dev, const void *rows_dev,
+                 const void *cols_dev, const void *ops_dev, int max_a, int max_w, int max_ct, const double *A,
+                 const double *Wp, double *C, void *stream);
+int qc_fgemm_f32(const void *items_dev, long long nitems, const void *groups_dev, const void *rows_dev,
+                 const void *cols_dev, const void *ops_dev, int max_a, int max_w, int max_ct, const float *A,
+                 const float *Wp, float *C, void *stream);
+/* W panels of the dense fiber-group GEMM: dst[i] = idx[i] >= 0 ? src[idx[i]] : 0 (once per dot). */
+int qc_wpanel_f64(const double *src, const long long *idx_dev, double *dst, long long n, void *stream);
+int qc_wpanel_f32(const float *src, const long long *idx_dev, float *dst, long long n, void *stream);
 
 /* ---------------------------------------------- tensor-core panel GEMM (TMA + tcgen05)
  * Replaces the pair loops of top1 = tensordot(L, psi) and top4 = tensordot(top3, R)

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "lib")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-CUDA_SOURCES = ["bgemm.cu", "bgemm_tc.cu", "tcpanel.cu", "fiber.cu", "pgemm.cu", "sigma_noalloc.cu", "mlp.cu",
+CUDA_SOURCES = ["bgemm.cu", "bgemm_tc.cu", "tcpanel.cu", "fiber.cu", "fgemm.cu", "pgemm.cu", "sigma_noalloc.cu", "mlp.cu",
                 "blockmap.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -1,0 +1,306 @@
+// Dense fiber-group GEMM for the two W contractions of sigma (the .W_i and .W_{i+1}
+// stages of HVecQt, source/mpo_dmrg_kernelQt.py:301-306).
+//
+// In those contractions an output block (fibers f = (l, r) x columns c = MPO bond x
+// physical index) is a sum over input blocks times small W blocks.  The blocks that
+// share their fiber sectors form a group, and inside a group every output block reads
+// every input block, so the group is one dense product
+//     C_g[F x CT] = alpha * A_g[F x R] . W_g[R x CT]
+// with R = the input blocks' contracted rows, CT = the output blocks' columns and
+// W_g the group's W blocks laid out once per dot as a dense panel (qc_wpanel_*).
+//
+// A work item is one tile of FT fibers of one group for a range of operators.  A
+// persistent grid of 128-thread CTAs walks the (item, operator) sequence with two
+// shared-memory buffers: while one (item, operator) is multiplied, the next one's A
+// tile, W panel and column records are in flight (cp.async, zero fill past the tile).
+// Each thread owns 4 fibers x mc columns (mc = 4 or 8) of the C tile: per contracted
+// row it reads one 16-byte A vector and mc/4 16-byte W vectors from shared memory for
+// 4*mc FMAs.  Every A and C element crosses HBM once; the W panels stay in L2.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include "qc_types.h"
+
+namespace {
+
+constexpr int FG_THREADS = 128;
+
+__device__ __forceinline__ void cp_async4(void *dst, const void *src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(float *dst, const float *src, bool valid) {
+  cp_async4(dst, valid ? src : nullptr, valid);
+}
+__device__ __forceinline__ void cp_async_elem(double *dst, const double *src, bool valid) {
+  cp_async8(dst, valid ? src : nullptr, valid);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// four consecutive elements from shared memory (16-byte aligned)
+__device__ __forceinline__ void lds4(const float *p, float *v) {
+  const float4 a = *reinterpret_cast<const float4 *>(p);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = a.z;
+  v[3] = a.w;
+}
+__device__ __forceinline__ void lds4(const double *p, double *v) {
+  const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = b.x;
+  v[3] = b.y;
+}
+
+// Stage (item, operator) into one buffer: the A tile [R][FT] (row r, fiber f at
+// A + a_base + row.off + (f0 + f) * row.fs; zero for f >= nf), the operator's W panel
+// [R][CTs] and the group's column records.
+template <typename T>
+__device__ __forceinline__ void fg_stage(const qc_fgitem &it, int op, const qc_fggrp *__restrict__ groups,
+                                         const qc_fgrow *__restrict__ rows, const qc_fgcol *__restrict__ cols,
+                                         const qc_op *__restrict__ ops, const T *__restrict__ A,
+                                         const T *__restrict__ Wp, T *as, T *ws, qc_fgcol *cs) {
+  const int tid = threadIdx.x;
+  const qc_fggrp g = groups[it.group];
+  const T *Ab = A + ops[op].a_base;
+  const int FT = g.FT;
+  const int n = g.R * FT;
+  int r = tid / FT, f = tid - r * FT;
+  const int dr = FG_THREADS / FT, df = FG_THREADS - dr * FT;
+  const qc_fgrow *rw = rows + g.row_b;
+#pragma unroll 4
+  for (int e = tid; e < n; e += FG_THREADS) {
+    const qc_fgrow w = rw[r];
+    cp_async_elem(as + e, Ab + w.off + (long long)(it.f0 + f) * w.fs, f < it.nf);
+    r += dr;
+    f += df;
+    if (f >= FT) {
+      f -= FT;
+      ++r;
+    }
+  }
+  const T *wsrc = Wp + it.wpan + (long long)(op - it.op_b) * it.wstride;
+  const int nw16 = g.R * g.CTs * (int)sizeof(T) / 16;
+  for (int e = tid; e < nw16; e += FG_THREADS)
+    cp_async16(reinterpret_cast<char *>(ws) + 16 * e, reinterpret_cast<const char *>(wsrc) + 16 * e);
+  const int nc16 = g.CT * (int)(sizeof(qc_fgcol) / 16);
+  for (int e = tid; e < nc16; e += FG_THREADS)
+    cp_async16(reinterpret_cast<char *>(cs) + 16 * e, reinterpret_cast<const char *>(cols + g.col_b) + 16 * e);
+}
+
+// One thread tile: fibers 4*fc .. 4*fc+3 of the item x columns mc*cc .. mc*cc+mc-1.
+template <typename T, int MC>
+__device__ __forceinline__ void fg_tile(const T *as, const T *ws, const qc_fgcol *cs, const qc_fggrp &g, int f0,
+                                        int nf, int fc, int cc, T alpha, T *Cb) {
+  T acc[4][MC];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int c = 0; c < MC; ++c) acc[i][c] = T(0);
+  const T *a = as + 4 * fc;
+  const T *w = ws + MC * cc;
+  const int FT = g.FT, CTs = g.CTs, R = g.R;
+#pragma unroll 4
+  for (int r = 0; r < R; ++r) {
+    T av[4], wv[MC];
+    lds4(a + r * FT, av);
+#pragma unroll
+    for (int q = 0; q < MC; q += 4) lds4(w + r * CTs + q, wv + q);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int c = 0; c < MC; ++c) acc[i][c] = fma(av[i], wv[c], acc[i][c]);
+  }
+  // fibers -> (f / flo, f % flo), advanced one fiber at a time
+  const int fl0 = 4 * fc;
+  const int fg0 = f0 + fl0;
+  int qf[4], rf[4];
+  if (g.flo >= g.F) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      qf[i] = 0;
+      rf[i] = fg0 + i;
+    }
+  } else {
+    int q = fg0 / g.flo, rm = fg0 - q * g.flo;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      qf[i] = q;
+      rf[i] = rm;
+      if (++rm == g.flo) {
+        rm = 0;
+        ++q;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < MC; ++c) {
+    const int col = MC * cc + c;
+    if (col < g.CT) {
+      const qc_fgcol cl = cs[col];
+      T *dst = Cb + cl.off;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (fl0 + i < nf) dst[(long long)qf[i] * cl.fhs + (long long)rf[i] * cl.fs] = alpha * acc[i][c];
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FG_THREADS, 4)
+k_fgemm(const qc_fgitem *__restrict__ items, int nitems, const qc_fggrp *__restrict__ groups,
+        const qc_fgrow *__restrict__ rows, const qc_fgcol *__restrict__ cols, const qc_op *__restrict__ ops,
+        int max_a, int max_w, int max_ct, const T *__restrict__ A, const T *__restrict__ Wp, T *__restrict__ C) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  qc_fgcol *const cs0 = reinterpret_cast<qc_fgcol *>(smem_raw);   // [2][max_ct]
+  T *const as0 = reinterpret_cast<T *>(cs0 + 2 * max_ct);         // [2][max_a]
+  T *const ws0 = as0 + 2 * max_a;                                 // [2][max_w]
+  int i = blockIdx.x;
+  if (i >= nitems) return;
+  int op = items[i].op_b;
+  fg_stage<T>(items[i], op, groups, rows, cols, ops, A, Wp, as0, ws0, cs0);
+  cp_async_commit();
+  for (int k = 0;; ++k) {
+    const int buf = k & 1;
+    // the next (item, operator) of this CTA's sequence
+    int ni = i, nop = op + 1;
+    if (nop >= items[i].op_e) {
+      ni = i + (int)gridDim.x;
+      nop = ni < nitems ? items[ni].op_b : 0;
+    }
+    if (ni < nitems)
+      fg_stage<T>(items[ni], nop, groups, rows, cols, ops, A, Wp, as0 + (buf ^ 1) * max_a,
+                  ws0 + (buf ^ 1) * max_w, cs0 + (buf ^ 1) * max_ct);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    {
+      const qc_fgitem it = items[i];
+      const qc_fggrp g = groups[it.group];
+      const qc_op o = ops[op];
+      const T alpha = T(o.alpha);
+      T *Cb = C + o.c_base;
+      const T *as = as0 + buf * max_a;
+      const T *ws = ws0 + buf * max_w;
+      const qc_fgcol *cs = cs0 + buf * max_ct;
+      const int chunks = g.CTs / g.mc;
+      const int ntile = ((it.nf + 3) >> 2) * chunks;
+      for (int m = threadIdx.x; m < ntile; m += FG_THREADS) {
+        const int fc = m / chunks, cc = m - fc * chunks;
+        if (g.mc == 4) {
+          fg_tile<T, 4>(as, ws, cs, g, it.f0, it.nf, fc, cc, alpha, Cb);
+        } else if (sizeof(T) == 4) {
+          fg_tile<T, 8>(as, ws, cs, g, it.f0, it.nf, fc, cc, alpha, Cb);
+        } else {      // FP64: an 8-column tile as two 4-column tiles (register budget)
+          fg_tile<T, 4>(as, ws, cs, g, it.f0, it.nf, fc, 2 * cc, alpha, Cb);
+          fg_tile<T, 4>(as, ws, cs, g, it.f0, it.nf, fc, 2 * cc + 1, alpha, Cb);
+        }
+      }
+    }
+    __syncthreads();
+    if (ni >= nitems) break;
+    i = ni;
+    op = nop;
+  }
+  cp_async_wait<0>();
+}
+
+template <typename T>
+__global__ void k_wpanel(const T *__restrict__ src, const long long *__restrict__ idx, T *__restrict__ dst,
+                         long long n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long j = idx[e];
+    dst[e] = j >= 0 ? src[j] : T(0);
+  }
+}
+
+size_t fg_smem(int max_a, int max_w, int max_ct, size_t elem) {
+  return 2 * (size_t)max_ct * sizeof(qc_fgcol) + 2 * ((size_t)max_a + (size_t)max_w) * elem;
+}
+
+template <typename T>
+int launch_fgemm(const void *items, long long nitems, const void *groups, const void *rows, const void *cols,
+                 const void *ops, int max_a, int max_w, int max_ct, const T *A, const T *Wp, T *C, cudaStream_t s) {
+  if (nitems <= 0) return QC_OK;
+  if (nitems > 0x7fffffffLL || !items || !groups || !ops || max_a < 4 || max_w < 0 || max_ct < 0 ||
+      (max_a % 4) || (max_w % 4))
+    return QC_ERR_ARG;
+  const size_t smem = fg_smem(max_a, max_w, max_ct, sizeof(T));
+  if (smem > 220 * 1024) return QC_ERR_ARG;
+  static int attr_smem = 0, nsm = 0;
+  if ((int)smem > attr_smem) {
+    cudaError_t ea = cudaFuncSetAttribute(k_fgemm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (ea != cudaSuccess) {
+      fprintf(stderr, "[qcgpu] qc_fgemm: %s\n", cudaGetErrorString(ea));
+      return QC_ERR_CUDA;
+    }
+    attr_smem = (int)smem;
+  }
+  if (nsm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fgemm<T>, FG_THREADS, smem);
+  if (per_sm < 1) per_sm = 1;
+  long long g = (long long)nsm * per_sm;
+  if (g > nitems) g = nitems;
+  k_fgemm<T><<<(int)g, FG_THREADS, smem, s>>>((const qc_fgitem *)items, (int)nitems, (const qc_fggrp *)groups,
+                                               (const qc_fgrow *)rows, (const qc_fgcol *)cols, (const qc_op *)ops,
+                                               max_a, max_w, max_ct, A, Wp, C);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "[qcgpu] qc_fgemm: %s\n", cudaGetErrorString(e));
+    return QC_ERR_CUDA;
+  }
+  return QC_OK;
+}
+
+template <typename T>
+int launch_wpanel(const T *src, const long long *idx, T *dst, long long n, cudaStream_t s) {
+  if (n <= 0) return QC_OK;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 4096) blocks = 4096;
+  k_wpanel<T><<<(int)blocks, 256, 0, s>>>(src, idx, dst, n);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "[qcgpu] qc_wpanel: %s\n", cudaGetErrorString(e));
+    return QC_ERR_CUDA;
+  }
+  return QC_OK;
+}
+
+}  // namespace
+
+extern "C" int qc_fgemm_f64(const void *items, long long nitems, const void *groups, const void *rows,
+                            const void *cols, const void *ops, int max_a, int max_w, int max_ct, const double *A,
+                            const double *Wp, double *C, void *stream) {
+  return launch_fgemm<double>(items, nitems, groups, rows, cols, ops, max_a, max_w, max_ct, A, Wp, C,
+                              (cudaStream_t)stream);
+}
+
+extern "C" int qc_fgemm_f32(const void *items, long long nitems, const void *groups, const void *rows,
+                            const void *cols, const void *ops, int max_a, int max_w, int max_ct, const float *A,
+                            const float *Wp, float *C, void *stream) {
+  return launch_fgemm<float>(items, nitems, groups, rows, cols, ops, max_a, max_w, max_ct, A, Wp, C,
+                             (cudaStream_t)stream);
+}
+
+extern "C" int qc_wpanel_f64(const double *src, const long long *idx, double *dst, long long n, void *stream) {
+  return launch_wpanel<double>(src, idx, dst, n, (cudaStream_t)stream);
+}
+
+extern "C" int qc_wpanel_f32(const float *src, const long long *idx, float *dst, long long n, void *stream) {
+  return launch_wpanel<float>(src, idx, dst, n, (cudaStream_t)stream);
+}

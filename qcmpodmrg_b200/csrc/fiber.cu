@@ -122,10 +122,17 @@ k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, cons
       const int fl = lane + 32 * q;
       if (fl < nf) {
         const int fg = t.f0 + fl;
-        T *dst = Cb + ob.c_off + (long long)(fg / ob.flo) * ob.fhs + (long long)(fg % ob.flo) * nc + c0;
+        if (ob.colmajor) {
+          T *dst = Cb + ob.c_off + (long long)c0 * t.F + fg;
 #pragma unroll
-        for (int i = 0; i < CB; ++i)
-          if (i < nb) dst[i] = alpha * acc[q][i];
+          for (int i = 0; i < CB; ++i)
+            if (i < nb) dst[(long long)i * t.F] = alpha * acc[q][i];
+        } else {
+          T *dst = Cb + ob.c_off + (long long)(fg / ob.flo) * ob.fhs + (long long)(fg % ob.flo) * nc + c0;
+#pragma unroll
+          for (int i = 0; i < CB; ++i)
+            if (i < nb) dst[i] = alpha * acc[q][i];
+        }
       }
     }
     // advance NW items
@@ -138,196 +145,6 @@ k_fiber(const qc_ftask *__restrict__ tasks, const qc_fin *__restrict__ fin, cons
       ++j;
     }
   }
-}
-
-// ---------------------------------------------------------------------------------------
-// Persistent fiber-group kernel.  Same work items as k_fiber, processed as a flat list of
-// (task, operator) items by a grid of resident CTAs.  While a CTA multiplies one item out
-// of shared memory, the next item's input rows and every W block it needs are already in
-// flight into the other shared-memory buffer (cp.async, zero fill beyond the tile), so the
-// HBM reads of T overlap the FMAs.  W blocks are staged with their rows padded to a
-// multiple of 4 elements (16-byte aligned), read as float4 / double2 broadcasts.
-__device__ __forceinline__ void cp_async4(void *dst, const void *src, bool valid) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void *dst, const void *src, bool valid) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
-}
-template <typename T>
-__device__ __forceinline__ void cp_async_elem(T *dst, const T *src, bool valid) {
-  if (sizeof(T) == 8) cp_async8(dst, valid ? src : nullptr, valid);
-  else cp_async4(dst, valid ? src : nullptr, valid);
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-// eight consecutive W values (16-byte aligned) from shared memory
-__device__ __forceinline__ void ld8(const float *p, float (&w)[CB]) {
-  const float4 a = *reinterpret_cast<const float4 *>(p), b = *reinterpret_cast<const float4 *>(p + 4);
-  w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w; w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
-}
-__device__ __forceinline__ void ld8(const double *p, double (&w)[CB]) {
-#pragma unroll
-  for (int i = 0; i < CB; i += 2) {
-    const double2 a = *reinterpret_cast<const double2 *>(p + i);
-    w[i] = a.x;
-    w[i + 1] = a.y;
-  }
-}
-
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-
-// Persistent, software-pipelined fiber kernel.  Item i's metadata blob is fetched two
-// items ahead, its input rows and W blocks one item ahead (cp.async, double buffer),
-// so neither the multiply loop nor the staging loop waits on a dependent global load.
-// Work inside an item: (output block, 8-column block, 32-fiber half) units spread over
-// the warps; lane = fiber.
-template <typename T, int FPL>
-__global__ void __launch_bounds__(FT_THREADS, 2)
-k_fiber2(const qc_fwork *__restrict__ work, int nwork, const int4 *__restrict__ blobs, const qc_op *__restrict__ ops,
-         int max_rows, int max_w, int max_blob, const T *__restrict__ A, const T *__restrict__ W, T *__restrict__ C) {
-  constexpr int FT = 32 * FPL;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  int4 *const meta0 = reinterpret_cast<int4 *>(smem_raw);                    // [3][max_blob]
-  T *const As0 = reinterpret_cast<T *>(meta0 + 3 * max_blob);                // [2][max_rows * FT]
-  T *const Ws0 = As0 + 2 * max_rows * FT;                                    // [2][max_w + 8]
-  const int a_stride = max_rows * FT, w_stride = max_w + 8;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  constexpr int NW = FT_THREADS / 32;
-
-  auto issue_meta = [&](int wi, int slot) {
-    if (wi < nwork) {
-      const qc_fwork wk = work[wi];
-      int4 *dst = meta0 + slot * max_blob;
-      for (int i = tid; i < wk.blob_len; i += FT_THREADS) cp_async16(dst + i, blobs + wk.blob + i);
-    }
-    cp_async_commit();
-  };
-  auto issue_data = [&](int wi, int slot, int b) {
-    if (wi < nwork) {
-      const qc_fwork wk = work[wi];
-      const int4 *m = meta0 + slot * max_blob;
-      const qc_fblob_head h = *reinterpret_cast<const qc_fblob_head *>(m);
-      const qc_fin *fin = reinterpret_cast<const qc_fin *>(m + 1);
-      const qc_fout *fout = reinterpret_cast<const qc_fout *>(m + 1 + 2 * h.n_in);
-      const qc_fpair2 *fpair = reinterpret_cast<const qc_fpair2 *>(m + 1 + 2 * h.n_in + 2 * h.n_out);
-      const qc_op o = ops[wk.op];
-      const int nf = min(FT, wk.F - wk.f0);
-      const T *Ab = A + o.a_base;
-      T *as = As0 + b * a_stride;
-      for (int i = 0; i < h.n_in; ++i) {
-        const qc_fin bk = fin[i];
-        const T *src = Ab + bk.a_off;
-        const int n = bk.rows * FT;
-        T *dst = as + bk.srow * FT;
-        if (!bk.fiber_major) {
-          for (int idx = tid; idx < n; idx += FT_THREADS) {
-            const int r = idx / FT, f = idx - r * FT;
-            cp_async_elem(dst + idx, src + (long long)r * wk.F + wk.f0 + f, f < nf);
-          }
-        } else {
-          for (int idx = tid; idx < n; idx += FT_THREADS) {
-            const int f = idx / bk.rows, r = idx - f * bk.rows;
-            cp_async_elem(dst + r * FT + f, src + (long long)(wk.f0 + f) * bk.rows + r, f < nf);
-          }
-        }
-      }
-      const T *Wb = W + o.b_base;
-      T *ws = Ws0 + b * w_stride;
-      for (int j = 0; j < h.n_out; ++j) {
-        const qc_fout ob = fout[j];
-        const int nc = ob.ncols, ncp = (nc + 3) & ~3;
-        for (int p = ob.pair_b; p < ob.pair_e; ++p) {
-          const qc_fpair2 pr = fpair[p];
-          const T *src = Wb + pr.w_off;
-          T *dst = ws + pr.wsm;
-          const int n = pr.rows * nc;
-          for (int e = tid; e < n; e += FT_THREADS) {
-            const int r = e / nc, c = e - r * nc;
-            cp_async_elem(dst + r * ncp + c, src + e, true);
-          }
-        }
-      }
-    }
-    cp_async_commit();
-  };
-
-  const int w0 = blockIdx.x;
-  if (w0 >= nwork) return;
-  issue_meta(w0, 0);
-  issue_meta(w0 + gridDim.x, 1);
-  cp_async_wait<1>();
-  __syncthreads();
-  issue_data(w0, 0, 0);
-  int k = 0;
-  for (int wi = w0; wi < nwork; wi += gridDim.x, ++k) {
-    const int slot = k % 3, buf = k & 1;
-    issue_meta(wi + 2 * gridDim.x, (k + 2) % 3);
-    cp_async_wait<1>();
-    __syncthreads();
-    issue_data(wi + gridDim.x, (k + 1) % 3, buf ^ 1);
-    // ---- multiply item wi out of shared memory
-    const qc_fwork wk = work[wi];
-    const int4 *m = meta0 + slot * max_blob;
-    const qc_fblob_head h = *reinterpret_cast<const qc_fblob_head *>(m);
-    const qc_fout *fout = reinterpret_cast<const qc_fout *>(m + 1 + 2 * h.n_in);
-    const qc_fpair2 *fpair = reinterpret_cast<const qc_fpair2 *>(m + 1 + 2 * h.n_in + 2 * h.n_out);
-    const qc_op o = ops[wk.op];
-    const int nf = min(FT, wk.F - wk.f0);
-    const T alpha = T(o.alpha);
-    T *Cb = C + o.c_base;
-    const T *as = As0 + buf * a_stride;
-    const T *ws = Ws0 + buf * w_stride;
-    // units (output j, column block cb, fiber half q), output by output; warp w takes units w, w+NW, ...
-    int j = 0, u0 = 0;
-    for (int target = warp;; target += NW) {
-      while (j < h.n_out) {
-        const int nu = ((fout[j].ncols + CB - 1) / CB) * FPL;
-        if (target < u0 + nu) break;
-        u0 += nu;
-        ++j;
-      }
-      if (j >= h.n_out) break;
-      const qc_fout ob = fout[j];
-      const int nc = ob.ncols, ncp = (nc + 3) & ~3;
-      const int uu = target - u0;
-      const int cb = uu / FPL, q = uu - cb * FPL;
-      const int c0 = cb * CB;
-      const int nb = min(CB, nc - c0);
-      const int fl = lane + 32 * q;
-      T acc[CB];
-#pragma unroll
-      for (int i = 0; i < CB; ++i) acc[i] = T(0);
-      for (int p = ob.pair_b; p < ob.pair_e; ++p) {
-        const qc_fpair2 pr = fpair[p];
-        const T *w = ws + pr.wsm + c0;
-        const T *a = as + pr.srow * FT + fl;
-#pragma unroll 4
-        for (int r = 0; r < pr.rows; ++r) {
-          const T av = a[r * FT];
-          T wv[CB];
-          ld8(w + r * ncp, wv);
-#pragma unroll
-          for (int i = 0; i < CB; ++i) acc[i] = fma(av, wv[i], acc[i]);
-        }
-      }
-      if (fl < nf) {
-        const int fg = wk.f0 + fl;
-        T *dst = Cb + ob.c_off + (long long)(fg / ob.flo) * ob.fhs + (long long)(fg % ob.flo) * nc + c0;
-#pragma unroll
-        for (int i = 0; i < CB; ++i)
-          if (i < nb) dst[i] = alpha * acc[i];
-      }
-    }
-    __syncthreads();
-  }
-  cp_async_wait<0>();
 }
 
 // dst[dst_off + i0*s0 + i1*s1 + i2*s2] = src[src_off + (i0*d1 + i1)*d2 + i2] for every
@@ -392,69 +209,7 @@ int launch_fiber(const void *tasks, long long ntasks, int opspan, const void *fi
   return QC_OK;
 }
 
-template <typename T>
-int launch_fiber2(const void *work, long long nwork, const void *blobs, const void *ops, int max_rows, int max_w,
-                  int max_blob, int fiber_tile, const T *A, const T *W, T *C, cudaStream_t s) {
-  if (nwork <= 0) return QC_OK;
-  if (nwork > 0x7fffffffLL || max_rows < 1 || max_w < 0 || max_blob < 1 || !work || !blobs) return QC_ERR_ARG;
-  if (fiber_tile != 32 && fiber_tile != 64) return QC_ERR_ARG;
-  const size_t smem = (size_t)3 * max_blob * 16 + (size_t)(2 * max_rows * fiber_tile + 2 * (max_w + 8)) * sizeof(T);
-  if (smem > 200 * 1024) return QC_ERR_ARG;
-  static bool attr_set[2] = {false, false};
-  static int nsm = 0;
-  const int v = (fiber_tile == 32) ? 0 : 1;
-  if (!attr_set[v]) {
-    cudaError_t ea = (v == 0) ? cudaFuncSetAttribute(k_fiber2<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     200 * 1024)
-                              : cudaFuncSetAttribute(k_fiber2<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     200 * 1024);
-    if (ea != cudaSuccess) {
-      fprintf(stderr, "[qcgpu] qc_fiber2: %s\n", cudaGetErrorString(ea));
-      return QC_ERR_CUDA;
-    }
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    attr_set[v] = true;
-  }
-  int per_sm = 1;
-  if (v == 0)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fiber2<T, 1>, FT_THREADS, smem);
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fiber2<T, 2>, FT_THREADS, smem);
-  if (per_sm < 1) per_sm = 1;
-  long long g = (long long)nsm * per_sm;
-  if (g > nwork) g = nwork;
-  const int grid = (int)g;
-  if (v == 0)
-    k_fiber2<T, 1><<<grid, FT_THREADS, smem, s>>>((const qc_fwork *)work, (int)nwork, (const int4 *)blobs,
-                                                  (const qc_op *)ops, max_rows, max_w, max_blob, A, W, C);
-  else
-    k_fiber2<T, 2><<<grid, FT_THREADS, smem, s>>>((const qc_fwork *)work, (int)nwork, (const int4 *)blobs,
-                                                  (const qc_op *)ops, max_rows, max_w, max_blob, A, W, C);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) {
-    fprintf(stderr, "[qcgpu] qc_fiber2: %s\n", cudaGetErrorString(e));
-    return QC_ERR_CUDA;
-  }
-  return QC_OK;
-}
-
 }  // namespace
-
-extern "C" int qc_fiber2_f64(const void *work, long long nwork, const void *blobs, const void *ops, int max_rows,
-                             int max_w, int max_blob, int fiber_tile, const double *A, const double *W, double *C,
-                             void *stream) {
-  return launch_fiber2<double>(work, nwork, blobs, ops, max_rows, max_w, max_blob, fiber_tile, A, W, C,
-                               (cudaStream_t)stream);
-}
-
-extern "C" int qc_fiber2_f32(const void *work, long long nwork, const void *blobs, const void *ops, int max_rows,
-                             int max_w, int max_blob, int fiber_tile, const float *A, const float *W, float *C,
-                             void *stream) {
-  return launch_fiber2<float>(work, nwork, blobs, ops, max_rows, max_w, max_blob, fiber_tile, A, W, C,
-                              (cudaStream_t)stream);
-}
 
 extern "C" int qc_block_permute(const void *descs, long long ndescs, int opspan, const void *ops, const double *src,
                                 void *dst, int dst_f32, void *stream) {

@@ -70,7 +70,8 @@ static_assert(sizeof(qc_fin) == 32, "qc_fin is 32 bytes");
 
 struct alignas(16) qc_fout {
   long long c_off;     // output block offset (relative to the operator's C base)
-  long long fhs;       // (f, c) at c_off + (f / flo)*fhs + (f % flo)*ncols + c
+  int fhs;             // (f, c) at c_off + (f / flo)*fhs + (f % flo)*ncols + c, or,
+  int colmajor;        // when colmajor is set, at c_off + c*F + f (block stored [ncols][F])
   int ncols;
   int pair_b, pair_e;  // contributions [pair_b, pair_e) of qc_fpair (empty: the block is zeroed)
   int flo;             // >= F for a block stored [F][ncols]
@@ -157,29 +158,45 @@ struct alignas(16) qc_tmdesc {
 };
 static_assert(sizeof(qc_tmdesc) == 112, "qc_tmdesc is 112 bytes");
 
-// ---- persistent fiber kernel: per-item work records and per-group metadata blobs ----
-// A fiber group's records (inputs, outputs, pairs with their W places) are packed on the
-// host into one contiguous blob of 16-byte units: [header][fin x n_in][fout x n_out][fpair2 x n_pair]
-// (fout.pair_b / pair_e index the blob's pairs).  A work item is one tile of fibers of one
-// group for one operator.
-struct alignas(16) qc_fwork {
-  int blob;            // first 16-byte unit of the group's blob
-  int blob_len;        // blob length in 16-byte units
-  int f0, F;           // first fiber of the tile, fibers of the group
-  int op;              // operator (index into the operator table)
-  int pad0, pad1, pad2;
+// ---- dense fiber-group GEMM (k_fgemm) -------------------------------------------
+// Every output block of a fiber group reads every input block of the group, so one
+// group is one dense product  C_g[F x CT] = A_g[F x R] . W_g[R x CT]: A_g's R rows are
+// the input blocks' contracted rows, W_g's CT columns the output blocks' columns, and
+// W_g is the group's W blocks laid out as one dense panel (zeros where a pair is
+// absent).  A work item is one tile of fibers of one group for a range of operators.
+struct alignas(16) qc_fggrp {
+  long long row_b;     // first row record (qc_fgrow) of the group
+  long long col_b;     // first column record (qc_fgcol) of the group
+  int F;               // fibers of the group
+  int R;               // rows (contracted extent summed over the input blocks)
+  int CT;              // columns (summed over the output blocks)
+  int CTs;             // CT padded to a multiple of mc: row stride of the W panel
+  int FT;              // fibers per tile (multiple of 4): row stride of the staged A tile
+  int mc;              // columns per thread tile (4 or 8)
+  int flo;             // two-level fiber split of the outputs (>= F: none)
+  int pad;
 };
-static_assert(sizeof(qc_fwork) == 32, "qc_fwork is 32 bytes");
+static_assert(sizeof(qc_fggrp) == 48, "qc_fggrp is 48 bytes");
 
-struct alignas(16) qc_fblob_head {
-  int n_in, n_out, n_pair, pad;
+struct alignas(16) qc_fgrow {
+  long long off;       // A element (row, fiber f) at a_base + off + f * fs
+  long long fs;
 };
-static_assert(sizeof(qc_fblob_head) == 16, "qc_fblob_head is 16 bytes");
+static_assert(sizeof(qc_fgrow) == 16, "qc_fgrow is 16 bytes");
 
-struct alignas(16) qc_fpair2 {
-  long long w_off;     // W block offset (relative to the operator's B base)
-  int srow, rows;      // shared-memory rows of the input block, contracted extent
-  int wsm;             // place of this pair's W block in the item's W area (rows padded to 4)
-  int pad0, pad1, pad2;
+struct alignas(16) qc_fgcol {
+  long long off;       // C element (fiber f, column) at c_base + off + (f / flo) * fhs + (f % flo) * fs
+  long long fhs;
+  long long fs;
+  long long pad;
 };
-static_assert(sizeof(qc_fpair2) == 32, "qc_fpair2 is 32 bytes");
+static_assert(sizeof(qc_fgcol) == 32, "qc_fgcol is 32 bytes");
+
+struct alignas(16) qc_fgitem {
+  long long wpan;      // W panel of operator op_b (element offset; multiple of 4)
+  int group;           // qc_fggrp index
+  int f0, nf;          // first fiber of the tile, fibers in the tile (<= FT)
+  int op_b, op_e;      // operators; operator op's panel is wpan + (op - op_b) * wstride
+  int wstride;         // multiple of 4
+};
+static_assert(sizeof(qc_fgitem) == 32, "qc_fgitem is 32 bytes");

@@ -562,8 +562,8 @@ FTASK_DT = numpy.dtype([("f0", "<i4"), ("F", "<i4"), ("in_b", "<i4"), ("in_e", "
                         ("out_e", "<i4"), ("op_b", "<i4"), ("op_e", "<i4")])
 FIN_DT = numpy.dtype([("a_off", "<i8"), ("rows", "<i4"), ("fiber_major", "<i4"), ("srow", "<i4"), ("pad", "<i4"),
                       ("pad2", "<i8")])
-FOUT_DT = numpy.dtype([("c_off", "<i8"), ("fhs", "<i8"), ("ncols", "<i4"), ("pair_b", "<i4"), ("pair_e", "<i4"),
-                       ("flo", "<i4")])
+FOUT_DT = numpy.dtype([("c_off", "<i8"), ("fhs", "<i4"), ("colmajor", "<i4"), ("ncols", "<i4"), ("pair_b", "<i4"),
+                       ("pair_e", "<i4"), ("flo", "<i4")])
 BPERM_DT = numpy.dtype([("src_off", "<i8"), ("dst_off", "<i8"), ("d0", "<i4"), ("d1", "<i4"), ("d2", "<i4"),
                         ("s0", "<i4"), ("s1", "<i4"), ("s2", "<i4"), ("op_b", "<i4"), ("op_e", "<i4"),
                         ("pad", "<i4", (4,))])
@@ -571,17 +571,23 @@ assert BPERM_DT.itemsize == 64
 FPAIR_DT = numpy.dtype([("w_off", "<i8"), ("srow", "<i4"), ("rows", "<i4")])
 assert FTASK_DT.itemsize == 32 and FIN_DT.itemsize == 32 and FOUT_DT.itemsize == 32 and FPAIR_DT.itemsize == 16
 FIBER_TILE = 32
-FIBER_PERSISTENT = True   # the persistent, double-buffered fiber kernel (qc_fiber2_*); False: qc_fiber_*
-FWORK_DT = numpy.dtype([("blob", "<i4"), ("blob_len", "<i4"), ("f0", "<i4"), ("F", "<i4"), ("op", "<i4"),
-                        ("pad", "<i4", (3,))])
-FPAIR2_DT = numpy.dtype([("w_off", "<i8"), ("srow", "<i4"), ("rows", "<i4"), ("wsm", "<i4"), ("pad", "<i4", (3,))])
-assert FWORK_DT.itemsize == 32 and FPAIR2_DT.itemsize == 32
+FIBER_FGEMM = True        # fiber groups as dense GEMMs (qc_fgemm_*); False: one CTA per fiber tile (qc_fiber_*)
+FGITEM_DT = numpy.dtype([("wpan", "<i8"), ("group", "<i4"), ("f0", "<i4"), ("nf", "<i4"), ("op_b", "<i4"),
+                         ("op_e", "<i4"), ("wstride", "<i4")])
+FGGRP_DT = numpy.dtype([("row_b", "<i8"), ("col_b", "<i8"), ("F", "<i4"), ("R", "<i4"), ("CT", "<i4"), ("CTs", "<i4"),
+                        ("FT", "<i4"), ("mc", "<i4"), ("flo", "<i4"), ("pad", "<i4")])
+FGROW_DT = numpy.dtype([("off", "<i8"), ("fs", "<i8")])
+FGCOL_DT = numpy.dtype([("off", "<i8"), ("fhs", "<i8"), ("fs", "<i8"), ("pad", "<i8")])
+assert FGITEM_DT.itemsize == 32 and FGGRP_DT.itemsize == 48 and FGROW_DT.itemsize == 16 and FGCOL_DT.itemsize == 32
+FG_THREADS = 128          # threads per CTA of qc_fgemm (one thread tile = 4 fibers x mc columns)
+FG_A_BUDGET = 4096        # staged A elements (rows x tile fibers) per buffer
+FG_W_BUDGET = 4096        # W panel elements (rows x padded columns) per buffer: wider groups are cut into column slices
 FIBER_ROWS_WIDE = 128     # staged rows up to which a tile holds 64 fibers (two per lane)
 FIBER_MAX_ROWS = 256
 
 
 def compile_fiber(c, triples, rows_axis, fiber_major, extra_out=None, in_off=None, out_off=None, out_fhs=None,
-                  out_flo=None):
+                  out_flo=None, out_colmajor=False):
     """Fiber-group work items of a W contraction (template for one operator).
 
     The first three output axes form the fiber group (their block dims multiply
@@ -590,7 +596,9 @@ def compile_fiber(c, triples, rows_axis, fiber_major, extra_out=None, in_off=Non
     in_off / out_off (block offsets by flat block index, instead of the packed
     layouts' ioff), out_fhs / out_flo (two-level fiber strides of output blocks),
     extra_out (output blocks that must be written: those without pairs are
-    written as zeros; with out_off, pairs into any other output block are dropped).
+    written as zeros; with out_off, pairs into any other output block are dropped),
+    out_colmajor (output blocks stored column by column, [ncols][F]: the next W
+    contraction then reads them with contiguous fibers, fiber_major=0).
     """
     empty = (numpy.zeros(0, FTASK_DT), numpy.zeros(0, FIN_DT), numpy.zeros(0, FOUT_DT), numpy.zeros(0, FPAIR_DT), 1,
              0.0, FIBER_TILE)
@@ -666,6 +674,9 @@ def compile_fiber(c, triples, rows_axis, fiber_major, extra_out=None, in_off=Non
     fouts["ncols"] = dO[:, 3] * dO[:, 4]
     fouts["flo"] = Fo if out_flo is None else out_flo[allo]
     fouts["fhs"] = 0 if out_fhs is None else out_fhs[allo]
+    if out_fhs is not None and len(allo) and int(out_fhs[allo].max()) >= 2 ** 31:
+        return None
+    fouts["colmajor"] = 1 if out_colmajor else 0
     fouts["pair_b"] = pb
     fouts["pair_e"] = pe
     pairs = numpy.zeros(len(ob), FPAIR_DT)
@@ -726,110 +737,206 @@ class FiberStage(object):
         self.span = int(max(1, (self.h_tasks["op_e"] - self.h_tasks["op_b"]).max())) if self.ntasks else 1
         self.name = name
         self.bytes = 0.0
-        # persistent kernel: per fiber group one metadata blob (inputs, outputs, pairs with the
-        # place of their W block in the item's W area, rows padded to 4), per (task, operator)
-        # one work record
-        self.persistent = FIBER_PERSISTENT
-        if self.ntasks:
-            self._build_persistent(device)
+        # dense fiber-group GEMM: per group a row table, a column table and a W panel map
+        self.fgemm = FIBER_FGEMM
+        self._wpan = {}
+        if self.ntasks and self.fgemm:
+            self._build_fgemm(device)
 
-    def _build_persistent(self, device):
-        fo, fi, fp = self.h_fout, self.h_fin, self.h_fpair
+    def _build_fgemm(self, device):
+        """Tables of qc_fgemm_* from the fiber-group records (vectorised over groups).
+
+        Group g (the tasks sharing their first output) is the product
+        C_g[F x CT] = A_g[F x R] . W_g[R x CT]: row srow + r of A_g is row r of an input
+        block, column col0_j + c of C_g column c of output block j, and W_g[srow_p + r,
+        col0_j + c] = W[w_off_p + r * ncols_j + c] for the pairs p of output j (zero where a
+        pair is absent).  W panel maps are shared by the groups of an operator range that
+        have the same one; the panels are gathered once per W tensor (qc_wpanel_*).
+        """
+        fo, fi, fp, ops = self.h_fout, self.h_fin, self.h_fpair, self.host_ops
+        i64 = numpy.int64
         tk = self.h_tasks[self.h_tasks["out_e"] > self.h_tasks["out_b"]]
-        gs, first = numpy.unique(tk["out_b"].astype(numpy.int64), return_index=True)
-        g_in_b = tk["in_b"][first].astype(numpy.int64)
-        g_in_e = tk["in_e"][first].astype(numpy.int64)
-        g_out_b = gs
-        g_out_e = tk["out_e"][first].astype(numpy.int64)
-        n_in, n_out = g_in_e - g_in_b, g_out_e - g_out_b
-        # outputs written as zeros have an empty pair range at an arbitrary index: a group's
-        # pairs are the union of its outputs' non-empty ranges (contiguous, in output order)
-        pb_all = fo["pair_b"].astype(numpy.int64)
-        pe_all = fo["pair_e"].astype(numpy.int64)
-        nonempty = pe_all > pb_all
-        big = numpy.iinfo(numpy.int64).max
-        g_of_out = numpy.searchsorted(gs, numpy.arange(len(fo)), side="right") - 1
-        in_grp = (g_of_out >= 0) & (numpy.arange(len(fo)) < g_out_e[numpy.maximum(g_of_out, 0)]) & nonempty
-        g_pb = numpy.full(len(gs), big, dtype=numpy.int64)
-        g_pe = numpy.zeros(len(gs), dtype=numpy.int64)
-        numpy.minimum.at(g_pb, g_of_out[in_grp], pb_all[in_grp])
-        numpy.maximum.at(g_pe, g_of_out[in_grp], pe_all[in_grp])
-        g_pb[g_pb == big] = 0
-        g_pe = numpy.maximum(g_pe, g_pb)
-        n_pair = g_pe - g_pb
-        owner = numpy.zeros(len(fp), dtype=numpy.int64)
-        ne = numpy.flatnonzero(nonempty)
-        cnt = pe_all[ne] - pb_all[ne]
-        owner[numpy.repeat(pb_all[ne], cnt) + (numpy.arange(int(cnt.sum())) - numpy.repeat(numpy.cumsum(cnt) - cnt, cnt))] = \
-            numpy.repeat(ne, cnt)
-        blen = 1 + 2 * (n_in + n_out + n_pair)
-        boff = numpy.cumsum(blen) - blen
-        tot = int(blen.sum())
-        blob = numpy.zeros((tot, 4), dtype=numpy.int32)
-        blob[boff, 0], blob[boff, 1], blob[boff, 2] = n_in, n_out, n_pair
+        gs, first = numpy.unique(tk["out_b"].astype(i64), return_index=True)
+        t0 = tk[first]
+        ng = len(gs)
+        F = t0["F"].astype(i64)
+        in_b, in_e = t0["in_b"].astype(i64), t0["in_e"].astype(i64)
+        out_b, out_e = gs, t0["out_e"].astype(i64)
 
-        def ranges(b, n):
-            g = numpy.repeat(numpy.arange(len(n)), n)
-            return g, numpy.arange(int(n.sum())) - numpy.repeat(numpy.cumsum(n) - n, n)
+        def ranges(n):
+            n = numpy.asarray(n, dtype=i64)
+            own = numpy.repeat(numpy.arange(len(n)), n)
+            return own, numpy.arange(int(n.sum()), dtype=i64) - numpy.repeat(numpy.cumsum(n) - n, n)
 
-        def put(rec_i32, g, loc, base):
-            dst = boff[g] + base[g] + 2 * loc
-            blob[dst] = rec_i32[:, 0:4]
-            blob[dst + 1] = rec_i32[:, 4:8]
+        # rows: the contracted rows of every input block, in staging order
+        gi, li = ranges(in_e - in_b)
+        fidx = in_b[gi] + li
+        frows = fi["rows"][fidx].astype(i64)
+        R = numpy.bincount(gi, weights=frows, minlength=ng).astype(i64)
+        e, r_in = ranges(frows)
+        fin_e, g_r = fidx[e], gi[e]
+        fm = fi["fiber_major"][fin_e] != 0
+        row_pos = (numpy.cumsum(R) - R)[g_r] + fi["srow"][fin_e].astype(i64) + r_in
+        rows_rec = numpy.zeros(int(R.sum()), FGROW_DT)
+        rows_rec["off"][row_pos] = fi["a_off"][fin_e] + numpy.where(fm, r_in, r_in * F[g_r])
+        rows_rec["fs"][row_pos] = numpy.where(fm, fi["rows"][fin_e].astype(i64), 1)
+        row_b = numpy.cumsum(R) - R
+        # columns: every output block's columns, output by output
+        go, lo = ranges(out_e - out_b)
+        oidx = out_b[go] + lo
+        nco = fo["ncols"][oidx].astype(i64)
+        CT = numpy.bincount(go, weights=nco, minlength=ng).astype(i64)
+        col_b = numpy.cumsum(CT) - CT
+        c0o = numpy.cumsum(nco) - nco - col_b[go]           # first column of each output in its group
+        e, c_in = ranges(nco)
+        o_e, g_c = oidx[e], go[e]
+        cm = fo["colmajor"][o_e] != 0
+        nc_e = nco[e]
+        cols_rec = numpy.zeros(int(CT.sum()), FGCOL_DT)
+        cols_rec["off"] = fo["c_off"][o_e] + numpy.where(cm, c_in * F[g_c], c_in)
+        cols_rec["fhs"] = numpy.where(cm, 0, fo["fhs"][o_e].astype(i64))
+        cols_rec["fs"] = numpy.where(cm, 1, nc_e)
+        cmo = fo["colmajor"][oidx] != 0
+        flo_o = numpy.where(cmo | (fo["flo"][oidx].astype(i64) >= F[go]), F[go], fo["flo"][oidx].astype(i64))
+        flo = numpy.full(ng, numpy.iinfo(i64).max, dtype=i64)
+        numpy.minimum.at(flo, go, flo_o)
+        flo_hi = numpy.zeros(ng, dtype=i64)
+        numpy.maximum.at(flo_hi, go, flo_o)
+        if numpy.any(flo != flo_hi):
+            raise ValueError("fiber group with outputs of different fiber splits")
+        flo = numpy.where(flo == numpy.iinfo(i64).max, F, flo)
+        # column tile width and padded panel rows
+        p4, p8 = (CT + 3) // 4 * 4, (CT + 7) // 8 * 8
+        mc = numpy.where((CT > 12) & (p8 * 10 <= p4 * 11), 8, 4).astype(i64)
+        CTs = (CT + mc - 1) // mc * mc
+        # W panel maps (index relative to the operator's W base, -1: zero), group by group
+        pan_sz = R * CTs
+        pan_b = numpy.cumsum(pan_sz) - pan_sz
+        wmap = numpy.full(int(pan_sz.sum()), -1, dtype=i64)
+        npo = (fo["pair_e"][oidx] - fo["pair_b"][oidx]).astype(i64)
+        npo = numpy.maximum(npo, 0)
+        e, lp = ranges(npo)
+        pidx = fo["pair_b"][oidx][e].astype(i64) + lp
+        p_g, p_nc, p_c0 = go[e], nco[e], c0o[e]
+        p_rows = fp["rows"][pidx].astype(i64)
+        e2, rr = ranges(p_rows * p_nc)
+        q = e2
+        r_, c_ = rr // p_nc[q], rr % p_nc[q]
+        dst = pan_b[p_g[q]] + (fp["srow"][pidx][q].astype(i64) + r_) * CTs[p_g[q]] + p_c0[q] + c_
+        wmap[dst] = fp["w_off"][pidx][q] + r_ * p_nc[q] + c_
+        # group records (groups wider than the W budget become column slices)
+        op_b, op_e = t0["op_b"].astype(i64), t0["op_e"].astype(i64)
+        recs = []          # (group, first column, columns, padded columns)
+        for g in range(ng):
+            if R[g] * CTs[g] <= FG_W_BUDGET:
+                recs.append((g, 0, CT[g], CTs[g]))
+                continue
+            width = max(int(mc[g]), FG_W_BUDGET // max(int(R[g]), 1) // int(mc[g]) * int(mc[g]))
+            for c0 in range(0, int(CT[g]), width):
+                n = min(width, int(CT[g]) - c0)
+                recs.append((g, c0, n, (n + mc[g] - 1) // mc[g] * mc[g]))
+        rg = numpy.array([x[0] for x in recs], dtype=i64)
+        rc0 = numpy.array([x[1] for x in recs], dtype=i64)
+        rct = numpy.array([x[2] for x in recs], dtype=i64)
+        rcts = numpy.array([x[3] for x in recs], dtype=i64)
+        nrec = len(recs)
+        # fibers per tile: a multiple of 4 that fills the CTA's threads with thread tiles
+        chunks = rcts // mc[rg]
+        nn = numpy.arange(1, 65, dtype=i64)
+        tot = nn[None, :] * chunks[:, None]
+        util = tot / (FG_THREADS * ((tot + FG_THREADS - 1) // FG_THREADS))
+        valid = (4 * nn[None, :] * numpy.maximum(R[rg], 1)[:, None] <= FG_A_BUDGET)
+        valid &= nn[None, :] <= numpy.maximum((F[rg] + 3) // 4, 1)[:, None]
+        valid[:, 0] = True
+        util = numpy.where(valid, util, -1.0)
+        good = util >= 0.97 * util.max(axis=1)[:, None]
+        FT = 4 * (nn.size - numpy.argmax(good[:, ::-1], axis=1))
+        grp = numpy.zeros(nrec, FGGRP_DT)
+        grp["row_b"] = row_b[rg]
+        grp["col_b"] = col_b[rg] + rc0
+        grp["F"], grp["R"], grp["CT"], grp["CTs"] = F[rg], R[rg], rct, rcts
+        grp["FT"], grp["mc"], grp["flo"] = FT, mc[rg], flo[rg]
+        # W panels: one per distinct map of an operator range, stored [operator][panel]
+        panel_of = numpy.zeros(nrec, dtype=i64)
+        stride_of = numpy.zeros(nrec, dtype=i64)
+        widx_parts = []
+        base = 0
+        for ob in numpy.unique(op_b[rg]):
+            recs_c = numpy.flatnonzero(op_b[rg] == ob)
+            seen, maps, off = {}, [], 0
+            for k in recs_c:
+                g = int(rg[k])
+                m = wmap[pan_b[g]:pan_b[g] + pan_sz[g]].reshape(int(R[g]), int(CTs[g]))
+                if rc0[k] or rct[k] != CT[g]:
+                    sub = numpy.full((int(R[g]), int(rcts[k])), -1, dtype=i64)
+                    sub[:, :rct[k]] = m[:, rc0[k]:rc0[k] + rct[k]]
+                    m = sub
+                key = (m.shape, m.tobytes())
+                if key not in seen:
+                    seen[key] = off
+                    maps.append(m.ravel())
+                    off += m.size
+                panel_of[k] = seen[key]
+            stride = off
+            oe = int(op_e[rg][recs_c[0]])
+            bb = ops["b_base"][int(ob):oe].astype(i64)
+            mm = numpy.concatenate(maps) if maps else numpy.zeros(0, dtype=i64)
+            widx_parts.append(numpy.where(mm[None, :] >= 0, bb[:, None] + mm[None, :], -1).ravel())
+            panel_of[recs_c] += base
+            stride_of[recs_c] = stride
+            base += stride * (oe - int(ob))
+        if base and int(stride_of.max()) >= 2 ** 31:
+            raise ValueError("W panel stride exceeds the work-item field")
+        self.h_widx = numpy.concatenate(widx_parts) if widx_parts else numpy.zeros(0, dtype=i64)
+        # items: tiles of fibers, operator ranges kept whole (the kernel walks them in order)
+        nt = (F[rg] + FT - 1) // FT
+        it_r, t = ranges(nt)
+        items = numpy.zeros(len(it_r), FGITEM_DT)
+        items["group"] = it_r
+        items["f0"] = t * FT[it_r]
+        items["nf"] = numpy.minimum(FT[it_r], F[rg][it_r] - t * FT[it_r])
+        items["op_b"], items["op_e"] = op_b[rg][it_r], op_e[rg][it_r]
+        items["wpan"] = panel_of[it_r]
+        items["wstride"] = stride_of[it_r]
+        self.h_items, self.h_groups, self.h_rows, self.h_cols = items, grp, rows_rec, cols_rec
+        self.max_a = int(max(4, ((R[rg] * FT).max() + 3) // 4 * 4)) if nrec else 4
+        self.max_w = int((R[rg] * rcts).max()) if nrec else 0
+        self.max_ct = int(rct.max()) if nrec else 0
+        self.d_items = upload(items, device)
+        self.d_groups = upload(grp, device)
+        self.d_rows = upload(rows_rec if len(rows_rec) else numpy.zeros(1, FGROW_DT), device)
+        self.d_cols = upload(cols_rec if len(cols_rec) else numpy.zeros(1, FGCOL_DT), device)
+        self.d_widx = torch.from_numpy(self.h_widx if len(self.h_widx) else numpy.full(1, -1, dtype=i64)).to(device)
 
-        g, loc = ranges(g_in_b, n_in)
-        put(fi[g_in_b[g] + loc].view(numpy.int32).reshape(-1, 8), g, loc, numpy.ones(len(gs), dtype=numpy.int64))
-        g, loc = ranges(g_out_b, n_out)
-        fo_g = fo[g_out_b[g] + loc].copy()
-        empty = fo_g["pair_e"] <= fo_g["pair_b"]
-        fo_g["pair_b"] = numpy.where(empty, 0, fo_g["pair_b"] - g_pb[g]).astype(numpy.int32)
-        fo_g["pair_e"] = numpy.where(empty, 0, fo_g["pair_e"] - g_pb[g]).astype(numpy.int32)
-        put(fo_g.view(numpy.int32).reshape(-1, 8), g, loc, 1 + 2 * n_in)
-        # W places: exclusive prefix of the padded W sizes inside the group
-        g, loc = ranges(g_pb, n_pair)
-        pidx = g_pb[g] + loc
-        own = owner[pidx]
-        ncp = (fo["ncols"].astype(numpy.int64) + 3) // 4 * 4
-        wsz = fp["rows"][pidx].astype(numpy.int64) * ncp[own]
-        excl = numpy.cumsum(wsz) - wsz
-        gstart = numpy.cumsum(n_pair) - n_pair
-        wsm = excl - excl[numpy.minimum(gstart[g], max(len(excl) - 1, 0))] if len(excl) else excl
-        p2 = numpy.zeros(len(pidx), FPAIR2_DT)
-        p2["w_off"], p2["srow"], p2["rows"], p2["wsm"] = fp["w_off"][pidx], fp["srow"][pidx], fp["rows"][pidx], wsm
-        put(p2.view(numpy.int32).reshape(-1, 8), g, loc, 1 + 2 * (n_in + n_out))
-        gw = numpy.bincount(g, weights=wsz, minlength=len(gs)) if len(g) else numpy.zeros(len(gs))
-        self.max_w = (int(gw.max()) + 3) // 4 * 4 if len(gw) else 0
-        self.max_blob = int(blen.max()) if len(blen) else 1
-        # work records: every (task, operator)
-        gid = numpy.searchsorted(gs, tk["out_b"].astype(numpy.int64))
-        n_op = (tk["op_e"] - tk["op_b"]).astype(numpy.int64)
-        t_of = numpy.repeat(numpy.arange(len(tk)), n_op)
-        opx = numpy.repeat(tk["op_b"].astype(numpy.int64), n_op) + \
-            (numpy.arange(int(n_op.sum())) - numpy.repeat(numpy.cumsum(n_op) - n_op, n_op))
-        wk = numpy.zeros(len(t_of), FWORK_DT)
-        wk["blob"] = boff[gid[t_of]]
-        wk["blob_len"] = blen[gid[t_of]]
-        wk["f0"], wk["F"] = tk["f0"][t_of], tk["F"][t_of]
-        wk["op"] = opx
-        self.h_work, self.h_blob = wk, blob
-        self.h_wsm_pairs = (pidx, wsm, own)
-        self.d_work = upload(wk, device)
-        self.d_blob = upload(blob, device)
+    def wpanel(self, B, stream):
+        """The stage's W panels for the W values B (gathered on the first call for B)."""
+        key = (B.data_ptr(), B.dtype, B.numel())
+        P = self._wpan.get(key)
+        if P is None:
+            n = len(self.h_widx)
+            P = torch.zeros(max(n, 4), dtype=B.dtype, device=B.device)
+            fn = native.lib().qc_wpanel_f64 if B.dtype == torch.float64 else native.lib().qc_wpanel_f32
+            check(fn(B.data_ptr(), self.d_widx.data_ptr(), P.data_ptr(), n, stream), "qc_wpanel")
+            LOG.launches += 1
+            self._wpan[key] = P
+        return P
 
     def run(self, A, B, C, kind="f64", stream=None):
         if self.ntasks == 0:
             return
         lib = native.lib()
         s = stream if stream is not None else torch.cuda.current_stream(C.device).cuda_stream
+        if self.fgemm:
+            P = self.wpanel(B, s)
         if LOG.enabled:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-        if self.persistent:
-            fn = lib.qc_fiber2_f64 if kind == "f64" else lib.qc_fiber2_f32
-            check(fn(self.d_work.data_ptr(), len(self.h_work), self.d_blob.data_ptr(), self.d[4].data_ptr(),
-                     self.max_rows, self.max_w, self.max_blob, self.tile, A.data_ptr(), B.data_ptr(), C.data_ptr(),
-                     s), "qc_fiber2_" + kind)
+        if self.fgemm:
+            fn = lib.qc_fgemm_f64 if kind == "f64" else lib.qc_fgemm_f32
+            check(fn(self.d_items.data_ptr(), len(self.h_items), self.d_groups.data_ptr(), self.d_rows.data_ptr(),
+                     self.d_cols.data_ptr(), self.d[4].data_ptr(), self.max_a, self.max_w, self.max_ct,
+                     A.data_ptr(), P.data_ptr(), C.data_ptr(), s), "qc_fgemm_" + kind)
         else:
             fn = lib.qc_fiber_f64 if kind == "f64" else lib.qc_fiber_f32
             check(fn(self.d[0].data_ptr(), self.ntasks, self.span, self.d[1].data_ptr(), self.d[2].data_ptr(),

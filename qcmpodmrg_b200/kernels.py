@@ -153,6 +153,15 @@ def _ncols(c, triples):
     return numpy.prod(c.out.block_dims(ob)[:, ne1:], axis=1)
 
 
+def unit_phys_t2(lay):
+    """True when every block of the intermediate T2 = T1 . W_i, axes (l', n2, r, b, n1'),
+    has extent 1 on its two physical axes (1 and 4)."""
+    if lay.rank != 5 or len(lay.idx_allowed) == 0:
+        return False
+    d = lay.block_dims(lay.idx_allowed)
+    return bool(numpy.all(d[:, 1] == 1) and numpy.all(d[:, 4] == 1))
+
+
 def pair_flops(c, t):
     """2*M*N*K summed over the block pairs of one contraction (one operator)."""
     if len(t) == 0:
@@ -220,7 +229,7 @@ class SigmaOperator(object):
             o3 = {} if pan4 is None else {"out_off": pan4["t3off"], "out_fhs": pan4["t3fhs"],
                                           "out_flo": pan4["t3flo"], "extra_out": pan4["needed"]}
             fused = None
-            fib3 = None
+            fib2 = fib3 = None
             if use_fiber and fuse_w:
                 cW = Contraction(W1, W2, ([1], [0]))
                 cF = Contraction(c1.out, cW.out, ([0, 2, 3], [0, 2, 5]))
@@ -229,14 +238,28 @@ class SigmaOperator(object):
                     fp = compile_fiber(cF, tF, 0, 0, in_off=t1off, **o3)
                     if fp is not None:
                         fused = (cW, cF, tF, fp)
-            elif use_fiber and pan4 is not None:
-                fib3 = compile_fiber(c3, t3, 3, 1, **o3)
+            elif use_fiber:
+                # .W_i and .W_{i+1} on the fiber kernel: T2 stored column by column (its
+                # physical axes have extent 1, so a T2 block's columns are the next
+                # contraction's rows and its fibers that contraction's fibers), read back
+                # with contiguous fibers
+                cm = bool(unit_phys_t2(c2.out))
+                fib2 = compile_fiber(c2, t2, 0, 0, in_off=t1off, out_colmajor=cm)
+                cm = cm and fib2 is not None
+                if pan4 is not None:
+                    fib3 = compile_fiber(c3, t3, 3, 0 if cm else 1, **o3)
+                    if fib3 is None:
+                        pan4 = None
+                if fib3 is None:
+                    fib3 = compile_fiber(c3, t3, 3, 0 if cm else 1)
+                if fib3 is None and cm:
+                    fib2 = compile_fiber(c2, t2, 0, 0, in_off=t1off)       # T2 packed for the grouped GEMM
             if pan4 is not None and fused is None and fib3 is None:
                 pan4 = None                 # T3 comes from the grouped GEMM in the packed layout
             t4 = prune(t4all, live1=live_blocks(c3.out, fused[2] if fused else t3))
             if c4.out is not psi_layout:
                 raise ValueError("sigma output layout differs from the wavefunction template")
-            plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3), (c4, t4), Rl, fused, pan, pan4, fib3)
+            plans[key] = (ops, (c1, t1), (c2, t2), (c3, t3), (c4, t4), Rl, fused, pan, pan4, fib2, fib3)
             for s, c in enumerate((c1, c2, c3)):
                 if s == 1 and fused is not None:
                     continue            # no T2 for fused classes
@@ -270,7 +293,6 @@ class SigmaOperator(object):
         pos = 0
         # W contractions: fiber-group kernel (inputs staged once per fiber tile) where
         # every group fits in shared memory, generic grouped GEMM otherwise
-        fiber_spec = {1: (0, 0), 2: (3, 1)}      # stage -> (rows axis of operand 1, fiber-major storage)
         lperm = []
         pst, pst_tc = {}, {}            # panel GEMM parts of the L.psi contraction
         rperm = []
@@ -279,7 +301,7 @@ class SigmaOperator(object):
         tc4_classes = []                # (operator range, pan4, row-table base) for the tensor-core .R
         tc1_classes = []                # (operator range, pan["tc"]) for the tensor-core L.psi
         any4 = any(v[8] is not None for v in plans.values())
-        for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
+        for key, (ops, *cs, Rl, fused, pan, pan4, fib2, fib3) in sorted(plans.items()):
             rng = (pos, pos + len(ops))
             pos += len(ops)
             t1off = pan["t1off"] if pan is not None else None
@@ -349,13 +371,11 @@ class SigmaOperator(object):
                         pst.setdefault(cfg, []).append(part)
                     continue
                 off1 = t1off if si == 1 else None
-                if use_fiber and si in fiber_spec:
-                    fp = compile_fiber(c, t, *fiber_spec[si], in_off=off1)
-                    if fp is not None:
-                        fib[si].append(fp + (rng,))
-                        self.w_paths["fiber"] += 1
-                        continue
-                if si in fiber_spec:
+                if si == 1 and fib2 is not None:
+                    fib[1].append(fib2 + (rng,))
+                    self.w_paths["fiber"] += 1
+                    continue
+                if si in (1, 2):
                     self.w_paths["generic"] += 1
                 add_parts(st[si], compile_classes(c, t, ax[si], tensor_cores=tc if si in (0, 3) else False,
                                                   off1=off1), op_range=rng)
@@ -426,13 +446,13 @@ class SigmaOperator(object):
         fb = 0
         for si in range(4 if LOG.enabled else 0):       # only the launch log reads the byte counts
             tot_b = 0
-            for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
+            for key, (ops, *cs, Rl, fused, pan, pan4, fib2, fib3) in sorted(plans.items()):
                 if fused is not None and si in (1, 2):
                     continue
                 c, t = cs[si]
                 tot_b += stage_bytes(c, t, len(ops), si == 0)      # psi is read by every operator
             self.stages[si].bytes = float(tot_b)
-        for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
+        for key, (ops, *cs, Rl, fused, pan, pan4, fib2, fib3) in sorted(plans.items()):
             if fused is not None and LOG.enabled:
                 fb += stage_bytes(fused[1], fused[2], len(ops), False)
         if self.fused is not None:
@@ -444,7 +464,7 @@ class SigmaOperator(object):
         # FLOPs of the reference's four-contraction chain (tensordotCAL pair GEMMs),
         # whatever the fusion used here
         self.flops = 0.0
-        for key, (ops, *cs, Rl, fused, pan, pan4, fib3) in sorted(plans.items()):
+        for key, (ops, *cs, Rl, fused, pan, pan4, fib2, fib3) in sorted(plans.items()):
             for (c, t) in cs:
                 self.flops += pair_flops(c, t) * len(ops)
         self.ndim0 = psi_layout.size

@@ -75,8 +75,10 @@ _SIGS = {
     "qc_tcpanel_status": (c_int, [c_int]),
     "qc_tcpanel_seg_f32": (c_int, [c_vp, c_ll, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "qc_gather_split_f32": (c_int, [c_vp, c_vp, c_ll, c_vp, c_vp, c_vp]),
-    "qc_fiber2_f64": (c_int, [c_vp, c_ll, c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
-    "qc_fiber2_f32": (c_int, [c_vp, c_ll, c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
+    "qc_fgemm_f64": (c_int, [c_vp, c_ll, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
+    "qc_fgemm_f32": (c_int, [c_vp, c_ll, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
+    "qc_wpanel_f64": (c_int, [c_vp, c_vp, c_vp, c_ll, c_vp]),
+    "qc_wpanel_f32": (c_int, [c_vp, c_vp, c_vp, c_ll, c_vp]),
 }
 
 

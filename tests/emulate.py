@@ -41,8 +41,8 @@ def patch_stage_run(monkeypatch):
         a = _f64(A)
         w = _f64(B)
         c = _f64(C)
-        if self.persistent:
-            _run_fiber2(self, a, w, c)
+        if self.fgemm:
+            _run_fgemm(self, a, w, c)
         else:
             _run_fiber(self, a, w, c)
         C.copy_(torch.from_numpy(c).to(C.dtype))
@@ -164,8 +164,12 @@ def _run_fiber(st, A, W, C):
                         numpy.arange(fo["ncols"])[None, :]
                     acc += blk.T @ W[wi]
                 fg = t["f0"] + numpy.arange(nf)
-                ci = o["c_base"] + fo["c_off"] + ((fg // fo["flo"]) * fo["fhs"] + (fg % fo["flo"]) * fo["ncols"])[:, None] \
-                    + numpy.arange(fo["ncols"])[None, :]
+                cc = numpy.arange(fo["ncols"])[None, :]
+                if fo["colmajor"]:
+                    ci = o["c_base"] + fo["c_off"] + cc * t["F"] + fg[:, None]
+                else:
+                    ci = o["c_base"] + fo["c_off"] + ((fg // fo["flo"]) * fo["fhs"] + (fg % fo["flo"]) * fo["ncols"])[:, None] \
+                        + cc
                 C[ci] = o["alpha"] * acc
 
 
@@ -223,38 +227,25 @@ def _run_tcpanel(st, A, B, C):
                 C[idx] = tile[:, int(sg["col0"]) + c]
 
 
-def decode_blob(st, wk):
-    """The metadata blob of a persistent-fiber work record: (fins, fouts, pairs2)."""
-    from qcmpodmrg_b200.engine import FIN_DT, FOUT_DT, FPAIR2_DT
-    b = st.h_blob[int(wk["blob"]):int(wk["blob"]) + int(wk["blob_len"])]
-    n_in, n_out, n_pair = (int(x) for x in b[0, :3])
-    raw = b[1:].copy().view(numpy.uint8).ravel()
-    fins = raw[:32 * n_in].view(FIN_DT)
-    fouts = raw[32 * n_in:32 * (n_in + n_out)].view(FOUT_DT)
-    pairs = raw[32 * (n_in + n_out):32 * (n_in + n_out + n_pair)].view(FPAIR2_DT)
-    return fins, fouts, pairs
-
-
-def _run_fiber2(st, A, W, C):
-    """Reference semantics of the persistent fiber kernel, from its work records and blobs only."""
-    FT = st.tile
-    for wk in st.h_work:
-        fins, fouts, pairs = decode_blob(st, wk)
-        o = st.host_ops[int(wk["op"])]
-        nf = min(FT, int(wk["F"]) - int(wk["f0"]))
-        f = int(wk["f0"]) + numpy.arange(nf)
-        rows = {}
-        for fi in fins:
-            base = o["a_base"] + fi["a_off"]
-            r = numpy.arange(fi["rows"])[:, None]
-            idx = base + (f[None, :] * fi["rows"] + r if fi["fiber_major"] else r * int(wk["F"]) + f[None, :])
-            rows[int(fi["srow"])] = A[idx]
-        for fo in fouts:
-            nc = int(fo["ncols"])
-            acc = numpy.zeros((nf, nc))
-            for p in pairs[int(fo["pair_b"]):int(fo["pair_e"])]:
-                wi = o["b_base"] + p["w_off"] + numpy.arange(p["rows"])[:, None] * nc + numpy.arange(nc)[None, :]
-                acc += rows[int(p["srow"])].T @ W[wi]
-            ci = o["c_base"] + fo["c_off"] + ((f // fo["flo"]) * fo["fhs"] + (f % fo["flo"]) * nc)[:, None] \
-                + numpy.arange(nc)[None, :]
-            C[ci] = o["alpha"] * acc
+def _run_fgemm(st, A, W, C):
+    """Reference semantics of k_fgemm, from its items, group / row / column records and
+    W panel map only: C_g tile = alpha * A_g tile . W_g for every (item, operator)."""
+    P = numpy.where(st.h_widx >= 0, W[numpy.maximum(st.h_widx, 0)], 0.0)
+    for it in st.h_items:
+        g = st.h_groups[int(it["group"])]
+        R, CT, CTs = int(g["R"]), int(g["CT"]), int(g["CTs"])
+        assert int(it["nf"]) <= int(g["FT"]) and R * int(g["FT"]) <= st.max_a and R * CTs <= st.max_w
+        assert CT <= st.max_ct and int(it["wpan"]) % 4 == 0 and int(it["wstride"]) % 4 == 0 and CTs % int(g["mc"]) == 0
+        f = int(it["f0"]) + numpy.arange(int(it["nf"]))
+        rows = st.h_rows[int(g["row_b"]):int(g["row_b"]) + R]
+        cols = st.h_cols[int(g["col_b"]):int(g["col_b"]) + CT]
+        flo = int(g["flo"])
+        for op in range(int(it["op_b"]), int(it["op_e"])):
+            o = st.host_ops[op]
+            a = A[o["a_base"] + rows["off"][:, None] + f[None, :] * rows["fs"][:, None]]       # [R, nf]
+            w0 = int(it["wpan"]) + (op - int(it["op_b"])) * int(it["wstride"])
+            w = P[w0:w0 + R * CTs].reshape(R, CTs)[:, :CT]
+            tile = o["alpha"] * (a.T @ w)                                                   # [nf, CT]
+            ci = o["c_base"] + cols["off"][None, :] + (f // flo)[:, None] * cols["fhs"][None, :] + \
+                (f % flo)[:, None] * cols["fs"][None, :]
+            C[ci] = tile

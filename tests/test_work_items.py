@@ -25,9 +25,31 @@ def _fiber_writes(fs):
             cb = int(fs.host_ops[op]["c_base"])
             for ob in fs.h_fout[int(t["out_b"]):int(t["out_e"])]:
                 nc = int(ob["ncols"])
+                if ob["colmajor"]:
+                    out.append((cb + int(ob["c_off"]) + numpy.arange(nc)[None, :] * int(t["F"]) + f[:, None]).ravel())
+                    continue
                 rows = cb + int(ob["c_off"]) + (f // int(ob["flo"])) * int(ob["fhs"]) + (f % int(ob["flo"])) * nc
                 out.append((rows[:, None] + numpy.arange(nc)[None, :]).ravel())
     return numpy.concatenate(out) if out else numpy.zeros(0, dtype=numpy.int64)
+
+
+def _fgemm_writes_reads(fs):
+    """Elements the dense fiber-group GEMM writes (from its own tables) and its highest read."""
+    out, hi = [], -1
+    for it in fs.h_items:
+        g = fs.h_groups[int(it["group"])]
+        f = int(it["f0"]) + numpy.arange(int(it["nf"]))
+        cols = fs.h_cols[int(g["col_b"]):int(g["col_b"]) + int(g["CT"])]
+        rows = fs.h_rows[int(g["row_b"]):int(g["row_b"]) + int(g["R"])]
+        flo = int(g["flo"])
+        for op in range(int(it["op_b"]), int(it["op_e"])):
+            o = fs.host_ops[op]
+            out.append((int(o["c_base"]) + cols["off"][None, :] + (f // flo)[:, None] * cols["fhs"][None, :]
+                        + (f % flo)[:, None] * cols["fs"][None, :]).ravel())
+            if len(rows):
+                hi = max(hi, int((int(o["a_base"]) + rows["off"] + int(f[-1]) * rows["fs"]).max()))
+                assert int((int(o["a_base"]) + rows["off"]).min()) >= 0
+    return (numpy.concatenate(out) if out else numpy.zeros(0, dtype=numpy.int64)), hi
 
 
 def _fiber_reads(fs):
@@ -72,6 +94,10 @@ def _check_sigma_writes(sig):
                 assert len(numpy.unique(w)) == len(w), "overlapping writes in " + sub.name
                 src = {"sigma2": sig.tot[0], "sigma3": sig.tot[1], "sigma23": sig.tot[0]}[sub.name]
                 assert _fiber_reads(sub) < src, sub.name
+                if sub.fgemm:
+                    wg, hi = _fgemm_writes_reads(sub)
+                    assert numpy.array_equal(numpy.sort(wg), numpy.sort(w)), sub.name
+                    assert hi < src, sub.name
             if isinstance(sub, PanelStage) and sub.groups:
                 w = _panel_writes(sub)
                 assert w.min() >= 0 and w.max() < ndst[sub.name], sub.name
@@ -123,13 +149,13 @@ def test_panel_layouts_cover_the_intermediates_once(tag, monkeypatch):
             assert (cover == 1).all()
 
 
-@pytest.mark.parametrize("tag", ["K5", "K6"])
-def test_persistent_fiber_staging_in_bounds(tag, monkeypatch):
-    """Persistent fiber kernel: one work record per (task, operator); every group's metadata
-    blob fits max_blob and repeats the group's records (outputs' pair ranges rebased); inside
-    an item the W blocks of its pairs get disjoint shared-memory areas (rows padded to 4)
-    within max_w, and the 8-wide W reads of the last column block stay inside max_w + 8."""
-    from emulate import decode_blob
+@pytest.mark.parametrize("tag", ["K5", "K6", "K5N8"])
+def test_dense_fiber_group_tables(tag, monkeypatch):
+    """Dense fiber-group GEMM tables: items tile every group's fibers exactly once for its
+    operator range; every item's staged A tile, W panel and columns fit the launch's
+    max_a / max_w / max_ct (and the shared memory of both precisions); W panels stay inside
+    the gathered panel buffer at 16-byte offsets; T2 is written column by column and read
+    back with contiguous fibers."""
     patch_stage_run(monkeypatch)
     for r in load("kernels_%s.npz" % tag)["records"]:
         sig, _, _ = record_operators(r, "cpu", use_fiber=True, fuse_w=False)
@@ -137,24 +163,27 @@ def test_persistent_fiber_staging_in_bounds(tag, monkeypatch):
             for sub in _subs(st):
                 if not (isinstance(sub, FiberStage) and sub.ntasks):
                     continue
-                t = sub.h_tasks
-                live = t["out_e"] > t["out_b"]
-                assert len(sub.h_work) == int((t["op_e"] - t["op_b"])[live].sum())
-                assert int(sub.h_work["blob_len"].max()) <= sub.max_blob
-                assert (sub.h_work["blob"] + sub.h_work["blob_len"]).max() <= len(sub.h_blob)
-                for wk in sub.h_work[:: max(1, len(sub.h_work) // 200)]:
-                    fins, fouts, pairs = decode_blob(sub, wk)
-                    assert fouts["pair_b"].min() >= 0 and fouts["pair_e"].max() <= len(pairs)
-                    if len(fins):                  # groups of zero-filled outputs stage nothing
-                        assert (fins["srow"] + fins["rows"]).max() <= sub.max_rows
-                    spans = []
-                    for fo in fouts:
-                        ncp = (int(fo["ncols"]) + 3) // 4 * 4
-                        for p in pairs[int(fo["pair_b"]):int(fo["pair_e"])]:
-                            lo, hi = int(p["wsm"]), int(p["wsm"]) + int(p["rows"]) * ncp
-                            assert lo % 4 == 0 and hi <= sub.max_w
-                            last = lo + (int(p["rows"]) - 1) * ncp + ((int(fo["ncols"]) - 1) // 8) * 8 + 7
-                            assert last < sub.max_w + 8
-                            spans.append((lo, hi))
-                    spans.sort()
-                    assert all(a[1] <= b[0] for a, b in zip(spans, spans[1:]))
+                assert sub.fgemm
+                it, gr = sub.h_items, sub.h_groups
+                g = gr[it["group"]]
+                assert (it["nf"] >= 1).all() and (it["nf"] <= g["FT"]).all() and (g["FT"] % 4 == 0).all()
+                assert (g["R"].astype(numpy.int64) * g["FT"] <= sub.max_a).all()
+                assert (g["R"].astype(numpy.int64) * g["CTs"] <= sub.max_w).all()
+                assert (g["CT"] <= sub.max_ct).all() and (g["CTs"] % g["mc"] == 0).all()
+                assert sub.max_a % 4 == 0 and sub.max_w % 4 == 0
+                for elem in (4, 8):
+                    assert 2 * sub.max_ct * 32 + 2 * (sub.max_a + sub.max_w) * elem <= 220 * 1024
+                assert (it["wpan"] % 4 == 0).all() and (it["wstride"] % 4 == 0).all()
+                last = it["wpan"] + (it["op_e"] - 1 - it["op_b"]).astype(numpy.int64) * it["wstride"] + \
+                    g["R"].astype(numpy.int64) * g["CTs"]
+                assert last.max() <= len(sub.h_widx)
+                for k in numpy.unique(it["group"]):
+                    sel = it[it["group"] == k]
+                    cover = numpy.zeros(int(gr[k]["F"]), dtype=numpy.int64)
+                    for x in sel:
+                        cover[int(x["f0"]):int(x["f0"]) + int(x["nf"])] += 1
+                    assert (cover == 1).all()
+                if sub.name == "sigma2":
+                    assert (sub.h_fout["colmajor"] == 1).all()
+                if sub.name == "sigma3":
+                    assert (sub.h_fin["fiber_major"] == 0).all()
