@@ -74,20 +74,15 @@ __device__ __forceinline__ void fg_stage(const qc_fgitem &it, int op, const qc_f
   const qc_fggrp g = groups[it.group];
   const T *Ab = A + ops[op].a_base;
   const int FT = g.FT;
-  const int n = g.R * FT;
-  int r = tid / FT, f = tid - r * FT;
-  const int dr = FG_THREADS / FT, df = FG_THREADS - dr * FT;
+  // warp w stages rows w, w + 4, ...: one (uniform) row record per row, lanes along fibers
+  const int lane = tid & 31, warp = tid >> 5;
   const qc_fgrow *rw = rows + g.row_b;
-#pragma unroll 4
-  for (int e = tid; e < n; e += FG_THREADS) {
+#pragma unroll 2
+  for (int r = warp; r < g.R; r += FG_THREADS / 32) {
     const qc_fgrow w = rw[r];
-    cp_async_elem(as + e, Ab + w.off + (long long)(it.f0 + f) * w.fs, f < it.nf);
-    r += dr;
-    f += df;
-    if (f >= FT) {
-      f -= FT;
-      ++r;
-    }
+    const T *src = Ab + w.off + (long long)it.f0 * w.fs;
+    T *dst = as + r * FT;
+    for (int f = lane; f < FT; f += 32) cp_async_elem(dst + f, src + (long long)f * w.fs, f < it.nf);
   }
   const T *wsrc = Wp + it.wpan + (long long)(op - it.op_b) * it.wstride;
   const int nw16 = g.R * g.CTs * (int)sizeof(T) / 16;
@@ -98,24 +93,26 @@ __device__ __forceinline__ void fg_stage(const qc_fgitem &it, int op, const qc_f
     cp_async16(reinterpret_cast<char *>(cs) + 16 * e, reinterpret_cast<const char *>(cols + g.col_b) + 16 * e);
 }
 
-// One thread tile: fibers 4*fc .. 4*fc+3 of the item x columns mc*cc .. mc*cc+mc-1.
+// One thread tile: fibers 4*fc .. 4*fc+3 of the item x columns col0 .. col0+MC-1.  The W
+// panel stores an 8-column tile as two 4-column halves, half q of chunk cc at
+// q * CTs/2 + 4*cc, so the chunks one load instruction reads are contiguous (no bank
+// conflicts); w0 points at half 0 of the tile's chunk, qstride = CTs/2.
 template <typename T, int MC>
-__device__ __forceinline__ void fg_tile(const T *as, const T *ws, const qc_fgcol *cs, const qc_fggrp &g, int f0,
-                                        int nf, int fc, int cc, T alpha, T *Cb) {
+__device__ __forceinline__ void fg_tile(const T *as, const T *w0, int qstride, const qc_fgcol *cs,
+                                        const qc_fggrp &g, int f0, int nf, int fc, int col0, T alpha, T *Cb) {
   T acc[4][MC];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int c = 0; c < MC; ++c) acc[i][c] = T(0);
   const T *a = as + 4 * fc;
-  const T *w = ws + MC * cc;
   const int FT = g.FT, CTs = g.CTs, R = g.R;
 #pragma unroll 4
   for (int r = 0; r < R; ++r) {
     T av[4], wv[MC];
     lds4(a + r * FT, av);
 #pragma unroll
-    for (int q = 0; q < MC; q += 4) lds4(w + r * CTs + q, wv + q);
+    for (int q = 0; q < MC / 4; ++q) lds4(w0 + r * CTs + q * qstride, wv + 4 * q);
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -145,7 +142,7 @@ __device__ __forceinline__ void fg_tile(const T *as, const T *ws, const qc_fgcol
   }
 #pragma unroll
   for (int c = 0; c < MC; ++c) {
-    const int col = MC * cc + c;
+    const int col = col0 + c;
     if (col < g.CT) {
       const qc_fgcol cl = cs[col];
       T *dst = Cb + cl.off;
@@ -198,12 +195,12 @@ k_fgemm(const qc_fgitem *__restrict__ items, int nitems, const qc_fggrp *__restr
       for (int m = threadIdx.x; m < ntile; m += FG_THREADS) {
         const int fc = m / chunks, cc = m - fc * chunks;
         if (g.mc == 4) {
-          fg_tile<T, 4>(as, ws, cs, g, it.f0, it.nf, fc, cc, alpha, Cb);
+          fg_tile<T, 4>(as, ws + 4 * cc, 0, cs, g, it.f0, it.nf, fc, 4 * cc, alpha, Cb);
         } else if (sizeof(T) == 4) {
-          fg_tile<T, 8>(as, ws, cs, g, it.f0, it.nf, fc, cc, alpha, Cb);
+          fg_tile<T, 8>(as, ws + 4 * cc, g.CTs / 2, cs, g, it.f0, it.nf, fc, 8 * cc, alpha, Cb);
         } else {      // FP64: an 8-column tile as two 4-column tiles (register budget)
-          fg_tile<T, 4>(as, ws, cs, g, it.f0, it.nf, fc, 2 * cc, alpha, Cb);
-          fg_tile<T, 4>(as, ws, cs, g, it.f0, it.nf, fc, 2 * cc + 1, alpha, Cb);
+          fg_tile<T, 4>(as, ws + 4 * cc, 0, cs, g, it.f0, it.nf, fc, 8 * cc, alpha, Cb);
+          fg_tile<T, 4>(as, ws + g.CTs / 2 + 4 * cc, 0, cs, g, it.f0, it.nf, fc, 8 * cc + 4, alpha, Cb);
         }
       }
     }

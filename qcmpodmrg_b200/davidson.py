@@ -12,6 +12,10 @@ the reference's HVecs does (:67-78).
 """
 import torch
 
+# a start vector of smaller norm carries no usable direction (a projected guess whose
+# weight lies outside the dot's blocks is rounding noise)
+V0_MIN_NORM = 1.e-8
+
 
 def _ortho(vbas, rbas, crit_indp, times=5):
     rbas = rbas.clone()
@@ -70,7 +74,13 @@ def davidson_steps(diag, neig=1, v0=None, crit_e=1.e-8, crit_vec=1.e-8, maxcycle
     if neig > ndim:
         raise ValueError("neig > ndim")
     vbas = gen_v0(diag, neig) if v0 is None else v0.reshape(neig, ndim).to(torch.float64).clone()
-    vbas[0] = vbas[0] / torch.linalg.norm(vbas[0])
+    n0 = float(torch.linalg.norm(vbas[0]))
+    if not n0 > V0_MIN_NORM:
+        # the guess has (numerically) no weight in this dot's blocks: the reference's
+        # genOrthoBas would divide by ~0 here; start from the diagonal instead (genV0)
+        vbas = gen_v0(diag, neig)
+        n0 = 1.0
+    vbas[0] = vbas[0] / n0
     if neig > 1:
         n, v2 = _ortho(vbas[0:1], vbas[1:], crit_indp)
         if n + 1 != neig:

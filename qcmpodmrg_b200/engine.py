@@ -586,6 +586,18 @@ FIBER_ROWS_WIDE = 128     # staged rows up to which a tile holds 64 fibers (two 
 FIBER_MAX_ROWS = 256
 
 
+def fg_col_perm(col, width, mc):
+    """Place of panel column col in a W panel row of the dense fiber-group GEMM: with
+    8-column thread tiles the row is stored as two halves, column 8k + 4q + j at
+    q * width/2 + 4k + j (each load instruction then reads contiguous 16-byte chunks)."""
+    col = numpy.asarray(col, dtype=numpy.int64)
+    width = numpy.asarray(width, dtype=numpy.int64)
+    mc = numpy.asarray(mc, dtype=numpy.int64)
+    half = (col % 8) // 4
+    perm = half * (width // 2) + (col // 8) * 4 + col % 4
+    return numpy.where(mc == 8, perm, col)
+
+
 def compile_fiber(c, triples, rows_axis, fiber_major, extra_out=None, in_off=None, out_off=None, out_fhs=None,
                   out_flo=None, out_colmajor=False):
     """Fiber-group work items of a W contraction (template for one operator).
@@ -809,37 +821,99 @@ class FiberStage(object):
         p4, p8 = (CT + 3) // 4 * 4, (CT + 7) // 8 * 8
         mc = numpy.where((CT > 12) & (p8 * 10 <= p4 * 11), 8, 4).astype(i64)
         CTs = (CT + mc - 1) // mc * mc
-        # W panel maps (index relative to the operator's W base, -1: zero), group by group
-        pan_sz = R * CTs
-        pan_b = numpy.cumsum(pan_sz) - pan_sz
-        wmap = numpy.full(int(pan_sz.sum()), -1, dtype=i64)
-        npo = (fo["pair_e"][oidx] - fo["pair_b"][oidx]).astype(i64)
-        npo = numpy.maximum(npo, 0)
+        # the pairs of every group (in group order): W block, its rows and columns in the panel
+        npo = numpy.maximum((fo["pair_e"][oidx] - fo["pair_b"][oidx]).astype(i64), 0)
         e, lp = ranges(npo)
         pidx = fo["pair_b"][oidx][e].astype(i64) + lp
-        p_g, p_nc, p_c0 = go[e], nco[e], c0o[e]
-        p_rows = fp["rows"][pidx].astype(i64)
-        e2, rr = ranges(p_rows * p_nc)
-        q = e2
-        r_, c_ = rr // p_nc[q], rr % p_nc[q]
-        dst = pan_b[p_g[q]] + (fp["srow"][pidx][q].astype(i64) + r_) * CTs[p_g[q]] + p_c0[q] + c_
-        wmap[dst] = fp["w_off"][pidx][q] + r_ * p_nc[q] + c_
-        # group records (groups wider than the W budget become column slices)
+        PA = numpy.stack([fp["srow"][pidx].astype(i64), c0o[e], fp["rows"][pidx].astype(i64), nco[e],
+                          fp["w_off"][pidx].astype(i64)], axis=1)
+        p_g = go[e]
+        gp_n = numpy.bincount(p_g, minlength=ng).astype(i64) if len(p_g) else numpy.zeros(ng, dtype=i64)
+        gp_b = numpy.cumsum(gp_n) - gp_n
+
+        def group_map(g, width):
+            """Dense W panel map of group g ([R][width], relative W index, -1: zero)."""
+            m = numpy.full((int(R[g]), int(width)), -1, dtype=i64)
+            for sr, c0, nr, nc, wo in PA[gp_b[g]:gp_b[g] + gp_n[g]]:
+                m[sr:sr + nr, c0:c0 + nc] = wo + numpy.arange(nr)[:, None] * nc + numpy.arange(nc)[None, :]
+            return m
+
+        # group records: whole groups, and column slices of groups wider than the W budget;
+        # records of one operator range with the same panel map share one panel
         op_b, op_e = t0["op_b"].astype(i64), t0["op_e"].astype(i64)
-        recs = []          # (group, first column, columns, padded columns)
-        for g in range(ng):
-            if R[g] * CTs[g] <= FG_W_BUDGET:
-                recs.append((g, 0, CT[g], CTs[g]))
-                continue
-            width = max(int(mc[g]), FG_W_BUDGET // max(int(R[g]), 1) // int(mc[g]) * int(mc[g]))
-            for c0 in range(0, int(CT[g]), width):
-                n = min(width, int(CT[g]) - c0)
-                recs.append((g, c0, n, (n + mc[g] - 1) // mc[g] * mc[g]))
-        rg = numpy.array([x[0] for x in recs], dtype=i64)
-        rc0 = numpy.array([x[1] for x in recs], dtype=i64)
-        rct = numpy.array([x[2] for x in recs], dtype=i64)
-        rcts = numpy.array([x[3] for x in recs], dtype=i64)
-        nrec = len(recs)
+        wide = R * CTs > FG_W_BUDGET
+        width = numpy.maximum(mc, FG_W_BUDGET // numpy.maximum(R, 1) // mc * mc)
+        nsl = numpy.where(wide, (CT + width - 1) // width, 1)
+        rg, sl = ranges(nsl)
+        rc0 = numpy.where(wide[rg], sl * width[rg], 0)
+        rct = numpy.where(wide[rg], numpy.minimum(width[rg], CT[rg] - rc0), CT[rg])
+        rcts = (rct + mc[rg] - 1) // mc[rg] * mc[rg]
+        nrec = len(rg)
+        seen, panels = {}, []           # key -> panel id; per panel (operator range, R, padded width, rep)
+        pan_id = numpy.zeros(nrec, dtype=i64)
+        for k in range(nrec):
+            g = int(rg[k])
+            if not wide[g]:
+                key = (int(op_b[g]), int(R[g]), int(CTs[g]), int(CT[g]), PA[gp_b[g]:gp_b[g] + gp_n[g]].tobytes())
+                rep = ("group", g)
+            else:
+                m = group_map(g, CTs[g])
+                sub = numpy.full((int(R[g]), int(rcts[k])), -1, dtype=i64)
+                sub[:, fg_col_perm(numpy.arange(rct[k]), rcts[k], mc[g])] = m[:, rc0[k]:rc0[k] + rct[k]]
+                key = (int(op_b[g]), "slice", sub.shape, sub.tobytes())
+                rep = ("map", sub)
+            pid = seen.get(key)
+            if pid is None:
+                pid = seen[key] = len(panels)
+                panels.append((int(op_b[g]), int(op_e[g]), int(R[g]) * int(rcts[k]), rep))
+            pan_id[k] = pid
+        # panels stored [operator][panel] per operator range
+        npan = len(panels)
+        p_ob = numpy.array([x[0] for x in panels], dtype=i64)
+        p_oe = numpy.array([x[1] for x in panels], dtype=i64)
+        p_sz = numpy.array([x[2] for x in panels], dtype=i64)
+        cls_ob, cls_first, cls_of_p = numpy.unique(p_ob, return_index=True, return_inverse=True)
+        cls_of_p = cls_of_p.ravel()
+        order = numpy.argsort(cls_of_p, kind="stable")
+        p_off = numpy.zeros(npan, dtype=i64)
+        stride_c = numpy.zeros(len(cls_ob), dtype=i64)
+        for pid in order:
+            c = cls_of_p[pid]
+            p_off[pid] = stride_c[c]
+            stride_c[c] += p_sz[pid]
+        nops_c = p_oe[cls_first] - cls_ob
+        base_c = numpy.cumsum(stride_c * nops_c) - stride_c * nops_c
+        panel_of = (base_c[cls_of_p] + p_off)[pan_id]
+        stride_of = stride_c[cls_of_p][pan_id]
+        if nrec and int(stride_of.max()) >= 2 ** 31:
+            raise ValueError("W panel stride exceeds the work-item field")
+        # the maps of the distinct panels, class by class: whole-group panels expanded from
+        # their pairs in one vectorised pass
+        mtot = int(stride_c.sum())
+        M = numpy.full(mtot, -1, dtype=i64)
+        m_base = (numpy.cumsum(stride_c) - stride_c)[cls_of_p] + p_off
+        grp_rep = numpy.full(ng, -1, dtype=i64)
+        for pid, (_, _, _, rep) in enumerate(panels):
+            if rep[0] == "group":
+                grp_rep[rep[1]] = pid
+            else:
+                M[m_base[pid]:m_base[pid] + p_sz[pid]] = rep[1].ravel()
+        sel = numpy.flatnonzero(grp_rep[p_g] >= 0) if len(p_g) else numpy.zeros(0, dtype=i64)
+        if len(sel):
+            sr, c0, nr, nc, wo = (PA[sel, i] for i in range(5))
+            pid_s = grp_rep[p_g[sel]]
+            q, kk = ranges(nr * nc)
+            r_, c_ = kk // nc[q], kk % nc[q]
+            gs_ = p_g[sel][q]
+            M[m_base[pid_s[q]] + (sr[q] + r_) * CTs[gs_] + fg_col_perm(c0[q] + c_, CTs[gs_], mc[gs_])] = \
+                wo[q] + r_ * nc[q] + c_
+        widx_parts = []
+        mb = numpy.cumsum(stride_c) - stride_c
+        for c in range(len(cls_ob)):
+            mm = M[mb[c]:mb[c] + stride_c[c]]
+            bb = ops["b_base"][int(cls_ob[c]):int(cls_ob[c] + nops_c[c])].astype(i64)
+            widx_parts.append(numpy.where(mm[None, :] >= 0, bb[:, None] + mm[None, :], -1).ravel())
+        self.h_widx = numpy.concatenate(widx_parts) if widx_parts else numpy.zeros(0, dtype=i64)
         # fibers per tile: a multiple of 4 that fills the CTA's threads with thread tiles
         chunks = rcts // mc[rg]
         nn = numpy.arange(1, 65, dtype=i64)
@@ -856,38 +930,6 @@ class FiberStage(object):
         grp["col_b"] = col_b[rg] + rc0
         grp["F"], grp["R"], grp["CT"], grp["CTs"] = F[rg], R[rg], rct, rcts
         grp["FT"], grp["mc"], grp["flo"] = FT, mc[rg], flo[rg]
-        # W panels: one per distinct map of an operator range, stored [operator][panel]
-        panel_of = numpy.zeros(nrec, dtype=i64)
-        stride_of = numpy.zeros(nrec, dtype=i64)
-        widx_parts = []
-        base = 0
-        for ob in numpy.unique(op_b[rg]):
-            recs_c = numpy.flatnonzero(op_b[rg] == ob)
-            seen, maps, off = {}, [], 0
-            for k in recs_c:
-                g = int(rg[k])
-                m = wmap[pan_b[g]:pan_b[g] + pan_sz[g]].reshape(int(R[g]), int(CTs[g]))
-                if rc0[k] or rct[k] != CT[g]:
-                    sub = numpy.full((int(R[g]), int(rcts[k])), -1, dtype=i64)
-                    sub[:, :rct[k]] = m[:, rc0[k]:rc0[k] + rct[k]]
-                    m = sub
-                key = (m.shape, m.tobytes())
-                if key not in seen:
-                    seen[key] = off
-                    maps.append(m.ravel())
-                    off += m.size
-                panel_of[k] = seen[key]
-            stride = off
-            oe = int(op_e[rg][recs_c[0]])
-            bb = ops["b_base"][int(ob):oe].astype(i64)
-            mm = numpy.concatenate(maps) if maps else numpy.zeros(0, dtype=i64)
-            widx_parts.append(numpy.where(mm[None, :] >= 0, bb[:, None] + mm[None, :], -1).ravel())
-            panel_of[recs_c] += base
-            stride_of[recs_c] = stride
-            base += stride * (oe - int(ob))
-        if base and int(stride_of.max()) >= 2 ** 31:
-            raise ValueError("W panel stride exceeds the work-item field")
-        self.h_widx = numpy.concatenate(widx_parts) if widx_parts else numpy.zeros(0, dtype=i64)
         # items: tiles of fibers, operator ranges kept whole (the kernel walks them in order)
         nt = (F[rg] + FT - 1) // FT
         it_r, t = ranges(nt)

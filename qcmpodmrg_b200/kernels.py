@@ -468,6 +468,17 @@ class SigmaOperator(object):
             for (c, t) in cs:
                 self.flops += pair_flops(c, t) * len(ops)
         self.ndim0 = psi_layout.size
+        # W panels of the dense fiber-group stages, gathered now (per dot) rather than in
+        # the first matrix-vector product
+        if torch.device(dev).type == "cuda":
+            s = torch.cuda.current_stream(dev).cuda_stream
+            wsets = [(self.stages[1], self.Wi), (self.stages[2], self.Wj)]
+            for st, wset in wsets:
+                for sub in (st.subs if isinstance(st, CompositeStage) else [st]):
+                    if isinstance(sub, FiberStage) and sub.ntasks and sub.fgemm:
+                        sub.wpanel(wset.values, s)
+                        if precision != "f64":
+                            sub.wpanel(wset.f32(), s)
 
     def rebind(self, L, R):
         """Use new environment values with the same block layouts (cached plan)."""

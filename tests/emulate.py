@@ -230,6 +230,7 @@ def _run_tcpanel(st, A, B, C):
 def _run_fgemm(st, A, W, C):
     """Reference semantics of k_fgemm, from its items, group / row / column records and
     W panel map only: C_g tile = alpha * A_g tile . W_g for every (item, operator)."""
+    from qcmpodmrg_b200.engine import fg_col_perm
     P = numpy.where(st.h_widx >= 0, W[numpy.maximum(st.h_widx, 0)], 0.0)
     for it in st.h_items:
         g = st.h_groups[int(it["group"])]
@@ -244,7 +245,7 @@ def _run_fgemm(st, A, W, C):
             o = st.host_ops[op]
             a = A[o["a_base"] + rows["off"][:, None] + f[None, :] * rows["fs"][:, None]]       # [R, nf]
             w0 = int(it["wpan"]) + (op - int(it["op_b"])) * int(it["wstride"])
-            w = P[w0:w0 + R * CTs].reshape(R, CTs)[:, :CT]
+            w = P[w0:w0 + R * CTs].reshape(R, CTs)[:, fg_col_perm(numpy.arange(CT), CTs, int(g["mc"]))]
             tile = o["alpha"] * (a.T @ w)                                                   # [nf, CT]
             ci = o["c_base"] + cols["off"][None, :] + (f // flo)[:, None] * cols["fhs"][None, :] + \
                 (f % flo)[:, None] * cols["fs"][None, :]

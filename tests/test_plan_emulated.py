@@ -79,3 +79,27 @@ def test_sigma_tma_tensor_core_units_emulated(tag, monkeypatch):
         ref = numpy.asarray(r["hvec_y"])
         y = sig(x).numpy()
         assert numpy.linalg.norm(y - ref) <= 2e-6 * numpy.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("tag", ["K5", "K6", "K5N8"])
+def test_sigma_fgemm_slices_and_small_tiles_emulated(tag, monkeypatch):
+    """Dense fiber-group GEMM with W panels cut into column slices and fiber tiles of a few
+    fibers (small shared-memory budgets), T2 column by column: same sigma."""
+    from qcmpodmrg_b200 import engine
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(engine, "FG_W_BUDGET", 40)
+    monkeypatch.setattr(engine, "FG_A_BUDGET", 96)
+    sliced = 0
+    for r in load("kernels_%s.npz" % tag)["records"]:
+        sig, dg, ws = record_operators(r, "cpu", use_fiber=True, fuse_w=False)
+        for st in sig.stages:
+            for s in getattr(st, "subs", [st]):
+                if isinstance(s, engine.FiberStage) and s.ntasks:
+                    g = s.h_groups
+                    assert (g["R"].astype(numpy.int64) * g["FT"] <= max(96, 4 * g["R"].max())).all()
+                    key = numpy.stack([g["row_b"], g["F"], g["R"]], 1)[g["R"] > 0]
+                    sliced += len(key) - len(numpy.unique(key, axis=0))     # records cut from one group
+        x = torch.from_numpy(numpy.asarray(r["hvec_x"], dtype=numpy.float64))
+        ref = numpy.asarray(r["hvec_y"])
+        assert numpy.abs(sig(x).numpy() - ref).max() <= 1e-12 * max(1.0, numpy.abs(ref).max())
+    assert sliced > 0
