@@ -62,29 +62,67 @@ __device__ __forceinline__ void lds4(const double *p, double *v) {
   v[3] = b.y;
 }
 
-// Stage (item, operator) into one buffer: the A tile [R][FT] (row r, fiber f at
-// A + a_base + row.off + (f0 + f) * row.fs; zero for f >= nf), the operator's W panel
-// [R][CTs] and the group's column records.
-template <typename T>
-__device__ __forceinline__ void fg_stage(const qc_fgitem &it, int op, const qc_fggrp *__restrict__ groups,
-                                         const qc_fgrow *__restrict__ rows, const qc_fgcol *__restrict__ cols,
-                                         const qc_op *__restrict__ ops, const T *__restrict__ A,
-                                         const T *__restrict__ Wp, T *as, T *ws, qc_fgcol *cs) {
-  const int tid = threadIdx.x;
-  const qc_fggrp g = groups[it.group];
-  const T *Ab = A + ops[op].a_base;
-  const int FT = g.FT;
-  // warp w stages rows w, w + 4, ...: one (uniform) row record per row, lanes along fibers
-  const int lane = tid & 31, warp = tid >> 5;
-  const qc_fgrow *rw = rows + g.row_b;
-#pragma unroll 2
-  for (int r = warp; r < g.R; r += FG_THREADS / 32) {
-    const qc_fgrow w = rw[r];
-    const T *src = Ab + w.off + (long long)it.f0 * w.fs;
-    T *dst = as + r * FT;
-    for (int f = lane; f < FT; f += 32) cp_async_elem(dst + f, src + (long long)f * w.fs, f < it.nf);
+// One (item, operator) step of a CTA: the item, its group and the operator's bases.
+struct FgStep {
+  qc_fgitem it;
+  qc_fggrp g;
+  long long a_base, c_base;
+  double alpha;
+  int op;
+};
+
+__device__ __forceinline__ void fg_load_op(FgStep &st, const qc_op *__restrict__ ops) {
+  const qc_op o = ops[st.op];
+  st.a_base = o.a_base;
+  st.c_base = o.c_base;
+  st.alpha = o.alpha;
+}
+
+// The row records a warp stages (rows warp, warp + 4, ...): lane l holds those of the
+// warp's rows l and l + 32, loaded in one round trip when a new item begins.
+struct FgRows {
+  long long off[2], fs[2];
+};
+
+__device__ __forceinline__ void fg_load_rows(FgRows &rr, const qc_fggrp &g, const qc_fgrow *__restrict__ rows) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int r = warp + (FG_THREADS / 32) * (lane + 32 * h);
+    if (r < g.R) {
+      const qc_fgrow w = rows[g.row_b + r];
+      rr.off[h] = w.off;
+      rr.fs[h] = w.fs;
+    } else {
+      rr.off[h] = 0;
+      rr.fs[h] = 0;
+    }
   }
-  const T *wsrc = Wp + it.wpan + (long long)(op - it.op_b) * it.wstride;
+}
+
+// Stage a step into one buffer: the A tile [R][FT] (row r, fiber f at
+// A + a_base + row.off + (f0 + f) * row.fs; zero for f >= nf), the operator's W panel
+// [R][CTs] and the group's column records.  No global load on the way: the row records
+// come from the warp's registers (shuffles), the rest is cp.async.
+template <typename T>
+__device__ __forceinline__ void fg_stage(const FgStep &st, const FgRows &rr, const qc_fgcol *__restrict__ cols,
+                                         const T *__restrict__ A, const T *__restrict__ Wp, T *as, T *ws,
+                                         qc_fgcol *cs) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const qc_fggrp &g = st.g;
+  const T *Ab = A + st.a_base;
+  const int FT = g.FT, nf = st.it.nf;
+  const int nrw = (g.R - warp + (FG_THREADS / 32) - 1) / (FG_THREADS / 32);     // rows of this warp
+  for (int j = 0; j < nrw; ++j) {
+    const int h = j >> 5, src_lane = j & 31;
+    const long long off = __shfl_sync(0xffffffffu, h ? rr.off[1] : rr.off[0], src_lane);
+    const long long fs = __shfl_sync(0xffffffffu, h ? rr.fs[1] : rr.fs[0], src_lane);
+    const int r = warp + (FG_THREADS / 32) * j;
+    const T *src = Ab + off + (long long)st.it.f0 * fs;
+    T *dst = as + r * FT;
+    for (int f = lane; f < FT; f += 32) cp_async_elem(dst + f, src + (long long)f * fs, f < nf);
+  }
+  const T *wsrc = Wp + st.it.wpan + (long long)(st.op - st.it.op_b) * st.it.wstride;
   const int nw16 = g.R * g.CTs * (int)sizeof(T) / 16;
   for (int e = tid; e < nw16; e += FG_THREADS)
     cp_async16(reinterpret_cast<char *>(ws) + 16 * e, reinterpret_cast<const char *>(wsrc) + 16 * e);
@@ -162,52 +200,103 @@ k_fgemm(const qc_fgitem *__restrict__ items, int nitems, const qc_fggrp *__restr
   qc_fgcol *const cs0 = reinterpret_cast<qc_fgcol *>(smem_raw);   // [2][max_ct]
   T *const as0 = reinterpret_cast<T *>(cs0 + 2 * max_ct);         // [2][max_a]
   T *const ws0 = as0 + 2 * max_a;                                 // [2][max_w]
-  int i = blockIdx.x;
-  if (i >= nitems) return;
-  int op = items[i].op_b;
-  fg_stage<T>(items[i], op, groups, rows, cols, ops, A, Wp, as0, ws0, cs0);
+  // this CTA's steps: items blockIdx.x, + gridDim.x, ..., each for its operators in order.
+  // Records are fetched ahead: the next step's item and operator before the multiply, its
+  // group and row records (only when a new item begins) right after it.
+  const int G = (int)gridDim.x;
+  int ci = blockIdx.x;
+  if (ci >= nitems) return;
+  FgStep cur;
+  cur.it = items[ci];
+  cur.op = cur.it.op_b;
+  cur.g = groups[cur.it.group];
+  fg_load_op(cur, ops);
+  FgRows rr;
+  fg_load_rows(rr, cur.g, rows);
+  fg_stage<T>(cur, rr, cols, A, Wp, as0, ws0, cs0);
   cp_async_commit();
+  // step 1
+  FgStep nxt;
+  int ni = ci;
+  nxt.it = cur.it;
+  nxt.g = cur.g;
+  nxt.op = cur.op + 1;
+  bool nxt_new = false;
+  if (nxt.op >= cur.it.op_e) {
+    ni = ci + G;
+    nxt_new = true;
+    if (ni < nitems) {
+      nxt.it = items[ni];
+      nxt.op = nxt.it.op_b;
+      nxt.g = groups[nxt.it.group];
+    }
+  }
+  bool has_nxt = ni < nitems;
+  if (has_nxt) {
+    fg_load_op(nxt, ops);
+    if (nxt_new) fg_load_rows(rr, nxt.g, rows);
+  }
   for (int k = 0;; ++k) {
     const int buf = k & 1;
-    // the next (item, operator) of this CTA's sequence
-    int ni = i, nop = op + 1;
-    if (nop >= items[i].op_e) {
-      ni = i + (int)gridDim.x;
-      nop = ni < nitems ? items[ni].op_b : 0;
-    }
-    if (ni < nitems)
-      fg_stage<T>(items[ni], nop, groups, rows, cols, ops, A, Wp, as0 + (buf ^ 1) * max_a,
-                  ws0 + (buf ^ 1) * max_w, cs0 + (buf ^ 1) * max_ct);
+    if (has_nxt)
+      fg_stage<T>(nxt, rr, cols, A, Wp, as0 + (buf ^ 1) * max_a, ws0 + (buf ^ 1) * max_w,
+                  cs0 + (buf ^ 1) * max_ct);
     cp_async_commit();
+    // the step after next: item (if a new one) and operator records now
+    FgStep n2;
+    int n2i = ni;
+    bool n2_new = false, has_n2 = false;
+    if (has_nxt) {
+      n2.it = nxt.it;
+      n2.g = nxt.g;
+      n2.op = nxt.op + 1;
+      if (n2.op >= nxt.it.op_e) {
+        n2i = ni + G;
+        n2_new = true;
+        if (n2i < nitems) {
+          n2.it = items[n2i];
+          n2.op = n2.it.op_b;
+        }
+      }
+      has_n2 = n2i < nitems;
+      if (has_n2 && !n2_new) fg_load_op(n2, ops);
+    }
     cp_async_wait<1>();
     __syncthreads();
     {
-      const qc_fgitem it = items[i];
-      const qc_fggrp g = groups[it.group];
-      const qc_op o = ops[op];
-      const T alpha = T(o.alpha);
-      T *Cb = C + o.c_base;
+      const qc_fggrp &g = cur.g;
+      const T alpha = T(cur.alpha);
+      T *Cb = C + cur.c_base;
       const T *as = as0 + buf * max_a;
       const T *ws = ws0 + buf * max_w;
       const qc_fgcol *cs = cs0 + buf * max_ct;
       const int chunks = g.CTs / g.mc;
-      const int ntile = ((it.nf + 3) >> 2) * chunks;
+      const int ntile = ((cur.it.nf + 3) >> 2) * chunks;
       for (int m = threadIdx.x; m < ntile; m += FG_THREADS) {
         const int fc = m / chunks, cc = m - fc * chunks;
         if (g.mc == 4) {
-          fg_tile<T, 4>(as, ws + 4 * cc, 0, cs, g, it.f0, it.nf, fc, 4 * cc, alpha, Cb);
+          fg_tile<T, 4>(as, ws + 4 * cc, 0, cs, g, cur.it.f0, cur.it.nf, fc, 4 * cc, alpha, Cb);
         } else if (sizeof(T) == 4) {
-          fg_tile<T, 8>(as, ws + 4 * cc, g.CTs / 2, cs, g, it.f0, it.nf, fc, 8 * cc, alpha, Cb);
+          fg_tile<T, 8>(as, ws + 4 * cc, g.CTs / 2, cs, g, cur.it.f0, cur.it.nf, fc, 8 * cc, alpha, Cb);
         } else {      // FP64: an 8-column tile as two 4-column tiles (register budget)
-          fg_tile<T, 4>(as, ws + 4 * cc, 0, cs, g, it.f0, it.nf, fc, 8 * cc, alpha, Cb);
-          fg_tile<T, 4>(as, ws + g.CTs / 2 + 4 * cc, 0, cs, g, it.f0, it.nf, fc, 8 * cc + 4, alpha, Cb);
+          fg_tile<T, 4>(as, ws + 4 * cc, 0, cs, g, cur.it.f0, cur.it.nf, fc, 8 * cc, alpha, Cb);
+          fg_tile<T, 4>(as, ws + g.CTs / 2 + 4 * cc, 0, cs, g, cur.it.f0, cur.it.nf, fc, 8 * cc + 4, alpha, Cb);
         }
       }
     }
+    // a new item two steps ahead: its group, operator and row records (the row records of
+    // the step staged above are no longer needed)
+    if (has_n2 && n2_new) {
+      n2.g = groups[n2.it.group];
+      fg_load_op(n2, ops);
+      fg_load_rows(rr, n2.g, rows);
+    }
     __syncthreads();
-    if (ni >= nitems) break;
-    i = ni;
-    op = nop;
+    if (!has_nxt) break;
+    cur = nxt;
+    nxt = n2;
+    ni = n2i;
+    has_nxt = has_n2;
   }
   cp_async_wait<0>();
 }
