@@ -13,6 +13,7 @@ decimation and renormalisation of every operator's environment.
   python bench.py --impl reference      # the reference algorithm (oracle port) on the host CPU
   python bench.py --workload batched    # lockstep independent instances vs one after another
   python bench.py --workload sp --sites 12 --dmax 100 --npts 4   # spin-projected (S=0) sweeps, FP64
+  python bench.py --workload dot --sites 24 --dmax 200   # one mid-chain dot's sigma (kernel profiles)
 
 Prints one JSON line.  value = seconds per sweep (lower is better).
 """
@@ -193,7 +194,7 @@ def run_ours(args):
     sp = args.workload == "sp"
     d = _make_dmrg(args, prec, dev, rank)
     warm = [_step(d, args) for _ in range(args.warmup)]
-    snap = d.snapshot() if args.e2e else None
+    snap = d.snapshot()          # the state the timed sweeps start from (e2e, accuracy and FP64 legs)
     # ---- timed region (device events on the launching stream, barrier + sync both sides)
     s0 = {k: v for k, v in d.stats.items() if not isinstance(v, dict)}
     LOG.reset()
@@ -271,7 +272,8 @@ def run_ours(args):
         e2e = e2e_leg(d, args, snap, per_sweep[0], energies[0][2])
         e2e["value"] = round(max_over_ranks(dist, e2e["value"], dev) / world, 3)
         line["e2e"] = e2e
-    del snap
+    if args.shadow and prec != "f64" and not sp:
+        line["same_input_dots"] = shadow_leg(d, args, snap)
     if rank == 0:
         acc = accuracy_leg(d, prec, args.cpu_baseline, sp)
         if args.cpu_baseline:
@@ -280,12 +282,13 @@ def run_ours(args):
     if hasattr(d.preconditioner, "summary"):
         line["precond_stats"] = d.preconditioner.summary()
     if args.f64_steps > 0 and prec != "f64" and not sp:
-        # the FP64 GPU arm: same workload, same schedule, same sweeps timed
+        # the FP64 GPU arm: the same sweeps from the same state (the snapshot the timed
+        # sweeps started from), timed the same way
         del d
         gc.collect()
         torch.cuda.empty_cache()
-        line["f64_arm"] = f64_arm(args, dev, dist, rank, [w[0] for w in warm] + [e[0] for e in energies],
-                                  per_sweep)
+        line["f64_arm"] = f64_arm(args, dev, dist, rank, snap, [e[0] for e in energies], per_sweep)
+    del snap
     if dist is not None:
         dist.destroy_process_group()
     if rank == 0:
@@ -368,27 +371,46 @@ def accuracy_leg(d, prec, with_oracle, sp):
     return out
 
 
-def f64_arm(args, dev, dist, rank, e_mixed, ms_mixed):
-    """The plain FP64 GPU path on the same workload and schedule (ramp, warm-up sweeps),
-    timing the first f64_steps sweeps after the warm-up; compared with the mixed arm's
-    energy after the same number of sweeps and its time for the same sweeps."""
-    import torch
+def shadow_leg(d, args, snap):
+    """The first timed sweep again from the same state, with every dot's low-precision
+    solve repeated in plain FP64 from the same start vector on the same operators: the
+    largest |E_mixed - E_FP64| over the dots (same inputs), and the matvec counts."""
+    d.restore(snap)
+    d.shadow = []
+    d.sweep("R", args.dmax, 1e-7)
+    d.sweep("L", args.dmax, 1e-7)
+    sh, d.shadow = d.shadow, None
+    de = [abs(r["e_mixed"] - r["e_f64"]) for r in sh]
+    return {"dots": len(sh), "max_abs_dE": max(de) if de else None,
+            "mean_abs_dE": float(numpy.mean(de)) if de else None,
+            "matvecs_mixed": sum(r["nmvp_mixed"] for r in sh), "matvecs_f64": sum(r["nmvp_f64"] for r in sh),
+            "definition": "one sweep from the timed sweeps' start state; at every dot the mixed-precision "
+                          "Davidson and the plain FP64 Davidson from the same start vector on the same "
+                          "operators; |dE| between their energies"}
+
+
+def f64_arm(args, dev, dist, rank, snap, e_mixed, ms_mixed):
+    """The plain FP64 GPU path from the same state as the timed sweeps (the snapshot they
+    started from), timing the first f64_steps of the same sweeps; compared with the mixed
+    arm's energy after the same number of sweeps and its time for those sweeps."""
+    from qcmpodmrg_b200.hamiltonian import make_hamiltonian
+    from qcmpodmrg_b200.dmrg import DMRG
     n = min(args.f64_steps, args.steps)
-    d = _make_dmrg(args, "f64", dev, rank)
-    for _ in range(args.warmup):
-        _step(d, args)
+    ham = make_hamiltonian(args.sites, args.sites, SEED, DECAY)
+    d = DMRG(ham, device=dev, precision="f64", w_path=args.w_path, plan_cache=args.plan_cache)
+    d.restore(snap)
     ms, per, res = _timed_sweeps(d, args, n, dist)
     ms = max_over_ranks(dist, ms, dev)
     e64 = res[-1][0]
-    em = e_mixed[args.warmup + n - 1]
+    em = e_mixed[n - 1]
     t_mixed = max_over_ranks(dist, sum(ms_mixed[:n]), dev)
     out = {"sweeps_timed": n, "s_per_sweep": round(ms / n / 1e3, 3), "sweep_ms": [round(x, 1) for x in per],
            "energy_f64": e64, "energy_mixed_same_sweep": em, "abs_dE_vs_f64": abs(em - e64),
            "energy_mixed_final": e_mixed[-1], "matvecs_per_sweep": sum(r[2] for r in res) / n,
            "speedup_vs_f64": round(ms / t_mixed, 3),
-           "definition": "same schedule from the same start: sweeps %d..%d after the warm-up, FP64 GPU time / "
-                         "mixed time for those sweeps; |dE| between the two arms' energies after sweep %d"
-                         % (args.warmup + 1, args.warmup + n, args.warmup + n)}
+           "definition": "both arms start from the same state (after the ramp and %d warm-up sweeps of the "
+                         "mixed arm) and run the same %d sweep(s): FP64 GPU time / mixed time for those "
+                         "sweeps; |dE| between the two arms' energies after them" % (args.warmup, n)}
     del d
     return out
 
@@ -417,6 +439,47 @@ def run_reference(args):
                              "sample": res[-1]["sample"]},
             "dots_sampled": {str(r["dot"]): round(r["dot_cost_s"], 2) for r in res},
             "e2e": {"value": round(v, 1), "unit": "s/sweep", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_dot(args):
+    """One mid-chain dot, for kernel profiles: the ramp up to D = dmax (one sweep pair per
+    bond dimension of RAMP below dmax, then one at dmax), then the sigma of the middle dot
+    applied once to warm up and --steps times under the NVTX range "dot" (the range an
+    ncu capture selects with --nvtx --nvtx-include "dot/"), in the bench's precision and
+    in FP64.  Prints one JSON line: per launch the stage, kernel, algorithmic bytes and
+    FLOPs and the CUDA-event time."""
+    import torch
+    from qcmpodmrg_b200.engine import LOG
+    dev = torch.device("cuda:0")
+    prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32", "mixed-tc": "tf32x3"}[args.precision]
+    d = _make_dmrg(args, prec, dev)
+    d.sweep("R", args.dmax, 1e-7)
+    d.sweep("L", args.dmax, 1e-7)
+    isite = d.nsite // 2
+    lay, idl, s, dg = d.dot_operators(isite)
+    x = torch.from_numpy(numpy.random.default_rng(0).standard_normal(s.ndim0)).to(dev)
+    precs = [prec] if prec == "f64" else [prec, "f64"]
+    for p in precs:
+        s(x, precision=p)
+    torch.cuda.synchronize()
+    LOG.reset()
+    LOG.enabled = True
+    torch.cuda.nvtx.range_push("dot")
+    for _ in range(args.steps):
+        for p in precs:
+            s(x, precision=p)
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    LOG.enabled = False
+    recs = []
+    for (name, e0, e1, fl, by) in LOG.records:
+        ms = e0.elapsed_time(e1)
+        recs.append({"stage": name, "kernel": stage_kernel(name, args.w_path, prec), "ms": round(ms, 4),
+                     "algo_bytes": int(by), "flops": float(fl), "gbs": round(by / (ms / 1e3) / 1e9, 1) if ms else None})
+    line = {"workload": "mid-chain dot sigma, K=%d N=%d D=%d" % (args.sites, args.sites, args.dmax),
+            "dot": isite, "ndim0": int(s.ndim0), "precisions": precs, "repeats": args.steps,
+            "launches_logged": len(recs), "gpu_launches": LOG.launches, "launches": recs}
     print(json.dumps(line), flush=True)
 
 
@@ -490,13 +553,16 @@ def main():
                     help="kernels of the two MPO-site contractions of sigma")
     ap.add_argument("--plan-cache", action="store_true",
                     help="reuse the compiled plans of dots whose sectors did not change")
+    ap.add_argument("--no-shadow", dest="shadow", action="store_false",
+                    help="skip the same-input leg (each dot of one sweep also solved in plain FP64)")
     ap.add_argument("--f64-steps", type=int, default=3,
-                    help="sweeps timed on the plain FP64 GPU arm after the same warm-up (0: no FP64 arm)")
+                    help="sweeps timed on the plain FP64 GPU arm from the timed sweeps' start state (0: no FP64 arm)")
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "learned"],
                     help="Davidson preconditioner of the mixed-precision arm")
     ap.add_argument("--precond-train", type=int, default=2, help="sweeps whose solver pairs train the network")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "sp"],
-                    help="sp: spin-projected sweeps (SP-MPS, S=0) with --npts quadrature points")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "sp", "dot"],
+                    help="sp: spin-projected sweeps (SP-MPS, S=0) with --npts quadrature points; dot: the "
+                         "mid-chain dot's sigma under the NVTX range 'dot' (kernel profiles)")
     ap.add_argument("--npts", type=int, default=4)
     ap.add_argument("--instances", type=int, default=16)
     ap.add_argument("--no-graphs", dest="graphs", action="store_false",
@@ -516,6 +582,8 @@ def main():
         sys.exit("bench.py: --gpus %d but WORLD_SIZE=%s" % (args.gpus, world))
     if args.workload == "batched":
         run_batched(args)
+    elif args.workload == "dot":
+        run_dot(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

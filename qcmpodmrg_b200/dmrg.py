@@ -121,6 +121,9 @@ class DMRG(object):
         self.recorder = None      # callback(residual, diag, e, x) fed by Davidson (preconditioner training)
         self.h2d_bytes = 0
         self.d2h_bytes = 0
+        # list: every low-precision dot solve is repeated in plain FP64 from the same start
+        # vector and both energies are appended here (off when None)
+        self.shadow = None
 
     # ------------------------------------------------------------- set-up
     def _setup_operators(self, ham):
@@ -221,6 +224,13 @@ class DMRG(object):
             res = self._mixed_davidson(hv, lambda v: sig(v, precision="f64"), diag, v0, crit_e)
         torch.cuda.synchronize(dev)
         self.stats["hvec_s"] += time.time() - t0
+        if self.shadow is not None and self.precision != "f64":
+            # the plain FP64 solve of the same dot from the same start vector (accuracy
+            # check: same operators, same inputs); its result does not enter the sweep
+            r64 = davidson(lambda v: sig(v, precision="f64"), diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec)
+            self.shadow.append({"isite": isite, "status": status, "e_f64": float(r64.eigs[0]),
+                                "e_mixed": float(res.eigs[0]), "nmvp_f64": int(r64.nmvp),
+                                "nmvp_mixed": int(res.nmvp)})
         self.stats["nmvp"] += res.nmvp
         self.stats["sigma_flops"] += res.nmvp * sig.flops
         if learned:
@@ -306,9 +316,11 @@ class DMRG(object):
         crit_e or the residual below the precision's floor.  Phase 2 applies the
         FP64 sigma to the final vector: its Rayleigh quotient has an error of second
         order in the vector's error.  The vector is accepted when its FP64 residual is
-        at most 1e-4, or when phase 1 converged by the reference's criteria and the FP64
-        Rayleigh quotient agrees with the low-precision Ritz value within ACCEPT_DE (the
-        low-precision sigma then did not bias the solve); otherwise FP64 Davidson
+        at most 1e-4, or when phase 1 converged by the reference's criteria and either
+        the FP64 residual is at most twice the low-precision one plus the precision's
+        floor, or the FP64 Rayleigh quotient agrees with the low-precision Ritz value
+        within ACCEPT_DE (the low-precision sigma then did not bias the solve beyond
+        the point where the FP64 solver itself stops); otherwise FP64 Davidson
         iterations (reference criteria) continue from that vector.  Vectors are device
         tensors, or host tensors when hv / hv64 are the host-buffer entry points.
         """
@@ -326,7 +338,12 @@ class DMRG(object):
         self.stats["nmvp_f64"] = self.stats.get("nmvp_f64", 0) + 1
         self.stats["nmvp_low"] = self.stats.get("nmvp_low", 0) + r1.nmvp
         converged = r1.niter < 19             # phase 1 met its criteria (not the iteration cap)
-        if rn <= max(self.crit_vec, accept) or (converged and abs(e64 - float(r1.eigs[0])) <= ACCEPT_DE):
+        # residual the low-precision solver saw for its final vector: when the FP64 residual
+        # is no larger than that (plus the precision's floor), the low-precision products did
+        # not bias the vector beyond the point where the FP64 solver itself stops
+        rn_low = float(r1.rnorms[-1][0]) if r1.rnorms else float("inf")
+        unbiased = rn <= 2.0 * rn_low + floor
+        if rn <= max(self.crit_vec, accept) or (converged and (unbiased or abs(e64 - float(r1.eigs[0])) <= ACCEPT_DE)):
             r1.eigs = numpy.array([e64])
             r1.vecs = x.reshape(1, -1)
             r1.nmvp += 1

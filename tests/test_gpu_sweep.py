@@ -9,11 +9,19 @@ undone by the next sweep.  Converged (final-sweep) energies and discarded
 weights are held to 1e-8 / 1e-10; earlier sweeps to 1e-5.
 
 The K=12, N=12, D=100 six-sweep run (C1) stops before convergence (discarded
-weight ~6e-3 per sweep) and its Davidson solves stop at |de| <= 1e-7, so after
-the first degenerate truncation the two trajectories are different but equally
-valid unconverged states.  For it the test holds the dots before the first
-truncation to 1e-10 (bit-level agreement of the sigma, Davidson and
-decimation) and the sweep energies to C1_TOL_E.
+weight ~6e-3 per sweep) and its Davidson solves stop at |de| <= 1e-7.  Its trajectory
+is set by rounding noise: from the occupation-number start the Davidson vector of a dot
+can lie in a subspace that H leaves invariant (a spin sector of the start state), and
+only rounding noise takes the solver out of it.  Exact diagonalisation of the dot
+Hamiltonians shows it: at the ninth dot of the first sweep the reference's own solver
+returns -17.4394 Eh where the dot's lowest eigenvalue is -18.8792 Eh; the reference
+leaves the subspace four dots later, the CPU interpreter of the kernels not within the
+first sweep, the B200 at yet another dot, and each then follows its own unconverged
+trajectory.  So the test holds the dots before the first truncation to 1e-10
+(bit-level agreement of sigma, Davidson and decimation), and the sweep energies only as
+variational upper bounds of one another: the GPU run's last sweep at least as low as
+the reference's up to C1_TOL_FINAL, and within C1_TOL_E of it.  The converged
+comparison is test_sweeps_config1_converged.
 """
 import os
 
@@ -26,8 +34,8 @@ from qcmpodmrg_b200.hamiltonian import make_hamiltonian
 pytestmark = pytest.mark.gpu
 
 
-C1_TOL_E = 3e-3       # unconverged run: sweep-energy spread between valid trajectories
-C1_TOL_FINAL = 5e-4   # last of the six sweeps (observed 1e-4 .. 3e-4 across summation orders)
+C1_TOL_E = 1e-2       # unconverged runs: spread of the last sweep's energy between trajectories
+C1_TOL_FINAL = 5e-4   # the GPU's last sweep may lie above the reference's by at most this
 C1_EXACT_DOTS = 7     # dots of the first sweep before the first truncating decimation
 
 
@@ -60,8 +68,9 @@ def test_sweeps_config1_partial(cuda):
     e_ref = numpy.asarray(fx["esweeps"])
     e_gpu = numpy.asarray(out["esweeps"])
     assert numpy.abs(e_gpu[:C1_EXACT_DOTS] - e_ref[:C1_EXACT_DOTS]).max() <= 1e-10
-    assert numpy.abs(out["eav"] - fx["eav"]).max() <= C1_TOL_E
-    assert abs(out["eav"][-1] - fx["eav"][-1]) <= C1_TOL_FINAL
+    print("C1 6 sweeps: GPU", list(out["eav"]), "reference", list(fx["eav"]))
+    assert out["eav"][-1] <= fx["eav"][-1] + C1_TOL_FINAL
+    assert abs(out["eav"][-1] - fx["eav"][-1]) <= C1_TOL_E
 
 
 
