@@ -381,12 +381,19 @@ def shadow_leg(d, args, snap):
     d.sweep("L", args.dmax, 1e-7)
     sh, d.shadow = d.shadow, None
     de = [abs(r["e_mixed"] - r["e_f64"]) for r in sh]
+    # a solve that ends at the iteration cap (19 Rayleigh-Ritz steps) is unconverged in
+    # either precision; |dE| is then the two solvers' distance from convergence
+    conv = [abs(r["e_mixed"] - r["e_f64"]) for r in sh if r["niter_f64"] < 19 and r["niter_mixed"] < 19]
+    worst = max(sh, key=lambda r: abs(r["e_mixed"] - r["e_f64"])) if sh else None
     return {"dots": len(sh), "max_abs_dE": max(de) if de else None,
             "mean_abs_dE": float(numpy.mean(de)) if de else None,
+            "dots_both_converged": len(conv), "max_abs_dE_converged": max(conv) if conv else None,
+            "median_abs_dE": float(numpy.median(de)) if de else None, "worst_dot": worst,
             "matvecs_mixed": sum(r["nmvp_mixed"] for r in sh), "matvecs_f64": sum(r["nmvp_f64"] for r in sh),
             "definition": "one sweep from the timed sweeps' start state; at every dot the mixed-precision "
                           "Davidson and the plain FP64 Davidson from the same start vector on the same "
-                          "operators; |dE| between their energies"}
+                          "operators; |dE| between their energies (converged: neither solve at the "
+                          "iteration cap)"}
 
 
 def f64_arm(args, dev, dist, rank, snap, e_mixed, ms_mixed):
@@ -453,11 +460,16 @@ def run_dot(args):
     from qcmpodmrg_b200.engine import LOG
     dev = torch.device("cuda:0")
     prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32", "mixed-tc": "tf32x3"}[args.precision]
-    d = _make_dmrg(args, prec, dev)
+    # the state is prepared by FP64 sweeps for --precision f64 and by FP32-sigma sweeps
+    # otherwise; the profiled dot's plan is then compiled for the requested precision
+    d = _make_dmrg(args, "f64" if prec == "f64" else "f32", dev)
     d.sweep("R", args.dmax, 1e-7)
-    d.sweep("L", args.dmax, 1e-7)
+    n, e, dw, el, dl = d.sweep("L", args.dmax, 1e-7)
+    d.precision = prec
     isite = d.nsite // 2
+    LOG.enabled = True            # the plan records its algorithmic byte counts for the launch log
     lay, idl, s, dg = d.dot_operators(isite)
+    LOG.enabled = False
     x = torch.from_numpy(numpy.random.default_rng(0).standard_normal(s.ndim0)).to(dev)
     precs = [prec] if prec == "f64" else [prec, "f64"]
     for p in precs:
@@ -466,19 +478,26 @@ def run_dot(args):
     LOG.reset()
     LOG.enabled = True
     torch.cuda.nvtx.range_push("dot")
+    marks = []
     for _ in range(args.steps):
         for p in precs:
+            marks.append((len(LOG.records), p))
             s(x, precision=p)
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     LOG.enabled = False
     recs = []
-    for (name, e0, e1, fl, by) in LOG.records:
+    prec_of = {}
+    for i0, p in marks:
+        for i in range(i0, len(LOG.records)):
+            prec_of[i] = p
+    for i, (name, e0, e1, fl, by) in enumerate(LOG.records):
         ms = e0.elapsed_time(e1)
-        recs.append({"stage": name, "kernel": stage_kernel(name, args.w_path, prec), "ms": round(ms, 4),
+        p = prec_of.get(i, prec)
+        recs.append({"stage": name, "precision": p, "kernel": stage_kernel(name, args.w_path, p), "ms": round(ms, 4),
                      "algo_bytes": int(by), "flops": float(fl), "gbs": round(by / (ms / 1e3) / 1e9, 1) if ms else None})
     line = {"workload": "mid-chain dot sigma, K=%d N=%d D=%d" % (args.sites, args.sites, args.dmax),
-            "dot": isite, "ndim0": int(s.ndim0), "precisions": precs, "repeats": args.steps,
+            "set_up_energy": e, "set_up_matvecs": int(d.stats["nmvp"]), "dot": isite, "ndim0": int(s.ndim0), "precisions": precs, "repeats": args.steps,
             "launches_logged": len(recs), "gpu_launches": LOG.launches, "launches": recs}
     print(json.dumps(line), flush=True)
 

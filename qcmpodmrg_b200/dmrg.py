@@ -193,6 +193,11 @@ class DMRG(object):
         dev = self.device
         t0 = time.time()
         lay, idl, sig, dg = self.dot_operators(isite)
+        if lay.size == 0:
+            raise RuntimeError("dot (%d, %d), sweep %s: the wavefunction has no allowed block (left bond sectors "
+                               "%s, right bond sectors %s, target %s)" % (
+                                   isite, isite + 1, status, numpy.unique(self.qnuml[isite], axis=0).tolist(),
+                                   numpy.unique(self.qnumr[isite + 2], axis=0).tolist(), self.qkey.tolist()))
         prj = torch.from_numpy(lay.prjmap(idl)).to(dev)
         self.stats["plan_s"] += time.time() - t0
         ldim, rdim = len(self.qnuml[isite]), len(self.qnumr[isite + 2])
@@ -230,7 +235,8 @@ class DMRG(object):
             r64 = davidson(lambda v: sig(v, precision="f64"), diag, 1, v0, crit_e=crit_e, crit_vec=self.crit_vec)
             self.shadow.append({"isite": isite, "status": status, "e_f64": float(r64.eigs[0]),
                                 "e_mixed": float(res.eigs[0]), "nmvp_f64": int(r64.nmvp),
-                                "nmvp_mixed": int(res.nmvp)})
+                                "nmvp_mixed": int(res.nmvp), "niter_f64": int(r64.niter),
+                                "niter_mixed": int(res.niter)})
         self.stats["nmvp"] += res.nmvp
         self.stats["sigma_flops"] += res.nmvp * sig.flops
         if learned:
@@ -477,11 +483,21 @@ class DMRG(object):
                 keys.append(k)
             first[k].append(i)
         nrows = rho.shape[0]
+        # classes the wavefunction has no weight in give exactly zero blocks: their
+        # eigenpairs are (0, unit vectors), as LAPACK returns them for a zero matrix; the
+        # device eigensolver is not called on them (on the B200 it returned NaN for an
+        # all-zero 41 x 41 block, which poisoned the global sort)
+        zero_row = (rho.abs().amax(dim=1) == 0).cpu().numpy() if nrows else numpy.zeros(0, dtype=bool)
         qsym, cols, sig = [], [], []
         for k in keys:
             rows = torch.tensor(first[k], dtype=torch.int64, device=rho.device)
-            blk = rho[rows][:, rows]
-            s2, u = torch.linalg.eigh(blk)
+            n = len(first[k])
+            if zero_row[first[k]].all():
+                s2 = torch.zeros(n, dtype=rho.dtype, device=rho.device)
+                u = torch.eye(n, dtype=rho.dtype, device=rho.device)
+            else:
+                blk = rho[rows][:, rows]
+                s2, u = torch.linalg.eigh(blk)
             qsym += [list(numpy.array(k) / 2.0)] * len(first[k])
             col = torch.zeros((nrows, len(first[k])), dtype=rho.dtype, device=rho.device)
             col[rows, :] = u
