@@ -8,7 +8,7 @@ step = one full two-site sweep (right-to-left then left-to-right) at D=500:
 per dot the sigma/diagonal plans, Davidson (FP64 Rayleigh-Ritz), RDM
 decimation and renormalisation of every operator's environment.
 
-  python bench.py [--steps K] [--warmup W] [--precision mixed|f64|mixed-tc|tf32] [--gpus N]
+  python bench.py [--steps K] [--warmup W] [--precision mixed-tc|mixed|f64|tf32] [--gpus N]
                   [--w-path fiber|generic|fused] [--plan-cache] [--sites K] [--dmax D]
   python bench.py --impl reference      # the reference algorithm (oracle port) on the host CPU
   python bench.py --workload batched    # lockstep independent instances vs one after another
@@ -227,7 +227,9 @@ def run_ours(args):
     kname = stage_kernel(top[0], args.w_path, prec)
     roof = {"kernel": "%s (%s)" % (kname, top[0]), "bound": "hbm", "achieved": round(gbs, 1),
             "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(gbs / pk["hbm_gbs"], 4),
-            "peak_source": src, "traffic": traffic_per_launch(top[0], b_l / max(n_l, 1)), "launches": n_l,
+            "peak_source": src, "traffic": traffic_per_launch(top[0], prec, b_l / max(n_l, 1)),
+            "traffic_source": "ncu DRAM bytes per algorithmic byte of this stage at K=24 D=200, times this "
+                              "launch's algorithmic bytes", "launches": n_l,
             "achieved_tflops": round(f_l / (t_l / 1e3) / 1e12, 3)}
     # whole job: world replicas each did args.steps sweeps in ms (slowest rank)
     line = {
@@ -305,13 +307,21 @@ def stage_kernel(stage, w_path, prec):
             "sigma4": tc if panel else "k_bgemm"}.get(stage, "k_bgemm")
 
 
-# DRAM bytes per launch measured by ncu for a stage's kernel, scaled to the launch's
-# algorithmic bytes (profiles/ holds the captures); None where no capture exists
-TRAFFIC_RATIO = {}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, ncu) per algorithmic byte of a
+# stage's launches, measured on the mid-chain dot of K=24, D=200 (bench.py --workload dot;
+# profiles/ holds the captures and the commands); the traffic of a D=500 launch is its
+# algorithmic bytes times this ratio (the kernels stream their operands once, so the
+# traffic grows in proportion to the blocks processed)
+TRAFFIC_RATIO = {("sigma1", "f32"): 0.987, ("sigma2", "f32"): 1.024, ("sigma3", "f32"): 1.007,
+                 ("sigma4", "f32"): 1.010,
+                 ("sigma1", "tf32x3"): 1.035, ("sigma2", "tf32x3"): 1.024, ("sigma3", "tf32x3"): 1.007,
+                 ("sigma4", "tf32x3"): 1.146,
+                 ("sigma1", "f64"): 1.083, ("sigma2", "f64"): 1.041, ("sigma3", "f64"): 1.029,
+                 ("sigma4", "f64"): 1.008}
 
 
-def traffic_per_launch(stage, algo_bytes):
-    r = TRAFFIC_RATIO.get(stage)
+def traffic_per_launch(stage, prec, algo_bytes):
+    r = TRAFFIC_RATIO.get((stage, prec))
     return None if r is None else round(r * algo_bytes)
 
 
@@ -563,7 +573,11 @@ def main():
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "f64", "tf32", "mixed-tc"])
+    ap.add_argument("--precision", default=None, choices=["mixed", "f64", "tf32", "mixed-tc"],
+                    help="mixed-tc (default): L.psi and .R on the tensor cores in split TF32, the MPO-site "
+                         "contractions in FP32, FP64 Rayleigh-Ritz / residual check / decimation; mixed: FP32 "
+                         "CUDA cores for all of sigma; f64: everything FP64 (the parity path); tf32: plain TF32 "
+                         "(default for --workload sp: mixed)")
     ap.add_argument("--sites", type=int, default=K_SITES)
     ap.add_argument("--dmax", type=int, default=DMAX)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
@@ -587,6 +601,8 @@ def main():
     ap.add_argument("--no-graphs", dest="graphs", action="store_false",
                     help="batched workload: plain lockstep launches instead of CUDA-graph replay")
     args = ap.parse_args()
+    if args.precision is None:
+        args.precision = "mixed" if args.workload == "sp" else "mixed-tc"
     world = os.environ.get("WORLD_SIZE")
     if args.gpus > 1 and world is None:
         # one process per GPU: relaunch under torch.distributed.run (replicas, see dist_init)
