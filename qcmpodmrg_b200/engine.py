@@ -1191,6 +1191,13 @@ def tc_sigma4_units(classes, order_pos, t3_base_of_class, rt_base_of_class, rt_o
     return u, maps
 
 
+def _ranges(n):
+    """(owner, local index) of the concatenation of arange(n[i]) (vectorised)."""
+    n = numpy.asarray(n, dtype=numpy.int64)
+    own = numpy.repeat(numpy.arange(len(n)), n)
+    return own, numpy.arange(int(n.sum()), dtype=numpy.int64) - numpy.repeat(numpy.cumsum(n) - n, n)
+
+
 def psi_panels(psi):
     """The wavefunction as the B operand of the tensor-core L.psi GEMMs: per first-index
     sector l' the psi blocks (l', n1, n2, r) of that sector side by side as columns,
@@ -1198,29 +1205,31 @@ def psi_panels(psi):
     rounded up to 4).  Returns (gather index into the packed vector, -1 for padding),
     {sector: (offset, N total, K, Kp)} and {block: (sector, first column)}."""
     blocks = numpy.asarray(psi.idx_allowed, dtype=numpy.int64)
-    sec = psi.block_sectors(blocks)[0]
+    if len(blocks) == 0:
+        return numpy.zeros(0, dtype=numpy.int64), {}, {}
+    sec = psi.block_sectors(blocks)[0].astype(numpy.int64)
     d = psi.block_dims(blocks)
-    K = d[:, 0]
-    N = numpy.prod(d[:, 1:], axis=1)
-    info, cols = {}, {}
-    idx = []
-    off = 0
-    for s_ in numpy.unique(sec):
-        sel = numpy.flatnonzero(sec == s_)
-        k = int(K[sel[0]])
-        kp = (k + 3) // 4 * 4
-        ntot = int(N[sel].sum())
-        info[int(s_)] = (off, ntot, k, kp)
-        g = numpy.full((ntot, kp), -1, dtype=numpy.int64)
-        c = 0
-        for j in sel:
-            n = int(N[j])
-            g[c:c + n, :k] = psi.ioff[blocks[j]] + numpy.arange(k)[None, :] * n + numpy.arange(n)[:, None]
-            cols[int(blocks[j])] = (int(s_), c)
-            c += n
-        idx.append(g.ravel())
-        off += ntot * kp
-    gidx = numpy.concatenate(idx) if idx else numpy.zeros(0, dtype=numpy.int64)
+    K = d[:, 0].astype(numpy.int64)
+    N = numpy.prod(d[:, 1:], axis=1).astype(numpy.int64)
+    o = numpy.argsort(sec, kind="stable")                 # blocks grouped by sector, in block order
+    blocks, sec, K, N = blocks[o], sec[o], K[o], N[o]
+    us, first = numpy.unique(sec, return_index=True)
+    cnt = numpy.diff(numpy.r_[first, len(sec)])
+    ks = K[first]
+    kps = (ks + 3) // 4 * 4
+    ntot = numpy.add.reduceat(N, first)
+    size = ntot * kps
+    soff = numpy.cumsum(size) - size
+    col = numpy.cumsum(N) - N - numpy.repeat((numpy.cumsum(N) - N)[first], cnt)    # first column in its sector
+    sidx = numpy.repeat(numpy.arange(len(us)), cnt)                                   # sector position per block
+    # gather index: panel element (column c, k) of sector s at soff + c * Kp + k
+    gidx = numpy.full(int(size.sum()), -1, dtype=numpy.int64)
+    b, e = _ranges(N * K[...])                       # (block, local element) over each block's N x K values
+    nb, kb = N[b], K[b]
+    cc, kk = e % nb, e // nb                         # element (k, column) of the block: psi offset k * N + c
+    gidx[soff[sidx[b]] + (col[b] + cc) * kps[sidx[b]] + kk] = psi.ioff[blocks[b]] + kk * nb + cc
+    info = {int(s_): (int(a), int(n), int(k), int(kp)) for s_, a, n, k, kp in zip(us, soff, ntot, ks, kps)}
+    cols = {int(bb): (int(s_), int(c)) for bb, s_, c in zip(blocks, sec, col)}
     return gidx, info, cols
 
 
@@ -1229,7 +1238,9 @@ def tc_sigma1_units(classes, psi_info, psi_cols, lp_base, lp_opstride, lp_total,
 
     classes: list of (op positions, pan["tc"] dict).  A: the class's TC L panels (pre-split
     planes, lp_total apart); B: the psi panels of the sector (psi_info, planes psi_total apart).
-    The T1 destination of psi block j is its panel [M x N_j] at t1pan_j (rows = L panel rows)."""
+    The T1 destination of psi block j is its panel [M x N_j] at t1pan_j (rows = L panel rows).
+    A unit is one 128-row tile of one 128-column tile of a sector's psi panel; its segments
+    are the pieces of the psi blocks that column tile holds (vectorised over blocks)."""
     units, maps, segs = [], [], []
     bmap = {}
     for s_, (off, ntot, k, kp) in sorted(psi_info.items()):
@@ -1238,42 +1249,68 @@ def tc_sigma1_units(classes, psi_info, psi_cols, lp_base, lp_opstride, lp_total,
     nseg = 0
     for ci, (poss, tc) in enumerate(classes):
         nops = len(poss)
-        col_of = {}
-        for b, t1p, nj in zip(tc["blocks"].tolist(), tc["t1pan"].tolist(), tc["Nj"].tolist()):
-            s_, c = psi_cols[b]
-            col_of.setdefault(s_, []).append((c, nj, t1p))
-        tl = []
-        for j, s_ in enumerate(tc["sectors"].tolist()):
-            amap = len(maps)
+        secs = numpy.asarray(tc["sectors"], dtype=numpy.int64)
+        amap = len(maps) + numpy.arange(len(secs))
+        for j in range(len(secs)):
             K, M, Kp = int(tc["K"][j]), int(tc["M"][j]), int(tc["Kp"][j])
             maps.append(("A", lp_base[ci] + int(tc["lpoff"][j]), (K, M, nops, 2), (Kp, lp_opstride[ci], lp_total),
                          (TC_BK, TC_BM, 1, 2)))
-            ntot = psi_info[s_][1]
-            blocks = sorted(col_of.get(s_, []))
-            m0 = numpy.arange(0, M, TC_BM)
-            for n0 in range(0, ntot, TC_BN):
-                w = min(TC_BN, ntot - n0)
-                sb = nseg
-                for (c, nj, t1p) in blocks:
-                    lo, hi = max(c, n0), min(c + nj, n0 + w)
-                    if hi > lo:
-                        segs.append((t1p + (lo - c), lo - n0, hi - lo, nj, (0, 0, 0)))
-                        nseg += 1
-                if nseg == sb:
-                    continue
-                t = numpy.zeros(len(m0), TCUNIT_DT)
-                t["a_map"], t["b_map"] = amap, bmap[s_]
-                t["a_c1"], t["b_c1"] = m0, n0
-                t["nk"] = (K + TC_BK - 1) // TC_BK
-                t["m_valid"] = numpy.minimum(TC_BM, M - m0)
-                t["n_valid"] = w
-                t["nseg"] = nseg - sb
-                t["c_off"] = sb
-                tl.append(t)
-        if tl:
-            u, q = _replicate_units(numpy.concatenate(tl), poss)
+        if len(secs) == 0:
+            continue
+        jpos = {int(s_): j for j, s_ in enumerate(secs.tolist())}
+        # the class's blocks: sector position j, first column c, width nj, T1 panel offset
+        bl = tc["blocks"].tolist()
+        bj = numpy.array([jpos.get(psi_cols[b][0], -1) for b in bl], dtype=numpy.int64)
+        bc = numpy.array([psi_cols[b][1] for b in bl], dtype=numpy.int64)
+        nj = numpy.asarray(tc["Nj"], dtype=numpy.int64)
+        t1p = numpy.asarray(tc["t1pan"], dtype=numpy.int64)
+        keep = bj >= 0
+        bj, bc, nj, t1p = bj[keep], bc[keep], nj[keep], t1p[keep]
+        # (block, column tile) pairs: tiles first .. last that the block's columns touch
+        t0 = bc // TC_BN
+        t1 = (bc + nj - 1) // TC_BN
+        pb, pl = _ranges(numpy.maximum(t1 - t0 + 1, 0))
+        tile = t0[pb] + pl
+        o = numpy.lexsort((bc[pb], tile, bj[pb]))            # by sector, column tile, first column
+        pb, tile = pb[o], tile[o]
+        n0 = tile * TC_BN
+        ntot_j = numpy.array([psi_info[int(s_)][1] for s_ in secs], dtype=numpy.int64)
+        w = numpy.minimum(TC_BN, ntot_j[bj[pb]] - n0)
+        lo = numpy.maximum(bc[pb], n0)
+        hi = numpy.minimum(bc[pb] + nj[pb], n0 + w)
+        ok = hi > lo
+        pb, tile, n0, lo, hi, w = pb[ok], tile[ok], n0[ok], lo[ok], hi[ok], w[ok]
+        sg = numpy.zeros(len(pb), TCSEG_DT)
+        sg["off"] = t1p[pb] + (lo - bc[pb])
+        sg["col0"] = lo - n0
+        sg["ncol"] = hi - lo
+        sg["ldc"] = nj[pb]
+        segs.append(sg)
+        # one unit group per (sector, column tile) that holds a segment
+        key = bj[pb] * (1 << 32) + tile
+        gstart = numpy.flatnonzero(numpy.r_[True, key[1:] != key[:-1]]) if len(key) else numpy.zeros(0, numpy.int64)
+        gn = numpy.diff(numpy.r_[gstart, len(key)])
+        gj, gn0, gw = bj[pb][gstart], n0[gstart], w[gstart]
+        Mj = numpy.asarray(tc["M"], dtype=numpy.int64)[gj]
+        nm = (Mj + TC_BM - 1) // TC_BM
+        ug, um = _ranges(nm)
+        t = numpy.zeros(len(ug), TCUNIT_DT)
+        t["a_map"] = amap[gj[ug]]
+        t["b_map"] = numpy.array([bmap[int(s_)] for s_ in secs], dtype=numpy.int64)[gj[ug]]
+        t["a_c1"] = um * TC_BM
+        t["b_c1"] = gn0[ug]
+        Kj = numpy.asarray(tc["K"], dtype=numpy.int64)[gj]
+        t["nk"] = ((Kj + TC_BK - 1) // TC_BK)[ug]
+        t["m_valid"] = numpy.minimum(TC_BM, Mj[ug] - um * TC_BM)
+        t["n_valid"] = gw[ug]
+        t["nseg"] = gn[ug]
+        t["c_off"] = nseg + gstart[ug]
+        nseg += len(pb)
+        if len(t):
+            u, q = _replicate_units(t, poss)
             u["a_c2"] = q
             units.append(u)
     u = numpy.concatenate(units) if units else numpy.zeros(0, TCUNIT_DT)
-    sg = numpy.array(segs, dtype=TCSEG_DT) if segs else numpy.zeros(1, TCSEG_DT)
+    sg = numpy.concatenate(segs) if segs and sum(len(x) for x in segs) else numpy.zeros(1, TCSEG_DT)
     return u, maps, sg
+
