@@ -193,6 +193,15 @@ def run_ours(args):
     prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32", "mixed-tc": "tf32x3"}[args.precision]
     sp = args.workload == "sp"
     d = _make_dmrg(args, prec, dev, rank)
+    tuned = {}
+    if args.autotune and not sp:
+        # measured choice of the fiber-GEMM schedule at the mid-chain dot, for this arm's
+        # precision and for the FP64 arm (both applied to every later plan of their run)
+        from qcmpodmrg_b200.autotune import tune_fiber_budget
+        tuned[prec] = tune_fiber_budget(d)
+        if prec != "f64" and args.f64_steps > 0:
+            tuned["f64"] = tune_fiber_budget(d, precision="f64")
+            d.sigma_opts["fg_budget"] = tuned[prec]["choice"]
     warm = [_step(d, args) for _ in range(args.warmup)]
     snap = d.snapshot()          # the state the timed sweeps start from (e2e, accuracy and FP64 legs)
     # ---- timed region (device events on the launching stream, barrier + sync both sides)
@@ -281,6 +290,8 @@ def run_ours(args):
         if args.cpu_baseline:
             line["cpu_baseline"] = acc.pop("cpu_baseline")
         line["accuracy"] = acc
+    if tuned:
+        line["autotune"] = tuned
     if hasattr(d.preconditioner, "summary"):
         line["precond_stats"] = d.preconditioner.summary()
     if args.f64_steps > 0 and prec != "f64" and not sp:
@@ -289,7 +300,8 @@ def run_ours(args):
         del d
         gc.collect()
         torch.cuda.empty_cache()
-        line["f64_arm"] = f64_arm(args, dev, dist, rank, snap, [e[0] for e in energies], per_sweep)
+        line["f64_arm"] = f64_arm(args, dev, dist, rank, snap, [e[0] for e in energies], per_sweep,
+                                  tuned.get("f64", {}).get("choice"))
     del snap
     if dist is not None:
         dist.destroy_process_group()
@@ -406,7 +418,7 @@ def shadow_leg(d, args, snap):
                           "iteration cap)"}
 
 
-def f64_arm(args, dev, dist, rank, snap, e_mixed, ms_mixed):
+def f64_arm(args, dev, dist, rank, snap, e_mixed, ms_mixed, fg_budget=None):
     """The plain FP64 GPU path from the same state as the timed sweeps (the snapshot they
     started from), timing the first f64_steps of the same sweeps; compared with the mixed
     arm's energy after the same number of sweeps and its time for those sweeps."""
@@ -415,6 +427,8 @@ def f64_arm(args, dev, dist, rank, snap, e_mixed, ms_mixed):
     n = min(args.f64_steps, args.steps)
     ham = make_hamiltonian(args.sites, args.sites, SEED, DECAY)
     d = DMRG(ham, device=dev, precision="f64", w_path=args.w_path, plan_cache=args.plan_cache)
+    if fg_budget is not None and d.sigma_opts.get("use_fiber"):
+        d.sigma_opts["fg_budget"] = tuple(fg_budget)
     d.restore(snap)
     ms, per, res = _timed_sweeps(d, args, n, dist)
     ms = max_over_ranks(dist, ms, dev)
@@ -477,6 +491,11 @@ def run_dot(args):
     n, e, dw, el, dl = d.sweep("L", args.dmax, 1e-7)
     d.precision = prec
     isite = d.nsite // 2
+    tune = None
+    if args.autotune:
+        from qcmpodmrg_b200.autotune import tune_fiber_budget
+        tune = {p: tune_fiber_budget(d, isite, precision=p) for p in ([prec] if prec == "f64" else [prec, "f64"])}
+        d.sigma_opts["fg_budget"] = tune[prec]["choice"]
     LOG.enabled = True            # the plan records its algorithmic byte counts for the launch log
     lay, idl, s, dg = d.dot_operators(isite)
     LOG.enabled = False
@@ -508,7 +527,7 @@ def run_dot(args):
                      "algo_bytes": int(by), "flops": float(fl), "gbs": round(by / (ms / 1e3) / 1e9, 1) if ms else None})
     line = {"workload": "mid-chain dot sigma, K=%d N=%d D=%d" % (args.sites, args.sites, args.dmax),
             "set_up_energy": e, "set_up_matvecs": int(d.stats["nmvp"]), "dot": isite, "ndim0": int(s.ndim0), "precisions": precs, "repeats": args.steps,
-            "launches_logged": len(recs), "gpu_launches": LOG.launches, "launches": recs}
+            "launches_logged": len(recs), "gpu_launches": LOG.launches, "autotune": tune, "launches": recs}
     print(json.dumps(line), flush=True)
 
 
@@ -586,6 +605,8 @@ def main():
                     help="kernels of the two MPO-site contractions of sigma")
     ap.add_argument("--plan-cache", action="store_true",
                     help="reuse the compiled plans of dots whose sectors did not change")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default fiber-GEMM schedule instead of the measured choice")
     ap.add_argument("--no-shadow", dest="shadow", action="store_false",
                     help="skip the same-input leg (each dot of one sweep also solved in plain FP64)")
     ap.add_argument("--f64-steps", type=int, default=3,

@@ -104,8 +104,9 @@ def davidson_steps(diag, neig=1, v0=None, crit_e=1.e-8, crit_vec=1.e-8, maxcycle
         xbas = vr @ vbas
         rbas = vr @ wbas - eigs[:, None] * xbas
         rn = torch.linalg.norm(rbas, dim=1)
-        rn_h = rn.cpu().tolist()
-        ec_h = econv.cpu().tolist()
+        hh = torch.cat([rn, econv.to(rn.dtype)]).cpu().tolist()      # one device->host copy per step
+        rn_h = hh[:neig]
+        ec_h = [v != 0.0 for v in hh[neig:]]
         rnorms.append(rn_h)
         rconv = [x <= crit_vec for x in rn_h]
         rindx = [i for i in range(neig) if not rconv[i] and not ec_h[i]]

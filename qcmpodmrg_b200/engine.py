@@ -712,8 +712,12 @@ def compile_fiber(c, triples, rows_axis, fiber_major, extra_out=None, in_off=Non
 class FiberStage(object):
     """Fiber-group work items of several symmetry classes, resident on the device."""
 
-    def __init__(self, parts, device, name, ops):
-        """parts: list of (tasks, fin, fout, fpair, max_rows, flops, fiber_tile, op_range), one fiber tile."""
+    def __init__(self, parts, device, name, ops, budget=None):
+        """parts: list of (tasks, fin, fout, fpair, max_rows, flops, fiber_tile, op_range), one fiber tile.
+        budget: (A, W) elements staged per shared-memory buffer by qc_fgemm (fibers per tile and
+        the width of W panel slices follow from it)."""
+        self.a_budget, self.w_budget = (FG_A_BUDGET, FG_W_BUDGET) if budget is None else (int(budget[0]),
+                                                                                          int(budget[1]))
         tks, fis, fos, fps = [], [], [], []
         nin = nout = npair = 0
         self.max_rows = 1
@@ -841,8 +845,8 @@ class FiberStage(object):
         # group records: whole groups, and column slices of groups wider than the W budget;
         # records of one operator range with the same panel map share one panel
         op_b, op_e = t0["op_b"].astype(i64), t0["op_e"].astype(i64)
-        wide = R * CTs > FG_W_BUDGET
-        width = numpy.maximum(mc, FG_W_BUDGET // numpy.maximum(R, 1) // mc * mc)
+        wide = R * CTs > self.w_budget
+        width = numpy.maximum(mc, self.w_budget // numpy.maximum(R, 1) // mc * mc)
         nsl = numpy.where(wide, (CT + width - 1) // width, 1)
         rg, sl = ranges(nsl)
         rc0 = numpy.where(wide[rg], sl * width[rg], 0)
@@ -919,7 +923,7 @@ class FiberStage(object):
         nn = numpy.arange(1, 65, dtype=i64)
         tot = nn[None, :] * chunks[:, None]
         util = tot / (FG_THREADS * ((tot + FG_THREADS - 1) // FG_THREADS))
-        valid = (4 * nn[None, :] * numpy.maximum(R[rg], 1)[:, None] <= FG_A_BUDGET)
+        valid = (4 * nn[None, :] * numpy.maximum(R[rg], 1)[:, None] <= self.a_budget)
         valid &= nn[None, :] <= numpy.maximum((F[rg] + 3) // 4, 1)[:, None]
         valid[:, 0] = True
         util = numpy.where(valid, util, -1.0)
@@ -1057,12 +1061,13 @@ def prune(triples, live1=None, live2=None):
     return triples[keep]
 
 
-def fiber_stages(parts, device, name, ops):
-    """FiberStage per fiber tile (parts compiled with 32- and 64-fiber tiles)."""
+def fiber_stages(parts, device, name, ops, budget=None):
+    """FiberStage per fiber tile (parts compiled with 32- and 64-fiber tiles); budget: the
+    dense fiber-group GEMM's (A, W) shared-memory budgets, default (FG_A_BUDGET, FG_W_BUDGET)."""
     by = {}
     for p in parts:
         by.setdefault(p[6], []).append(p)
-    return [FiberStage(v, device, name, ops) for k, v in sorted(by.items())]
+    return [FiberStage(v, device, name, ops, budget) for k, v in sorted(by.items())]
 
 
 # ---------------------------------------------------------------- tensor-core panel GEMM (qc_tcpanel_f32)

@@ -176,8 +176,11 @@ class SigmaOperator(object):
     """sigma = sum_p w_p R_p W_p[i+1] W_p[i] L_p psi for the dot (isite, isite+1)."""
 
     def __init__(self, ws, isite, psi_layout, L, R, Wi, Wj, qkey, opers, hpwts, precision="f64",
-                 tensor_cores=None, use_fiber=False, fuse_w=True, panel1=True, panel4=True, live=None):
-        """live: optional mask over the wavefunction layout's flat blocks.  Blocks outside it
+                 tensor_cores=None, use_fiber=False, fuse_w=True, panel1=True, panel4=True, live=None,
+                 fg_budget=None):
+        """fg_budget: (A, W) shared-memory budgets of the dense fiber-group GEMM (qc_fgemm), as
+        chosen by qcmpodmrg_b200.autotune; None keeps the engine's defaults.
+        live: optional mask over the wavefunction layout's flat blocks.  Blocks outside it
         are zero in every input vector and discarded in every output (the blocks that N
         symmetry adds to an (N, Sz) wavefunction under spin projection): block pairs that
         read them in the first contraction or write them in the last are not compiled."""
@@ -382,7 +385,7 @@ class SigmaOperator(object):
         self.stages = []
         for si in range(4):
             g = Stage(st[si], dev, "sigma%d" % (si + 1), tabs[si]) if st[si] else None
-            f = fiber_stages(fib[si], dev, "sigma%d" % (si + 1), tabs[si]) if fib[si] else []
+            f = fiber_stages(fib[si], dev, "sigma%d" % (si + 1), tabs[si], fg_budget) if fib[si] else []
             if si == 0:
                 self._s0_generic = g
             if si == 0 and (pst or pst_tc):
@@ -426,7 +429,7 @@ class SigmaOperator(object):
         self.wtot = wtot
         if fuse_parts:
             ftab = op_table(bases[0][order], wbase[order], bases[2][order], 1.0)
-            self.fused = CompositeStage(fiber_stages(fuse_parts, dev, "sigma23", ftab), "sigma23")
+            self.fused = CompositeStage(fiber_stages(fuse_parts, dev, "sigma23", ftab, fg_budget), "sigma23")
             wst = Stage(wij_parts, dev, "wij", op_table(Wi.offsets[order], Wj.offsets[order], wbase[order], 1.0))
             self.Wij = torch.zeros(max(wtot, 1), dtype=torch.float64, device=dev)
             wst.run(Wi.values, Wj.values, self.Wij, "f64")
