@@ -322,11 +322,11 @@ class DMRG(object):
         crit_e or the residual below the precision's floor.  Phase 2 applies the
         FP64 sigma to the final vector: its Rayleigh quotient has an error of second
         order in the vector's error.  The vector is accepted when its FP64 residual is
-        at most 1e-4, or when phase 1 converged by the reference's criteria and either
-        the FP64 residual is at most twice the low-precision one plus the precision's
-        floor, or the FP64 Rayleigh quotient agrees with the low-precision Ritz value
-        within ACCEPT_DE (the low-precision sigma then did not bias the solve beyond
-        the point where the FP64 solver itself stops); otherwise FP64 Davidson
+        at most 1e-4, or at most twice the low-precision one plus the precision's floor
+        (the low-precision sigma did not bias the vector beyond the point where the FP64
+        solver itself stops, by its criteria or at the same iteration cap), or when phase 1
+        converged and the FP64 Rayleigh quotient agrees with the low-precision Ritz value
+        within ACCEPT_DE; otherwise FP64 Davidson
         iterations (reference criteria) continue from that vector.  Vectors are device
         tensors, or host tensors when hv / hv64 are the host-buffer entry points.
         """
@@ -346,10 +346,11 @@ class DMRG(object):
         converged = r1.niter < 19             # phase 1 met its criteria (not the iteration cap)
         # residual the low-precision solver saw for its final vector: when the FP64 residual
         # is no larger than that (plus the precision's floor), the low-precision products did
-        # not bias the vector beyond the point where the FP64 solver itself stops
+        # not bias the vector beyond the point where the FP64 solver itself stops -- also when
+        # phase 1 ended at the iteration cap, where the FP64 solver stops as well
         rn_low = float(r1.rnorms[-1][0]) if r1.rnorms else float("inf")
         unbiased = rn <= 2.0 * rn_low + floor
-        if rn <= max(self.crit_vec, accept) or (converged and (unbiased or abs(e64 - float(r1.eigs[0])) <= ACCEPT_DE)):
+        if rn <= max(self.crit_vec, accept) or unbiased or (converged and abs(e64 - float(r1.eigs[0])) <= ACCEPT_DE):
             r1.eigs = numpy.array([e64])
             r1.vecs = x.reshape(1, -1)
             r1.nmvp += 1
