@@ -9,9 +9,9 @@ per dot the sigma/diagonal plans, Davidson (FP64 Rayleigh-Ritz), RDM
 decimation and renormalisation of every operator's environment.
 
   python bench.py [--steps K] [--warmup W] [--precision mixed-tc|mixed|f64|tf32] [--gpus N]
-                  [--w-path fiber|generic|fused] [--plan-cache] [--sites K] [--dmax D]
+                  [--w-path fiber|generic|fused] [--no-plan-cache] [--sites K] [--dmax D]
   python bench.py --impl reference      # the reference algorithm (oracle port) on the host CPU
-  python bench.py --workload batched    # lockstep independent instances vs one after another
+  python bench.py --workload batched    # 64 independent instances in lockstep vs one after another
   python bench.py --workload sp --sites 12 --dmax 100 --npts 4   # spin-projected (S=0) sweeps, FP64
   python bench.py --workload dot --sites 24 --dmax 200   # one mid-chain dot's sigma (kernel profiles)
 
@@ -532,10 +532,11 @@ def run_dot(args):
 
 
 def run_batched(args):
-    """Independent instances (K in [8, 14], D in [64, 128], --instances of them) swept in lockstep:
-    one launch per sigma contraction for all instances per Davidson step, replayed from CUDA
-    graphs (or launched directly with --no-graphs), against the same instances swept one after
-    another.  Prints one JSON line."""
+    """Independent instances (the batched configuration: K uniform in 8..20 with N = K, Sz = 0
+    or 1/2, D uniform in 64..256, seeded decayed integrals; --instances of them) swept in
+    lockstep: one launch per sigma contraction for all instances per Davidson step, replayed
+    from CUDA graphs (or launched directly with --no-graphs), against the same instances swept
+    one after another.  Prints one JSON line."""
     import torch
     from qcmpodmrg_b200.hamiltonian import make_hamiltonian
     from qcmpodmrg_b200.synthetic import product_mps
@@ -543,13 +544,13 @@ def run_batched(args):
     from qcmpodmrg_b200.batched import BatchedDMRG
     dev = torch.device("cuda:0")
     rng = numpy.random.default_rng(1000)
-    shapes = [(2 * int(rng.integers(4, 8)), int(rng.integers(64, 129))) for _ in range(args.instances)]
+    shapes = [(int(rng.integers(8, 21)), int(rng.integers(64, 257))) for _ in range(args.instances)]
 
     def make():
         out = []
         for i, (K, D) in enumerate(shapes):
             ham = make_hamiltonian(K, K, 1000 + i, 3.0)
-            d = DMRG(ham, device=dev, precision="f64")
+            d = DMRG(ham, device=dev, precision="f64", sz=0.5 * (K % 2))
             d.load_mps(product_mps(ham))
             for st in ("R", "L"):          # set-up sweep at a small bond dimension
                 d.sweep(st, 16, 1e-7)
@@ -578,8 +579,8 @@ def run_batched(args):
     line = {"metric": "instance-sweeps per second, lockstep batched vs sequential", "value":
             round(len(shapes) / t_bat, 3), "unit": "instance-sweeps/s", "n_gpus": 1, "steps": 1, "warmup": 0,
             "higher_is_better": True, "dtype": "f64", "data": "synthetic: seeded integrals per instance",
-            "config": {"workload": "%d independent two-site DMRG instances, K in [8, 14], D in [64, 128]"
-                                   % len(shapes), "shapes": shapes},
+            "config": {"workload": "%d independent two-site DMRG instances, K in [8, 20] (N = K), D in [64, 256], "
+                                   "one sweep each after a D=16 set-up sweep" % len(shapes), "shapes": shapes},
             "sequential_instance_sweeps_per_s": round(len(shapes) / t_seq, 3),
             "batched_s": round(t_bat, 2), "sequential_s": round(t_seq, 2),
             "graphs": args.graphs, "graph_captures": b.captures, "lockstep_steps": b.steps}
@@ -603,8 +604,9 @@ def main():
     ap.add_argument("--no-cpu", dest="cpu_baseline", action="store_false")
     ap.add_argument("--w-path", default="fiber", choices=["generic", "fiber", "fused"],
                     help="kernels of the two MPO-site contractions of sigma")
-    ap.add_argument("--plan-cache", action="store_true",
-                    help="reuse the compiled plans of dots whose sectors did not change")
+    ap.add_argument("--no-plan-cache", dest="plan_cache", action="store_false",
+                    help="compile every dot's plans afresh instead of reusing those of dots whose sectors "
+                         "did not change")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the default fiber-GEMM schedule instead of the measured choice")
     ap.add_argument("--no-shadow", dest="shadow", action="store_false",
@@ -618,7 +620,7 @@ def main():
                     help="sp: spin-projected sweeps (SP-MPS, S=0) with --npts quadrature points; dot: the "
                          "mid-chain dot's sigma under the NVTX range 'dot' (kernel profiles)")
     ap.add_argument("--npts", type=int, default=4)
-    ap.add_argument("--instances", type=int, default=16)
+    ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--no-graphs", dest="graphs", action="store_false",
                     help="batched workload: plain lockstep launches instead of CUDA-graph replay")
     args = ap.parse_args()

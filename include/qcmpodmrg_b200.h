@@ -228,6 +228,17 @@ int qc_fgemm_f32(const void *items_dev, long long nitems, const void *groups_dev
 /* W panels of the dense fiber-group GEMM: dst[i] = idx[i] >= 0 ? src[idx[i]] : 0 (once per dot). */
 int qc_wpanel_f64(const double *src, const long long *idx_dev, double *dst, long long n, void *stream);
 int qc_wpanel_f32(const float *src, const long long *idx_dev, float *dst, long long n, void *stream);
+/* W panels of the dense fiber-group GEMM assembled from their W blocks (the form the plan
+ * compiler emits; the W blocks are those of the pair lists of tensordotSYM for
+ * top2 = tensordot(top1, W_i) / top3 = tensordot(top2, W_j), kernelQt.py:301-306):
+ * recs_dev holds nrec qc_wpair records (64 B; see qc_types.h), maxops the largest operator
+ * count of a record, ops_dev the stage's operator table (b_base: the operator's W).  P
+ * (psize elements) must be zero-filled by the caller; W holds wsize elements.  Indices
+ * outside either buffer are skipped. */
+int qc_wpanel_pairs_f64(const double *W, long long wsize, const void *recs_dev, long long nrec, int maxops,
+                        const void *ops_dev, double *P, long long psize, void *stream);
+int qc_wpanel_pairs_f32(const float *W, long long wsize, const void *recs_dev, long long nrec, int maxops,
+                        const void *ops_dev, float *P, long long psize, void *stream);
 
 /* ---------------------------------------------- tensor-core panel GEMM (TMA + tcgen05)
  * Replaces the pair loops of top1 = tensordot(L, psi) and top4 = tensordot(top3, R)

@@ -64,6 +64,8 @@ def tune_fiber_budget(d, isite=None, candidates=CANDIDATES, repeats=4, precision
     isite = d.nsite // 2 if isite is None else int(isite)
     t0 = time.time()
     saved = d.sigma_opts.get("fg_budget")
+    cache_size, d.plan_cache_size = d.plan_cache_size, 0       # every candidate compiles its own plan
+    d.plan_cache.clear()
     table, ref, ndim0 = [], None, 0
     x = None
     for cand in candidates:
@@ -83,6 +85,8 @@ def tune_fiber_budget(d, isite=None, candidates=CANDIDATES, repeats=4, precision
         del sig, dg
     best = min(table, key=lambda t: t[1])[0]
     d.sigma_opts["fg_budget"] = best if best != (FG_A_BUDGET, FG_W_BUDGET) else saved
+    d.plan_cache_size = cache_size
+    d.plan_cache.clear()
     rep = {"choice": best, "table": table, "dot": isite, "ndim0": ndim0, "precision": prec, "bond": dmax,
            "s": round(time.time() - t0, 2)}
     _CACHE[key] = rep

@@ -367,7 +367,56 @@ int launch_wpanel(const T *src, const long long *idx, T *dst, long long n, cudaS
   return QC_OK;
 }
 
+// W panels assembled from their W blocks (one CTA per (block, operator)), into panels the
+// caller zero-filled; every index is checked against the two buffers' sizes.
+template <typename T>
+__global__ void k_wpanel_pairs(const T *__restrict__ W, long long wsize, const qc_wpair *__restrict__ recs,
+                               long long nrec, const qc_op *__restrict__ ops, T *__restrict__ P, long long psize) {
+  const int o = (int)blockIdx.y;
+  for (long long k = blockIdx.x; k < nrec; k += gridDim.x) {
+    const qc_wpair w = recs[k];
+    if (o >= w.nops) continue;
+    const long long sb = ops[w.op_b + o].b_base + w.src;
+    const long long db = w.dst + (long long)o * w.opstride;
+    const int n = w.nr * w.ncol, half = w.width >> 1;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      const int r = e / w.ncol, j = e - r * w.ncol;
+      const int c = w.j0 + j;
+      const int pc = (w.mc == 8) ? ((c & 7) >> 2) * half + (c >> 3) * 4 + (c & 3) : c;
+      const long long d = db + (long long)(w.r0 + r) * w.width + pc;
+      const long long si = sb + (long long)r * w.src_ld + j;
+      if (d >= 0 && d < psize && si >= 0 && si < wsize) P[d] = W[si];
+    }
+  }
+}
+
+template <typename T>
+int launch_wpanel_pairs(const T *W, long long wsize, const void *recs, long long nrec, int maxops, const void *ops,
+                        T *P, long long psize, cudaStream_t s) {
+  if (nrec <= 0) return QC_OK;
+  if (!W || !recs || !ops || !P || maxops < 1 || maxops > 65535 || wsize < 0 || psize < 0) return QC_ERR_ARG;
+  const long long gx = nrec < (1LL << 30) ? nrec : (1LL << 30);
+  k_wpanel_pairs<T><<<dim3((unsigned)gx, (unsigned)maxops), 128, 0, s>>>(W, wsize, (const qc_wpair *)recs, nrec,
+                                                                         (const qc_op *)ops, P, psize);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "[qcgpu] qc_wpanel_pairs: %s\n", cudaGetErrorString(e));
+    return QC_ERR_CUDA;
+  }
+  return QC_OK;
+}
+
 }  // namespace
+
+extern "C" int qc_wpanel_pairs_f64(const double *W, long long wsize, const void *recs, long long nrec, int maxops,
+                                   const void *ops, double *P, long long psize, void *stream) {
+  return launch_wpanel_pairs<double>(W, wsize, recs, nrec, maxops, ops, P, psize, (cudaStream_t)stream);
+}
+
+extern "C" int qc_wpanel_pairs_f32(const float *W, long long wsize, const void *recs, long long nrec, int maxops,
+                                   const void *ops, float *P, long long psize, void *stream) {
+  return launch_wpanel_pairs<float>(W, wsize, recs, nrec, maxops, ops, P, psize, (cudaStream_t)stream);
+}
 
 extern "C" int qc_fgemm_f64(const void *items, long long nitems, const void *groups, const void *rows,
                             const void *cols, const void *ops, int max_a, int max_w, int max_ct, const double *A,

@@ -200,3 +200,13 @@ struct alignas(16) qc_fgitem {
   int wstride;         // multiple of 4
 };
 static_assert(sizeof(qc_fgitem) == 32, "qc_fgitem is 32 bytes");
+
+// One W block of a dense fiber-group W panel: for operators o < nops (of op_b ..), rows
+// r < nr, columns j < ncol: P[dst + o * opstride + (r0 + r) * width + perm(j0 + j)] =
+// W[b_base(op_b + o) + src + r * src_ld + j]; perm places column c of an 8-column thread
+// tile as the kernel reads it (two 4-column halves, width / 2 apart) when mc == 8.
+struct alignas(16) qc_wpair {
+  long long dst, opstride, src;
+  int width, mc, r0, nr, j0, ncol, src_ld, op_b, nops, pad;
+};
+static_assert(sizeof(qc_wpair) == 64, "qc_wpair is 64 bytes");

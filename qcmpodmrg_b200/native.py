@@ -79,6 +79,8 @@ _SIGS = {
     "qc_fgemm_f32": (c_int, [c_vp, c_ll, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp]),
     "qc_wpanel_f64": (c_int, [c_vp, c_vp, c_vp, c_ll, c_vp]),
     "qc_wpanel_f32": (c_int, [c_vp, c_vp, c_vp, c_ll, c_vp]),
+    "qc_wpanel_pairs_f64": (c_int, [c_vp, c_ll, c_vp, c_ll, c_int, c_vp, c_vp, c_ll, c_vp]),
+    "qc_wpanel_pairs_f32": (c_int, [c_vp, c_ll, c_vp, c_ll, c_int, c_vp, c_vp, c_ll, c_vp]),
 }
 
 

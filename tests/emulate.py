@@ -227,11 +227,27 @@ def _run_tcpanel(st, A, B, C):
                 C[idx] = tile[:, int(sg["col0"]) + c]
 
 
+def wpanel_pairs(st, W):
+    """Reference semantics of qc_wpanel_pairs: the zero-filled W panels with every W block
+    of every record copied in for each operator of its range (columns permuted)."""
+    from qcmpodmrg_b200.engine import fg_col_perm
+    P = numpy.zeros(max(st.wpanel_size, 4), dtype=W.dtype)
+    for w in st.h_wpairs:
+        r = numpy.arange(int(w["nr"]))[:, None]
+        j = numpy.arange(int(w["ncol"]))[None, :]
+        pc = fg_col_perm(int(w["j0"]) + j, int(w["width"]), int(w["mc"]))
+        for o in range(int(w["nops"])):
+            sb = int(st.host_ops[int(w["op_b"]) + o]["b_base"]) + int(w["src"])
+            d = int(w["dst"]) + o * int(w["opstride"]) + (int(w["r0"]) + r) * int(w["width"]) + pc
+            P[d] = W[sb + r * int(w["src_ld"]) + j]
+    return P
+
+
 def _run_fgemm(st, A, W, C):
     """Reference semantics of k_fgemm, from its items, group / row / column records and
     W panel map only: C_g tile = alpha * A_g tile . W_g for every (item, operator)."""
     from qcmpodmrg_b200.engine import fg_col_perm
-    P = numpy.where(st.h_widx >= 0, W[numpy.maximum(st.h_widx, 0)], 0.0)
+    P = wpanel_pairs(st, W)
     for it in st.h_items:
         g = st.h_groups[int(it["group"])]
         R, CT, CTs = int(g["R"]), int(g["CT"]), int(g["CTs"])

@@ -9,7 +9,7 @@ import torch
 
 from helpers import load, record_operators, record_sp_operators
 from emulate import patch_stage_run
-from qcmpodmrg_b200.engine import CompositeStage, FiberStage, PanelStage, PANEL_TILES
+from qcmpodmrg_b200.engine import fg_col_perm, CompositeStage, FiberStage, PanelStage, PANEL_TILES
 
 
 def _subs(st):
@@ -176,7 +176,27 @@ def test_dense_fiber_group_tables(tag, monkeypatch):
                 assert (it["wpan"] % 4 == 0).all() and (it["wstride"] % 4 == 0).all()
                 last = it["wpan"] + (it["op_e"] - 1 - it["op_b"]).astype(numpy.int64) * it["wstride"] + \
                     g["R"].astype(numpy.int64) * g["CTs"]
-                assert last.max() <= len(sub.h_widx)
+                assert last.max() <= sub.wpanel_size
+                # W blocks: inside the panels and the W tensor set, every panel element
+                # written at most once per operator, columns inside the panel width
+                wp = sub.h_wpairs
+                assert (wp["j0"] >= 0).all() and (wp["j0"] + wp["ncol"] <= wp["width"]).all()
+                assert (wp["nr"] >= 1).all() and (wp["ncol"] >= 1).all() and (wp["nops"] >= 1).all()
+                count = numpy.zeros(sub.wpanel_size, dtype=numpy.int64)
+                wtot = int(sub.host_ops["b_base"].max()) + 1
+                for w in wp:
+                    rr = numpy.arange(int(w["nr"]))[:, None]
+                    jj = numpy.arange(int(w["ncol"]))[None, :]
+                    pc = fg_col_perm(int(w["j0"]) + jj, int(w["width"]), int(w["mc"]))
+                    for o in range(int(w["nops"])):
+                        dd = int(w["dst"]) + o * int(w["opstride"]) + (int(w["r0"]) + rr) * int(w["width"]) + pc
+                        numpy.add.at(count, dd.ravel(), 1)
+                        si = int(sub.host_ops[int(w["op_b"]) + o]["b_base"]) + int(w["src"]) + \
+                            rr * int(w["src_ld"]) + jj
+                        assert si.min() >= 0
+                    assert int(w["src"]) + (int(w["nr"]) - 1) * int(w["src_ld"]) + int(w["ncol"]) - 1 >= 0
+                assert count.max() <= 1
+                assert wtot >= 1
                 for k in numpy.unique(it["group"]):
                     sel = it[it["group"] == k]
                     cover = numpy.zeros(int(gr[k]["F"]), dtype=numpy.int64)
