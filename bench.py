@@ -14,6 +14,7 @@ decimation and renormalisation of every operator's environment.
   python bench.py --workload batched    # 64 independent instances in lockstep vs one after another
   python bench.py --workload sp --sites 12 --dmax 100 --npts 4   # spin-projected (S=0) sweeps, FP64
   python bench.py --workload dot --sites 24 --dmax 200   # one mid-chain dot's sigma (kernel profiles)
+  python bench.py --workload converge --dmax 200 --steps 30   # mixed and FP64 to convergence, same start
 
 Prints one JSON line.  value = seconds per sweep (lower is better).
 """
@@ -531,6 +532,66 @@ def run_dot(args):
     print(json.dumps(line), flush=True)
 
 
+def run_converge(args):
+    """Time to convergence, both arms from the same state: the ramp (RAMP below dmax) in the
+    mixed precision, then sweeps (R then L) at dmax until the sweep energy changes by less
+    than --tol, at most --steps sweeps, first in the mixed precision and then, from the same
+    state, in plain FP64.  Prints one JSON line with both arms' sweeps, seconds (CUDA events)
+    and energies, |E_mixed - E_FP64| and the speed-up."""
+    import torch
+    from qcmpodmrg_b200.hamiltonian import make_hamiltonian
+    from qcmpodmrg_b200.dmrg import DMRG
+    dev = torch.device("cuda:0")
+    prec = {"mixed": "f32", "f64": "f64", "tf32": "tf32", "mixed-tc": "tf32x3"}[args.precision]
+    d = _make_dmrg(args, prec, dev)
+    if args.autotune:
+        from qcmpodmrg_b200.autotune import tune_fiber_budget
+        budgets = {prec: tune_fiber_budget(d)["choice"], "f64": tune_fiber_budget(d, precision="f64")["choice"]}
+        d.sigma_opts["fg_budget"] = tuple(budgets[prec])
+    snap = d.snapshot()
+
+    def converge(dm):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        hist, eold = [], None
+        for k in range(args.steps):
+            e, dw, nmv = _step(dm, args)
+            hist.append((e, dw, nmv))
+            if eold is not None and abs(e - eold) < args.tol:
+                break
+            eold = e
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3, hist
+
+    t_mix, h_mix = converge(d)
+    st_mix = {k: d.stats.get(k, 0) for k in ("nmvp_f64", "nmvp_low")}
+    del d
+    torch.cuda.empty_cache()
+    ham = make_hamiltonian(args.sites, args.sites, SEED, DECAY)
+    d64 = DMRG(ham, device=dev, precision="f64", w_path=args.w_path, plan_cache=args.plan_cache)
+    if args.autotune and d64.sigma_opts.get("use_fiber"):
+        d64.sigma_opts["fg_budget"] = tuple(budgets["f64"])
+    d64.restore(snap)
+    t64, h64 = converge(d64)
+    line = {"metric": "time to convergence (sweep energy change < %g Eh), mixed vs FP64" % args.tol,
+            "value": round(t_mix, 2), "unit": "s", "higher_is_better": False, "n_gpus": 1,
+            "config": {"workload": "two-site Qt DMRG, K=%d N=%d Sz=0 D=%d, decay 3, seed 1, from the same "
+                                   "ramped state (D %s)" % (args.sites, args.sites, args.dmax,
+                                                            "/".join(str(x) for x in RAMP if x < args.dmax)),
+                       "precision": args.precision, "tol": args.tol, "max_sweeps": args.steps},
+            "mixed": {"s": round(t_mix, 2), "sweeps": len(h_mix), "energy": h_mix[-1][0], "dwt": h_mix[-1][1],
+                      "matvecs": sum(h[2] for h in h_mix), "energies": [h[0] for h in h_mix],
+                      "matvecs_f64_low": [st_mix["nmvp_f64"], st_mix["nmvp_low"]]},
+            "f64": {"s": round(t64, 2), "sweeps": len(h64), "energy": h64[-1][0], "dwt": h64[-1][1],
+                    "matvecs": sum(h[2] for h in h64), "energies": [h[0] for h in h64]},
+            "abs_dE_vs_f64": abs(h_mix[-1][0] - h64[-1][0]),
+            "speedup_vs_f64": round(t64 / t_mix, 3) if t_mix > 0 else None}
+    print(json.dumps(line), flush=True)
+
+
 def run_batched(args):
     """Independent instances (the batched configuration: K uniform in 8..20 with N = K, Sz = 0
     or 1/2, D uniform in 64..256, seeded decayed integrals; --instances of them) swept in
@@ -550,7 +611,7 @@ def run_batched(args):
         out = []
         for i, (K, D) in enumerate(shapes):
             ham = make_hamiltonian(K, K, 1000 + i, 3.0)
-            d = DMRG(ham, device=dev, precision="f64", sz=0.5 * (K % 2))
+            d = DMRG(ham, device=dev, precision="f64", sz=0.5 * (K % 2), plan_cache=False)
             d.load_mps(product_mps(ham))
             for st in ("R", "L"):          # set-up sweep at a small bond dimension
                 d.sweep(st, 16, 1e-7)
@@ -568,6 +629,7 @@ def run_batched(args):
     torch.cuda.synchronize()
     t_seq = time.time() - t0
     del seq
+    torch.cuda.empty_cache()
     bat = make()
     b = BatchedDMRG(bat, kind="f64", use_graphs=args.graphs)
     torch.cuda.synchronize()
@@ -616,7 +678,8 @@ def main():
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "learned"],
                     help="Davidson preconditioner of the mixed-precision arm")
     ap.add_argument("--precond-train", type=int, default=2, help="sweeps whose solver pairs train the network")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "sp", "dot"],
+    ap.add_argument("--tol", type=float, default=1e-8, help="--workload converge: sweep energy change")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "sp", "dot", "converge"],
                     help="sp: spin-projected sweeps (SP-MPS, S=0) with --npts quadrature points; dot: the "
                          "mid-chain dot's sigma under the NVTX range 'dot' (kernel profiles)")
     ap.add_argument("--npts", type=int, default=4)
@@ -642,6 +705,8 @@ def main():
         run_batched(args)
     elif args.workload == "dot":
         run_dot(args)
+    elif args.workload == "converge":
+        run_converge(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

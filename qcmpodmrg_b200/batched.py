@@ -31,10 +31,22 @@ def _abs_ops(ops, a, b, c):
 class BatchedSigma(object):
     """sigma for several (SigmaOperator, input, output) triples in one launch per stage group."""
 
-    def __init__(self, items, device, kind="f64"):
+    def __init__(self, items, device, kind="f64", ws=None):
+        """ws: optional dict of grow-only scratch buffers shared by the batches of one run
+        (one batch is live at a time); without it every batch allocates its own."""
         self.device = device
         self.kind = kind
         dt = torch.float64 if kind == "f64" else torch.float32
+
+        def buf(name, n):
+            if ws is None:
+                return torch.zeros(n, dtype=dt, device=device)
+            b = ws.get((name, dt))
+            if b is None or b.numel() < n:
+                ws.pop((name, dt), None)
+                b = torch.empty(max(int(n), 1) + 64, dtype=dt, device=device)
+                ws[(name, dt)] = b
+            return b
         self.dtype = dt
         self.items = items
         n = len(items)
@@ -49,11 +61,11 @@ class BatchedSigma(object):
                 offs[i, k] = o
                 o += pad(int(tot[i, k]) + 1)
             sizes.append(o)
-        self.T = [torch.zeros(sizes[k], dtype=dt, device=device) for k in range(4)]
+        self.T = [buf("t%d" % k, sizes[k]) for k in range(4)]
         nd = [s.ndim0 for s in items]
         self.xoff = numpy.concatenate([[0], numpy.cumsum([pad(v + 1) for v in nd])])
-        self.X = torch.zeros(int(self.xoff[-1]), dtype=dt, device=device)
-        self.Y = torch.zeros(int(self.xoff[-1]), dtype=dt, device=device)
+        self.X = buf("x", int(self.xoff[-1]))
+        self.Y = buf("y", int(self.xoff[-1]))
         self.offs = offs
         groups = {}
         fibers = {}
@@ -205,18 +217,29 @@ class BatchedSigma(object):
             LOG.launches += 1
 
     def capture(self):
-        """Capture the launch sequence in a CUDA graph (inputs/outputs are the static X / Y)."""
-        self._launch_all()            # warm-up outside capture
+        """Capture the launch sequence in a CUDA graph (inputs/outputs are the static X / Y);
+        the launches run once directly first (the warm-up capture needs)."""
+        self._launch_all()
         torch.cuda.synchronize(self.device)
+        self._capture()
+
+    def _capture(self):
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
             self._launch_all()
         self.graph = g
 
-    def __call__(self, xs):
+    def __call__(self, xs, graph_after=None):
+        """graph_after: capture the launch sequence once the batch has run this many times
+        directly (the direct runs are the capture's warm-up), then replay it; None: never."""
         for i, x in enumerate(xs):
             if x is not None:
                 self.X[int(self.xoff[i]):int(self.xoff[i]) + x.numel()].copy_(x)
+        self.calls = getattr(self, "calls", 0) + 1
+        if self.graph is None and graph_after is not None and self.calls > graph_after:
+            torch.cuda.synchronize(self.device)
+            self._capture()
+            self.captured = True
         if self.graph is not None:
             self.graph.replay()
         else:
@@ -238,6 +261,7 @@ class BatchedDMRG(object):
         self.device = instances[0].device
         self.steps = 0
         self.captures = 0
+        self.ws = {}              # scratch shared by the run's batches
 
     def sweep(self, status, dmax, crit_e):
         """One sweep of every instance; dmax is one bond dimension or one per instance."""
@@ -266,13 +290,16 @@ class BatchedDMRG(object):
                 break
             if changed or batch is None or active != batch_ids:
                 items = [ctx[i]["sig"] for i in active]
-                batch = BatchedSigma(items, self.device, self.kind)
+                batch = None                      # the previous batch's graph goes before its buffers move
+                batch = BatchedSigma(items, self.device, self.kind, self.ws)
                 batch_ids = active
-                if self.use_graphs:
-                    batch.capture()
-                    self.captures += 1
             xs = [pend[i] if ctx[i] is not None else None for i in batch_ids]
-            ys = batch(xs)
+            # a batch runs directly the first time and is captured in a CUDA graph when it is
+            # used again (most batches live one step: an instance moves to its next dot)
+            had = batch.graph is not None
+            ys = batch(xs, graph_after=1 if self.use_graphs else None)
+            if batch.graph is not None and not had:
+                self.captures += 1
             self.steps += 1
             for k, i in enumerate(batch_ids):
                 if ctx[i] is None:
