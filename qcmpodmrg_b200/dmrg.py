@@ -123,6 +123,8 @@ class DMRG(object):
         # list: every low-precision dot solve is repeated in plain FP64 from the same start
         # vector and both energies are appended here (off when None)
         self.shadow = None
+        # mixed precision: one FP64 Davidson step after every accepted low-precision solve
+        self.fp64_step = True
 
     # ------------------------------------------------------------- set-up
     def _setup_operators(self, ham):
@@ -327,8 +329,9 @@ class DMRG(object):
         solver itself stops, by its criteria or at the same iteration cap), or when phase 1
         converged and the FP64 Rayleigh quotient agrees with the low-precision Ritz value
         within ACCEPT_DE; otherwise FP64 Davidson
-        iterations (reference criteria) continue from that vector.  Vectors are device
-        tensors, or host tensors when hv / hv64 are the host-buffer entry points.
+        iterations (reference criteria) continue from that vector.  With fp64_step on, an
+        accepted vector gets one more Davidson step on FP64 products.  Vectors are
+        device tensors, or host tensors when hv / hv64 are the host-buffer entry points.
         """
         # residual floor of the low-precision sigma (relative sigma error ~1e-7 FP32,
         # ~1e-3 TF32), and the FP64 residual accepted without FP64 iterations: the
@@ -351,15 +354,46 @@ class DMRG(object):
         rn_low = float(r1.rnorms[-1][0]) if r1.rnorms else float("inf")
         unbiased = rn <= 2.0 * rn_low + floor
         if rn <= max(self.crit_vec, accept) or unbiased or (converged and abs(e64 - float(r1.eigs[0])) <= ACCEPT_DE):
+            r1.nmvp += 1
+            if self.fp64_step and rn > self.crit_vec:
+                # one FP64 Davidson step from the accepted vector (Rayleigh-Ritz in the span of
+                # the vector and its preconditioned FP64 residual): the last step the FP64
+                # solver takes runs on FP64 products
+                x, e64 = self._fp64_step(hv64, diag, x, y, e64)
+                self.stats["nmvp_f64"] += 1
+                r1.nmvp += 1
             r1.eigs = numpy.array([e64])
             r1.vecs = x.reshape(1, -1)
-            r1.nmvp += 1
             return r1
         r2 = davidson(hv64, diag, 1, x.reshape(1, -1), crit_e=crit_e, crit_vec=self.crit_vec,
                       precond=self.preconditioner)
         self.stats["nmvp_f64"] += r2.nmvp
         r2.nmvp += r1.nmvp + 1
         return r2
+
+    def _fp64_step(self, hv64, diag, x, y, e):
+        """One FP64 Davidson step from the normalised vector x (y = H x in FP64, e its
+        Rayleigh quotient): the residual preconditioned as the solver does it (iop=4, or
+        the preconditioner of the run), orthogonalised against x, one FP64 product, and
+        the lower Ritz pair of the 2 x 2 projected problem.  Returns (vector, energy)."""
+        r = y - e * x
+        if self.preconditioner is None:
+            d = r / ((diag.to(r.device) - e).abs() + 1.e-4)
+        else:
+            d = self.preconditioner(r, diag, torch.tensor(e, dtype=torch.float64, device=r.device), x)
+        for _ in range(2):
+            d = d - torch.dot(x, d) * x
+        nd = float(torch.linalg.norm(d))
+        if not nd > 1.e-14:
+            return x, e
+        d = d / nd
+        yd = hv64(d)
+        hh = torch.stack([torch.dot(d, y), torch.dot(x, yd), torch.dot(d, yd)]).cpu().numpy()
+        h = numpy.array([[e, 0.5 * (hh[0] + hh[1])], [0.5 * (hh[0] + hh[1]), hh[2]]])
+        w, u = numpy.linalg.eigh(h)
+        x2 = float(u[0, 0]) * x + float(u[1, 0]) * d
+        x2 = x2 / torch.linalg.norm(x2)
+        return x2, float(w[0])
 
     def _solve_dot_host(self, isite, status, dmax, crit_e):
         """The same dot, through mpo_dmrg_kernel.HDiag/HVec with host buffers."""
