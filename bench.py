@@ -702,6 +702,9 @@ def main():
     if world is not None and int(world) != args.gpus:
         sys.exit("bench.py: --gpus %d but WORLD_SIZE=%s" % (args.gpus, world))
     if args.workload == "batched":
+        # 64 instances hold ~90 GB of environments next to the batches' scratch: let the
+        # caching allocator grow segments instead of fragmenting (set before CUDA starts)
+        os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
         run_batched(args)
     elif args.workload == "dot":
         run_dot(args)

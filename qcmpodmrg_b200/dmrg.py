@@ -229,6 +229,8 @@ class DMRG(object):
                            record=self.recorder)
         else:
             res = self._mixed_davidson(hv, lambda v: sig(v, precision="f64"), diag, v0, crit_e)
+            if hasattr(sig, "check_device_status"):
+                sig.check_device_status()
         torch.cuda.synchronize(dev)
         self.stats["hvec_s"] += time.time() - t0
         if self.shadow is not None and self.precision != "f64":

@@ -641,6 +641,15 @@ class SigmaOperator(object):
     def scratch_bytes(self):
         return 8 * sum(self.tot)
 
+    def check_device_status(self):
+        """Raise if a tensor-core launch of this plan gave up a bounded wait (its device
+        error flag, qc_tcpanel_status): its output would be incomplete.  Reads one int."""
+        if (self.tc1 is not None or self.tc4 is not None) and torch.device(self.ws.device).type == "cuda":
+            st = native.lib().qc_tcpanel_status(1)
+            if st != 0:
+                raise RuntimeError("tensor-core panel kernel: a bounded wait expired (status %d); the sigma of "
+                                   "this dot is incomplete" % st)
+
     def work_groups(self):
         """The plan's device work-item groups in stage order, as the C-ABI's
         qc_sigma_f64_noalloc takes them: (stage, kind, tasks, ntasks, opspan, contribs,

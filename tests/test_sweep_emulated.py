@@ -60,3 +60,18 @@ def test_odd_electron_number_sector(monkeypatch):
     ham = make_hamiltonian(4, 3, 1, None)
     out = DMRG(ham, device="cpu", sz=0.5).run(product_mps(ham), 16, 2)
     assert abs(out["eav"][-1] - fci_energy(ham)) <= 1e-8
+
+
+def test_mixed_precision_sweep_emulated(monkeypatch):
+    """The mixed-precision solve (low-precision Davidson, one FP64 product for the energy and
+    the residual check, one FP64 Davidson step) with the tensor-core plan, on the CPU
+    interpreter (whose split-TF32 products are exact): the reference's converged energies."""
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    from qcmpodmrg_b200.dmrg import DMRG
+    fx = load("sweep_K5N8.npz")
+    ham = make_hamiltonian(int(fx["K"]), int(fx["N"]), int(fx["seed"]), None if fx["decay"] < 0 else fx["decay"])
+    d = DMRG(ham, device="cpu", precision="tf32x3")
+    out = d.run(fx["init_mps"], int(fx["D"]), int(fx["nsweeps"]))
+    assert abs(out["eav"][-1] - fx["eav"][-1]) <= 1e-8
+    assert d.stats["nmvp_low"] > d.stats["nmvp_f64"] > 0
