@@ -64,7 +64,7 @@ def test_odd_electron_number_sector(monkeypatch):
 
 def test_mixed_precision_sweep_emulated(monkeypatch):
     """The mixed-precision solve (low-precision Davidson, one FP64 product for the energy and
-    the residual check, one FP64 Davidson step) with the tensor-core plan, on the CPU
+    the residual check, and the optional closing FP64 Davidson step) with the tensor-core plan, on the CPU
     interpreter (whose split-TF32 products are exact): the reference's converged energies."""
     patch_stage_run(monkeypatch)
     monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
@@ -72,6 +72,7 @@ def test_mixed_precision_sweep_emulated(monkeypatch):
     fx = load("sweep_K5N8.npz")
     ham = make_hamiltonian(int(fx["K"]), int(fx["N"]), int(fx["seed"]), None if fx["decay"] < 0 else fx["decay"])
     d = DMRG(ham, device="cpu", precision="tf32x3")
+    d.fp64_step = True                 # the optional closing FP64 step too
     out = d.run(fx["init_mps"], int(fx["D"]), int(fx["nsweeps"]))
     assert abs(out["eav"][-1] - fx["eav"][-1]) <= 1e-8
     assert d.stats["nmvp_low"] > d.stats["nmvp_f64"] > 0
