@@ -13,9 +13,10 @@ from .blocks import QTensor, classification
 from .kernels import SigmaOracle, hdiag, RenormOracle, boundary_env
 from .mpo import QPHYS, build_mpo, site_operator
 
-# Davidson matrix-vector products per dot at K=24, D=500 (FP64 GPU sweeps of the
-# same workload: 398 products over the 46 dots of one sweep).
-MATVECS_PER_DOT = 8.7
+# Davidson matrix-vector products per dot at K=24, D=500 (the FP64 GPU arm of the same
+# workload, the algorithm of the reference's pdvdson: 355 products over the 46 dots of one
+# sweep after the ramp and three warm-up sweeps).
+MATVECS_PER_DOT = 7.7
 
 
 def _qt(status, qsyms, ndims, values=None, rng=None):
