@@ -777,9 +777,10 @@ class FiberStage(object):
         """
         fo, fi, fp, ops = self.h_fout, self.h_fin, self.h_fpair, self.host_ops
         i64 = numpy.int64
-        tk = self.h_tasks[self.h_tasks["out_e"] > self.h_tasks["out_b"]]
-        gs, first = numpy.unique(tk["out_b"].astype(i64), return_index=True)
-        t0 = tk[first]
+        ht = self.h_tasks
+        live = numpy.flatnonzero(ht["out_e"] > ht["out_b"])
+        gs, first = numpy.unique(ht["out_b"][live].astype(i64), return_index=True)
+        t0 = ht[live[first]]
         ng = len(gs)
         F = t0["F"].astype(i64)
         in_b, in_e = t0["in_b"].astype(i64), t0["in_e"].astype(i64)
@@ -854,12 +855,17 @@ class FiberStage(object):
         nrec = len(rg)
         seen, panels = {}, []           # key -> panel id; per panel (operator range, size, representative record)
         pan_id = numpy.zeros(nrec, dtype=i64)
+        # the loop reads plain Python values: the pair rows of group g are the bytes
+        # [gp_b[g], gp_b[g] + gp_n[g]) x 40 of PA (five int64 columns, row-major)
+        pab = numpy.ascontiguousarray(PA, dtype=i64).tobytes()
+        opb_l, ope_l, R_l, CTs_l, CT_l = op_b.tolist(), op_e.tolist(), R.tolist(), CTs.tolist(), CT.tolist()
+        wide_l, gpb_l, gpn_l, rg_l, rcts_l = wide.tolist(), gp_b.tolist(), gp_n.tolist(), rg.tolist(), rcts.tolist()
         for k in range(nrec):
-            g = int(rg[k])
-            pa = PA[gp_b[g]:gp_b[g] + gp_n[g]]
-            if not wide[g]:
-                key = (int(op_b[g]), int(R[g]), int(CTs[g]), int(CT[g]), pa.tobytes())
+            g = rg_l[k]
+            if not wide_l[g]:
+                key = (opb_l[g], R_l[g], CTs_l[g], CT_l[g], pab[40 * gpb_l[g]:40 * (gpb_l[g] + gpn_l[g])])
             else:
+                pa = PA[gp_b[g]:gp_b[g] + gp_n[g]]
                 # the W blocks of the slice, clipped to its columns [rc0, rc0 + rct)
                 lo = numpy.maximum(pa[:, 1], rc0[k])
                 hi = numpy.minimum(pa[:, 1] + pa[:, 3], rc0[k] + rct[k])
@@ -870,7 +876,7 @@ class FiberStage(object):
             pid = seen.get(key)
             if pid is None:
                 pid = seen[key] = len(panels)
-                panels.append((int(op_b[g]), int(op_e[g]), int(R[g]) * int(rcts[k]), k))
+                panels.append((opb_l[g], ope_l[g], R_l[g] * rcts_l[k], k))
             pan_id[k] = pid
         # panels stored [operator][panel] per operator range
         npan = len(panels)
@@ -921,16 +927,24 @@ class FiberStage(object):
         self.h_wpairs = wp
         self.wpanel_size = int((stride_c * nops_c).sum())
         # fibers per tile: a multiple of 4 that fills the CTA's threads with thread tiles
+        # (decided once per distinct (column chunks, rows, fiber quads) of the records)
         chunks = rcts // mc[rg]
+        combo = numpy.stack([chunks, numpy.maximum(R[rg], 1), numpy.maximum((F[rg] + 3) // 4, 1)], axis=1)
+        if len(combo) and int(combo.max()) < (1 << 20):
+            ck = (combo[:, 0] << 40) | (combo[:, 1] << 20) | combo[:, 2]       # one int64 key per record
+            uk, cinv = numpy.unique(ck, return_inverse=True)
+            ucombo = numpy.stack([uk >> 40, (uk >> 20) & ((1 << 20) - 1), uk & ((1 << 20) - 1)], axis=1)
+        else:
+            ucombo, cinv = numpy.unique(combo, axis=0, return_inverse=True)
         nn = numpy.arange(1, 65, dtype=i64)
-        tot = nn[None, :] * chunks[:, None]
+        tot = nn[None, :] * ucombo[:, 0:1]
         util = tot / (FG_THREADS * ((tot + FG_THREADS - 1) // FG_THREADS))
-        valid = (4 * nn[None, :] * numpy.maximum(R[rg], 1)[:, None] <= self.a_budget)
-        valid &= nn[None, :] <= numpy.maximum((F[rg] + 3) // 4, 1)[:, None]
+        valid = (4 * nn[None, :] * ucombo[:, 1:2] <= self.a_budget)
+        valid &= nn[None, :] <= ucombo[:, 2:3]
         valid[:, 0] = True
         util = numpy.where(valid, util, -1.0)
         good = util >= 0.97 * util.max(axis=1)[:, None]
-        FT = 4 * (nn.size - numpy.argmax(good[:, ::-1], axis=1))
+        FT = (4 * (nn.size - numpy.argmax(good[:, ::-1], axis=1)))[cinv.ravel()]
         grp = numpy.zeros(nrec, FGGRP_DT)
         grp["row_b"] = row_b[rg]
         grp["col_b"] = col_b[rg] + rc0
