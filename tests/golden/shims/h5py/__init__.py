@@ -19,7 +19,8 @@ class Dataset(object):
 
     @property
     def value(self):
-        return self._data.copy()
+        # as h5py: a scalar dataset reads as a NumPy scalar, an array dataset as an array
+        return self._data[()] if self._data.ndim == 0 else self._data.copy()
 
     @property
     def shape(self):
