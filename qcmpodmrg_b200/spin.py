@@ -293,8 +293,9 @@ class SPDMRG(DMRG):
         """Generalised Davidson with FP32 H and S products, then one FP64 pair of products:
         the FP64 Rayleigh quotient e = x.Hx / x.Sx is accurate to second order in the
         vector's error.  Accepted when the FP64 residual |Hx - e Sx| (x S-normalised) is at
-        most 1e-4, or when the FP32 solve converged by the reference's criteria and e agrees
-        with its Ritz value within 1e-6 Eh; otherwise FP64 iterations continue from x."""
+        most 1e-4 or at most twice the FP32 solve's own residual plus 1e-5, or when the FP32
+        solve converged by the reference's criteria and e agrees with its Ritz value within
+        1e-6 Eh; otherwise FP64 iterations continue from x."""
         from .dmrg import ACCEPT_DE
         r1 = gdavidson(sig, sv, diag, 1, v0, crit_e=crit_e, crit_vec=max(self.crit_vec, 1e-5))
         x = r1.vecs[0]
@@ -307,7 +308,11 @@ class SPDMRG(DMRG):
         self.stats["nmvp_f64"] = self.stats.get("nmvp_f64", 0) + 1
         self.stats["nmvp_low"] = self.stats.get("nmvp_low", 0) + r1.nmvp
         converged = r1.niter < 19
-        if rn <= max(self.crit_vec, 1e-4) or (converged and abs(e64 - float(r1.eigs[0])) <= ACCEPT_DE):
+        # as in DMRG._mixed_davidson: an FP64 residual no larger than twice the FP32 solver's
+        # own (plus its floor) means the FP32 products did not bias the vector
+        rn_low = float(r1.rnorms[-1][0]) if r1.rnorms else float("inf")
+        unbiased = rn <= 2.0 * rn_low + 1e-5
+        if rn <= max(self.crit_vec, 1e-4) or unbiased or (converged and abs(e64 - float(r1.eigs[0])) <= ACCEPT_DE):
             r1.eigs = numpy.array([e64])
             r1.vecs = (x / xsx ** 0.5).reshape(1, -1)
             r1.nmvp += 1
