@@ -76,3 +76,22 @@ def test_mixed_precision_sweep_emulated(monkeypatch):
     out = d.run(fx["init_mps"], int(fx["D"]), int(fx["nsweeps"]))
     assert abs(out["eav"][-1] - fx["eav"][-1]) <= 1e-8
     assert d.stats["nmvp_low"] > d.stats["nmvp_f64"] > 0
+
+
+def test_plan_cache_keys_on_the_sigma_options(monkeypatch):
+    """A cached plan is reused only under the sigma options it was compiled with: another
+    fiber-GEMM schedule (as the autotuner sets it) compiles a new plan, the same one hits."""
+    patch_stage_run(monkeypatch)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    from qcmpodmrg_b200.dmrg import DMRG
+    fx = load("sweep_K4.npz")
+    ham = make_hamiltonian(int(fx["K"]), int(fx["N"]), int(fx["seed"]), None if fx["decay"] < 0 else fx["decay"])
+    d = DMRG(ham, device="cpu")
+    d.load_mps(fx["init_mps"])
+    d.sweep("R", int(fx["D"]), 1e-8)
+    lay, idl, sig, dg = d.dot_operators(1)
+    assert d.dot_operators(1)[2] is sig                      # same options: reused
+    d.sigma_opts["fg_budget"] = (2048, 2048)
+    sig2 = d.dot_operators(1)[2]
+    assert sig2 is not sig                                   # other schedule: compiled anew
+    assert d.dot_operators(1)[2] is sig2
