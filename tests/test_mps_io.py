@@ -92,3 +92,32 @@ def test_reference_reads_our_files_and_we_read_its_tensors(monkeypatch, tmp_path
     dense = numpy.zeros(int(numpy.prod(lay.shape)))
     dense[lay.prjmap(idlst)] = values
     assert numpy.array_equal(dense.reshape(lay.shape), t.toDenseTensor(t.idlst))
+
+
+@needs_ref
+def test_we_read_files_the_reference_writes(monkeypatch, tmp_path):
+    """An MPS written by the reference's own saveSite / saveQnum (dense and qtensor sites)
+    loads into the same start state."""
+    import reference_runner  # noqa: F401
+    from qcmpodmrg.source import mpo_dmrg_io
+    from qcmpodmrg.source.qtensor import qtensor
+    from qcmpodmrg_b200.mps_io import load_mps
+    d = _swept(monkeypatch)
+    for qt in (False, True):
+        f = _h5(tmp_path, "mps_written_by_ref_%d" % qt)
+        f["nsite"] = d.nsite
+        for i in range(d.nsite + 1):
+            mpo_dmrg_io.saveQnum(f, i, numpy.asarray(d.qnuml[i]))
+        for i in range(d.nsite):
+            dense = d.lmps[i].dense.numpy()
+            if qt:
+                t = qtensor.qtensor(numpy.array([False, False, True]))
+                t.fromDenseTensor(dense, [d.qnuml[i], numpy.array([[0., 0.], [1., -0.5], [1., 0.5], [2., 0.]]),
+                                          d.qnuml[i + 1]])
+                mpo_dmrg_io.saveSite(f, i, t)
+            else:
+                mpo_dmrg_io.saveSite(f, i, dense)
+        got = load_mps(f)
+        for i in range(d.nsite):
+            assert numpy.array_equal(got["site%d" % i], d.lmps[i].dense.numpy())
+            assert numpy.array_equal(got["qnum%d" % i], d.qnuml[i])
